@@ -1,0 +1,40 @@
+"""finitevolx_b200: B200-native (sm_100a) drop-in for finitevolX's explicit-step
+and elliptic-inversion hot path.
+
+Public names mirror ``finitevolx`` (finitevolx/__init__.py).  Every operator
+runs in libfvx.so, a C-ABI CUDA library built for sm_100a; arrays are CUDA
+``torch.Tensor`` objects (NumPy inputs are copied to the device).
+"""
+
+from finitevolx_b200.grid import ArakawaCGrid2D, CartesianGrid2D
+from finitevolx_b200.mask import (
+    Mask2D,
+    StencilCapability2D,
+    count_contiguous,
+    make_sponge,
+    narrow_mask_hierarchy,
+)
+from finitevolx_b200.advection import (
+    Advection2D,
+    Reconstruction2D,
+    upwind_flux,
+    uv_center_flux,
+    uv_node_flux,
+)
+from finitevolx_b200.operators import (
+    Difference2D,
+    Interpolation2D,
+    arakawa_jacobian,
+    divergence_2d,
+)
+from finitevolx_b200.diffusion import BiharmonicDiffusion2D, Diffusion2D, diffusion_2d
+from finitevolx_b200.boundary import enforce_periodic, enforce_periodic_, pad_interior
+from finitevolx_b200.timestepping import euler_step, heun_step, rk3_ssp_step
+
+__all__ = [
+    "ArakawaCGrid2D", "CartesianGrid2D", "Mask2D", "StencilCapability2D", "count_contiguous",
+    "make_sponge", "narrow_mask_hierarchy", "Advection2D", "Reconstruction2D", "upwind_flux",
+    "uv_center_flux", "uv_node_flux", "Difference2D", "Interpolation2D", "arakawa_jacobian",
+    "divergence_2d", "BiharmonicDiffusion2D", "Diffusion2D", "diffusion_2d", "enforce_periodic",
+    "enforce_periodic_", "pad_interior", "euler_step", "heun_step", "rk3_ssp_step",
+]

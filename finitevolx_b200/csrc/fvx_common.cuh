@@ -1,0 +1,53 @@
+// Shared definitions for the finitevolx_b200 CUDA library (sm_100a).
+//
+// Conventions (same as finitevolX): fields are row-major [Ny, Nx] arrays
+// with a one-cell ghost ring; U[j,i] sits at i+1/2, V[j,i] at j+1/2 and
+// X[j,i] at the north-east corner of T[j,i].  Every entry point takes
+// caller-owned device pointers and a cudaStream_t, allocates nothing on the
+// hot path, and returns an int status (fvx_status below).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define DEV __device__ __forceinline__
+
+enum fvx_status {
+  FVX_OK = 0,
+  FVX_ERR_SHAPE = 1,      // a size or stride is out of the supported range
+  FVX_ERR_METHOD = 2,     // unknown scheme / operator code
+  FVX_ERR_DTYPE = 3,      // unsupported dtype combination
+  FVX_ERR_CUDA = 4,       // a CUDA runtime call failed
+  FVX_ERR_NOT_CONVERGED = 5,
+  FVX_ERR_ARG = 6,        // a required pointer is null or an argument is invalid
+  FVX_ERR_TIMEOUT = 7,    // a bounded device-side wait gave up
+};
+
+// Advection schemes (Advection2D method strings, advection/advection.py:360-368).
+enum fvx_scheme {
+  FVX_NAIVE = 0,
+  FVX_UPWIND1 = 1,
+  FVX_UPWIND2 = 2,
+  FVX_UPWIND3 = 3,
+  FVX_WENO3 = 4,
+  FVX_WENO5 = 5,
+  FVX_WENOZ5 = 6,
+  FVX_WENO7 = 7,
+  FVX_WENO9 = 8,
+  FVX_MINMOD = 9,
+  FVX_VAN_LEER = 10,
+  FVX_SUPERBEE = 11,
+  FVX_MC = 12,
+  FVX_WENOZ3 = 13,  // face-flux only (Reconstruction2D.wenoz3_x/_y)
+  FVX_NUM_SCHEMES = 14,
+};
+
+static inline int fvx_cuda_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? FVX_OK : FVX_ERR_CUDA;
+}
+
+static inline cudaStream_t fvx_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+template <typename T>
+DEV T ldg(const T* p) { return __ldg(p); }
