@@ -1,0 +1,337 @@
+"""Benchmark: QG 1.5-layer RK3-SSP step (WENO5 + beta + DST Helmholtz), FP32, 2048^2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 2048]
+
+One "step" = one rk3_ssp_step of the QG PV tendency on a 2048^2 interior
+(2050^2 with the ghost ring), periodic q, DST (Dirichlet) psi with
+lambda = 1/Ld^2 (Ld = 40 km), beta = 1.7e-11, Lx = Ly = 5.12e6 m, WENO5,
+dt at CFL 0.5 for max|u| = 1 m/s.  Metric: Mcell-steps/s = interior cells x
+steps / s / 1e6 (whole job, all ranks).  Inputs: seeded k^-3 Gaussian PV
+field (std 1e-5 s^-1), synthetic.
+
+* value: device time (CUDA events on the launching stream) of K steps, each
+  replayed from a CUDA graph; L2 flushed (256 MiB write) before every step,
+  outside the timed events; max over ranks.
+* e2e: the same step through the public API (``QGModel.step``) from pinned
+  host memory: host->device copy of q, the step, device->host copy of
+  q_{n+1}, all inside the timed region.
+* roofline: the dominant kernel is the tcgen05 DST GEMM (one of the four
+  products per solve); achieved = algorithmic 2*M*N*K flops per launch /
+  its mean CUDA-event duration, vs the measured bf16 peak.
+* cpu_baseline: the FP64 NumPy oracle's QG step on this host.
+* --impl reference: the reference's CPU implementation of the path
+  (finitevolX's JAX stack is not installable here; the oracle port restates
+  it) on the same config, one bounded sample per step.
+
+Multi-GPU (--gpus N under torchrun): the single-field step does not shard;
+each rank runs an independent replica ("replicas only"), value sums ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+LX = 5.12e6
+BETA = 1.7e-11
+LD = 4.0e4
+METRIC = "QG RK3 Mcell-steps/s"
+UNIT = "Mcell-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--n", type=int, default=2048)
+    ap.add_argument("--method", default="weno5")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(n, method):
+    return {"workload": f"qg1.5_rk3ssp_{method}_dst_{n}x{n}_fp32", "interior": [n, n], "scheme": method,
+            "helmholtz": "DST-I dense GEMMs, 3xBF16 split, FP32 accumulate", "bc": "periodic q, Dirichlet psi",
+            "lambda": 1.0 / LD ** 2, "beta": BETA, "dt": 0.5 * LX / n, "l2": "flushed (256 MiB write) before every step",
+            "parallelism": "replicas"}
+
+
+def initial_q(n, seed=0):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    w = rng.standard_normal((n, n))
+    ky = np.fft.fftfreq(n)[:, None]
+    kx = np.fft.rfftfreq(n)[None, :]
+    k = np.sqrt(kx ** 2 + ky ** 2)
+    k[0, 0] = np.inf
+    f = np.fft.irfft2(np.fft.rfft2(w) * k ** -1.5, s=(n, n))
+    f = (f - f.mean()) * (1e-5 / f.std())
+    q = np.zeros((n + 2, n + 2))
+    q[1:-1, 1:-1] = f
+    q[0, :], q[-1, :] = q[-2, :], q[1, :]
+    q[:, 0], q[:, -1] = q[:, -2], q[:, 1]
+    return q
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+            t0 = time.time()
+            while not self.rows and time.time() - t0 < 5.0:  # sampler running before timing starts
+                time.sleep(0.01)
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in self.rows for n, v in zip(names, r[5:9]) if v.strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(n, method):
+    """One FP64 oracle QG step at the full size on this host (single core)."""
+    import numpy as np
+    import oracle.fvx_oracle as O
+    q = initial_q(n)
+    dx = LX / n
+    t = time.perf_counter()
+    O.qg_step(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, method)
+    t = time.perf_counter() - t
+    return {"value": n * n / t / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 rk3_ssp_step at {n}x{n}, FP64 NumPy/SciPy oracle (restatement of the reference "
+                      f"math; finitevolX's JAX stack is not installable offline), {t:.1f} s"}
+
+
+def run_reference(args, rank):
+    """Reference arm: the oracle port of the reference's CPU path, all host threads."""
+    if rank != 0:
+        return
+    import numpy as np
+    import scipy.fft
+    import oracle.fvx_oracle as O
+    # bounded per-step sample (same physics, smaller interior) so K + W steps stay within minutes
+    ns = min(args.n, 512 if args.steps + args.warmup <= 200 else 256)
+    q = initial_q(ns)
+    dx = LX / ns
+    cores = os.cpu_count() or 1
+    times = []
+    with scipy.fft.set_workers(cores):
+        for k in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            q = O.qg_step(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, args.method)
+            t = time.perf_counter() - t
+            if k >= args.warmup:
+                times.append(t)
+    tot = sum(times)
+    val = ns * ns * len(times) / tot / 1e6
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config(args.n, args.method),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"per step: 1 rk3_ssp_step at {ns}x{ns} (FP64 NumPy oracle port of the "
+                                   "reference path; SciPy FFT on all host threads)"},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200 import _lib as L
+    from finitevolx_b200.qg import QGModel
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    n = args.n
+    grid = fvx.ArakawaCGrid2D.from_interior(n, n, LX, LX)
+    dt = 0.5 * grid.dx / 1.0
+    model = QGModel(grid, BETA, 1.0 / LD ** 2, method=args.method, dtype=torch.float32)
+    q0 = torch.as_tensor(initial_q(n, seed=rank), dtype=torch.float32, device="cuda")
+    qa, qb = q0.clone(), torch.empty_like(q0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # warm-up (eager), leaves split(qb) in the DST workspace for the graphs
+    for _ in range(max(args.warmup, 3)):
+        model.step(qa, dt, out=qb)
+        qa.copy_(qb)
+    model.step(qa, dt, out=qb)
+    torch.cuda.synchronize()
+    # CUDA graphs of one step each way (qa -> qb, qb -> qa), chained presplit
+    graphs = []
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for src, dst in ((qb, qa), (qa, qb)):
+            g = torch.cuda.CUDAGraph()
+            launches0 = model.kernel_launches
+            with torch.cuda.graph(g, stream=s):
+                model.step(src, dt, out=dst, presplit=True)
+            per_step_launches = model.kernel_launches - launches0
+            graphs.append(g)
+    torch.cuda.current_stream().wait_stream(s)
+    for g in graphs:  # graph warm-up
+        g.replay()
+    torch.cuda.synchronize()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms = 0.0
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            graphs[k % 2].replay()
+            e1.record()
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+    torch.cuda.synchronize()
+    t_max = total_ms
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        dist.barrier()
+    cells = n * n
+    value = world * cells * args.steps / (t_max * 1e-3) / 1e6
+
+    # e2e through the public API with pinned host buffers
+    host_in = torch.empty(q0.shape, dtype=torch.float32, pin_memory=True)
+    host_in.copy_(q0.cpu())
+    host_out = torch.empty_like(host_in, pin_memory=True)
+    e2e_ms = 0.0
+    for k in range(args.warmup + args.steps):
+        flush.fill_(float(k))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        qd = host_in.to("cuda", non_blocking=True)
+        out = model.step(qd, dt)
+        host_out.copy_(out, non_blocking=True)
+        e1.record()
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_ms += e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e = world * cells * args.steps / (e2e_ms * 1e-3) / 1e6
+    nbytes = host_in.numel() * host_in.element_size()
+
+    # dominant kernel: one tcgen05 DST GEMM (2048 x 2048 x 2048, 3xBF16)
+    from finitevolx_b200._lib import I, fn, stream_ptr
+    h = model.plan.handle
+    gemm = fn("fvx_dst_gemm_step")
+    for _ in range(5):
+        gemm(h, I(0), I(1), stream_ptr())
+    reps = 20
+    gt = []
+    for _ in range(reps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        L.check(gemm(h, I(0), I(1), stream_ptr()), "gemm")
+        e1.record()
+        e1.synchronize()
+        gt.append(e0.elapsed_time(e1))
+    gemm_ms = statistics.mean(gt)
+    flops = 2.0 * n * n * n
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops")
+    peak_src = "measured burst bf16 (MEASURED_PEAKS.json)" if peak else "fallback 1590"
+    peak = peak or 1590.0
+    achieved = flops / (gemm_ms * 1e-3) / 1e12
+
+    if rank == 0:
+        res = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(n, args.method),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+                    "ms_per_step": e2e_ms / args.steps},
+            "gpu_launches": per_step_launches * args.steps,
+            "roofline": {"bound": "tensor", "kernel": "gemm_split_bf16_kernel (DST product, 3xBF16)",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": peak_src, "traffic": None,
+                         "per_launch_ms": gemm_ms, "algorithmic_flops_per_launch": flops},
+            "clocks": clk.summary(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(n, args.method)
+        print(json.dumps(res))
+    if world > 1:
+        dist.barrier()
+        del graphs
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,748 @@
+// Dirichlet Helmholtz solver by dense DST-I matrix products on the
+// tcgen05 tensor cores (sm_100a).
+//
+// Restates spectraldiffx v0.0.10 ``solve_helmholtz_dst`` (re-exported at
+// finitevolX solvers/spectral.py:14-98; math in docs/elliptic_solvers.md:
+// 55-76): psi = IDST2(DST2(f) / Lambda) with Lambda[j,i] = ey[j] + ex[i] -
+// lambda and ey[j] = -4/dy^2 sin^2(pi (j+1) / (2 (Ny+1))).  With the DST-I
+// matrix S[j,k] = sin(pi (j+1)(k+1) / (N+1)) (symmetric), scipy's
+// unnormalised DST-I is 2 S and its inverse S / (N+1), so
+//   psi = 4 / ((Ny+1)(Nx+1)) * S_y ((S_y f S_x) ./ Lambda) S_x.
+//
+// The four products run as one GEMM shape, C = X S (X row-major, S
+// symmetric, so both operands are K-major), whose epilogue stores C
+// transposed: the chain Q -> (Q S_x)^T -> (S_y Q S_x ./ Lambda) ->
+// (. S_x)^T -> psi needs no transpose kernels and every operand is a
+// K-major TMA tile.  Precision: 3xBF16 split (X = Xh + Xl, S = Sh + Sl,
+// C = Xh Sh + Xh Sl + Xl Sh) with FP32 accumulation in TMEM; the epilogue
+// writes the next product's operand already split into bf16 hi/lo.  An FP64
+// SIMT form of the same chain is the correctness path, and the FP64 solve
+// recovers full accuracy by iterative refinement with an FP64 residual.
+#include "fvx_common.cuh"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+namespace fvx {
+namespace dst {
+
+typedef __nv_bfloat16 bf16;
+
+constexpr int BM = 128, BN = 256, BK = 64, STAGES = 2;
+constexpr int A_TILE = BM * BK * 2;                        // 16 KiB
+constexpr int B_TILE = BN * BK * 2;                        // 32 KiB
+constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;       // 96 KiB
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr int THREADS = 192;                               // TMA warp, MMA warp, 4 epilogue warps
+constexpr long long kWaitCycles = 4000000000LL;            // ~2 s bound on every spin-wait
+
+enum EpiMode { EPI_SPLIT = 0, EPI_F32 = 1, EPI_F64 = 2, EPI_F64_ACC = 3 };
+
+struct Epi {
+  int mode;
+  int rows_per_batch;      // R: row m of C is (batch m / R, r = m % R)
+  int m_total;             // M
+  int n_cols;              // valid N
+  void* out0;              // hi / f32 / f64 output
+  void* out1;              // lo output (split mode)
+  long long batch_stride;  // elements between batches in the output
+  long long ld;            // elements between consecutive n rows of the (transposed) output
+  int off_n, off_r;        // index offsets into the output (e.g. a ghost ring)
+  double alpha;
+  const float* inv_eig;    // [n_eig][N][R] scale 1/Lambda, or null
+  const double* inv_eig64;
+  int n_eig;               // batch b uses grid b % n_eig
+  int* err;
+};
+
+// ---- PTX helpers ----------------------------------------------------------
+DEV uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+DEV void mbar_init(uint32_t a, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count));
+}
+DEV void mbar_expect_tx(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+DEV bool mbar_try(uint32_t a, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after ~2 s, raises the CTA abort flag and the
+// global error flag instead of spinning forever.
+DEV bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag, int* err) {
+  long long t0 = clock64();
+  while (!mbar_try(a, parity)) {
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kWaitCycles) {
+      *abort_flag = 1;
+      if (err) atomicExch(err, 1);
+      return false;
+    }
+  }
+  return true;
+}
+DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+DEV void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+DEV void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+DEV void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+DEV void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row core
+// groups 1024 B apart (SBO), sm_100 descriptor version 1.
+DEV uint64_t sdesc_sw128(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+// Instruction descriptor: kind::f16 with BF16 A/B, FP32 accumulator,
+// both operands K-major, M = 128, N = 256.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                            ((uint32_t)(BM >> 4) << 24);
+
+// ---- epilogue store ---------------------------------------------------------
+DEV void epi_store(const Epi& ep, int b, int r, int n, float acc) {
+  long long idx = (long long)b * ep.batch_stride + (long long)(n + ep.off_n) * ep.ld + (r + ep.off_r);
+  switch (ep.mode) {
+    case EPI_SPLIT: {
+      float x = acc * (float)ep.alpha;
+      if (ep.inv_eig) x *= ep.inv_eig[((long long)(b % ep.n_eig) * ep.n_cols + n) * ep.rows_per_batch + r];
+      bf16 hi = __float2bfloat16_rn(x);
+      bf16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+      ((bf16*)ep.out0)[idx] = hi;
+      ((bf16*)ep.out1)[idx] = lo;
+      break;
+    }
+    case EPI_F32: {
+      float x = acc * (float)ep.alpha;
+      if (ep.inv_eig) x *= ep.inv_eig[((long long)(b % ep.n_eig) * ep.n_cols + n) * ep.rows_per_batch + r];
+      ((float*)ep.out0)[idx] = x;
+      break;
+    }
+    case EPI_F64:
+      ((double*)ep.out0)[idx] = (double)acc * ep.alpha;
+      break;
+    default:
+      ((double*)ep.out0)[idx] += (double)acc * ep.alpha;
+      break;
+  }
+}
+
+// ---- the tcgen05 GEMM -------------------------------------------------------
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, int K,
+                       Epi ep) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + STAGES * STAGE_BYTES);  // full[S], empty[S], acc
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 1);
+  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int KT = (K + BK - 1) / BK;
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[STAGES + s]); };
+  const uint32_t accb = smem_u32(&bars[2 * STAGES]);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
+    mbar_init(accb, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(BN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    // TMA producer
+    for (int kt = 0; kt < KT; ++kt) {
+      const int s = kt % STAGES;
+      if (kt >= STAGES && !mbar_wait(empty(s), ((kt / STAGES) - 1) & 1, abort_flag, ep.err)) break;
+      mbar_expect_tx(full(s), STAGE_BYTES);
+      const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+      tma_load_2d(base, &mAh, full(s), kt * BK, m0);
+      tma_load_2d(base + A_TILE, &mAl, full(s), kt * BK, m0);
+      tma_load_2d(base + 2 * A_TILE, &mBh, full(s), kt * BK, n0);
+      tma_load_2d(base + 2 * A_TILE + B_TILE, &mBl, full(s), kt * BK, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: three split products per 16-wide K step
+    bool ok = true;
+    for (int kt = 0; kt < KT && ok; ++kt) {
+      const int s = kt % STAGES;
+      ok = mbar_wait(full(s), (kt / STAGES) & 1, abort_flag, ep.err);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
+      const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + A_TILE);
+      const uint64_t bh = sdesc_sw128(base + 2 * A_TILE), bl = sdesc_sw128(base + 2 * A_TILE + B_TILE);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint64_t o = (uint64_t)(kk * 32 >> 4);
+        umma_bf16(tmem, ah + o, bh + o, kIdesc, (kt | kk) != 0);
+        umma_bf16(tmem, ah + o, bl + o, kIdesc, 1u);
+        umma_bf16(tmem, al + o, bh + o, kIdesc, 1u);
+      }
+      umma_commit(empty(s));
+    }
+    umma_commit(accb);  // also issued after an abort so the epilogue never waits on MMAs in flight
+  } else if (warp >= 2) {
+    // epilogue: TMEM -> registers -> transposed global stores
+    const int wq = warp & 3;
+    const int row = wq * 32 + lane;
+    const int m = m0 + row;
+    const bool mvalid = m < ep.m_total;
+    const int b = mvalid ? m / ep.rows_per_batch : 0;
+    const int r = mvalid ? m - b * ep.rows_per_batch : 0;
+    if (mbar_wait(accb, 0, abort_flag, ep.err)) {
+      tc_fence_after();
+      if (!*abort_flag) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < BN; c0 += 32) {
+          uint32_t v[32];
+          tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + (uint32_t)c0, v);
+          tmem_wait_ld();
+          if (mvalid) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int n = n0 + c0 + j;
+              if (n < ep.n_cols) epi_store(ep, b, r, n, __uint_as_float(v[j]));
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
+  }
+}
+
+// ---- FP64 SIMT GEMM with the same transposed-store epilogue (correctness path)
+constexpr int DT = 64, DK = 16;
+__global__ void __launch_bounds__(256)
+gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict__ S, int lds, int M, int N, int K,
+                Epi ep) {
+  __shared__ double As[DK][DT + 1];
+  __shared__ double Ss[DK][DT + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  const int m0 = blockIdx.y * DT, n0 = blockIdx.x * DT;
+  double acc[4][4] = {};
+  for (int k0 = 0; k0 < K; k0 += DK) {
+    for (int t = threadIdx.x; t < DT * DK; t += 256) {
+      int mm = t / DK, kk = t % DK;
+      int gm = m0 + mm, gk = k0 + kk;
+      As[kk][mm] = (gm < M && gk < K) ? A[(long long)gm * lda + gk] : 0.0;
+      int kk2 = t / DT, nn = t % DT;
+      int gk2 = k0 + kk2, gn = n0 + nn;
+      Ss[kk2][nn] = (gk2 < K && gn < N) ? S[(long long)gk2 * lds + gn] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < DK; ++kk) {
+      double a[4], s[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) { a[i] = As[kk][ty + 16 * i]; s[i] = Ss[kk][tx + 16 * i]; }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], s[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int m = m0 + ty + 16 * i;
+    if (m >= M) continue;
+    const int b = m / ep.rows_per_batch, r = m - b * ep.rows_per_batch;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int n = n0 + tx + 16 * j;
+      if (n >= N) continue;
+      double x = acc[i][j] * ep.alpha;
+      if (ep.inv_eig64) x *= ep.inv_eig64[((long long)(b % ep.n_eig) * ep.n_cols + n) * ep.rows_per_batch + r];
+      long long idx = (long long)b * ep.batch_stride + (long long)(n + ep.off_n) * ep.ld + (r + ep.off_r);
+      if (ep.mode == EPI_F64_ACC) ((double*)ep.out0)[idx] += x;
+      else if (ep.mode == EPI_F32) ((float*)ep.out0)[idx] = (float)x;
+      else ((double*)ep.out0)[idx] = x;
+    }
+  }
+}
+
+// ---- input split / copy / residual kernels ---------------------------------
+template <typename T>
+__global__ void split_input_kernel(const T* __restrict__ in, long long bstride, long long ld, int ny, int nx,
+                                   int batch, bf16* __restrict__ hi, bf16* __restrict__ lo, double scale) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)batch * ny * nx;
+  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long b = k / ((long long)ny * nx);
+    long long rem = k - b * ny * nx;
+    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
+    float v = (float)((double)in[b * bstride + (long long)y * ld + x] * scale);
+    bf16 h = __float2bfloat16_rn(v);
+    hi[k] = h;
+    lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+}
+
+template <typename T>
+__global__ void copy_in_f64_kernel(const T* __restrict__ in, long long bstride, long long ld, int ny, int nx,
+                                   int batch, double* __restrict__ out) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)batch * ny * nx;
+  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long b = k / ((long long)ny * nx);
+    long long rem = k - b * ny * nx;
+    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
+    out[k] = (double)in[b * bstride + (long long)y * ld + x];
+  }
+}
+
+__global__ void zero_f64_kernel(double* p, long long bstride, long long ld, int ny, int nx, int batch) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)batch * ny * nx;
+  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long b = k / ((long long)ny * nx);
+    long long rem = k - b * ny * nx;
+    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
+    p[b * bstride + (long long)y * ld + x] = 0.0;
+  }
+}
+
+DEV double warp_sum(double v) {
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// r = f - (lap - lambda) psi (5-point, zero outside), FP64; writes r split
+// into bf16 hi/lo (the next correction's GEMM operand, scaled by 1/rscale)
+// and accumulates sum r^2, sum f^2, sum psi^2, sum |A|^2-weighted norm parts
+// into norms[0..3] with warp-shuffle reductions.
+template <typename T>
+__global__ void residual_kernel(const T* __restrict__ f, long long fb, long long fld, const double* __restrict__ psi,
+                                long long pb, long long pld, int ny, int nx, int batch, double dx, double dy,
+                                const double* __restrict__ lam, int nlam, bf16* __restrict__ hi,
+                                bf16* __restrict__ lo, double* norms) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n = (long long)batch * ny * nx;
+  double s_r = 0, s_f = 0, s_p = 0;
+  const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy);
+  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long b = k / ((long long)ny * nx);
+    long long rem = k - b * ny * nx;
+    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
+    const double* P = psi + b * pb + (long long)y * pld + x;
+    double c = P[0];
+    double e = x + 1 < nx ? P[1] : 0.0, w = x > 0 ? P[-1] : 0.0;
+    double nn = y + 1 < ny ? P[pld] : 0.0, s = y > 0 ? P[-pld] : 0.0;
+    double lap = ((e - 2.0 * c) + w) * idx2 + ((nn - 2.0 * c) + s) * idy2;
+    double fv = (double)f[b * fb + (long long)y * fld + x];
+    double r = fv - (lap - lam[b % nlam] * c);
+    float rv = (float)r;
+    bf16 h = __float2bfloat16_rn(rv);
+    hi[k] = h;
+    lo[k] = __float2bfloat16_rn(rv - __bfloat162float(h));
+    s_r += r * r;
+    s_f += fv * fv;
+    s_p += c * c;
+  }
+  s_r = warp_sum(s_r);
+  s_f = warp_sum(s_f);
+  s_p = warp_sum(s_p);
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&norms[0], s_r);
+    atomicAdd(&norms[1], s_f);
+    atomicAdd(&norms[2], s_p);
+  }
+}
+
+// ---- host side ----------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+// 2-D bf16 tensor map over [outer][inner] (inner contiguous), box
+// {BK, box_outer}, 128-byte swizzle, zero fill out of bounds.
+static bool make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint32_t box_outer) {
+  auto enc = encode_fn();
+  if (!enc) return false;
+  if (((uintptr_t)base & 15) != 0 || (inner * 2) % 16 != 0) return false;
+  cuuint64_t dims[2] = {inner, outer};
+  cuuint64_t strides[1] = {inner * 2};
+  cuuint32_t box[2] = {(cuuint32_t)BK, box_outer};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+// C[M, N] = X[M, K] S[K, N] (S symmetric, given as hi/lo rows of length K).
+static int gemm_split(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Sh, const bf16* Sl, int N,
+                      const Epi& ep, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(gemm_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
+        cudaSuccess)
+      return FVX_ERR_CUDA;
+    attr_set = true;
+  }
+  CUtensorMap a_h, a_l, b_h, b_l;
+  if (!make_map(&a_h, Xh, K, M, BM) || !make_map(&a_l, Xl, K, M, BM) || !make_map(&b_h, Sh, K, N, BN) ||
+      !make_map(&b_l, Sl, K, N, BN))
+    return FVX_ERR_ARG;
+  dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+  if (grid.y > 65535) return FVX_ERR_SHAPE;
+  gemm_split_bf16_kernel<<<grid, THREADS, SMEM_BYTES, st>>>(a_h, a_l, b_h, b_l, K, ep);
+  return fvx_cuda_status();
+}
+
+static int gemm_f64(const double* A, int lda, int M, int K, const double* S, int N, const Epi& ep, cudaStream_t st) {
+  dim3 grid((N + DT - 1) / DT, (M + DT - 1) / DT);
+  if (grid.y > 65535) return FVX_ERR_SHAPE;
+  gemm_f64_kernel<<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
+  return fvx_cuda_status();
+}
+
+static int grid1d(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b > 148 * 32 ? 148 * 32 : (b < 1 ? 1 : b));
+}
+
+}  // namespace dst
+}  // namespace fvx
+
+using namespace fvx;
+using namespace fvx::dst;
+
+struct fvx_dst_plan {
+  int ny, nx, batch_max, n_lam;
+  double dx, dy;
+  bool split_ok;
+  std::vector<double> lam_host;
+  double* lam_dev = nullptr;
+  bf16 *Sxh = nullptr, *Sxl = nullptr, *Syh = nullptr, *Syl = nullptr;
+  double *Sx64 = nullptr, *Sy64 = nullptr;
+  float* inv32 = nullptr;   // [n_lam][ny][nx]
+  double* inv64 = nullptr;  // [n_lam][ny][nx]
+  bf16 *W1h = nullptr, *W1l = nullptr, *W2h = nullptr, *W2l = nullptr;
+  double *V1 = nullptr, *V2 = nullptr;  // FP64 chain work
+  double* norms = nullptr;              // [4]
+  int* err = nullptr;
+};
+
+static void dst_free(fvx_dst_plan* p) {
+  void* ptrs[] = {p->lam_dev, p->Sxh, p->Sxl, p->Syh, p->Syl, p->Sx64, p->Sy64, p->inv32, p->inv64,
+                  p->W1h,     p->W1l, p->W2h, p->W2l, p->V1,  p->V2,  p->norms, p->err};
+  for (void* q : ptrs)
+    if (q) cudaFree(q);
+}
+
+extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int batch_max, const double* lambdas,
+                                   int n_lambda, int want_fp64, fvx_dst_plan** out) {
+  if (!out || !lambdas) return FVX_ERR_ARG;
+  *out = nullptr;
+  if (ny < 1 || nx < 1 || batch_max < 1 || n_lambda < 1) return FVX_ERR_SHAPE;
+  fvx_dst_plan* p = new fvx_dst_plan();
+  p->ny = ny; p->nx = nx; p->dx = dx; p->dy = dy; p->batch_max = batch_max; p->n_lam = n_lambda;
+  p->lam_host.assign(lambdas, lambdas + n_lambda);
+  p->split_ok = (nx % 8 == 0) && (ny % 8 == 0);
+  const size_t plane = (size_t)ny * nx, work = plane * batch_max;
+  bool ok = true;
+  auto A = [&](void** q, size_t bytes) { if (ok && cudaMalloc(q, bytes) != cudaSuccess) ok = false; };
+  A((void**)&p->lam_dev, sizeof(double) * n_lambda);
+  A((void**)&p->Sx64, sizeof(double) * nx * nx);
+  A((void**)&p->Sy64, sizeof(double) * ny * ny);
+  A((void**)&p->inv32, sizeof(float) * plane * n_lambda);
+  A((void**)&p->inv64, sizeof(double) * plane * n_lambda);
+  A((void**)&p->norms, sizeof(double) * 4);
+  A((void**)&p->err, sizeof(int));
+  if (p->split_ok) {
+    A((void**)&p->Sxh, sizeof(bf16) * nx * nx); A((void**)&p->Sxl, sizeof(bf16) * nx * nx);
+    A((void**)&p->Syh, sizeof(bf16) * ny * ny); A((void**)&p->Syl, sizeof(bf16) * ny * ny);
+    A((void**)&p->W1h, sizeof(bf16) * work); A((void**)&p->W1l, sizeof(bf16) * work);
+    A((void**)&p->W2h, sizeof(bf16) * work); A((void**)&p->W2l, sizeof(bf16) * work);
+  }
+  if (want_fp64 || !p->split_ok) {
+    A((void**)&p->V1, sizeof(double) * work);
+    A((void**)&p->V2, sizeof(double) * work);
+  }
+  if (!ok) { dst_free(p); delete p; return FVX_ERR_CUDA; }
+  // host-side tables in FP64
+  auto fill_S = [](int n, std::vector<double>& S) {
+    S.resize((size_t)n * n);
+    for (int j = 0; j < n; ++j)
+      for (int k = 0; k < n; ++k) {
+        // sin(pi (j+1)(k+1)/(n+1)) with the argument reduced mod 2(n+1) to keep it exact
+        long long q = ((long long)(j + 1) * (k + 1)) % (2LL * (n + 1));
+        S[(size_t)j * n + k] = std::sin(M_PI * (double)q / (double)(n + 1));
+      }
+  };
+  std::vector<double> Sx, Sy;
+  fill_S(nx, Sx);
+  fill_S(ny, Sy);
+  std::vector<double> ex(nx), ey(ny);
+  for (int i = 0; i < nx; ++i) { double s = std::sin(M_PI * (i + 1) / (2.0 * (nx + 1))); ex[i] = -4.0 / (dx * dx) * s * s; }
+  for (int j = 0; j < ny; ++j) { double s = std::sin(M_PI * (j + 1) / (2.0 * (ny + 1))); ey[j] = -4.0 / (dy * dy) * s * s; }
+  std::vector<double> inv64(plane * n_lambda);
+  std::vector<float> inv32(plane * n_lambda);
+  for (int l = 0; l < n_lambda; ++l)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        double v = 1.0 / ((ey[j] + ex[i]) - lambdas[l]);
+        inv64[(size_t)l * plane + (size_t)j * nx + i] = v;
+        inv32[(size_t)l * plane + (size_t)j * nx + i] = (float)v;
+      }
+  cudaMemcpy(p->lam_dev, lambdas, sizeof(double) * n_lambda, cudaMemcpyHostToDevice);
+  cudaMemcpy(p->Sx64, Sx.data(), sizeof(double) * Sx.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(p->Sy64, Sy.data(), sizeof(double) * Sy.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(p->inv64, inv64.data(), sizeof(double) * inv64.size(), cudaMemcpyHostToDevice);
+  cudaMemcpy(p->inv32, inv32.data(), sizeof(float) * inv32.size(), cudaMemcpyHostToDevice);
+  if (p->split_ok) {
+    auto split = [](const std::vector<double>& S, std::vector<bf16>& h, std::vector<bf16>& l) {
+      h.resize(S.size());
+      l.resize(S.size());
+      for (size_t k = 0; k < S.size(); ++k) {
+        h[k] = __float2bfloat16_rn((float)S[k]);
+        l[k] = __float2bfloat16_rn((float)(S[k] - (double)__bfloat162float(h[k])));
+      }
+    };
+    std::vector<bf16> h, l;
+    split(Sx, h, l);
+    cudaMemcpy(p->Sxh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(p->Sxl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+    split(Sy, h, l);
+    cudaMemcpy(p->Syh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(p->Syl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+  }
+  cudaMemset(p->err, 0, sizeof(int));
+  if (cudaDeviceSynchronize() != cudaSuccess) { dst_free(p); delete p; return FVX_ERR_CUDA; }
+  *out = p;
+  return FVX_OK;
+}
+
+extern "C" int fvx_dst_plan_destroy(fvx_dst_plan* p) {
+  if (!p) return FVX_ERR_ARG;
+  cudaDeviceSynchronize();
+  dst_free(p);
+  delete p;
+  return fvx_cuda_status();
+}
+
+// Device error flag of the plan's kernels (1 = a bounded wait gave up).
+// Synchronises the stream.
+extern "C" int fvx_dst_plan_check(fvx_dst_plan* p, void* stream) {
+  if (!p) return FVX_ERR_ARG;
+  int e = 0;
+  if (cudaMemcpyAsync(&e, p->err, sizeof(int), cudaMemcpyDeviceToHost, fvx_stream(stream)) != cudaSuccess ||
+      cudaStreamSynchronize(fvx_stream(stream)) != cudaSuccess)
+    return FVX_ERR_CUDA;
+  return e ? FVX_ERR_TIMEOUT : FVX_OK;
+}
+
+static Epi make_epi(fvx_dst_plan* p, int mode, int R, int M, int N, void* o0, void* o1, long long bstride,
+                    long long ld, int off_n, int off_r, double alpha, bool eig) {
+  Epi e;
+  e.mode = mode; e.rows_per_batch = R; e.m_total = M; e.n_cols = N; e.out0 = o0; e.out1 = o1;
+  e.batch_stride = bstride; e.ld = ld; e.off_n = off_n; e.off_r = off_r; e.alpha = alpha;
+  e.inv_eig = eig ? p->inv32 : nullptr; e.inv_eig64 = eig ? p->inv64 : nullptr; e.n_eig = p->n_lam;
+  e.err = p->err;
+  return e;
+}
+
+// The split-BF16 chain on operands already split into W1 ([B][ny][nx]).
+// Output: mode EPI_F32 / EPI_F64 / EPI_F64_ACC into ``out`` with batch
+// stride ``ob`` and row pitch ``old`` (interior [B][ny][nx] view).
+static int chain_split(fvx_dst_plan* p, int B, int out_mode, void* out, long long ob, long long old,
+                       cudaStream_t st) {
+  const int ny = p->ny, nx = p->nx;
+  const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
+  int rc;
+  // 1: (Q S_x)^T -> W2 [B][nx][ny]
+  Epi e1 = make_epi(p, EPI_SPLIT, ny, B * ny, nx, p->W2h, p->W2l, (long long)nx * ny, ny, 0, 0, 1.0, false);
+  if ((rc = gemm_split(p->W1h, p->W1l, B * ny, nx, p->Sxh, p->Sxl, nx, e1, st))) return rc;
+  // 2: (S_y Q S_x) ./ Lambda -> W1 [B][ny][nx]
+  Epi e2 = make_epi(p, EPI_SPLIT, nx, B * nx, ny, p->W1h, p->W1l, (long long)ny * nx, nx, 0, 0, 1.0, true);
+  // inv_eig is indexed [n][r] = [y'][x'] = the [ny][nx] grid
+  if ((rc = gemm_split(p->W2h, p->W2l, B * nx, ny, p->Syh, p->Syl, ny, e2, st))) return rc;
+  // 3: (G S_x)^T -> W2
+  if ((rc = gemm_split(p->W1h, p->W1l, B * ny, nx, p->Sxh, p->Sxl, nx, e1, st))) return rc;
+  // 4: c S_y G S_x -> out [B][ny][nx]
+  Epi e4 = make_epi(p, out_mode, nx, B * nx, ny, out, nullptr, ob, old, 0, 0, c, false);
+  return gemm_split(p->W2h, p->W2l, B * nx, ny, p->Syh, p->Syl, ny, e4, st);
+}
+
+static int chain_f64(fvx_dst_plan* p, int B, int out_mode, void* out, long long ob, long long old, cudaStream_t st) {
+  const int ny = p->ny, nx = p->nx;
+  const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
+  int rc;
+  Epi e1 = make_epi(p, EPI_F64, ny, B * ny, nx, p->V2, nullptr, (long long)nx * ny, ny, 0, 0, 1.0, false);
+  if ((rc = gemm_f64(p->V1, nx, B * ny, nx, p->Sx64, nx, e1, st))) return rc;
+  Epi e2 = make_epi(p, EPI_F64, nx, B * nx, ny, p->V1, nullptr, (long long)ny * nx, nx, 0, 0, 1.0, true);
+  if ((rc = gemm_f64(p->V2, ny, B * nx, ny, p->Sy64, ny, e2, st))) return rc;
+  if ((rc = gemm_f64(p->V1, nx, B * ny, nx, p->Sx64, nx, e1, st))) return rc;
+  Epi e4 = make_epi(p, out_mode, nx, B * nx, ny, out, nullptr, ob, old, 0, 0, c, false);
+  return gemm_f64(p->V2, ny, B * nx, ny, p->Sy64, ny, e4, st);
+}
+
+// FP32 solve through the split-BF16 tensor-core chain.  rhs / psi are
+// interior views: element (b, y, x) at ptr[b*bstride + y*ld + x].
+extern "C" int fvx_dst_solve_f32(fvx_dst_plan* p, const float* rhs, long long rhs_bstride, long long rhs_ld,
+                                 float* psi, long long psi_bstride, long long psi_ld, int batch, void* stream) {
+  if (!p || !rhs || !psi) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  long long n = (long long)batch * p->ny * p->nx;
+  if (!p->split_ok) {  // sizes the TMA tiles cannot address: FP64 SIMT chain, FP32 output
+    copy_in_f64_kernel<float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, p->ny, p->nx, batch, p->V1);
+    int rc0 = fvx_cuda_status();
+    if (rc0) return rc0;
+    return chain_f64(p, batch, EPI_F32, psi, psi_bstride, psi_ld, st);
+  }
+  split_input_kernel<float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, p->ny, p->nx, batch, p->W1h,
+                                                        p->W1l, 1.0);
+  int rc = fvx_cuda_status();
+  if (rc) return rc;
+  return chain_split(p, batch, EPI_F32, psi, psi_bstride, psi_ld, st);
+}
+
+// Same chain on operands the caller already split into the plan's first
+// workspace (fvx_dst_workspace); used by the fused QG stage kernel.
+extern "C" int fvx_dst_solve_presplit_f32(fvx_dst_plan* p, float* psi, long long psi_bstride, long long psi_ld,
+                                          int batch, void* stream) {
+  if (!p || !psi) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max || !p->split_ok) return FVX_ERR_SHAPE;
+  return chain_split(p, batch, EPI_F32, psi, psi_bstride, psi_ld, fvx_stream(stream));
+}
+
+extern "C" int fvx_dst_workspace(fvx_dst_plan* p, void** w1_hi, void** w1_lo) {
+  if (!p || !w1_hi || !w1_lo) return FVX_ERR_ARG;
+  *w1_hi = p->W1h;
+  *w1_lo = p->W1l;
+  return p->split_ok ? FVX_OK : FVX_ERR_SHAPE;
+}
+
+// FP64 solve.  method 0: FP64 SIMT chain (one pass).  method 1: split-BF16
+// chain + iterative refinement on the FP64 residual until the normwise
+// backward error ||r|| / (||A|| ||psi|| + ||f||) <= tol (||A|| the 2-norm
+// bound 8/h^2 + lambda) or max_iter passes.  info (host, may be null):
+// [passes, backward error, ||r||/||f||].
+extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long rhs_bstride, long long rhs_ld,
+                                 double* psi, long long psi_bstride, long long psi_ld, int batch, int method,
+                                 double tol, int max_iter, double* info, void* stream) {
+  if (!p || !rhs || !psi) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  const int ny = p->ny, nx = p->nx;
+  long long n = (long long)batch * ny * nx;
+  int rc;
+  if (method == 0 || !p->split_ok) {
+    if (!p->V1) return FVX_ERR_ARG;
+    copy_in_f64_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->V1);
+    if ((rc = fvx_cuda_status())) return rc;
+    rc = chain_f64(p, batch, EPI_F64, psi, psi_bstride, psi_ld, st);
+    if (info) { info[0] = 1; info[1] = -1; info[2] = -1; }
+    return rc;
+  }
+  double lam_max = 0;
+  for (double l : p->lam_host) lam_max = fmax(lam_max, fabs(l));
+  const double anorm = 4.0 / (p->dx * p->dx) + 4.0 / (p->dy * p->dy) + lam_max;
+  zero_f64_kernel<<<grid1d(n), 256, 0, st>>>(psi, psi_bstride, psi_ld, ny, nx, batch);
+  split_input_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->W1h, p->W1l, 1.0);
+  if ((rc = fvx_cuda_status())) return rc;
+  double be = 1, rr = 1;
+  int it = 0;
+  for (it = 1; it <= max_iter; ++it) {
+    if ((rc = chain_split(p, batch, EPI_F64_ACC, psi, psi_bstride, psi_ld, st))) return rc;
+    cudaMemsetAsync(p->norms, 0, sizeof(double) * 4, st);
+    residual_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
+                                                        batch, p->dx, p->dy, p->lam_dev, p->n_lam, p->W1h, p->W1l,
+                                                        p->norms);
+    double h[4];
+    if (cudaMemcpyAsync(h, p->norms, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    const double rn = sqrt(h[0]), fn = sqrt(h[1]), pn = sqrt(h[2]);
+    be = rn / (anorm * pn + fn + 1e-300);
+    rr = rn / (fn + 1e-300);
+    if (be <= tol) break;
+  }
+  if (info) { info[0] = it > max_iter ? max_iter : it; info[1] = be; info[2] = rr; }
+  return be <= tol ? FVX_OK : FVX_ERR_NOT_CONVERGED;
+}
+
+// One product of the split chain on the plan's workspaces, for timing the
+// tensor-core GEMM in isolation: which 0 = (W1 S_x)^T -> W2, 1 = (W2 S_y) ./
+// Lambda -> W1.  Operands are whatever the workspaces currently hold.
+extern "C" int fvx_dst_gemm_step(fvx_dst_plan* p, int which, int batch, void* stream) {
+  if (!p || !p->split_ok) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max) return FVX_ERR_SHAPE;
+  const int ny = p->ny, nx = p->nx;
+  cudaStream_t st = fvx_stream(stream);
+  if (which == 0) {
+    Epi e1 = make_epi(p, EPI_SPLIT, ny, batch * ny, nx, p->W2h, p->W2l, (long long)nx * ny, ny, 0, 0, 1.0, false);
+    return gemm_split(p->W1h, p->W1l, batch * ny, nx, p->Sxh, p->Sxl, nx, e1, st);
+  }
+  if (which == 1) {
+    Epi e2 = make_epi(p, EPI_SPLIT, nx, batch * nx, ny, p->W1h, p->W1l, (long long)ny * nx, nx, 0, 0, 1.0, true);
+    return gemm_split(p->W2h, p->W2l, batch * nx, ny, p->Syh, p->Syl, ny, e2, st);
+  }
+  return FVX_ERR_ARG;
+}

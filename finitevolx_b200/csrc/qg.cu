@@ -1,0 +1,249 @@
+// Fused QG 1.5-layer RK stage (scripts/qg_1p5_layer.py:115-145, 420-497 with
+// timestepping/explicit_rk.py:74-121).  One kernel per Runge-Kutta stage:
+//
+//   q_b   = BC(q_s)               periodic wrap (boundary.py:52-75) or zero ring
+//   X     = interior(T_to_X(psi)) psi from the DST solve, zero ghost ring
+//   u, v  = -diff_y_X_to_U(X), diff_x_X_to_V(X)
+//   rhs   = Advection2D(q_b, u, v, scheme)              [2:-2, 2:-2]
+//         + (-beta * V_to_T(v))                           [1:-1, 1:-1]
+//         + forcing - drag * laplacian(psi) + nu * laplacian(q_b)
+//   q_out = a * q_n + b * q_s + c * rhs                  (c = stage weight * dt)
+//
+// q_b is never materialised (ghost values come from wrap-around tile loads),
+// face fluxes and velocities stay in shared memory, and the kernel writes
+// q_out (interior, plus the ghost ring on the last stage) and optionally the
+// bf16 hi/lo split of q_out's interior that the next DST product reads.
+#include "recon.cuh"
+
+#include <cuda_bf16.h>
+
+namespace fvx {
+namespace qg {
+
+constexpr int TX = 64, TY = 16, THREADS = 256;
+
+struct StageArgs {
+  const void* qs;      // stage state [Ny][Nx]
+  const void* qn;      // step-start state (null on stage 1)
+  const void* psi;     // interior-only [Ny-2][Nx-2]
+  const void* forcing; // [Ny][Nx] or null
+  void* out;           // [Ny][Nx]
+  __nv_bfloat16* split_hi;  // [Ny-2][Nx-2] or null
+  __nv_bfloat16* split_lo;
+  int ny, nx;
+  double a, b, c;      // out = a*qn + b*qs + c*rhs
+  double dx, dy, beta, drag, visc;
+  int periodic;        // 1: periodic ghost ring, 0: zero (wall) ghost ring
+  int write_ghost;
+};
+
+template <typename T, int S>
+__global__ void __launch_bounds__(THREADS)
+stage_kernel(StageArgs A) {
+  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
+  constexpr int QW = TX + 2 * H, QH = TY + 2 * H;
+  extern __shared__ __align__(16) uint8_t sm[];
+  T* qt = (T*)sm;                          // [QH][QW]
+  T* pt = qt + QH * QW;                    // psi [TY+2][TX+2], origin (y0-1, x0-1)
+  T* xt = pt + (TY + 2) * (TX + 2);        // X [TY+1][TX+1], origin (y0-1, x0-1)
+  T* fe = xt + (TY + 1) * (TX + 1);        // [TY][TX+1]
+  T* fn = fe + TY * (TX + 1);              // [TY+1][TX]
+  const int ny = A.ny, nx = A.nx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int tid = threadIdx.x;
+  const T* qs = (const T*)A.qs;
+  const T* psi = (const T*)A.psi;
+  const int nxi = nx - 2;
+  // ---- loads: q with BC applied on the fly, psi with zero outside --------
+  for (int k = tid; k < QH * QW; k += THREADS) {
+    int ly = k / QW, lx = k - ly * QW;
+    int gy = y0 - H + ly, gx = x0 - H + lx;
+    T val = T(0);
+    if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
+      bool gh = gy == 0 || gy == ny - 1 || gx == 0 || gx == nx - 1;
+      if (!gh) val = qs[(size_t)gy * nx + gx];
+      else if (A.periodic) {
+        int sy = gy == 0 ? ny - 2 : (gy == ny - 1 ? 1 : gy);
+        int sx = gx == 0 ? nx - 2 : (gx == nx - 1 ? 1 : gx);
+        val = qs[(size_t)sy * nx + sx];
+      }
+    }
+    qt[k] = val;
+  }
+  for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
+    int ly = k / (TX + 2), lx = k - ly * (TX + 2);
+    int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
+    pt[k] = (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2) ? psi[(size_t)(gy - 1) * nxi + (gx - 1)] : T(0);
+  }
+  __syncthreads();
+  // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
+  for (int k = tid; k < (TY + 1) * (TX + 1); k += THREADS) {
+    int ly = k / (TX + 1), lx = k - ly * (TX + 1);
+    int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
+    T val = T(0);
+    if (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2) {
+      const T* p = pt + ly * (TX + 2) + lx;  // psi at (gy, gx)
+      val = T(0.25) * (p[0] + p[1] + p[TX + 2] + p[TX + 3]);
+    }
+    xt[k] = val;
+  }
+  __syncthreads();
+  const T dx = T(A.dx), dy = T(A.dy);
+  // u at U-point (j, i) = -(X[j,i] - X[j-1,i]) / dy on [1, N-2]^2
+  auto uvel = [&](int gy, int gx) -> T {
+    if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
+    const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
+    return -((p[0] - p[-(TX + 1)]) / dy);
+  };
+  auto vvel = [&](int gy, int gx) -> T {
+    if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
+    const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
+    return (p[0] - p[-1]) / dx;
+  };
+  // ---- face fluxes --------------------------------------------------------
+  for (int k = tid; k < TY * (TX + 1); k += THREADS) {
+    int ly = k / (TX + 1), lf = k - ly * (TX + 1);
+    int gj = y0 + ly, gi = x0 - 1 + lf;
+    T f = T(0);
+    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
+      T uu = uvel(gj, gi);
+      f = face_value<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
+    }
+    fe[k] = f;
+  }
+  for (int k = tid; k < (TY + 1) * TX; k += THREADS) {
+    int lf = k / TX, lx = k - lf * TX;
+    int gj = y0 - 1 + lf, gi = x0 + lx;
+    T f = T(0);
+    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
+      T vv = vvel(gj, gi);
+      f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+    }
+    fn[k] = f;
+  }
+  __syncthreads();
+  // ---- tendency, RK combination, stores ------------------------------------
+  const T* qn = (const T*)A.qn;
+  const T* F = (const T*)A.forcing;
+  T* out = (T*)A.out;
+  const T beta = T(A.beta), drag = T(A.drag), visc = T(A.visc);
+  const T ca = T(A.a), cb = T(A.b), cc = T(A.c);
+  for (int k = tid; k < TY * TX; k += THREADS) {
+    int ly = k / TX, lx = k - ly * TX;
+    int gj = y0 + ly, gi = x0 + lx;
+    if (gj < 1 || gj > ny - 2 || gi < 1 || gi > nx - 2) continue;  // ghost ring written below
+    T rhs = T(0);
+    if (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3)
+      rhs = -((fe[ly * (TX + 1) + lx + 1] - fe[ly * (TX + 1) + lx]) / dx +
+              (fn[(ly + 1) * TX + lx] - fn[ly * TX + lx]) / dy);
+    T vc = T(0.5) * (vvel(gj, gi) + vvel(gj - 1, gi));
+    rhs = rhs + (-beta * vc);
+    size_t g = (size_t)gj * nx + gi;
+    if (F) rhs = rhs + F[g];
+    if (A.drag != 0.0) {
+      const T* p = pt + (ly + 1) * (TX + 2) + (lx + 1);
+      T d2x = ((p[1] - p[0]) - (p[0] - p[-1])) / (dx * dx);
+      T d2y = ((p[TX + 2] - p[0]) - (p[0] - p[-(TX + 2)])) / (dy * dy);
+      rhs = rhs - drag * (d2x + d2y);
+    }
+    if (A.visc != 0.0) {
+      const T* q = qt + (ly + H) * QW + (lx + H);
+      T d2x = ((q[1] - q[0]) - (q[0] - q[-1])) / (dx * dx);
+      T d2y = ((q[QW] - q[0]) - (q[0] - q[-QW])) / (dy * dy);
+      rhs = rhs + visc * (d2x + d2y);
+    }
+    T qsv = qt[(ly + H) * QW + (lx + H)];
+    T r = cb * qsv;
+    if (qn) r = ca * qn[g] + r;
+    r = r + cc * rhs;
+    out[g] = r;
+    if (A.split_hi) {
+      size_t s = (size_t)(gj - 1) * nxi + (gi - 1);
+      float fv = (float)r;
+      __nv_bfloat16 h = __float2bfloat16_rn(fv);
+      A.split_hi[s] = h;
+      A.split_lo[s] = __float2bfloat16_rn(fv - __bfloat162float(h));
+    }
+    if (A.write_ghost && A.periodic) {
+      // copies of this interior cell into the ghost ring (S, N, W, E fill)
+      int ys[2] = {gj, gj == ny - 2 ? 0 : (gj == 1 ? ny - 1 : -1)};
+      int xs[2] = {gi, gi == nx - 2 ? 0 : (gi == 1 ? nx - 1 : -1)};
+      for (int a2 = 0; a2 < 2; ++a2)
+        for (int b2 = 0; b2 < 2; ++b2) {
+          if ((a2 == 0 && b2 == 0) || ys[a2] < 0 || xs[b2] < 0) continue;
+          out[(size_t)ys[a2] * nx + xs[b2]] = r;
+        }
+    }
+  }
+  if (A.write_ghost && !A.periodic) {
+    for (int k = tid; k < TY * TX; k += THREADS) {
+      int ly = k / TX, lx = k - ly * TX;
+      int gj = y0 + ly, gi = x0 + lx;
+      if (gj < ny && gi < nx && (gj == 0 || gj == ny - 1 || gi == 0 || gi == nx - 1))
+        out[(size_t)gj * nx + gi] = T(0);
+    }
+  }
+}
+
+template <typename T, int S>
+static size_t smem_bytes() {
+  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
+  size_t n = (size_t)(TY + 2 * H) * (TX + 2 * H) + (TY + 2) * (TX + 2) + (TY + 1) * (TX + 1) + TY * (TX + 1) +
+             (TY + 1) * TX;
+  return n * sizeof(T);
+}
+
+template <typename T, int S>
+static int launch(const StageArgs& a, cudaStream_t st) {
+  size_t sm = smem_bytes<T, S>();
+  static bool set = false;
+  if (!set) {
+    if (cudaFuncSetAttribute(stage_kernel<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    set = true;
+  }
+  dim3 g((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
+  stage_kernel<T, S><<<g, THREADS, sm, st>>>(a);
+  return fvx_cuda_status();
+}
+
+template <typename T>
+static int dispatch(int method, const StageArgs& a, cudaStream_t st) {
+  switch (method) {
+    case FVX_UPWIND1: return launch<T, FVX_UPWIND1>(a, st);
+    case FVX_UPWIND3: return launch<T, FVX_UPWIND3>(a, st);
+    case FVX_WENO3: return launch<T, FVX_WENO3>(a, st);
+    case FVX_WENO5: return launch<T, FVX_WENO5>(a, st);
+    case FVX_WENOZ5: return launch<T, FVX_WENOZ5>(a, st);
+    case FVX_WENO7: return launch<T, FVX_WENO7>(a, st);
+    case FVX_WENO9: return launch<T, FVX_WENO9>(a, st);
+    case FVX_VAN_LEER: return launch<T, FVX_VAN_LEER>(a, st);
+    case FVX_MINMOD: return launch<T, FVX_MINMOD>(a, st);
+    default: return FVX_ERR_METHOD;
+  }
+}
+
+}  // namespace qg
+}  // namespace fvx
+
+using namespace fvx;
+
+#define FVX_DEF_QG(SFX, T)                                                                                   \
+  extern "C" int fvx_qg_stage_##SFX(const T* q_stage, const T* q_start, const T* psi_interior,             \
+                                    const T* forcing, T* q_out, void* split_hi, void* split_lo, int ny, int nx, \
+                                    double dx, double dy, double beta, double drag, double viscosity,       \
+                                    double a, double b, double c, int method, int periodic, int write_ghost, \
+                                    void* stream) {                                                          \
+    if (!q_stage || !psi_interior || !q_out) return FVX_ERR_ARG;                                             \
+    if ((split_hi == nullptr) != (split_lo == nullptr)) return FVX_ERR_ARG;                                  \
+    if (ny < 6 || nx < 6) return FVX_ERR_SHAPE;                                                              \
+    qg::StageArgs A;                                                                                         \
+    A.qs = q_stage; A.qn = q_start; A.psi = psi_interior; A.forcing = forcing; A.out = q_out;              \
+    A.split_hi = (__nv_bfloat16*)split_hi; A.split_lo = (__nv_bfloat16*)split_lo;                          \
+    A.ny = ny; A.nx = nx; A.a = a; A.b = b; A.c = c; A.dx = dx; A.dy = dy; A.beta = beta;                    \
+    A.drag = drag; A.visc = viscosity; A.periodic = periodic; A.write_ghost = write_ghost;                   \
+    return qg::dispatch<T>(method, A, fvx_stream(stream));                                                   \
+  }
+
+FVX_DEF_QG(f32, float)
+FVX_DEF_QG(f64, double)

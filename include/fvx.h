@@ -148,6 +148,61 @@ int fvx_lincomb_f32(int64_t n, double a, const float* x, double b, const float* 
 int fvx_lincomb_f64(int64_t n, double a, const double* x, double b, const double* y, double c,
                     const double* z, double* out, void* stream);
 
+
+/* ---- Dirichlet Helmholtz by DST-I tensor-core GEMMs --------------------- */
+
+/* Replaces spectraldiffx solve_helmholtz_dst as re-exported by finitevolX
+ * (solvers/spectral.py:14-98; called at scripts/qg_1p5_layer.py:444-449):
+ * (nabla^2 - lambda) psi = rhs on an interior-only [ny, nx] array, psi = 0
+ * outside.  A plan holds the DST-I matrices, eigenvalue grids and
+ * workspaces; batch element b uses lambdas[b % n_lambda] (pv_inversion's
+ * per-layer lambda, solvers/elliptic.py:517-541).  Creating a plan is the
+ * only allocating call. */
+typedef struct fvx_dst_plan fvx_dst_plan;
+int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int batch_max, const double* lambdas, int n_lambda,
+                        int want_fp64, fvx_dst_plan** plan);
+int fvx_dst_plan_destroy(fvx_dst_plan* plan);
+/* Reads the plan's device error flag (7 if a bounded wait gave up); syncs. */
+int fvx_dst_plan_check(fvx_dst_plan* plan, void* stream);
+/* FP32: 3xBF16 split tcgen05 chain (ny, nx multiples of 8; otherwise the
+ * FP64 chain with FP32 output).  Element (b,y,x) at ptr[b*bstride + y*ld + x]. */
+int fvx_dst_solve_f32(fvx_dst_plan* plan, const float* rhs, long long rhs_bstride, long long rhs_ld, float* psi,
+                      long long psi_bstride, long long psi_ld, int batch, void* stream);
+/* FP64: method 0 = FP64 SIMT chain; 1 = split chain + FP64 iterative
+ * refinement to normwise backward error <= tol (info: passes, backward
+ * error, ||r||/||f||; returns 5 if max_iter passes do not reach tol). */
+int fvx_dst_solve_f64(fvx_dst_plan* plan, const double* rhs, long long rhs_bstride, long long rhs_ld, double* psi,
+                      long long psi_bstride, long long psi_ld, int batch, int method, double tol, int max_iter,
+                      double* info, void* stream);
+/* Same chain on an operand already split into the plan workspace (written
+ * by fvx_qg_stage_f32's split outputs); fvx_dst_workspace returns it. */
+int fvx_dst_solve_presplit_f32(fvx_dst_plan* plan, float* psi, long long psi_bstride, long long psi_ld, int batch,
+                               void* stream);
+int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
+/* One product of the chain on the current workspaces (timing only). */
+int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
+
+/* ---- fused QG RK stage ---------------------------------------------------- */
+
+/* One Runge-Kutta stage of the QG 1.5-layer PV equation
+ * (scripts/qg_1p5_layer.py:454-487 inside rk3_ssp_step,
+ * timestepping/explicit_rk.py:74-121): q_out = a*q_start + b*q_stage + c*rhs
+ * with rhs = Advection2D(BC(q_stage), u, v) - beta*V_to_T(v) + forcing
+ * - drag*laplacian(psi) + viscosity*laplacian(BC(q_stage)), (u, v) the
+ * geostrophic velocity of psi_interior (zero outside).  periodic: 1 periodic
+ * ghost ring, 0 zero ring.  write_ghost refills q_out's ring.  split_hi/lo
+ * (bf16 [ny-2][nx-2], may be NULL) receive q_out's interior for the next DST.
+ * method: 1 upwind1, 3 upwind3, 4 weno3, 5 weno5, 6 wenoz5, 7 weno7,
+ * 8 weno9, 9 minmod, 10 van_leer. */
+int fvx_qg_stage_f32(const float* q_stage, const float* q_start, const float* psi_interior, const float* forcing,
+                     float* q_out, void* split_hi, void* split_lo, int ny, int nx, double dx, double dy,
+                     double beta, double drag, double viscosity, double a, double b, double c, int method,
+                     int periodic, int write_ghost, void* stream);
+int fvx_qg_stage_f64(const double* q_stage, const double* q_start, const double* psi_interior,
+                     const double* forcing, double* q_out, void* split_hi, void* split_lo, int ny, int nx,
+                     double dx, double dy, double beta, double drag, double viscosity, double a, double b,
+                     double c, int method, int periodic, int write_ghost, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

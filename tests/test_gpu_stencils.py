@@ -297,7 +297,7 @@ def test_periodic_and_pad(cuda_ok):
 def test_rk3_with_advection_fp64(cuda_ok):
     ny, nx = 34, 34
     h, u, v = rand_fields(ny, nx, 3)
-    grid = fvx.ArakawaCGrid2D.from_interior(nx - 2, ny - 2, 1.0, 1.0)
+    grid = fvx.ArakawaCGrid2D(Nx=nx, Ny=ny, Lx=nx - 2.0, Ly=ny - 2.0, dx=1.0, dy=1.0)
     adv = fvx.Advection2D(grid)
     ud, vd = dev(u), dev(v)
     got = fvx.rk3_ssp_step(dev(h), lambda q: adv(fvx.enforce_periodic(q), ud, vd, "weno5"), 0.05)
