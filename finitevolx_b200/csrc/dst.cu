@@ -746,3 +746,132 @@ extern "C" int fvx_dst_gemm_step(fvx_dst_plan* p, int which, int batch, void* st
   }
   return FVX_ERR_ARG;
 }
+
+// ===========================================================================
+// Allocation-free FP32 DST Helmholtz solve.
+//
+// Some callers cannot call cudaMalloc at solve time: a framework custom call
+// (an XLA FFI handler, for instance) where the framework owns every byte of
+// device memory and a library-side allocation would bypass its allocator
+// and its limits; a host that budgets all device memory up front and
+// forbids allocation once it runs; or a latency-critical loop that cannot
+// afford cudaMalloc's implicit device synchronisation.  For them,
+// fvx_dst_solve_noalloc_f32 runs the same 3xBF16 tensor-core chain as
+// fvx_dst_solve_f32 without a plan: its scratch (DST matrices, inverse
+// eigenvalue grid, two split operand buffers and an error flag) lives in the
+// file-scope array below, which every GPU that loads this library holds
+// until the process exits.  The caller still passes rhs and psi.
+//
+// Limits and rules:
+//   * ny and nx (interior sizes) must be multiples of 8 and at most
+//     kNoAllocMaxN = 256, batch 1, one lambda; larger sizes return
+//     FVX_ERR_SHAPE (1) and touch nothing.
+//   * The first call on a device looks up the array's device address with
+//     cudaGetSymbolAddress (once per device, with that device current);
+//     make that first call before any stream capture.
+//   * Every call shares the one array and overwrites it (tables, operands
+//     and the error flag are rewritten or cleared by each call), so calls
+//     that overlap on the GPU -- on different streams, or from different
+//     host threads -- race and corrupt each other's results.
+// ===========================================================================
+namespace fvx {
+namespace dst {
+
+constexpr int kNoAllocMaxN = 256;
+constexpr size_t kNaPlane = (size_t)kNoAllocMaxN * kNoAllocMaxN;
+// bf16: S_x hi/lo, S_y hi/lo, W1 hi/lo, W2 hi/lo (8 planes); f32 1/Lambda;
+// int error flag (padded to 256 bytes)
+constexpr size_t kNoAllocBytes = 8 * kNaPlane * sizeof(bf16) + kNaPlane * sizeof(float) + 256;
+
+static __device__ __align__(256) unsigned char g_dst_noalloc_scratch[kNoAllocBytes];
+
+// DST-I matrices (split into bf16 hi/lo) and 1/Lambda for one (ny, nx, dx,
+// dy, lambda), computed in FP64 on the device.
+__global__ void noalloc_tables_kernel(int ny, int nx, double dx, double dy, double lam, bf16* sxh, bf16* sxl,
+                                      bf16* syh, bf16* syl, float* inv) {
+  const int n2 = nx * nx, m2 = ny * ny, p = ny * nx;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n2 + m2 + p; k += gridDim.x * blockDim.x) {
+    if (k < n2 + m2) {
+      const bool isx = k < n2;
+      const int n = isx ? nx : ny, kk = isx ? k : k - n2;
+      const int j = kk / n, c = kk - j * n;
+      const long long q = ((long long)(j + 1) * (c + 1)) % (2LL * (n + 1));
+      const double s = sinpi((double)q / (double)(n + 1));
+      const bf16 h = __float2bfloat16_rn((float)s);
+      const bf16 l = __float2bfloat16_rn((float)(s - (double)__bfloat162float(h)));
+      (isx ? sxh : syh)[kk] = h;
+      (isx ? sxl : syl)[kk] = l;
+    } else {
+      const int kk = k - n2 - m2, j = kk / nx, i = kk - j * nx;
+      const double sy = sinpi((double)(j + 1) / (2.0 * (ny + 1)));
+      const double sx = sinpi((double)(i + 1) / (2.0 * (nx + 1)));
+      const double ey = -4.0 / (dy * dy) * sy * sy, ex = -4.0 / (dx * dx) * sx * sx;
+      inv[kk] = (float)(1.0 / ((ey + ex) - lam));
+    }
+  }
+}
+
+}  // namespace dst
+}  // namespace fvx
+
+#include <mutex>
+
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[128] = {nullptr};
+
+extern "C" int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, float* psi, long long psi_ld, int ny,
+                                         int nx, double dx, double dy, double lambda, void* stream) {
+  using namespace fvx::dst;
+  if (!rhs || !psi) return FVX_ERR_ARG;
+  if (ny < 8 || nx < 8 || ny > kNoAllocMaxN || nx > kNoAllocMaxN || ny % 8 || nx % 8) return FVX_ERR_SHAPE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return FVX_ERR_CUDA;
+  unsigned char* base;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      // Load this file's module on the current device first (with lazy module
+      // loading nothing may have loaded it yet), then look up the array.
+      cudaFuncAttributes fa;
+      if (cudaFuncGetAttributes(&fa, noalloc_tables_kernel) != cudaSuccess) {
+        cudaGetLastError();
+        return FVX_ERR_CUDA;
+      }
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_dst_noalloc_scratch) != cudaSuccess || !ptr) {
+        cudaGetLastError();
+        return FVX_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = ptr;
+    }
+    base = (unsigned char*)g_noalloc_addr[dev];
+  }
+  cudaStream_t st = fvx_stream(stream);
+  bf16* pl = (bf16*)base;
+  bf16 *sxh = pl, *sxl = pl + kNaPlane, *syh = pl + 2 * kNaPlane, *syl = pl + 3 * kNaPlane;
+  bf16 *w1h = pl + 4 * kNaPlane, *w1l = pl + 5 * kNaPlane, *w2h = pl + 6 * kNaPlane, *w2l = pl + 7 * kNaPlane;
+  float* inv = (float*)(pl + 8 * kNaPlane);
+  int* err = (int*)(inv + kNaPlane);
+  if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return FVX_ERR_CUDA;
+  const int total = nx * nx + ny * ny + ny * nx;
+  noalloc_tables_kernel<<<(total + 255) / 256, 256, 0, st>>>(ny, nx, dx, dy, lambda, sxh, sxl, syh, syl, inv);
+  split_input_kernel<float><<<grid1d((long long)ny * nx), 256, 0, st>>>(rhs, 0, rhs_ld, ny, nx, 1, w1h, w1l, 1.0);
+  int rc = fvx_cuda_status();
+  if (rc) return rc;
+  auto epi = [&](int mode, int R, int M, int N, void* o0, void* o1, long long bs, long long ld, double alpha,
+                 bool eig) {
+    Epi e;
+    e.mode = mode; e.rows_per_batch = R; e.m_total = M; e.n_cols = N; e.out0 = o0; e.out1 = o1;
+    e.batch_stride = bs; e.ld = ld; e.off_n = 0; e.off_r = 0; e.alpha = alpha;
+    e.inv_eig = eig ? inv : nullptr; e.inv_eig64 = nullptr; e.n_eig = 1; e.err = err;
+    return e;
+  };
+  const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
+  if ((rc = gemm_split(w1h, w1l, ny, nx, sxh, sxl, nx, epi(EPI_SPLIT, ny, ny, nx, w2h, w2l, (long long)nx * ny, ny, 1.0, false), st)))
+    return rc;
+  if ((rc = gemm_split(w2h, w2l, nx, ny, syh, syl, ny, epi(EPI_SPLIT, nx, nx, ny, w1h, w1l, (long long)ny * nx, nx, 1.0, true), st)))
+    return rc;
+  if ((rc = gemm_split(w1h, w1l, ny, nx, sxh, sxl, nx, epi(EPI_SPLIT, ny, ny, nx, w2h, w2l, (long long)nx * ny, ny, 1.0, false), st)))
+    return rc;
+  return gemm_split(w2h, w2l, nx, ny, syh, syl, ny, epi(EPI_F32, nx, nx, ny, psi, nullptr, 0, psi_ld, c, false), st);
+}

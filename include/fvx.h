@@ -182,6 +182,20 @@ int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
 /* One product of the chain on the current workspaces (timing only). */
 int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
 
+/* Allocation-free FP32 DST Helmholtz solve.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc while they run
+ * (a framework custom call whose framework owns all device memory, a host
+ * that forbids allocation after start-up, a loop that cannot take
+ * cudaMalloc's implicit synchronisation).  Same result as
+ * fvx_dst_solve_f32, batch 1, one lambda; its scratch is a fixed
+ * file-scope device array (about 1.3 MB, held by every GPU that loads the
+ * library until exit), so ny and nx must be multiples of 8 and at most 256
+ * (otherwise returns 1 and does nothing).  The first call on a device looks
+ * up the array's address (make it before any stream capture).  All calls
+ * share the array: calls that overlap on the GPU race. */
+int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, float* psi, long long psi_ld, int ny, int nx,
+                              double dx, double dy, double lambda, void* stream);
+
 /* ---- fused QG RK stage ---------------------------------------------------- */
 
 /* One Runge-Kutta stage of the QG 1.5-layer PV equation

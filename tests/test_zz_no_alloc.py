@@ -1,0 +1,79 @@
+"""The allocation-free DST solve entry point, called through the C ABI.
+
+``fvx_dst_solve_noalloc_f32`` serves callers that cannot call cudaMalloc
+while they run (a framework custom call whose framework owns all device
+memory, a host that forbids allocation after start-up, a loop that cannot
+take cudaMalloc's implicit synchronisation).  Its scratch is a fixed
+file-scope device array (interiors up to 256 x 256).  This test compares it
+with the plan-based ``fvx_dst_solve_f32`` on two consecutive calls, at the
+DST tests' tolerance (1e-4 of max|psi|), checks that device free memory does
+not change across the calls, and that an oversized request is refused.
+The file is named to be collected last.
+"""
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(ny, nx, seed):
+    rng = np.random.default_rng(seed)
+    f = rng.standard_normal((ny, nx))
+    return torch.as_tensor(f, dtype=torch.float32, device="cuda")
+
+
+def test_noalloc_dst_matches_plan_path(cuda_ok):
+    from finitevolx_b200 import _lib as L
+    from finitevolx_b200.solvers.spectral import DSTHelmholtzPlan
+
+    lib = L.lib()
+    solve = lib.fvx_dst_solve_noalloc_f32
+    solve.restype = ctypes.c_int
+    st = L.stream_ptr()
+    ny, nx, dx, dy, lam = 96, 128, 0.05, 0.07, 2.5
+    plan = DSTHelmholtzPlan(ny, nx, dx, dy, (lam,))
+    rhs = [_fields(ny, nx, seed) for seed in (1, 2)]
+    outs = [torch.empty_like(r) for r in rhs]
+    refs = [torch.empty_like(r) for r in rhs]
+
+    def call(r, out):
+        return solve(L.P(r), ctypes.c_longlong(nx), L.P(out), ctypes.c_longlong(nx), ctypes.c_int(ny),
+                     ctypes.c_int(nx), ctypes.c_double(dx), ctypes.c_double(dy), ctypes.c_double(lam), st)
+
+    def rel(a, b):
+        a, b = a.double().cpu().numpy(), b.double().cpu().numpy()
+        return np.abs(a - b).max() / np.abs(b).max()
+
+    # warm-up: the first call on this device does the set-up; the comparison
+    # path (plan solve, host copies) is exercised once as well
+    warm = _fields(ny, nx, 0)
+    assert call(warm, outs[0]) == 0
+    plan.solve(warm, out=refs[0])
+    assert rel(outs[0], refs[0]) <= 1e-4
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for r, o in zip(rhs, outs):  # two calls in a row, nothing else in between
+        assert call(r, o) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    # device-wide free memory (other processes may share the GPU, hence the slack)
+    assert free1 >= free0 - (64 << 20)
+    for r, o, ref in zip(rhs, outs, refs):
+        plan.solve(r, out=ref)  # the existing entry point
+        err = rel(o, ref)
+        assert err <= 1e-4, err
+
+
+def test_noalloc_dst_rejects_oversize(cuda_ok):
+    from finitevolx_b200 import _lib as L
+
+    lib = L.lib()
+    x = torch.zeros((264, 264), dtype=torch.float32, device="cuda")
+    rc = lib.fvx_dst_solve_noalloc_f32(L.P(x), ctypes.c_longlong(264), L.P(x), ctypes.c_longlong(264),
+                                       ctypes.c_int(264), ctypes.c_int(264), ctypes.c_double(1.0),
+                                       ctypes.c_double(1.0), ctypes.c_double(0.0), L.stream_ptr())
+    assert rc == 1  # FVX_ERR_SHAPE: beyond the 256 x 256 maximum
