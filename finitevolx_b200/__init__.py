@@ -30,11 +30,36 @@ from finitevolx_b200.operators import (
 from finitevolx_b200.diffusion import BiharmonicDiffusion2D, Diffusion2D, diffusion_2d
 from finitevolx_b200.boundary import enforce_periodic, enforce_periodic_, pad_interior
 from finitevolx_b200.timestepping import euler_step, heun_step, rk3_ssp_step
+from finitevolx_b200.solvers import (
+    CGInfo,
+    DSTHelmholtzPlan,
+    MaskedHelmholtzPCG,
+    MultigridSolver,
+    build_multigrid_solver,
+    make_multigrid_preconditioner,
+    masked_laplacian,
+    pv_inversion,
+    solve_cg,
+    solve_helmholtz_dst,
+    solve_poisson_dst,
+    streamfunction_from_vorticity,
+)
+from finitevolx_b200.vertical import (
+    build_coupling_matrix,
+    decompose_vertical_modes,
+    layer_to_mode,
+    mode_to_layer,
+)
+from finitevolx_b200.qg import QGModel
 
 __all__ = [
     "ArakawaCGrid2D", "CartesianGrid2D", "Mask2D", "StencilCapability2D", "count_contiguous",
     "make_sponge", "narrow_mask_hierarchy", "Advection2D", "Reconstruction2D", "upwind_flux",
     "uv_center_flux", "uv_node_flux", "Difference2D", "Interpolation2D", "arakawa_jacobian",
     "divergence_2d", "BiharmonicDiffusion2D", "Diffusion2D", "diffusion_2d", "enforce_periodic",
-    "enforce_periodic_", "pad_interior", "euler_step", "heun_step", "rk3_ssp_step",
+    "enforce_periodic_", "pad_interior", "euler_step", "heun_step", "rk3_ssp_step", "CGInfo",
+    "DSTHelmholtzPlan", "MaskedHelmholtzPCG", "MultigridSolver", "build_multigrid_solver",
+    "make_multigrid_preconditioner", "masked_laplacian", "pv_inversion", "solve_cg", "solve_helmholtz_dst",
+    "solve_poisson_dst", "streamfunction_from_vorticity", "build_coupling_matrix",
+    "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel",
 ]

@@ -1,0 +1,859 @@
+// Geometric multigrid for the masked, variable-coefficient Helmholtz
+// operator and the preconditioned CG built on it.
+//
+// Restates finitevolX solvers/multigrid.py: _apply_operator (:327-405),
+// _weighted_jacobi (:408-461), _restrict (:464-507), _prolongate (:510-598),
+// MultigridSolver.v_cycle (:808-881) and build_multigrid_solver
+// (:905-1062, level hierarchy built on the host in FP64 like the
+// reference's offline NumPy setup), plus masked_laplacian
+// (solvers/iterative.py:144-191) and a PCG whose stopping test follows
+// solve_cg (iterative.py:48-136).
+//
+// Device layout per level: mask, cx, cy, inv_diag, u, f, tmp (T = float or
+// double, row-major [ny, nx]).  Levels at or below kCoarseCells cells run
+// inside one CTA (one launch for the whole coarse part of the V-cycle);
+// finer levels use one launch per sweep / transfer.
+#include "fvx_common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace fvx {
+namespace mg {
+
+constexpr int kCoarseCells = 128 * 128;
+constexpr int kCoarseThreads = 1024;
+
+template <typename T>
+struct Lev {
+  int ny, nx;
+  T rdx2, rdy2;    // 1/dx^2, 1/dy^2 at this level
+  T dx2, dy2;      // dx^2, dy^2 (FP64 divides like the reference)
+  T lam;
+  T *mask, *cx, *cy, *inv, *u, *f, *tmp;
+};
+
+template <typename T> DEV T divd(T a, T d2, T rd2) {
+  if constexpr (sizeof(T) == 8) return a / d2;
+  else return a * rd2;
+}
+
+// (A u)[j,i] of _apply_operator: u masked first, zero-padded neighbours,
+// conservative 5-point stencil, output masked.
+template <typename T>
+DEV T apply_at(const Lev<T>& L, const T* u, int j, int i) {
+  const int nx = L.nx, ny = L.ny;
+  const size_t c = (size_t)j * nx + i;
+  const T m = L.mask[c];
+  const T um = u[c] * m;
+  const T ue = i + 1 < nx ? u[c + 1] * L.mask[c + 1] : T(0);
+  const T uw = i > 0 ? u[c - 1] * L.mask[c - 1] : T(0);
+  const T un = j + 1 < ny ? u[c + nx] * L.mask[c + nx] : T(0);
+  const T us = j > 0 ? u[c - nx] * L.mask[c - nx] : T(0);
+  const T cxw = i > 0 ? L.cx[c - 1] : T(0);
+  const T cys = j > 0 ? L.cy[c - nx] : T(0);
+  const T lap = divd(L.cx[c] * (ue - um) - cxw * (um - uw), L.dx2, L.rdx2) +
+                divd(L.cy[c] * (un - um) - cys * (um - us), L.dy2, L.rdy2);
+  return (lap - L.lam * um) * m;
+}
+
+template <typename T>
+DEV void jacobi_at(const Lev<T>& L, const T* u, const T* f, T* out, T omega, size_t c) {
+  const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+  const T r = f[c] - apply_at(L, u, j, i);
+  out[c] = (u[c] + omega * L.inv[c] * r) * L.mask[c];
+}
+
+// coarse cell (J, I): r = (f - A u) * m on the 4 fine cells, mask-weighted mean
+template <typename T>
+DEV void restrict_at(const Lev<T>& F, const T* u, const T* f, const Lev<T>& C, T* fc, size_t cc) {
+  const int J = (int)(cc / C.nx), I = (int)(cc - (size_t)J * C.nx);
+  T s[4], m[4];
+  const int dj[4] = {0, 1, 0, 1}, di[4] = {0, 0, 1, 1};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int j = 2 * J + dj[k], i = 2 * I + di[k];
+    const size_t c = (size_t)j * F.nx + i;
+    const T mf = F.mask[c];
+    const T r = (f[c] - apply_at(F, u, j, i)) * mf;
+    s[k] = r * mf;
+    m[k] = mf;
+  }
+  const T sum4 = ((s[0] + s[1]) + s[2]) + s[3];
+  const T cnt = ((m[0] + m[1]) + m[2]) + m[3];
+  fc[cc] = (sum4 / (cnt > T(1) ? cnt : T(1))) * C.mask[cc];
+}
+
+// fine cell: u = (u + P e_c) * m_f, P the mask-normalised 9/3/3/1 bilinear form
+template <typename T>
+DEV void prolong_at(const Lev<T>& F, T* u, const Lev<T>& C, const T* ec, size_t c) {
+  const int j = (int)(c / F.nx), i = (int)(c - (size_t)j * F.nx);
+  const int J = j >> 1, I = i >> 1, dj = j & 1, di = i & 1;
+  const int sj = 2 * dj - 1, si = 2 * di - 1;
+  auto V = [&](int jj, int ii) -> T {
+    if (jj < 0 || jj >= C.ny || ii < 0 || ii >= C.nx) return T(0);
+    const size_t k = (size_t)jj * C.nx + ii;
+    return ec[k] * C.mask[k];
+  };
+  auto M = [&](int jj, int ii) -> T {
+    if (jj < 0 || jj >= C.ny || ii < 0 || ii >= C.nx) return T(0);
+    return C.mask[(size_t)jj * C.nx + ii];
+  };
+  const T ws = ((T(9) * V(J, I) + T(3) * V(J, I + si)) + T(3) * V(J + sj, I)) + T(1) * V(J + sj, I + si);
+  const T ds = ((T(9) * M(J, I) + T(3) * M(J, I + si)) + T(3) * M(J + sj, I)) + T(1) * M(J + sj, I + si);
+  const T e = (ws / (ds > T(1) ? ds : T(1))) * F.mask[c];
+  u[c] = (u[c] + e) * F.mask[c];
+}
+
+template <typename T>
+__global__ void jacobi_kernel(Lev<T> L, const T* u, const T* f, T* out, T omega) {
+  const size_t n = (size_t)L.ny * L.nx;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    jacobi_at(L, u, f, out, omega, c);
+}
+template <typename T>
+__global__ void restrict_kernel(Lev<T> F, const T* u, const T* f, Lev<T> C, T* fc) {
+  const size_t n = (size_t)C.ny * C.nx;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    restrict_at(F, u, f, C, fc, c);
+}
+template <typename T>
+__global__ void prolong_kernel(Lev<T> F, T* u, Lev<T> C, const T* ec) {
+  const size_t n = (size_t)F.ny * F.nx;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    prolong_at(F, u, C, ec, c);
+}
+template <typename T>
+__global__ void apply_kernel(Lev<T> L, const T* u, T* out) {
+  const size_t n = (size_t)L.ny * L.nx;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+    out[c] = apply_at(L, u, j, i);
+  }
+}
+template <typename T>
+__global__ void fill_kernel(T* p, size_t n, T v) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) p[c] = v;
+}
+template <typename T>
+__global__ void copy_kernel(T* dst, const T* src, size_t n) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    dst[c] = src[c];
+}
+
+constexpr int kMaxLevels = 16;
+template <typename T>
+struct LevArray {
+  Lev<T> L[kMaxLevels];
+};
+
+// Whole coarse part of a V-cycle in one CTA: levels lc .. nl-1, entered with
+// f[lc] set and u[lc] = 0 (the recursion's zero initial guess).
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads)
+coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
+  const int tid = threadIdx.x;
+  auto sweeps = [&](const Lev<T>& L, int n) {
+    const size_t cells = (size_t)L.ny * L.nx;
+    T* a = L.u;
+    T* b = L.tmp;
+    for (int s = 0; s < n; ++s) {
+      for (size_t c = tid; c < cells; c += kCoarseThreads) jacobi_at(L, a, L.f, b, omega, c);
+      __syncthreads();
+      T* t = a; a = b; b = t;
+    }
+    if (a != L.u) {
+      for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = a[c];
+      __syncthreads();
+    }
+  };
+  for (int l = lc; l < nl; ++l) {
+    const Lev<T>& L = A.L[l];
+    const size_t cells = (size_t)L.ny * L.nx;
+    for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = T(0);
+    __syncthreads();
+    if (l == nl - 1) { sweeps(L, n_coarse); break; }
+    sweeps(L, n_pre);
+    const Lev<T>& C = A.L[l + 1];
+    const size_t cc = (size_t)C.ny * C.nx;
+    for (size_t c = tid; c < cc; c += kCoarseThreads) restrict_at(L, L.u, L.f, C, C.f, c);
+    __syncthreads();
+  }
+  for (int l = nl - 2; l >= lc; --l) {
+    const Lev<T>& L = A.L[l];
+    const Lev<T>& C = A.L[l + 1];
+    const size_t cells = (size_t)L.ny * L.nx;
+    for (size_t c = tid; c < cells; c += kCoarseThreads) prolong_at(L, L.u, C, C.u, c);
+    __syncthreads();
+    sweeps(L, n_post);
+  }
+}
+
+// masked_laplacian (iterative.py:144-191): periodic roll, (lap - lam psi_m) * m
+template <typename T>
+__global__ void masked_laplacian_kernel(const T* psi, const T* m, T* out, int ny, int nx, T dx, T dy, T lam) {
+  const size_t n = (size_t)ny * nx;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / nx), i = (int)(c - (size_t)j * nx);
+    const int ie = i + 1 == nx ? 0 : i + 1, iw = i == 0 ? nx - 1 : i - 1;
+    const int jn = j + 1 == ny ? 0 : j + 1, js = j == 0 ? ny - 1 : j - 1;
+    auto P = [&](int jj, int ii) { size_t k = (size_t)jj * nx + ii; return psi[k] * m[k]; };
+    const T pm = P(j, i);
+    const T lap = ((P(j, iw) + P(j, ie)) - T(2) * pm) / (dx * dx) + ((P(js, i) + P(jn, i)) - T(2) * pm) / (dy * dy);
+    out[c] = (lap - lam * pm) * m[c];
+  }
+}
+
+static int grid_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+}  // namespace mg
+}  // namespace fvx
+
+using namespace fvx;
+using namespace fvx::mg;
+
+struct fvx_mg {
+  int nl = 0, lc = 0, n_pre = 6, n_post = 6, n_coarse = 50, dtype = 0;
+  double omega = 0.95, lam = 0.0;
+  std::vector<void*> allocs;
+  LevArray<float> A32;
+  LevArray<double> A64;
+  Lev<double> L0d;  // finest operator in FP64 (residual checks of FP32 solves)
+};
+
+template <typename T>
+static LevArray<T>& levs(fvx_mg* g);
+template <>
+LevArray<float>& levs<float>(fvx_mg* g) { return g->A32; }
+template <>
+LevArray<double>& levs<double>(fvx_mg* g) { return g->A64; }
+
+static void mg_free(fvx_mg* g) {
+  for (void* p : g->allocs) cudaFree(p);
+  g->allocs.clear();
+}
+
+// Host FP64 hierarchy (build_multigrid_solver, multigrid.py:905-1062).
+struct HostLevel {
+  int ny, nx;
+  double dx, dy;
+  std::vector<double> mask, coeff, cx, cy, inv;
+};
+
+static void host_level_ops(HostLevel& L, double lam) {
+  const int ny = L.ny, nx = L.nx;
+  const size_t n = (size_t)ny * nx;
+  L.cx.assign(n, 0.0);
+  L.cy.assign(n, 0.0);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t c = (size_t)j * nx + i;
+      if (i + 1 < nx) L.cx[c] = (0.5 * (L.coeff[c] + L.coeff[c + 1])) * (L.mask[c] * L.mask[c + 1]);
+      if (j + 1 < ny) L.cy[c] = (0.5 * (L.coeff[c] + L.coeff[c + nx])) * (L.mask[c] * L.mask[c + nx]);
+    }
+  L.inv.assign(n, 0.0);
+  for (int j = 0; j < ny; ++j)
+    for (int i = 0; i < nx; ++i) {
+      const size_t c = (size_t)j * nx + i;
+      const double cxw = i > 0 ? L.cx[c - 1] : 0.0, cys = j > 0 ? L.cy[c - nx] : 0.0;
+      double d = -(L.cx[c] + cxw) / (L.dx * L.dx) - (L.cy[c] + cys) / (L.dy * L.dy) - lam;
+      d *= L.mask[c];
+      L.inv[c] = (std::fabs(d) > 1e-30 ? 1.0 / d : 0.0) * L.mask[c];
+    }
+}
+
+template <typename T>
+static int upload_levels(fvx_mg* g, std::vector<HostLevel>& H) {
+  LevArray<T>& A = levs<T>(g);
+  for (int l = 0; l < g->nl; ++l) {
+    HostLevel& h = H[l];
+    Lev<T>& L = A.L[l];
+    L.ny = h.ny; L.nx = h.nx;
+    L.dx2 = (T)(h.dx * h.dx); L.dy2 = (T)(h.dy * h.dy);
+    L.rdx2 = (T)(1.0 / (h.dx * h.dx)); L.rdy2 = (T)(1.0 / (h.dy * h.dy));
+    L.lam = (T)g->lam;
+    const size_t n = (size_t)h.ny * h.nx;
+    T** bufs[7] = {&L.mask, &L.cx, &L.cy, &L.inv, &L.u, &L.f, &L.tmp};
+    for (T** b : bufs) {
+      if (cudaMalloc((void**)b, n * sizeof(T)) != cudaSuccess) return FVX_ERR_CUDA;
+      g->allocs.push_back(*b);
+      cudaMemset(*b, 0, n * sizeof(T));
+    }
+    std::vector<T> tmp(n);
+    const std::vector<double>* src[4] = {&h.mask, &h.cx, &h.cy, &h.inv};
+    T* dst[4] = {L.mask, L.cx, L.cy, L.inv};
+    for (int k = 0; k < 4; ++k) {
+      for (size_t c = 0; c < n; ++c) tmp[c] = (T)(*src[k])[c];
+      if (cudaMemcpy(dst[k], tmp.data(), n * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess) return FVX_ERR_CUDA;
+    }
+  }
+  return FVX_OK;
+}
+
+// mask: [ny, nx] float64 0/1 (host); coeff: [ny, nx] float64 or NULL.
+extern "C" int fvx_mg_create(const double* mask, const double* coeff, int ny, int nx, double dx, double dy,
+                             double lambda, int n_levels, int n_pre, int n_post, int n_coarse, double omega, int dtype,
+                             fvx_mg** out) {
+  if (!mask || !out) return FVX_ERR_ARG;
+  *out = nullptr;
+  if (ny < 1 || nx < 1 || n_pre < 0 || n_post < 0 || n_coarse < 0) return FVX_ERR_SHAPE;
+  if (dtype != 0 && dtype != 1) return FVX_ERR_DTYPE;
+  if (n_levels <= 0) {  // _compute_n_levels (multigrid.py:50-76)
+    int a = ny, b = nx;
+    n_levels = 1;
+    while (a % 2 == 0 && b % 2 == 0 && a / 2 >= 8 && b / 2 >= 8) { a /= 2; b /= 2; ++n_levels; }
+  }
+  if (n_levels > kMaxLevels) return FVX_ERR_SHAPE;
+  const int fac = 1 << (n_levels - 1);
+  if (ny % fac || nx % fac) return FVX_ERR_SHAPE;
+  std::vector<HostLevel> H(n_levels);
+  H[0].ny = ny; H[0].nx = nx; H[0].dx = dx; H[0].dy = dy;
+  const size_t n0 = (size_t)ny * nx;
+  H[0].mask.assign(mask, mask + n0);
+  H[0].coeff.resize(n0);
+  for (size_t c = 0; c < n0; ++c) H[0].coeff[c] = (coeff ? coeff[c] : 1.0) * H[0].mask[c];
+  for (int l = 0; l < n_levels; ++l) {
+    host_level_ops(H[l], lambda);
+    if (l + 1 < n_levels) {
+      HostLevel& F = H[l];
+      HostLevel& C = H[l + 1];
+      C.ny = F.ny / 2; C.nx = F.nx / 2; C.dx = F.dx * 2.0; C.dy = F.dy * 2.0;
+      const size_t nc = (size_t)C.ny * C.nx;
+      C.mask.resize(nc);
+      C.coeff.resize(nc);
+      for (int J = 0; J < C.ny; ++J)
+        for (int I = 0; I < C.nx; ++I) {
+          const size_t a = (size_t)(2 * J) * F.nx + 2 * I, b = a + F.nx, c = a + 1, d = b + 1;
+          const double avg = (((F.mask[a] + F.mask[b]) + F.mask[c]) + F.mask[d]) / 4.0;  // _restrict_mask
+          const double mc = avg >= 0.5 ? 1.0 : 0.0;
+          C.mask[(size_t)J * C.nx + I] = mc;
+          const double s4 = ((F.coeff[a] * F.mask[a] + F.coeff[b] * F.mask[b]) + F.coeff[c] * F.mask[c]) +
+                            F.coeff[d] * F.mask[d];
+          const double cnt = ((F.mask[a] + F.mask[b]) + F.mask[c]) + F.mask[d];
+          C.coeff[(size_t)J * C.nx + I] = (s4 / (cnt > 1.0 ? cnt : 1.0)) * mc;  // _restrict_coeff
+        }
+    }
+  }
+  fvx_mg* g = new fvx_mg();
+  g->nl = n_levels; g->n_pre = n_pre; g->n_post = n_post; g->n_coarse = n_coarse;
+  g->omega = omega; g->lam = lambda; g->dtype = dtype;
+  g->lc = n_levels - 1;
+  while (g->lc > 0 && (size_t)H[g->lc - 1].ny * H[g->lc - 1].nx <= (size_t)kCoarseCells) --g->lc;
+  int rc = dtype == 0 ? upload_levels<float>(g, H) : upload_levels<double>(g, H);
+  if (!rc) {
+    Lev<double>& D = g->L0d;
+    D.ny = ny; D.nx = nx; D.dx2 = dx * dx; D.dy2 = dy * dy; D.rdx2 = 1.0 / (dx * dx); D.rdy2 = 1.0 / (dy * dy);
+    D.lam = lambda; D.inv = D.u = D.f = D.tmp = nullptr;
+    double** bufs[3] = {&D.mask, &D.cx, &D.cy};
+    const std::vector<double>* src[3] = {&H[0].mask, &H[0].cx, &H[0].cy};
+    for (int k = 0; k < 3 && !rc; ++k) {
+      if (cudaMalloc((void**)bufs[k], n0 * sizeof(double)) != cudaSuccess) { rc = FVX_ERR_CUDA; break; }
+      g->allocs.push_back(*bufs[k]);
+      if (cudaMemcpy(*bufs[k], src[k]->data(), n0 * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess)
+        rc = FVX_ERR_CUDA;
+    }
+  }
+  if (rc) { mg_free(g); delete g; return rc; }
+  if (cudaDeviceSynchronize() != cudaSuccess) { mg_free(g); delete g; return FVX_ERR_CUDA; }
+  *out = g;
+  return FVX_OK;
+}
+
+extern "C" int fvx_mg_destroy(fvx_mg* g) {
+  if (!g) return FVX_ERR_ARG;
+  cudaDeviceSynchronize();
+  mg_free(g);
+  delete g;
+  return fvx_cuda_status();
+}
+
+// Level metadata and device arrays (mask, cx, cy, inv_diag) for inspection.
+extern "C" int fvx_mg_level(fvx_mg* g, int level, int* ny, int* nx, double* dx2, void** mask, void** cx, void** cy,
+                            void** inv) {
+  if (!g || level < 0 || level >= g->nl) return FVX_ERR_ARG;
+  if (g->dtype == 0) {
+    Lev<float>& L = g->A32.L[level];
+    *ny = L.ny; *nx = L.nx; *dx2 = L.dx2; *mask = L.mask; *cx = L.cx; *cy = L.cy; *inv = L.inv;
+  } else {
+    Lev<double>& L = g->A64.L[level];
+    *ny = L.ny; *nx = L.nx; *dx2 = L.dx2; *mask = L.mask; *cx = L.cx; *cy = L.cy; *inv = L.inv;
+  }
+  return FVX_OK;
+}
+
+extern "C" int fvx_mg_num_levels(fvx_mg* g) { return g ? g->nl : -1; }
+
+// V-cycle below the finest level of a host-driven cycle.
+template <typename T>
+static int vcycle_levels(fvx_mg* g, int l, cudaStream_t st) {
+  LevArray<T>& A = levs<T>(g);
+  const T om = (T)g->omega;
+  if (l >= g->lc) {
+    coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, l, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
+    return fvx_cuda_status();
+  }
+  Lev<T>& L = A.L[l];
+  const size_t n = (size_t)L.ny * L.nx;
+  const int gr = grid_for(n);
+  fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
+  T* a = L.u;
+  T* b = L.tmp;
+  for (int s = 0; s < g->n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+  Lev<T>& C = A.L[l + 1];
+  restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
+  int rc = vcycle_levels<T>(g, l + 1, st);
+  if (rc) return rc;
+  prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
+  a = L.u; b = L.tmp;
+  for (int s = 0; s < g->n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+  return fvx_cuda_status();
+}
+
+// One V-cycle at level 0: u_out = V(u_in, f) (u_in NULL = zero initial
+// guess).  u_in and u_out may alias.  Arrays are [ny, nx] of the plan dtype.
+template <typename T>
+static int vcycle0(fvx_mg* g, const T* u_in, const T* f, T* u_out, cudaStream_t st) {
+  LevArray<T>& A = levs<T>(g);
+  Lev<T>& L = A.L[0];
+  const size_t n = (size_t)L.ny * L.nx;
+  const int gr = grid_for(n);
+  const T om = (T)g->omega;
+  if (g->nl == 1) {
+    if (u_in) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, u_in, n);
+    else fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
+    copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
+    T* a = L.u; T* b = L.tmp;
+    for (int s = 0; s < g->n_coarse; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+    copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
+    return fvx_cuda_status();
+  }
+  if (g->lc == 0) {  // whole cycle fits the single-CTA kernel
+    copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
+    if (u_in) {
+      // a non-zero start at level 0 is run with the host-driven path below
+    } else {
+      coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, 0, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
+      copy_kernel<T><<<gr, 256, 0, st>>>(u_out, L.u, n);
+      return fvx_cuda_status();
+    }
+  }
+  if (u_in) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, u_in, n);
+  else fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
+  copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
+  T* a = L.u; T* b = L.tmp;
+  for (int s = 0; s < g->n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+  Lev<T>& C = A.L[1];
+  restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
+  int rc = vcycle_levels<T>(g, 1, st);
+  if (rc) return rc;
+  prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
+  a = L.u; b = L.tmp;
+  for (int s = 0; s < g->n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+  copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
+  return fvx_cuda_status();
+}
+
+extern "C" int fvx_mg_vcycle(fvx_mg* g, const void* u_in, const void* f, void* u_out, void* stream) {
+  if (!g || !f || !u_out) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  return g->dtype == 0 ? vcycle0<float>(g, (const float*)u_in, (const float*)f, (float*)u_out, st)
+                       : vcycle0<double>(g, (const double*)u_in, (const double*)f, (double*)u_out, st);
+}
+
+// MultigridSolver._run_vcycles (multigrid.py:885-897): n_cycles V-cycles from 0.
+extern "C" int fvx_mg_solve(fvx_mg* g, const void* f, void* u, int n_cycles, void* stream) {
+  if (!g || !f || !u || n_cycles < 0) return FVX_ERR_ARG;
+  int rc = FVX_OK;
+  for (int k = 0; k < n_cycles && rc == FVX_OK; ++k) rc = fvx_mg_vcycle(g, k == 0 ? nullptr : u, f, u, stream);
+  if (n_cycles == 0) {
+    const size_t n = g->dtype == 0 ? (size_t)g->A32.L[0].ny * g->A32.L[0].nx : (size_t)g->A64.L[0].ny * g->A64.L[0].nx;
+    rc = cudaMemsetAsync(u, 0, n * (g->dtype == 0 ? 4 : 8), fvx_stream(stream)) == cudaSuccess ? FVX_OK : FVX_ERR_CUDA;
+  }
+  return rc;
+}
+
+// _apply_operator at a level: out = A u.
+extern "C" int fvx_mg_apply(fvx_mg* g, int level, const void* u, void* out, void* stream) {
+  if (!g || !u || !out || level < 0 || level >= g->nl) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  if (g->dtype == 0) {
+    Lev<float>& L = g->A32.L[level];
+    apply_kernel<float><<<grid_for((size_t)L.ny * L.nx), 256, 0, st>>>(L, (const float*)u, (float*)out);
+  } else {
+    Lev<double>& L = g->A64.L[level];
+    apply_kernel<double><<<grid_for((size_t)L.ny * L.nx), 256, 0, st>>>(L, (const double*)u, (double*)out);
+  }
+  return fvx_cuda_status();
+}
+
+#define FVX_DEF_MLAP(SFX, T)                                                                                   \
+  extern "C" int fvx_masked_laplacian_##SFX(const T* psi, const T* mask, T* out, int ny, int nx, double dx,   \
+                                            double dy, double lambda, void* stream) {                         \
+    if (!psi || !mask || !out) return FVX_ERR_ARG;                                                             \
+    if (ny < 1 || nx < 1) return FVX_ERR_SHAPE;                                                                \
+    masked_laplacian_kernel<T><<<grid_for((size_t)ny * nx), 256, 0, fvx_stream(stream)>>>(psi, mask, out, ny,  \
+                                                                                          nx, T(dx), T(dy),     \
+                                                                                          T(lambda));           \
+    return fvx_cuda_status();                                                                                  \
+  }
+FVX_DEF_MLAP(f32, float)
+FVX_DEF_MLAP(f64, double)
+
+// ===========================================================================
+// Preconditioned CG on the finest operator A (negative definite, like
+// solve_cg's operators, iterative.py:97-127): CG with A and a negative-
+// definite preconditioner M is the SPD recurrence on (-A, -M) written with
+// the natural residual rho = b - A x.  x is FP64; rho, z, p, A p are T;
+// every inner product accumulates in FP64 (warp shuffles, then one block
+// per reduction in a fixed order, so results are deterministic); every
+// ``replace_every`` iterations rho is recomputed from x in FP64.  All
+// scalars stay on the device and every kernel returns at once when the
+// convergence flag is set, so the host only reads the flag every ``chunk``
+// iterations.
+// ===========================================================================
+namespace fvx {
+namespace mg {
+
+enum Slot { S_GAMMA = 0, S_PAP, S_ALPHA, S_BETA, S_RR, S_BB, S_CONV, S_ITER, S_TOL2, S_FLEX_A, S_NSLOTS = 16 };
+constexpr int kRedBlocks = 296;  // 2 per SM
+
+DEV double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+  if (w == 0)
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  return v;
+}
+
+template <typename T>
+__global__ void k_apply_dot(Lev<T> L, const T* p, T* Ap, double* part, const double* s) {
+  if (s[S_CONV] != 0.0) return;
+  const size_t n = (size_t)L.ny * L.nx;
+  double acc = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+    const T a = apply_at(L, p, j, i);
+    Ap[c] = a;
+    acc += (double)p[c] * (double)a;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+template <typename T>
+__global__ void k_update(double* x, const T* p, const T* Ap, T* rho, T* rho_prev, double* part, const double* s,
+                         size_t N) {
+  if (s[S_CONV] != 0.0) return;
+  const double a = s[S_ALPHA];
+  double acc = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += (size_t)gridDim.x * blockDim.x) {
+    x[c] += a * (double)p[c];
+    if (rho_prev) rho_prev[c] = rho[c];
+    const T r = rho[c] - (T)a * Ap[c];
+    rho[c] = r;
+    acc += (double)r * (double)r;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+// rho = b - A x in FP64 (x FP64, b of type T), rho stored as T; part = |rho|^2
+template <typename T>
+__global__ void k_residual64(Lev<double> D, const double* x, const T* b, T* rho, double* part, const double* s,
+                             int force) {
+  if (!force && s[S_CONV] != 0.0) return;
+  const size_t n = (size_t)D.ny * D.nx;
+  double acc = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / D.nx), i = (int)(c - (size_t)j * D.nx);
+    const double r = (double)b[c] - apply_at(D, x, j, i);
+    if (rho) rho[c] = (T)r;
+    acc += r * r;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+
+template <typename T>
+__global__ void k_dot(const T* a, const T* b, const T* c2, double* part, double* part2, const double* s, size_t n) {
+  if (s[S_CONV] != 0.0) return;
+  double acc = 0.0, acc2 = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    acc += (double)a[c] * (double)b[c];
+    if (c2) acc2 += (double)a[c] * (double)c2[c];
+  }
+  acc = block_sum(acc);
+  if (c2) acc2 = block_sum(acc2);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = acc;
+    if (c2) part2[blockIdx.x] = acc2;
+  }
+}
+
+template <typename T>
+__global__ void k_pupdate(T* p, const T* z, const double* s, size_t n) {
+  if (s[S_CONV] != 0.0) return;
+  const T b = (T)s[S_BETA];
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    p[c] = z[c] + b * p[c];
+}
+
+template <typename T>
+__global__ void k_copy_if(T* dst, const T* src, size_t n, const double* s) {
+  if (s[S_CONV] != 0.0) return;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    dst[c] = src[c];
+}
+
+enum RedMode { R_STORE = 0, R_ALPHA, R_BETA, R_RR, R_BETA_FLEX };
+
+// One block: fixed-order sum of the partials, then the scalar update.
+__global__ void k_reduce(const double* part, const double* part2, int np, double* s, int slot, int mode, int force) {
+  if (!force && s[S_CONV] != 0.0) return;
+  double v = 0.0, v2 = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) {
+    v += part[k];
+    if (part2) v2 += part2[k];
+  }
+  v = block_sum(v);
+  if (part2) v2 = block_sum(v2);
+  if (threadIdx.x != 0) return;
+  switch (mode) {
+    case R_STORE: s[slot] = v; break;
+    case R_ALPHA: s[S_PAP] = v; s[S_ALPHA] = s[S_GAMMA] / v; break;
+    case R_BETA: s[S_BETA] = v / s[S_GAMMA]; s[S_GAMMA] = v; break;
+    case R_BETA_FLEX: s[S_BETA] = (v - v2) / s[S_GAMMA]; s[S_GAMMA] = v; break;  // Polak-Ribiere
+    case R_RR:
+      s[S_RR] = v;
+      s[S_ITER] += 1.0;
+      if (v <= s[S_TOL2]) s[S_CONV] = 1.0;
+      break;
+  }
+}
+
+template <typename T>
+__global__ void k_zero_x(double* x, size_t n) {
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) x[c] = 0.0;
+}
+
+}  // namespace mg
+}  // namespace fvx
+
+struct fvx_pcg {
+  fvx_mg* mg = nullptr;
+  int dtype = 0;
+  size_t n = 0;
+  void *rho = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *rho_prev = nullptr;
+  void *own_rho = nullptr, *own_z = nullptr;  // allocations replaced by bound caller buffers
+  double *part = nullptr, *part2 = nullptr, *s = nullptr;
+};
+
+extern "C" int fvx_pcg_create(fvx_mg* g, fvx_pcg** out) {
+  if (!g || !out) return FVX_ERR_ARG;
+  fvx_pcg* P = new fvx_pcg();
+  P->mg = g;
+  P->dtype = g->dtype;
+  P->n = g->dtype == 0 ? (size_t)g->A32.L[0].ny * g->A32.L[0].nx : (size_t)g->A64.L[0].ny * g->A64.L[0].nx;
+  const size_t es = g->dtype == 0 ? 4 : 8;
+  bool ok = true;
+  void** vecs[5] = {&P->rho, &P->z, &P->p, &P->Ap, &P->rho_prev};
+  for (void** v : vecs)
+    if (ok && cudaMalloc(v, P->n * es) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->part, kRedBlocks * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->part2, kRedBlocks * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->s, (S_NSLOTS + 2) * sizeof(double)) != cudaSuccess) ok = false;
+  if (!ok) {
+    void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->part, P->part2, P->s};
+    for (void* q : ps) if (q) cudaFree(q);
+    delete P;
+    return FVX_ERR_CUDA;
+  }
+  *out = P;
+  return FVX_OK;
+}
+
+extern "C" int fvx_pcg_destroy(fvx_pcg* P) {
+  if (!P) return FVX_ERR_ARG;
+  cudaDeviceSynchronize();
+  if (P->own_rho) { P->rho = P->own_rho; P->z = P->own_z; }
+  void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->part, P->part2, P->s};
+  for (void* q : ps) if (q) cudaFree(q);
+  delete P;
+  return fvx_cuda_status();
+}
+
+// Preconditioner callback: z = M rho on the given stream; returns a status.
+typedef int (*fvx_precond_fn)(void* ctx, const void* rho, void* z, void* stream);
+
+template <typename T>
+static int pcg_run(fvx_pcg* P, const T* b, double* x, int max_iter, double rtol, int precond, fvx_precond_fn fn,
+                   void* ctx, int flexible, int replace_every, int chunk, double* info, cudaStream_t st) {
+  fvx_mg* g = P->mg;
+  Lev<T>& L = levs<T>(g).L[0];
+  const size_t n = P->n;
+  T *rho = (T*)P->rho, *z = (T*)P->z, *p = (T*)P->p, *Ap = (T*)P->Ap, *rp = (T*)P->rho_prev;
+  double* s = P->s;
+  const int G = kRedBlocks;
+  double init[S_NSLOTS] = {0};
+  cudaMemcpyAsync(s, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  k_zero_x<T><<<G, 256, 0, st>>>(x, n);
+  // rho = b (x = 0), bb = |b|^2 computed in FP64
+  k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 1);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_BB, R_STORE, 1);
+  double bb = 0;
+  cudaMemcpyAsync(&bb, s + S_BB, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
+  const double tol2 = rtol * rtol * bb;
+  cudaMemcpyAsync(s + S_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st);
+  auto apply_M = [&]() -> int {
+    if (precond == 1) return fvx_mg_vcycle(g, nullptr, rho, z, st);
+    if (precond == 2) return fn(ctx, rho, z, st);
+    k_copy_if<T><<<G, 256, 0, st>>>(z, rho, n, s);
+    return fvx_cuda_status();
+  };
+  int rc = FVX_OK;
+  if (bb == 0.0) {
+    if (info) { info[0] = 0; info[1] = 0; info[2] = 1; }
+    return FVX_OK;
+  }
+  if ((rc = apply_M())) return rc;
+  k_copy_if<T><<<G, 256, 0, st>>>(p, z, n, s);
+  k_dot<T><<<G, 256, 0, st>>>(rho, z, nullptr, P->part, nullptr, s, n);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_GAMMA, R_STORE, 0);
+  int it = 0;
+  double hs[S_NSLOTS];
+  bool conv = false;
+  while (it < max_iter && !conv) {
+    const int m = chunk < max_iter - it ? chunk : max_iter - it;
+    for (int k = 0; k < m; ++k, ++it) {
+      k_apply_dot<T><<<G, 256, 0, st>>>(L, p, Ap, P->part, s);
+      k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_ALPHA, 0);
+      k_update<T><<<G, 256, 0, st>>>(x, p, Ap, rho, flexible ? rp : nullptr, P->part, s, n);
+      if (replace_every > 0 && (it + 1) % replace_every == 0)
+        k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 0);
+      k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_RR, 0);
+      if ((rc = apply_M())) return rc;
+      k_dot<T><<<G, 256, 0, st>>>(z, rho, flexible ? rp : nullptr, P->part, P->part2, s, n);
+      k_reduce<<<1, 256, 0, st>>>(P->part, flexible ? P->part2 : nullptr, G, s, 0, flexible ? R_BETA_FLEX : R_BETA, 0);
+      k_pupdate<T><<<G, 256, 0, st>>>(p, z, s, n);
+    }
+    if ((rc = fvx_cuda_status())) return rc;
+    if (cudaMemcpyAsync(hs, s, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    conv = hs[S_CONV] != 0.0;
+  }
+  // final FP64 true residual
+  k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, (T*)nullptr, P->part, s, 1);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_RR, R_STORE, 1);
+  double rr = 0;
+  cudaMemcpyAsync(&rr, s + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
+  const double rel = sqrt(rr / bb);
+  if (info) { info[0] = hs[S_ITER]; info[1] = rel; info[2] = rel <= rtol ? 1.0 : 0.0; }
+  return rel <= rtol ? FVX_OK : FVX_ERR_NOT_CONVERGED;
+}
+
+// PCG on A x = b (A the plan's finest operator, negative definite) to
+// ||b - A x||_2 <= rtol ||b||_2 checked in FP64.  precond: 0 none, 1 one MG
+// V-cycle from zero (make_multigrid_preconditioner, preconditioners.py:
+// 207-244), 2 the callback ``fn(ctx, rho, z, stream)``.  flexible: Polak-
+// Ribiere beta (for preconditioners that change between iterations).
+// b: plan dtype; x: FP64 output.  info: [iterations, relative residual,
+// converged].
+extern "C" int fvx_pcg_solve(fvx_pcg* P, const void* b, double* x, int max_iter, double rtol, int precond,
+                             fvx_precond_fn fn, void* ctx, int flexible, int replace_every, int chunk, double* info,
+                             void* stream) {
+  if (!P || !b || !x || max_iter < 0 || chunk < 1) return FVX_ERR_ARG;
+  if (precond == 2 && !fn) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  return P->dtype == 0
+             ? pcg_run<float>(P, (const float*)b, x, max_iter, rtol, precond, fn, ctx, flexible, replace_every, chunk,
+                              info, st)
+             : pcg_run<double>(P, (const double*)b, x, max_iter, rtol, precond, fn, ctx, flexible, replace_every,
+                               chunk, info, st);
+}
+
+// Use caller-owned device buffers (plan dtype, [ny, nx]) as the residual rho
+// and preconditioned residual z, so a preconditioner callback can read rho
+// and write z through the caller's own handles.
+extern "C" int fvx_pcg_bind_vectors(fvx_pcg* P, void* rho, void* z) {
+  if (!P || !rho || !z) return FVX_ERR_ARG;
+  if (!P->own_rho) { P->own_rho = P->rho; P->own_z = P->z; }
+  P->rho = rho;
+  P->z = z;
+  return FVX_OK;
+}
+
+// ---- small linear-algebra helpers ----------------------------------------
+namespace fvx {
+namespace mg {
+template <typename T>
+__global__ void k_dot_plain(const T* a, const T* b, size_t n, double* part) {
+  double acc = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    acc += (double)a[c] * (double)b[c];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+}
+__global__ void k_sum_parts(const double* part, int np, double* out) {
+  double v = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) v += part[k];
+  v = block_sum(v);
+  if (threadIdx.x == 0) *out = v;
+}
+// out[b, k, c] = sum_l C[k][l] in[b, l, c]  (layer_to_mode / mode_to_layer,
+// vertical/vertical_modes.py:193-263), C given by value.
+constexpr int kMaxLayers = 8;
+struct Mix { double c[kMaxLayers * kMaxLayers]; };
+template <typename T>
+__global__ void k_layer_mix(Mix M, const T* in, T* out, int nl, size_t plane, int batch) {
+  const size_t n = plane * (size_t)batch;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = t / plane, c = t - b * plane;
+    const T* src = in + b * nl * plane + c;
+    T v[kMaxLayers];
+    for (int l = 0; l < nl; ++l) v[l] = src[l * plane];
+    T* dst = out + b * nl * plane + c;
+    for (int k = 0; k < nl; ++k) {
+      T acc = T(0);
+      for (int l = 0; l < nl; ++l) acc = acc + (T)M.c[k * nl + l] * v[l];
+      dst[k * plane] = acc;
+    }
+  }
+}
+}  // namespace mg
+}  // namespace fvx
+
+// sum a*b in FP64 into *out_dev (device double); ``part`` holds 296 doubles.
+#define FVX_DEF_LA(SFX, T)                                                                                      \
+  extern "C" int fvx_dot_##SFX(const T* a, const T* b, int64_t n, double* part, double* out_dev, void* stream) { \
+    if (!a || !b || !part || !out_dev || n < 0) return FVX_ERR_ARG;                                             \
+    cudaStream_t st = fvx_stream(stream);                                                                       \
+    fvx::mg::k_dot_plain<T><<<fvx::mg::kRedBlocks, 256, 0, st>>>(a, b, (size_t)n, part);                        \
+    fvx::mg::k_sum_parts<<<1, 256, 0, st>>>(part, fvx::mg::kRedBlocks, out_dev);                                \
+    return fvx_cuda_status();                                                                                   \
+  }                                                                                                             \
+  extern "C" int fvx_layer_mix_##SFX(const double* C, int nl, const T* in, T* out, int64_t plane, int batch,    \
+                                     void* stream) {                                                            \
+    if (!C || !in || !out || in == out) return FVX_ERR_ARG;                                                     \
+    if (nl < 1 || nl > fvx::mg::kMaxLayers || plane < 1 || batch < 1) return FVX_ERR_SHAPE;                     \
+    fvx::mg::Mix M;                                                                                             \
+    for (int k = 0; k < nl * nl; ++k) M.c[k] = C[k];                                                            \
+    fvx::mg::k_layer_mix<T><<<fvx::mg::grid_for((size_t)plane * batch), 256, 0, fvx_stream(stream)>>>(          \
+        M, in, out, nl, (size_t)plane, batch);                                                                  \
+    return fvx_cuda_status();                                                                                   \
+  }
+FVX_DEF_LA(f32, float)
+FVX_DEF_LA(f64, double)

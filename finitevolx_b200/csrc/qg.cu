@@ -22,6 +22,13 @@ namespace qg {
 
 constexpr int TX = 64, TY = 16, THREADS = 256;
 
+// a / d: exact division in FP64; multiplication by the rounded reciprocal in
+// FP32 (<= 1 ulp from the quotient).
+template <typename T> DEV T divr(T a, T d, T rd) {
+  if constexpr (sizeof(T) == 8) return a / d;
+  else return a * rd;
+}
+
 struct StageArgs {
   const void* qs;      // stage state [Ny][Nx]
   const void* qn;      // step-start state (null on stage 1)
@@ -48,6 +55,7 @@ stage_kernel(StageArgs A) {
   T* xt = pt + (TY + 2) * (TX + 2);        // X [TY+1][TX+1], origin (y0-1, x0-1)
   T* fe = xt + (TY + 1) * (TX + 1);        // [TY][TX+1]
   T* fn = fe + TY * (TX + 1);              // [TY+1][TX]
+  T* vs = fn + (TY + 1) * TX;              // v on north faces [TY+1][TX], origin (y0-1, x0)
   const int ny = A.ny, nx = A.nx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const int tid = threadIdx.x;
@@ -89,16 +97,17 @@ stage_kernel(StageArgs A) {
   }
   __syncthreads();
   const T dx = T(A.dx), dy = T(A.dy);
+  const T rdx = T(1.0 / A.dx), rdy = T(1.0 / A.dy);
   // u at U-point (j, i) = -(X[j,i] - X[j-1,i]) / dy on [1, N-2]^2
   auto uvel = [&](int gy, int gx) -> T {
     if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
     const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
-    return -((p[0] - p[-(TX + 1)]) / dy);
+    return -divr(p[0] - p[-(TX + 1)], dy, rdy);
   };
   auto vvel = [&](int gy, int gx) -> T {
     if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
     const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
-    return (p[0] - p[-1]) / dx;
+    return divr(p[0] - p[-1], dx, rdx);
   };
   // ---- face fluxes --------------------------------------------------------
   for (int k = tid; k < TY * (TX + 1); k += THREADS) {
@@ -115,11 +124,11 @@ stage_kernel(StageArgs A) {
     int lf = k / TX, lx = k - lf * TX;
     int gj = y0 - 1 + lf, gi = x0 + lx;
     T f = T(0);
-    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T vv = vvel(gj, gi);
+    T vv = vvel(gj, gi);
+    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)
       f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
-    }
     fn[k] = f;
+    vs[k] = vv;
   }
   __syncthreads();
   // ---- tendency, RK combination, stores ------------------------------------
@@ -134,22 +143,22 @@ stage_kernel(StageArgs A) {
     if (gj < 1 || gj > ny - 2 || gi < 1 || gi > nx - 2) continue;  // ghost ring written below
     T rhs = T(0);
     if (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3)
-      rhs = -((fe[ly * (TX + 1) + lx + 1] - fe[ly * (TX + 1) + lx]) / dx +
-              (fn[(ly + 1) * TX + lx] - fn[ly * TX + lx]) / dy);
-    T vc = T(0.5) * (vvel(gj, gi) + vvel(gj - 1, gi));
+      rhs = -(divr(fe[ly * (TX + 1) + lx + 1] - fe[ly * (TX + 1) + lx], dx, rdx) +
+              divr(fn[(ly + 1) * TX + lx] - fn[ly * TX + lx], dy, rdy));
+    T vc = T(0.5) * (vs[(ly + 1) * TX + lx] + vs[ly * TX + lx]);
     rhs = rhs + (-beta * vc);
     size_t g = (size_t)gj * nx + gi;
     if (F) rhs = rhs + F[g];
     if (A.drag != 0.0) {
       const T* p = pt + (ly + 1) * (TX + 2) + (lx + 1);
-      T d2x = ((p[1] - p[0]) - (p[0] - p[-1])) / (dx * dx);
-      T d2y = ((p[TX + 2] - p[0]) - (p[0] - p[-(TX + 2)])) / (dy * dy);
+      T d2x = divr((p[1] - p[0]) - (p[0] - p[-1]), dx * dx, rdx * rdx);
+      T d2y = divr((p[TX + 2] - p[0]) - (p[0] - p[-(TX + 2)]), dy * dy, rdy * rdy);
       rhs = rhs - drag * (d2x + d2y);
     }
     if (A.visc != 0.0) {
       const T* q = qt + (ly + H) * QW + (lx + H);
-      T d2x = ((q[1] - q[0]) - (q[0] - q[-1])) / (dx * dx);
-      T d2y = ((q[QW] - q[0]) - (q[0] - q[-QW])) / (dy * dy);
+      T d2x = divr((q[1] - q[0]) - (q[0] - q[-1]), dx * dx, rdx * rdx);
+      T d2y = divr((q[QW] - q[0]) - (q[0] - q[-QW]), dy * dy, rdy * rdy);
       rhs = rhs + visc * (d2x + d2y);
     }
     T qsv = qt[(ly + H) * QW + (lx + H)];
@@ -189,7 +198,7 @@ template <typename T, int S>
 static size_t smem_bytes() {
   constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
   size_t n = (size_t)(TY + 2 * H) * (TX + 2 * H) + (TY + 2) * (TX + 2) + (TY + 1) * (TX + 1) + TY * (TX + 1) +
-             (TY + 1) * TX;
+             2 * (TY + 1) * TX;
   return n * sizeof(T);
 }
 

@@ -18,18 +18,28 @@
 namespace fvx {
 
 template <typename T> DEV T sq(T x) { return x * x; }
+// Division in the reconstruction formulas: exact IEEE division in FP64 (the
+// correctness path tracks the reference's operation order), the fast
+// reciprocal form in FP32 (<= 2 ulp; its 2^126 < |b| < 2^128 corner maps to
+// the weights an FP32 reference overflows on anyway).
+template <typename T> DEV T fdiv(T a, T b) {
+  if constexpr (sizeof(T) == 8) return a / b;
+  else return __fdividef(a, b);
+}
 template <typename T> DEV T tabs(T x) { return x < T(0) ? -x : x; }
 template <typename T> DEV T tmax(T a, T b) { return a > b ? a : b; }
 template <typename T> DEV T tmin(T a, T b) { return a < b ? a : b; }
 
-// ---- WENO3 (advection/weno.py:297-347, :413-459) -------------------------
+// ---- WENO3 (advection/weno.py:297-347) ------------------------------------
+// The right-biased forms (:413-459, :462-522, :597-665) are these functions on
+// the mirrored stencil; face_value() below feeds them that way.
 template <typename T> DEV T weno3(T qm, T q0, T qp) {
   const T eps = T(1e-8);
   T qi1 = T(-0.5) * qm + T(1.5) * q0;
   T qi2 = T(0.5) * (q0 + qp);
-  T w1 = T(1.0 / 3.0) / sq(sq(q0 - qm) + eps);
-  T w2 = T(2.0 / 3.0) / sq(sq(qp - q0) + eps);
-  return (w1 * qi1 + w2 * qi2) / (w1 + w2);
+  T w1 = fdiv(T(1.0 / 3.0), sq(sq(q0 - qm) + eps));
+  T w2 = fdiv(T(2.0 / 3.0), sq(sq(qp - q0) + eps));
+  return fdiv(w1 * qi1 + w2 * qi2, w1 + w2);
 }
 template <typename T> DEV T wenoz3(T qm, T q0, T qp) {
   const T eps = T(1e-14);
@@ -37,45 +47,26 @@ template <typename T> DEV T wenoz3(T qm, T q0, T qp) {
   T qi2 = T(0.5) * (q0 + qp);
   T b1 = sq(q0 - qm), b2 = sq(qp - q0);
   T tau = tabs(b2 - b1);
-  T w1 = T(1.0 / 3.0) * (T(1) + tau / (b1 + eps));
-  T w2 = T(2.0 / 3.0) * (T(1) + tau / (b2 + eps));
-  return (w1 * qi1 + w2 * qi2) / (w1 + w2);
+  T w1 = T(1.0 / 3.0) * (T(1) + fdiv(tau, b1 + eps));
+  T w2 = T(2.0 / 3.0) * (T(1) + fdiv(tau, b2 + eps));
+  return fdiv(w1 * qi1 + w2 * qi2, w1 + w2);
 }
-template <typename T> DEV T weno3r(T q0, T qp, T qpp) {
-  const T eps = T(1e-8);
-  T qi1 = T(0.5) * (q0 + qp);
-  T qi2 = T(1.5) * qp - T(0.5) * qpp;
-  T w1 = T(2.0 / 3.0) / sq(sq(qp - q0) + eps);
-  T w2 = T(1.0 / 3.0) / sq(sq(qpp - qp) + eps);
-  return (w1 * qi1 + w2 * qi2) / (w1 + w2);
-}
-template <typename T> DEV T wenoz3r(T q0, T qp, T qpp) {
-  const T eps = T(1e-14);
-  T qi1 = T(0.5) * (q0 + qp);
-  T qi2 = T(1.5) * qp - T(0.5) * qpp;
-  T b1 = sq(qp - q0), b2 = sq(qpp - qp);
-  T tau = tabs(b2 - b1);
-  T w1 = T(2.0 / 3.0) * (T(1) + tau / (b1 + eps));
-  T w2 = T(1.0 / 3.0) * (T(1) + tau / (b2 + eps));
-  return (w1 * qi1 + w2 * qi2) / (w1 + w2);
-}
-
 // ---- WENO5 (advection/weno.py:350-410, :462-522) -------------------------
 template <typename T, bool Z>
 DEV T weno5_core(T qi1, T qi2, T qi3, T b1, T b2, T b3) {
   if (Z) {
     const T eps = T(1e-16);
     T tau5 = tabs(b1 - b3);
-    T w1 = T(0.1) * (T(1) + tau5 / (b1 + eps));
-    T w2 = T(0.6) * (T(1) + tau5 / (b2 + eps));
-    T w3 = T(0.3) * (T(1) + tau5 / (b3 + eps));
-    return (w1 * qi1 + w2 * qi2 + w3 * qi3) / (w1 + w2 + w3);
+    T w1 = T(0.1) * (T(1) + fdiv(tau5, b1 + eps));
+    T w2 = T(0.6) * (T(1) + fdiv(tau5, b2 + eps));
+    T w3 = T(0.3) * (T(1) + fdiv(tau5, b3 + eps));
+    return fdiv(w1 * qi1 + w2 * qi2 + w3 * qi3, w1 + w2 + w3);
   } else {
     const T eps = T(1e-8);
-    T w1 = T(0.1) / sq(b1 + eps);
-    T w2 = T(0.6) / sq(b2 + eps);
-    T w3 = T(0.3) / sq(b3 + eps);
-    return (w1 * qi1 + w2 * qi2 + w3 * qi3) / (w1 + w2 + w3);
+    T w1 = fdiv(T(0.1), sq(b1 + eps));
+    T w2 = fdiv(T(0.6), sq(b2 + eps));
+    T w3 = fdiv(T(0.3), sq(b3 + eps));
+    return fdiv(w1 * qi1 + w2 * qi2 + w3 * qi3, w1 + w2 + w3);
   }
 }
 template <typename T, bool Z> DEV T weno5(T qmm, T qm, T q0, T qp, T qpp) {
@@ -88,17 +79,6 @@ template <typename T, bool Z> DEV T weno5(T qmm, T qm, T q0, T qp, T qpp) {
   T b3 = k1 * sq(q0 - T(2) * qp + qpp) + k2 * sq(T(3) * q0 - T(4) * qp + qpp);
   return weno5_core<T, Z>(qi1, qi2, qi3, b1, b2, b3);
 }
-template <typename T, bool Z> DEV T weno5r(T qm, T q0, T qp, T qpp, T qppp) {
-  const T k1 = T(13.0 / 12.0), k2 = T(0.25);
-  T qi1 = T(1.0 / 3.0) * qppp - T(7.0 / 6.0) * qpp + T(11.0 / 6.0) * qp;
-  T qi2 = T(-1.0 / 6.0) * qpp + T(5.0 / 6.0) * qp + T(1.0 / 3.0) * q0;
-  T qi3 = T(1.0 / 3.0) * qp + T(5.0 / 6.0) * q0 - T(1.0 / 6.0) * qm;
-  T b1 = k1 * sq(qp - T(2) * qpp + qppp) + k2 * sq(T(3) * qp - T(4) * qpp + qppp);
-  T b2 = k1 * sq(q0 - T(2) * qp + qpp) + k2 * sq(q0 - qpp);
-  T b3 = k1 * sq(qm - T(2) * q0 + qp) + k2 * sq(qm - T(4) * q0 + T(3) * qp);
-  return weno5_core<T, Z>(qi1, qi2, qi3, b1, b2, b3);
-}
-
 // ---- WENO7 / WENO9, generic Jiang-Shu form (advection/weno.py:268-294) ---
 template <typename T> DEV T tab_c(int R, int k, int j) {
   if constexpr (sizeof(T) == 8) return R == 4 ? kW7_C[k][j] : kW9_C[k][j];
@@ -114,8 +94,8 @@ template <typename T> DEV T tab_b(int R, int k, int i, int j) {
 }
 
 // v[0..2R-2]: the 2R-1 cells of the big stencil ordered in the upwind
-// direction.  RIGHT selects the mirrored (negative-flow) tables, which is the
-// same as reading the reversed stencil with the left-biased tables.
+// direction (the mirrored, negative-flow tables of the reference are the
+// left-biased tables on the reversed stencil).
 //
 // FP32: the quadratic forms have O(10^3) alternating coefficients, so on raw
 // values they lose ~4 digits to cancellation against the local mean.  The
@@ -146,11 +126,11 @@ DEV T weno_generic(const T* vin) {
       for (int j = 0; j < R; ++j) row = row + tab_b<T>(R, k, i, j) * v[k + j];
       beta = beta + v[k + i] * row;
     }
-    T a = tab_w<T>(R, k) / sq(beta + eps);
+    T a = fdiv(tab_w<T>(R, k), sq(beta + eps));
     den = den + a;
     num = num + a * cand;
   }
-  return SHIFT ? s + num / den : num / den;
+  return SHIFT ? s + fdiv(num, den) : num / den;
 }
 
 // ---- limiters (advection/limiters.py:34-123) -----------------------------
@@ -204,42 +184,33 @@ DEV T face_value(const T* p, int st, int i, int N, bool pos) {
     return at(1) + T(0.5) * limiter<T, S>(r) * dn;
   }
   if constexpr (SchemeInfo<S>::is_weno) {
+    // Upwind-oriented stencil: e(k) is the cell k steps downstream of the
+    // upwind cell c (pos: h[i+k], neg: h[i+1-k]).  Every right-biased formula
+    // of the reference is the left-biased one on the mirrored stencil (same
+    // candidates, same smoothness squares, same weights), so both flow
+    // directions run one code path and warps do not diverge on the sign.
     constexpr bool Z = SchemeInfo<S>::zfam;
     const int c = pos ? i : i + 1;
     const int d = min(c, N - 1 - c);
     const int r = min(SchemeInfo<S>::reach, d);
-    if (pos) {
-      if (r >= 4) {
-        T v[9];
+    const T* b = pos ? p : p + st;
+    const int s = pos ? st : -st;
+    auto e = [&](int k) -> T { return b[k * s]; };
+    if (r >= 4) {
+      T v[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = at(k - 4);
-        return weno_generic<T, 5>(v);
-      }
-      if (r == 3) {
-        T v[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) v[k] = at(k - 3);
-        return weno_generic<T, 4>(v);
-      }
-      if (r == 2) return weno5<T, Z>(at(-2), at(-1), at(0), at(1), at(2));
-      return Z ? wenoz3(at(-1), at(0), at(1)) : weno3(at(-1), at(0), at(1));
-    } else {
-      if (r >= 4) {  // mirrored tables == left tables on the reversed stencil
-        T v[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = at(5 - k);
-        return weno_generic<T, 5>(v);
-      }
-      if (r == 3) {
-        T v[7];
-#pragma unroll
-        for (int k = 0; k < 7; ++k) v[k] = at(4 - k);
-        return weno_generic<T, 4>(v);
-      }
-      if (r == 2) return weno5r<T, Z>(at(-1), at(0), at(1), at(2), at(3));
-      if (r == 1) return Z ? wenoz3r(at(0), at(1), at(2)) : weno3r(at(0), at(1), at(2));
-      return at(1);
+      for (int k = 0; k < 9; ++k) v[k] = e(k - 4);
+      return weno_generic<T, 5>(v);
     }
+    if (r == 3) {
+      T v[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) v[k] = e(k - 3);
+      return weno_generic<T, 4>(v);
+    }
+    if (r == 2) return weno5<T, Z>(e(-2), e(-1), e(0), e(1), e(2));
+    if (r == 1) return Z ? wenoz3(e(-1), e(0), e(1)) : weno3(e(-1), e(0), e(1));
+    return e(0);
   }
   return T(0);
 }

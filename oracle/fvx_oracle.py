@@ -1118,7 +1118,9 @@ def build_coupling_matrix(H, gp):
 
 
 def decompose_vertical_modes(A, f0):
-    lam, R = np.linalg.eigh(A)
+    """decompose_vertical_modes (vertical_modes.py:124-190); jnp.linalg.eigh
+    symmetrises its input by default, so the restatement uses (A + A^T)/2."""
+    lam, R = np.linalg.eigh(0.5 * (A + A.T))
     pos = lam > 0
     safe = np.where(pos, lam, 1.0)
     rr = np.where(pos, 1.0 / (abs(f0) * np.sqrt(safe)), np.inf)
