@@ -49,5 +49,9 @@ static inline int fvx_cuda_status() {
 
 static inline cudaStream_t fvx_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Preconditioner / coarse-solver callback: z = M rho on the given stream;
+// returns a status.
+typedef int (*fvx_precond_fn)(void* ctx, const void* rho, void* z, void* stream);
+
 template <typename T>
 DEV T ldg(const T* p) { return __ldg(p); }

@@ -148,10 +148,10 @@ struct LevArray {
 };
 
 // Whole coarse part of a V-cycle in one CTA: levels lc .. nl-1, entered with
-// f[lc] set and u[lc] = 0 (the recursion's zero initial guess).
+// f[lc] set and u[lc] = 0 (the recursion's zero initial guess).  S is the
+// level table in shared memory.
 template <typename T>
-__global__ void __launch_bounds__(kCoarseThreads)
-coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
+DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
   const int tid = threadIdx.x;
   auto sweeps = [&](const Lev<T>& L, int n) {
     const size_t cells = (size_t)L.ny * L.nx;
@@ -168,24 +168,73 @@ coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n
     }
   };
   for (int l = lc; l < nl; ++l) {
-    const Lev<T>& L = A.L[l];
+    const Lev<T>& L = S[l];
     const size_t cells = (size_t)L.ny * L.nx;
     for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = T(0);
     __syncthreads();
     if (l == nl - 1) { sweeps(L, n_coarse); break; }
     sweeps(L, n_pre);
-    const Lev<T>& C = A.L[l + 1];
+    const Lev<T>& C = S[l + 1];
     const size_t cc = (size_t)C.ny * C.nx;
     for (size_t c = tid; c < cc; c += kCoarseThreads) restrict_at(L, L.u, L.f, C, C.f, c);
     __syncthreads();
   }
   for (int l = nl - 2; l >= lc; --l) {
-    const Lev<T>& L = A.L[l];
-    const Lev<T>& C = A.L[l + 1];
+    const Lev<T>& L = S[l];
+    const Lev<T>& C = S[l + 1];
     const size_t cells = (size_t)L.ny * L.nx;
     for (size_t c = tid; c < cells; c += kCoarseThreads) prolong_at(L, L.u, C, C.u, c);
     __syncthreads();
     sweeps(L, n_post);
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads)
+coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
+  __shared__ Lev<T> S[kMaxLevels];
+  if (threadIdx.x < nl) S[threadIdx.x] = A.L[threadIdx.x];
+  __syncthreads();
+  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
+}
+
+// Many independent solves of A_lc u = f at level lc, one CTA per right-hand
+// side: u = sum of n_cycles V-cycle corrections, u += V(f - A u).  Each
+// block's level arrays u, f, tmp come from its own slice of ``work``
+// (3 * sum of the cells of levels lc .. nl-1 per block).
+template <typename T>
+__global__ void __launch_bounds__(kCoarseThreads)
+coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega,
+                            const T* __restrict__ f, T* __restrict__ u, T* work, size_t work_per_block,
+                            int n_cycles) {
+  __shared__ Lev<T> S[kMaxLevels];
+  if (threadIdx.x == 0) {
+    T* w = work + (size_t)blockIdx.x * work_per_block;
+    for (int l = lc; l < nl; ++l) {
+      S[l] = A.L[l];
+      const size_t c = (size_t)S[l].ny * S[l].nx;
+      S[l].u = w;
+      S[l].f = w + c;
+      S[l].tmp = w + 2 * c;
+      w += 3 * c;
+    }
+  }
+  __syncthreads();
+  const Lev<T>& L = S[lc];
+  const size_t cells = (size_t)L.ny * L.nx;
+  const T* fb = f + (size_t)blockIdx.x * cells;
+  T* ub = u + (size_t)blockIdx.x * cells;
+  for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) ub[c] = T(0);
+  __syncthreads();
+  for (int k = 0; k < n_cycles; ++k) {
+    for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) {
+      const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+      L.f[c] = (fb[c] - apply_at(L, ub, j, i)) * L.mask[c];
+    }
+    __syncthreads();
+    coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
+    for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) ub[c] += L.u[c];
+    __syncthreads();
   }
 }
 
@@ -466,6 +515,155 @@ extern "C" int fvx_mg_vcycle(fvx_mg* g, const void* u_in, const void* f, void* u
                        : vcycle0<double>(g, (const double*)u_in, (const double*)f, (double*)u_out, st);
 }
 
+// ---------------------------------------------------------------------------
+// Hybrid cycle for a learned coarse solver: the V-cycle's legs on levels
+// 0 .. lvl-1 (n_pre / n_post weighted-Jacobi sweeps from a zero guess, the
+// reference's restriction and prolongation) with the level-lvl correction
+// supplied by ``coarse(ctx, f_lvl, u_lvl, stream)``, which reads the
+// restricted residual f_lvl and writes u_lvl (both [ny_lvl, nx_lvl], plan
+// dtype).  With ``coarse`` NULL the correction is zero.
+template <typename T>
+static int hybrid_down(fvx_mg* g, const T* f, int lvl, int n_pre, cudaStream_t st) {
+  LevArray<T>& A = levs<T>(g);
+  const T om = (T)g->omega;
+  Lev<T>& L0 = A.L[0];
+  copy_kernel<T><<<grid_for((size_t)L0.ny * L0.nx), 256, 0, st>>>(L0.f, f, (size_t)L0.ny * L0.nx);
+  for (int l = 0; l < lvl; ++l) {
+    Lev<T>& L = A.L[l];
+    const size_t n = (size_t)L.ny * L.nx;
+    const int gr = grid_for(n);
+    fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
+    T* a = L.u;
+    T* b = L.tmp;
+    for (int s = 0; s < n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+    if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+    Lev<T>& C = A.L[l + 1];
+    restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
+  }
+  return fvx_cuda_status();
+}
+
+template <typename T>
+static int hybrid_up(fvx_mg* g, T* u_out, int lvl, int n_post, cudaStream_t st) {
+  LevArray<T>& A = levs<T>(g);
+  const T om = (T)g->omega;
+  for (int l = lvl - 1; l >= 0; --l) {
+    Lev<T>& L = A.L[l];
+    Lev<T>& C = A.L[l + 1];
+    const size_t n = (size_t)L.ny * L.nx;
+    const int gr = grid_for(n);
+    prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
+    T* a = L.u;
+    T* b = L.tmp;
+    for (int s = 0; s < n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
+    if (l == 0) copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
+    else if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+  }
+  return fvx_cuda_status();
+}
+
+template <typename T>
+static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int n_post, fvx_precond_fn coarse,
+                        void* ctx, cudaStream_t st) {
+  int rc = hybrid_down<T>(g, f, lvl, n_pre, st);
+  if (rc) return rc;
+  Lev<T>& C = levs<T>(g).L[lvl];
+  if (coarse) {
+    if ((rc = coarse(ctx, C.f, C.u, st))) return rc;
+  } else {
+    fill_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(C.u, (size_t)C.ny * C.nx, T(0));
+  }
+  return hybrid_up<T>(g, u_out, lvl, n_post, st);
+}
+
+extern "C" int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
+                                    fvx_precond_fn coarse, void* ctx, void* stream) {
+  if (!g || !f || !u_out || n_pre < 0 || n_post < 0) return FVX_ERR_ARG;
+  if (lvl < 1 || lvl >= g->nl) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  return g->dtype == 0 ? hybrid_cycle<float>(g, (const float*)f, (float*)u_out, lvl, n_pre, n_post, coarse, ctx, st)
+                       : hybrid_cycle<double>(g, (const double*)f, (double*)u_out, lvl, n_pre, n_post, coarse, ctx,
+                                              st);
+}
+
+// The hybrid cycle packaged as a preconditioner callback (ctx = the
+// fvx_hybrid object) for fvx_pcg_solve / fvx_pcg_iterate with precond 2.
+struct fvx_hybrid {
+  fvx_mg* g;
+  int lvl, n_pre, n_post;
+  fvx_precond_fn coarse;
+  void* ctx;
+};
+
+extern "C" int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, fvx_precond_fn coarse, void* ctx,
+                                 fvx_hybrid** out) {
+  if (!g || !out || n_pre < 0 || n_post < 0) return FVX_ERR_ARG;
+  if (lvl < 1 || lvl >= g->nl) return FVX_ERR_SHAPE;
+  *out = new fvx_hybrid{g, lvl, n_pre, n_post, coarse, ctx};
+  return FVX_OK;
+}
+
+extern "C" int fvx_hybrid_destroy(fvx_hybrid* h) {
+  delete h;
+  return FVX_OK;
+}
+
+extern "C" int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* stream) {
+  fvx_hybrid* h = (fvx_hybrid*)ctx;
+  if (!h) return FVX_ERR_ARG;
+  return fvx_mg_vcycle_hybrid(h->g, rho, z, h->lvl, h->n_pre, h->n_post, h->coarse, h->ctx, stream);
+}
+
+// The downward leg only: the level-lvl restricted residual of f, copied to
+// f_lvl ([ny_lvl, nx_lvl]); used to generate training inputs.
+extern "C" int fvx_mg_restrict_residual(fvx_mg* g, const void* f, int lvl, int n_pre, void* f_lvl, void* stream) {
+  if (!g || !f || !f_lvl || n_pre < 0) return FVX_ERR_ARG;
+  if (lvl < 1 || lvl >= g->nl) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  if (g->dtype == 0) {
+    int rc = hybrid_down<float>(g, (const float*)f, lvl, n_pre, st);
+    Lev<float>& C = g->A32.L[lvl];
+    const size_t n = (size_t)C.ny * C.nx;
+    copy_kernel<float><<<grid_for(n), 256, 0, st>>>((float*)f_lvl, C.f, n);
+    return rc ? rc : fvx_cuda_status();
+  }
+  int rc = hybrid_down<double>(g, (const double*)f, lvl, n_pre, st);
+  Lev<double>& C = g->A64.L[lvl];
+  const size_t n = (size_t)C.ny * C.nx;
+  copy_kernel<double><<<grid_for(n), 256, 0, st>>>((double*)f_lvl, C.f, n);
+  return rc ? rc : fvx_cuda_status();
+}
+
+// Scratch elements per right-hand side for fvx_mg_solve_level_batched.
+extern "C" long long fvx_mg_level_work(fvx_mg* g, int lvl) {
+  if (!g || lvl < 0 || lvl >= g->nl) return -1;
+  long long w = 0;
+  for (int l = lvl; l < g->nl; ++l)
+    w += g->dtype == 0 ? 3LL * g->A32.L[l].ny * g->A32.L[l].nx : 3LL * g->A64.L[l].ny * g->A64.L[l].nx;
+  return w;
+}
+
+// ``batch`` independent solves A_lvl u_b = f_b at level lvl (MG cycles run
+// by one CTA each); f, u: [batch, ny_lvl, nx_lvl]; work: batch *
+// fvx_mg_level_work(g, lvl) elements of the plan dtype.
+extern "C" int fvx_mg_solve_level_batched(fvx_mg* g, int lvl, int batch, const void* f, void* u, int n_cycles,
+                                          void* work, void* stream) {
+  if (!g || !f || !u || !work || batch < 0 || n_cycles < 1) return FVX_ERR_ARG;
+  if (lvl < 0 || lvl >= g->nl) return FVX_ERR_SHAPE;
+  if (batch == 0) return FVX_OK;
+  cudaStream_t st = fvx_stream(stream);
+  const size_t wpb = (size_t)fvx_mg_level_work(g, lvl);
+  if (g->dtype == 0)
+    coarse_solve_batched_kernel<float><<<batch, kCoarseThreads, 0, st>>>(
+        g->A32, lvl, g->nl, g->n_pre, g->n_post, g->n_coarse, (float)g->omega, (const float*)f, (float*)u,
+        (float*)work, wpb, n_cycles);
+  else
+    coarse_solve_batched_kernel<double><<<batch, kCoarseThreads, 0, st>>>(
+        g->A64, lvl, g->nl, g->n_pre, g->n_post, g->n_coarse, g->omega, (const double*)f, (double*)u,
+        (double*)work, wpb, n_cycles);
+  return fvx_cuda_status();
+}
+
 // MultigridSolver._run_vcycles (multigrid.py:885-897): n_cycles V-cycles from 0.
 extern "C" int fvx_mg_solve(fvx_mg* g, const void* f, void* u, int n_cycles, void* stream) {
   if (!g || !f || !u || n_cycles < 0) return FVX_ERR_ARG;
@@ -693,96 +891,170 @@ extern "C" int fvx_pcg_destroy(fvx_pcg* P) {
   return fvx_cuda_status();
 }
 
-// Preconditioner callback: z = M rho on the given stream; returns a status.
-typedef int (*fvx_precond_fn)(void* ctx, const void* rho, void* z, void* stream);
+// The PCG in four entry points so a host can capture fvx_pcg_iterate (and
+// the preconditioner launches it makes) in a CUDA graph and replay it:
+// begin (rho = b, z = M rho, p = z, gamma), iterate (n iterations, no host
+// synchronisation; kernels return at once after convergence), status (reads
+// the flag, synchronises), finish (FP64 true residual).
+struct PcgCall {
+  int precond;
+  fvx_precond_fn fn;
+  void* ctx;
+  int flexible;
+  int replace_every;
+};
 
 template <typename T>
-static int pcg_run(fvx_pcg* P, const T* b, double* x, int max_iter, double rtol, int precond, fvx_precond_fn fn,
-                   void* ctx, int flexible, int replace_every, int chunk, double* info, cudaStream_t st) {
+static int pcg_apply_M(fvx_pcg* P, const PcgCall& c, cudaStream_t st) {
+  if (c.precond == 1) return fvx_mg_vcycle(P->mg, nullptr, P->rho, P->z, st);
+  if (c.precond == 2) return c.fn(c.ctx, P->rho, P->z, st);
+  k_copy_if<T><<<kRedBlocks, 256, 0, st>>>((T*)P->z, (const T*)P->rho, P->n, P->s);
+  return fvx_cuda_status();
+}
+
+template <typename T>
+static int pcg_begin_t(fvx_pcg* P, const T* b, double* x, double rtol, const PcgCall& c, double* bb_out,
+                       cudaStream_t st) {
+  fvx_mg* g = P->mg;
+  const size_t n = P->n;
+  double* s = P->s;
+  const int G = kRedBlocks;
+  double init[S_NSLOTS] = {0};
+  cudaMemcpyAsync(s, init, sizeof(init), cudaMemcpyHostToDevice, st);
+  k_zero_x<T><<<G, 256, 0, st>>>(x, n);
+  k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, (T*)P->rho, P->part, s, 1);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_BB, R_STORE, 1);
+  double bb = 0;
+  cudaMemcpyAsync(&bb, s + S_BB, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
+  *bb_out = bb;
+  const double tol2 = rtol * rtol * bb;
+  double conv = bb == 0.0 ? 1.0 : 0.0;
+  cudaMemcpyAsync(s + S_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s + S_CONV, &conv, sizeof(double), cudaMemcpyHostToDevice, st);
+  if (bb == 0.0) return FVX_OK;
+  int rc = pcg_apply_M<T>(P, c, st);
+  if (rc) return rc;
+  k_copy_if<T><<<G, 256, 0, st>>>((T*)P->p, (const T*)P->z, n, s);
+  k_dot<T><<<G, 256, 0, st>>>((const T*)P->rho, (const T*)P->z, nullptr, P->part, nullptr, s, n);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_GAMMA, R_STORE, 0);
+  return fvx_cuda_status();
+}
+
+// ``it0``: iterations already done (for the residual-replacement schedule).
+template <typename T>
+static int pcg_iterate_t(fvx_pcg* P, const T* b, double* x, int it0, int niter, const PcgCall& c, cudaStream_t st) {
   fvx_mg* g = P->mg;
   Lev<T>& L = levs<T>(g).L[0];
   const size_t n = P->n;
   T *rho = (T*)P->rho, *z = (T*)P->z, *p = (T*)P->p, *Ap = (T*)P->Ap, *rp = (T*)P->rho_prev;
   double* s = P->s;
   const int G = kRedBlocks;
-  double init[S_NSLOTS] = {0};
-  cudaMemcpyAsync(s, init, sizeof(init), cudaMemcpyHostToDevice, st);
-  k_zero_x<T><<<G, 256, 0, st>>>(x, n);
-  // rho = b (x = 0), bb = |b|^2 computed in FP64
-  k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 1);
-  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_BB, R_STORE, 1);
-  double bb = 0;
-  cudaMemcpyAsync(&bb, s + S_BB, sizeof(double), cudaMemcpyDeviceToHost, st);
+  for (int k = 0; k < niter; ++k) {
+    const int it = it0 + k;
+    k_apply_dot<T><<<G, 256, 0, st>>>(L, p, Ap, P->part, s);
+    k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_ALPHA, 0);
+    k_update<T><<<G, 256, 0, st>>>(x, p, Ap, rho, c.flexible ? rp : nullptr, P->part, s, n);
+    if (c.replace_every > 0 && (it + 1) % c.replace_every == 0)
+      k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 0);
+    k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_RR, 0);
+    int rc = pcg_apply_M<T>(P, c, st);
+    if (rc) return rc;
+    k_dot<T><<<G, 256, 0, st>>>(z, rho, c.flexible ? rp : nullptr, P->part, P->part2, s, n);
+    k_reduce<<<1, 256, 0, st>>>(P->part, c.flexible ? P->part2 : nullptr, G, s, 0,
+                                c.flexible ? R_BETA_FLEX : R_BETA, 0);
+    k_pupdate<T><<<G, 256, 0, st>>>(p, z, s, n);
+  }
+  return fvx_cuda_status();
+}
+
+template <typename T>
+static int pcg_finish_t(fvx_pcg* P, const T* b, double* x, double bb, double* rel_out, cudaStream_t st) {
+  const int G = kRedBlocks;
+  k_residual64<T><<<G, 256, 0, st>>>(P->mg->L0d, x, b, (T*)nullptr, P->part, P->s, 1);
+  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, P->s, S_RR, R_STORE, 1);
+  double rr = 0;
+  cudaMemcpyAsync(&rr, P->s + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
-  const double tol2 = rtol * rtol * bb;
-  cudaMemcpyAsync(s + S_TOL2, &tol2, sizeof(double), cudaMemcpyHostToDevice, st);
-  auto apply_M = [&]() -> int {
-    if (precond == 1) return fvx_mg_vcycle(g, nullptr, rho, z, st);
-    if (precond == 2) return fn(ctx, rho, z, st);
-    k_copy_if<T><<<G, 256, 0, st>>>(z, rho, n, s);
-    return fvx_cuda_status();
-  };
-  int rc = FVX_OK;
+  *rel_out = bb > 0 ? sqrt(rr / bb) : 0.0;
+  return FVX_OK;
+}
+
+extern "C" int fvx_pcg_begin(fvx_pcg* P, const void* b, double* x, double rtol, int precond, fvx_precond_fn fn,
+                             void* ctx, double* bb_out, void* stream) {
+  if (!P || !b || !x || !bb_out || (precond == 2 && !fn)) return FVX_ERR_ARG;
+  PcgCall c{precond, fn, ctx, 0, 0};
+  cudaStream_t st = fvx_stream(stream);
+  return P->dtype == 0 ? pcg_begin_t<float>(P, (const float*)b, x, rtol, c, bb_out, st)
+                       : pcg_begin_t<double>(P, (const double*)b, x, rtol, c, bb_out, st);
+}
+
+extern "C" int fvx_pcg_iterate(fvx_pcg* P, const void* b, double* x, int it0, int niter, int precond,
+                               fvx_precond_fn fn, void* ctx, int flexible, int replace_every, void* stream) {
+  if (!P || !b || !x || niter < 0 || (precond == 2 && !fn)) return FVX_ERR_ARG;
+  PcgCall c{precond, fn, ctx, flexible, replace_every};
+  cudaStream_t st = fvx_stream(stream);
+  return P->dtype == 0 ? pcg_iterate_t<float>(P, (const float*)b, x, it0, niter, c, st)
+                       : pcg_iterate_t<double>(P, (const double*)b, x, it0, niter, c, st);
+}
+
+// Reads [converged flag, iterations, last |rho|^2]; synchronises the stream.
+extern "C" int fvx_pcg_status(fvx_pcg* P, double* out3, void* stream) {
+  if (!P || !out3) return FVX_ERR_ARG;
+  double hs[S_NSLOTS];
+  cudaStream_t st = fvx_stream(stream);
+  if (cudaMemcpyAsync(hs, P->s, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return FVX_ERR_CUDA;
+  out3[0] = hs[S_CONV];
+  out3[1] = hs[S_ITER];
+  out3[2] = hs[S_RR];
+  return FVX_OK;
+}
+
+extern "C" int fvx_pcg_finish(fvx_pcg* P, const void* b, double* x, double bb, double* rel_out, void* stream) {
+  if (!P || !b || !x || !rel_out) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  return P->dtype == 0 ? pcg_finish_t<float>(P, (const float*)b, x, bb, rel_out, st)
+                       : pcg_finish_t<double>(P, (const double*)b, x, bb, rel_out, st);
+}
+
+template <typename T>
+static int pcg_run(fvx_pcg* P, const T* b, double* x, int max_iter, double rtol, int precond, fvx_precond_fn fn,
+                   void* ctx, int flexible, int replace_every, int chunk, double* info, cudaStream_t st) {
+  PcgCall c{precond, fn, ctx, flexible, replace_every};
+  double bb = 0;
+  int rc = pcg_begin_t<T>(P, b, x, rtol, c, &bb, st);
+  if (rc) return rc;
   if (bb == 0.0) {
     if (info) { info[0] = 0; info[1] = 0; info[2] = 1; }
     return FVX_OK;
   }
-  if ((rc = apply_M())) return rc;
-  k_copy_if<T><<<G, 256, 0, st>>>(p, z, n, s);
-  k_dot<T><<<G, 256, 0, st>>>(rho, z, nullptr, P->part, nullptr, s, n);
-  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_GAMMA, R_STORE, 0);
   int it = 0;
-  double hs[S_NSLOTS];
-  bool conv = false;
-  while (it < max_iter && !conv) {
+  double hs[3] = {0, 0, 0};
+  while (it < max_iter && hs[0] == 0.0) {
     const int m = chunk < max_iter - it ? chunk : max_iter - it;
-    for (int k = 0; k < m; ++k, ++it) {
-      k_apply_dot<T><<<G, 256, 0, st>>>(L, p, Ap, P->part, s);
-      k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_ALPHA, 0);
-      k_update<T><<<G, 256, 0, st>>>(x, p, Ap, rho, flexible ? rp : nullptr, P->part, s, n);
-      if (replace_every > 0 && (it + 1) % replace_every == 0)
-        k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 0);
-      k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_RR, 0);
-      if ((rc = apply_M())) return rc;
-      k_dot<T><<<G, 256, 0, st>>>(z, rho, flexible ? rp : nullptr, P->part, P->part2, s, n);
-      k_reduce<<<1, 256, 0, st>>>(P->part, flexible ? P->part2 : nullptr, G, s, 0, flexible ? R_BETA_FLEX : R_BETA, 0);
-      k_pupdate<T><<<G, 256, 0, st>>>(p, z, s, n);
-    }
-    if ((rc = fvx_cuda_status())) return rc;
-    if (cudaMemcpyAsync(hs, s, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-        cudaStreamSynchronize(st) != cudaSuccess)
-      return FVX_ERR_CUDA;
-    conv = hs[S_CONV] != 0.0;
+    if ((rc = pcg_iterate_t<T>(P, b, x, it, m, c, st))) return rc;
+    it += m;
+    if ((rc = fvx_pcg_status(P, hs, st))) return rc;
   }
-  // final FP64 true residual
-  k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, (T*)nullptr, P->part, s, 1);
-  k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_RR, R_STORE, 1);
-  double rr = 0;
-  cudaMemcpyAsync(&rr, s + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
-  const double rel = sqrt(rr / bb);
-  if (info) { info[0] = hs[S_ITER]; info[1] = rel; info[2] = rel <= rtol ? 1.0 : 0.0; }
+  double rel = 0;
+  if ((rc = pcg_finish_t<T>(P, b, x, bb, &rel, st))) return rc;
+  if (info) { info[0] = hs[1]; info[1] = rel; info[2] = rel <= rtol ? 1.0 : 0.0; }
   return rel <= rtol ? FVX_OK : FVX_ERR_NOT_CONVERGED;
 }
 
-// PCG on A x = b (A the plan's finest operator, negative definite) to
-// ||b - A x||_2 <= rtol ||b||_2 checked in FP64.  precond: 0 none, 1 one MG
-// V-cycle from zero (make_multigrid_preconditioner, preconditioners.py:
-// 207-244), 2 the callback ``fn(ctx, rho, z, stream)``.  flexible: Polak-
-// Ribiere beta (for preconditioners that change between iterations).
-// b: plan dtype; x: FP64 output.  info: [iterations, relative residual,
-// converged].
+// Whole solve: begin, chunks of ``chunk`` iterations between reads of the
+// device convergence flag, FP64 true residual at the end.
 extern "C" int fvx_pcg_solve(fvx_pcg* P, const void* b, double* x, int max_iter, double rtol, int precond,
                              fvx_precond_fn fn, void* ctx, int flexible, int replace_every, int chunk, double* info,
                              void* stream) {
-  if (!P || !b || !x || max_iter < 0 || chunk < 1) return FVX_ERR_ARG;
-  if (precond == 2 && !fn) return FVX_ERR_ARG;
+  if (!P || !b || !x || max_iter < 0 || chunk < 1 || (precond == 2 && !fn)) return FVX_ERR_ARG;
   cudaStream_t st = fvx_stream(stream);
-  return P->dtype == 0
-             ? pcg_run<float>(P, (const float*)b, x, max_iter, rtol, precond, fn, ctx, flexible, replace_every, chunk,
-                              info, st)
-             : pcg_run<double>(P, (const double*)b, x, max_iter, rtol, precond, fn, ctx, flexible, replace_every,
-                               chunk, info, st);
+  return P->dtype == 0 ? pcg_run<float>(P, (const float*)b, x, max_iter, rtol, precond, fn, ctx, flexible,
+                                        replace_every, chunk, info, st)
+                       : pcg_run<double>(P, (const double*)b, x, max_iter, rtol, precond, fn, ctx, flexible,
+                                         replace_every, chunk, info, st);
 }
 
 // Use caller-owned device buffers (plan dtype, [ny, nx]) as the residual rho

@@ -1,0 +1,641 @@
+// Learned coarse-grid preconditioner: a 4-level U-Net (16/16/32/32
+// channels) with hand-written forward, backward and Adam kernels.
+//
+// Tensors are FP32 [B, C, h, w]; convolution weights are [Cout, Cin, 3, 3]
+// with FP32 master copies for training and BF16 copies for the forward pass
+// (BF16 weights, FP32 accumulation).  One conv layer reads its input through
+// an optional 2x2 average pool (from a 2h x 2w tensor) or a nearest 2x
+// upsample (from an h/2 x w/2 tensor), adds a bias and an optional skip
+// tensor, and applies ReLU.  The reference has no learned component; this
+// is new work measured against its multigrid preconditioner.
+#include "fvx_common.cuh"
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
+
+namespace fvx {
+namespace nn {
+
+enum InMode { IN_DIRECT = 0, IN_POOL = 1, IN_UP = 2 };
+constexpr int TILE = 16;           // 16 x 16 output pixels per block
+constexpr int THREADS = TILE * TILE;
+constexpr int CMAX = 32;
+
+// value of the conv input (channel plane ``src`` of the source tensor) at
+// conv-grid pixel (y, x); zero outside [0, h) x [0, w)
+DEV float in_at(const float* src, int mode, int h, int w, int y, int x) {
+  if (y < 0 || y >= h || x < 0 || x >= w) return 0.f;
+  if (mode == IN_DIRECT) return src[(size_t)y * w + x];
+  if (mode == IN_POOL) {
+    const int W2 = 2 * w;
+    const float* p = src + (size_t)(2 * y) * W2 + 2 * x;
+    return 0.25f * ((p[0] + p[1]) + (p[W2] + p[W2 + 1]));
+  }
+  return src[(size_t)(y >> 1) * (w >> 1) + (x >> 1)];  // IN_UP
+}
+
+__host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
+  return mode == IN_DIRECT ? (size_t)h * w : (mode == IN_POOL ? (size_t)4 * h * w : (size_t)(h / 2) * (w / 2));
+}
+
+// y = act(W * in + b [+ skip]); one thread per output pixel, all Cout
+// accumulators in registers, input tiles and weights staged in smem.
+template <int COUT>
+__global__ void __launch_bounds__(THREADS)
+conv_fwd_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
+                const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
+                int w, int relu) {
+  __shared__ float tile[TILE + 2][TILE + 2];
+  __shared__ float ws[CMAX * 9 * COUT];
+  const int b = blockIdx.z;
+  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+  const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
+  for (int k = threadIdx.x; k < cin * 9 * COUT; k += THREADS) {
+    // ws[(ci*9 + t)*COUT + co] = W[co][ci][t]
+    const int co = k % COUT, rest = k / COUT;
+    ws[k] = __bfloat162float(wb[(size_t)co * cin * 9 + rest]);
+  }
+  float acc[COUT];
+#pragma unroll
+  for (int co = 0; co < COUT; ++co) acc[co] = 0.f;
+  const size_t sp = src_plane(mode, h, w);
+  const float* inb = in + (size_t)b * cin * sp;
+  for (int ci = 0; ci < cin; ++ci) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < (TILE + 2) * (TILE + 2); k += THREADS) {
+      const int ly = k / (TILE + 2), lx = k % (TILE + 2);
+      tile[ly][lx] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const float v = tile[ty + t / 3][tx + t % 3];
+      const float* wr = ws + (ci * 9 + t) * COUT;
+#pragma unroll
+      for (int co = 0; co < COUT; ++co) acc[co] = fmaf(wr[co], v, acc[co]);
+    }
+  }
+  const int y = y0 + ty, x = x0 + tx;
+  if (y >= h || x >= w) return;
+  const size_t plane = (size_t)h * w, base = (size_t)b * COUT * plane + (size_t)y * w + x;
+#pragma unroll
+  for (int co = 0; co < COUT; ++co) {
+    float v = acc[co] + bias[co];
+    if (skip) v += skip[base + co * plane];
+    if (relu) v = fmaxf(v, 0.f);
+    out[base + co * plane] = v;
+  }
+}
+
+// G = dL/d(pre-activation) = dY * (y > 0) (or dY when the layer is linear);
+// dskip += G.
+__global__ void act_grad_kernel(const float* dy, const float* y, float* g, float* dskip, size_t n, int relu) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float v = relu ? (y[k] > 0.f ? dy[k] : 0.f) : dy[k];
+    g[k] = v;
+    if (dskip) dskip[k] += v;
+  }
+}
+
+// dXin[b, ci, p] = sum_co sum_t W[co][ci][t] G[b, co, p - (t - 1)] (the conv's
+// adjoint on the conv-input grid), W the BF16 weights the forward pass used.
+template <int CIN>
+__global__ void __launch_bounds__(THREADS)
+conv_bwd_data_kernel(const float* __restrict__ g, int cout, const __nv_bfloat16* __restrict__ wb,
+                     float* __restrict__ dxin, int h, int w) {
+  __shared__ float tile[TILE + 2][TILE + 2];
+  __shared__ float ws[CMAX * 9 * CIN];
+  const int b = blockIdx.z;
+  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+  const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
+  for (int k = threadIdx.x; k < cout * 9 * CIN; k += THREADS) {
+    // ws[(co*9 + t)*CIN + ci] = W[co][ci][t]
+    const int ci = k % CIN, rest = k / CIN, co = rest / 9, t = rest % 9;
+    ws[k] = __bfloat162float(wb[((size_t)co * CIN + ci) * 9 + t]);
+  }
+  float acc[CIN];
+#pragma unroll
+  for (int ci = 0; ci < CIN; ++ci) acc[ci] = 0.f;
+  const size_t plane = (size_t)h * w;
+  const float* gb = g + (size_t)b * cout * plane;
+  for (int co = 0; co < cout; ++co) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < (TILE + 2) * (TILE + 2); k += THREADS) {
+      const int ly = k / (TILE + 2), lx = k % (TILE + 2);
+      const int yy = y0 - 1 + ly, xx = x0 - 1 + lx;
+      tile[ly][lx] = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? gb[co * plane + (size_t)yy * w + xx] : 0.f;
+    }
+    __syncthreads();
+    // input pixel p receives G at p - (t - 1): tile offset (2 - dy, 2 - dx)
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const float v = tile[ty + 2 - t / 3][tx + 2 - t % 3];
+      const float* wr = ws + (co * 9 + t) * CIN;
+#pragma unroll
+      for (int ci = 0; ci < CIN; ++ci) acc[ci] = fmaf(wr[ci], v, acc[ci]);
+    }
+  }
+  const int y = y0 + ty, x = x0 + tx;
+  if (y >= h || x >= w) return;
+  const size_t base = (size_t)b * CIN * plane + (size_t)y * w + x;
+#pragma unroll
+  for (int ci = 0; ci < CIN; ++ci) dxin[base + ci * plane] = acc[ci];
+}
+
+// Adjoint of the input transform: dsrc += T^T dxin.
+__global__ void in_adjoint_kernel(const float* dxin, float* dsrc, int mode, int bc, int h, int w) {
+  // bc = B * Cin planes; conv grid h x w
+  const size_t sp = src_plane(mode, h, w);
+  const size_t n = (size_t)bc * sp;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const size_t pl = k / sp, r = k - pl * sp;
+    const float* d = dxin + pl * (size_t)h * w;
+    float v;
+    if (mode == IN_DIRECT) v = d[r];
+    else if (mode == IN_POOL) {  // source (Y, X) on the 2h x 2w grid
+      const int Y = (int)(r / (2 * w)), X = (int)(r % (2 * w));
+      v = 0.25f * d[(size_t)(Y >> 1) * w + (X >> 1)];
+    } else {  // IN_UP: source (Y, X) on the h/2 x w/2 grid gathers its 4 children
+      const int w2 = w / 2;
+      const int Y = (int)(r / w2), X = (int)(r % w2);
+      const float* c = d + (size_t)(2 * Y) * w + 2 * X;
+      v = (c[0] + c[1]) + (c[w] + c[w + 1]);
+    }
+    dsrc[k] += v;
+  }
+}
+
+// dW partials: block (tile, b) sums G[co] * Xin[ci] shifted over its 16x16
+// pixels for every (co, ci, t); db partials likewise.
+__global__ void __launch_bounds__(THREADS)
+conv_bwd_weight_kernel(const float* __restrict__ in, int mode, int cin, const float* __restrict__ g, int cout, int h,
+                       int w, float* __restrict__ part_w, float* __restrict__ part_b) {
+  __shared__ float gs[CMAX][TILE * TILE];
+  __shared__ float xs[TILE + 2][TILE + 2];
+  const int b = blockIdx.z;
+  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
+  const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const size_t plane = (size_t)h * w;
+  for (int k = threadIdx.x; k < cout * TILE * TILE; k += THREADS) {
+    const int co = k / (TILE * TILE), p = k % (TILE * TILE);
+    const int y = y0 + p / TILE, x = x0 + p % TILE;
+    gs[co][p] = (y < h && x < w) ? g[((size_t)b * cout + co) * plane + (size_t)y * w + x] : 0.f;
+  }
+  __syncthreads();
+  if (threadIdx.x < cout) {
+    float s = 0.f;
+    for (int p = 0; p < TILE * TILE; ++p) s += gs[threadIdx.x][p];
+    part_b[(size_t)blk * cout + threadIdx.x] = s;
+  }
+  const size_t sp = src_plane(mode, h, w);
+  const float* inb = in + (size_t)b * cin * sp;
+  const int combos = cout * 9;
+  for (int ci = 0; ci < cin; ++ci) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < (TILE + 2) * (TILE + 2); k += THREADS) {
+      const int ly = k / (TILE + 2), lx = k % (TILE + 2);
+      xs[ly][lx] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < combos; c += THREADS) {
+      const int co = c / 9, t = c % 9, dy = t / 3, dx = t % 3;
+      float s = 0.f;
+      for (int p = 0; p < TILE * TILE; ++p) s = fmaf(gs[co][p], xs[p / TILE + dy][p % TILE + dx], s);
+      part_w[(size_t)blk * cout * cin * 9 + ((size_t)co * cin + ci) * 9 + t] = s;
+    }
+  }
+}
+
+// sum over blocks (fixed order) of the partials into grad
+__global__ void reduce_parts_kernel(const float* part, int nblk, int len, float* grad) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int j = 0; j < nblk; ++j) s += part[(size_t)j * len + k];
+    grad[k] = s;
+  }
+}
+
+// L = sum(mask * (pred - target)^2) / sum(mask); dpred = 2 mask (pred - target) / sum(mask)
+// (mask of sample b at mask + b * mstride)
+__global__ void mse_kernel(const float* pred, const float* target, const float* mask, size_t mstride, size_t plane,
+                           int batch, float* dpred, double* loss_acc, double msum) {
+  double acc = 0.0;
+  const size_t n = plane * batch;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const size_t b = k / plane;
+    const float m = mask ? mask[b * mstride + (k - b * plane)] : 1.f;
+    const float d = (pred[k] - target[k]) * m;
+    dpred[k] = (float)(2.0 * d / msum);
+    acc += (double)d * d;
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss_acc, acc / msum);
+}
+
+// Adam (Kingma & Ba 2015) on FP32 master weights, refreshing the BF16 copy.
+__global__ void adam_kernel(float* wgt, __nv_bfloat16* wb, const float* grad, float* m, float* v, int n, float lr,
+                            float b1, float b2, float eps, float c1, float c2) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float g = grad[k];
+    const float mk = b1 * m[k] + (1.f - b1) * g;
+    const float vk = b2 * v[k] + (1.f - b2) * g * g;
+    m[k] = mk;
+    v[k] = vk;
+    const float wk = wgt[k] - lr * (mk / c1) / (sqrtf(vk / c2) + eps);
+    wgt[k] = wk;
+    if (wb) wb[k] = __float2bfloat16_rn(wk);
+  }
+}
+
+__global__ void to_bf16_kernel(const float* src, __nv_bfloat16* dst, int n) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    dst[k] = __float2bfloat16_rn(src[k]);
+}
+
+static int blocks_for(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
+}
+
+}  // namespace nn
+}  // namespace fvx
+
+using namespace fvx;
+using namespace fvx::nn;
+
+extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
+                               const float* skip, float* out, int cout, int h, int w, int relu, void* stream) {
+  if (!in || !w_bf16 || !bias || !out) return FVX_ERR_ARG;
+  if (cin < 1 || cin > CMAX || batch < 1 || h < 1 || w < 1 || mode < 0 || mode > 2) return FVX_ERR_SHAPE;
+  if ((mode == IN_UP) && ((h % 2) || (w % 2))) return FVX_ERR_SHAPE;
+  dim3 g((w + TILE - 1) / TILE, (h + TILE - 1) / TILE, batch);
+  cudaStream_t st = fvx_stream(stream);
+  const __nv_bfloat16* wb = (const __nv_bfloat16*)w_bf16;
+  switch (cout) {
+    case 1: conv_fwd_kernel<1><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
+    case 16: conv_fwd_kernel<16><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
+    case 32: conv_fwd_kernel<32><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
+    default: return FVX_ERR_SHAPE;
+  }
+  return fvx_cuda_status();
+}
+
+// Backward of one conv layer (wb: the BF16 weights of the forward pass).
+// dy: dL/dy (post-activation); y: the layer's output (for the ReLU mask).  Writes g (scratch [B, Cout, h, w]), adds the
+// skip gradient into dskip (if non-null), adds the input gradient into
+// dsrc (if non-null; dxin scratch [B, Cin, h, w]), and writes dW, db.
+// part: scratch of nblocks * Cout * (Cin * 9 + 1) floats.
+extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, const void* wb, const float* dy,
+                               const float* y, int cout, int h, int w, int relu, float* g, float* dskip, float* dxin,
+                               float* dsrc, float* dw, float* db, float* part, void* stream) {
+  if (!in || !wb || !dy || !y || !g || !dw || !db || !part) return FVX_ERR_ARG;
+  const __nv_bfloat16* wf = (const __nv_bfloat16*)wb;
+  if (cin < 1 || cin > CMAX || cout < 1 || cout > CMAX) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  const size_t n = (size_t)batch * cout * h * w;
+  act_grad_kernel<<<blocks_for(n), 256, 0, st>>>(dy, y, g, dskip, n, relu);
+  dim3 gr((w + TILE - 1) / TILE, (h + TILE - 1) / TILE, batch);
+  const int nblk = gr.x * gr.y * gr.z;
+  float* pw = part;
+  float* pb = part + (size_t)nblk * cout * cin * 9;
+  conv_bwd_weight_kernel<<<gr, THREADS, 0, st>>>(in, mode, cin, g, cout, h, w, pw, pb);
+  reduce_parts_kernel<<<blocks_for((size_t)cout * cin * 9), 256, 0, st>>>(pw, nblk, cout * cin * 9, dw);
+  reduce_parts_kernel<<<1, 256, 0, st>>>(pb, nblk, cout, db);
+  if (dsrc) {
+    if (!dxin) return FVX_ERR_ARG;
+    switch (cin) {
+      case 1: conv_bwd_data_kernel<1><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+      case 2: conv_bwd_data_kernel<2><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+      case 3: conv_bwd_data_kernel<3><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+      case 16: conv_bwd_data_kernel<16><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+      case 32: conv_bwd_data_kernel<32><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+      default: return FVX_ERR_SHAPE;
+    }
+    const size_t sp = src_plane(mode, h, w);
+    in_adjoint_kernel<<<blocks_for((size_t)batch * cin * sp), 256, 0, st>>>(dxin, dsrc, mode, batch * cin, h, w);
+  }
+  return fvx_cuda_status();
+}
+
+// Number of blocks a conv_bwd call uses for its partials (scratch sizing).
+extern "C" int fvx_nn_conv_bwd_blocks(int batch, int h, int w) {
+  return ((w + TILE - 1) / TILE) * ((h + TILE - 1) / TILE) * batch;
+}
+
+extern "C" int fvx_nn_mse(const float* pred, const float* target, const float* mask, long long plane, int batch,
+                          float* dpred, double* loss_dev, double mask_sum, void* stream) {
+  if (!pred || !target || !dpred || !loss_dev || mask_sum <= 0) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  cudaMemsetAsync(loss_dev, 0, sizeof(double), st);
+  mse_kernel<<<blocks_for((size_t)plane * batch), 256, 0, st>>>(pred, target, mask, 0, (size_t)plane, batch, dpred,
+                                                                 loss_dev, mask_sum);
+  return fvx_cuda_status();
+}
+
+extern "C" int fvx_nn_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, double lr,
+                           double beta1, double beta2, double eps, int step, void* stream) {
+  if (!w || !grad || !m || !v || n < 0 || step < 1) return FVX_ERR_ARG;
+  const float c1 = (float)(1.0 - pow(beta1, step)), c2 = (float)(1.0 - pow(beta2, step));
+  adam_kernel<<<blocks_for((size_t)n), 256, 0, fvx_stream(stream)>>>(w, (__nv_bfloat16*)w_bf16, grad, m, v, n,
+                                                                      (float)lr, (float)beta1, (float)beta2,
+                                                                      (float)eps, c1, c2);
+  return fvx_cuda_status();
+}
+
+extern "C" int fvx_nn_to_bf16(const float* src, void* dst, int n, void* stream) {
+  if (!src || !dst || n < 0) return FVX_ERR_ARG;
+  to_bf16_kernel<<<blocks_for((size_t)n), 256, 0, fvx_stream(stream)>>>(src, (__nv_bfloat16*)dst, n);
+  return fvx_cuda_status();
+}
+
+// ===========================================================================
+// The network object: parameters, Adam state, activations and scratch for up
+// to batch_max samples on an h x w grid (h, w multiples of 8).
+//
+//   x  [B, 3, h, w]      input: f / s, level mask, log coefficient
+//   E0 conv 3->16, ReLU                       a0 [16, h]
+//   E1 pool, conv 16->16, ReLU                a1 [16, h/2]
+//   E2 pool, conv 16->32, ReLU                a2 [32, h/4]
+//   E3 pool, conv 32->32, ReLU                a3 [32, h/8]
+//   D2 upsample a3, conv 32->32, + a2, ReLU   a4 [32, h/4]
+//   D1 upsample a4, conv 32->16, + a1, ReLU   a5 [16, h/2]
+//   D0 upsample a5, conv 16->16, + a0, ReLU   a6 [16, h]
+//   OUT conv 16->1, linear                    y  [1, h]
+//
+// Parameters are one flat FP32 vector (layer by layer: W[Cout][Cin][3][3]
+// then b[Cout]); the forward pass uses its BF16 copy.
+// ===========================================================================
+namespace fvx {
+namespace nn {
+
+struct LayerDef {
+  int cin, cout, mode, in, skip, out, div, relu;
+};
+// activation slots: 0 x, 1 a0, 2 a1, 3 a2, 4 a3, 5 a4, 6 a5, 7 a6, 8 y
+constexpr int kSlots = 9;
+constexpr int kSlotC[kSlots] = {3, 16, 16, 32, 32, 32, 16, 16, 1};
+constexpr int kSlotDiv[kSlots] = {0, 0, 1, 2, 3, 2, 1, 0, 0};
+constexpr int kLayers = 8;
+constexpr LayerDef kNet[kLayers] = {
+    {3, 16, IN_DIRECT, 0, -1, 1, 0, 1},  {16, 16, IN_POOL, 1, -1, 2, 1, 1}, {16, 32, IN_POOL, 2, -1, 3, 2, 1},
+    {32, 32, IN_POOL, 3, -1, 4, 3, 1},   {32, 32, IN_UP, 4, 3, 5, 2, 1},    {32, 16, IN_UP, 5, 2, 6, 1, 1},
+    {16, 16, IN_UP, 6, 1, 7, 0, 1},      {16, 1, IN_DIRECT, 7, -1, 8, 0, 0},
+};
+
+static size_t layer_params(const LayerDef& L) { return (size_t)L.cout * L.cin * 9 + L.cout; }
+static size_t total_params() {
+  size_t n = 0;
+  for (const LayerDef& L : kNet) n += layer_params(L);
+  return n;
+}
+
+// s = sqrt(sum(f^2 m) / max(sum m, 1)), stored as [s, 1/s] (1/s = 0 when s = 0)
+__global__ void rms_kernel(const float* f, const float* mask, size_t n, float* scale) {
+  __shared__ double sh[2][32];
+  double a = 0.0, c = 0.0;
+  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+    const double m = mask[k];
+    a += (double)f[k] * f[k] * m;
+    c += m;
+  }
+  for (int o = 16; o; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = a; sh[1][threadIdx.x >> 5] = c; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double A = 0.0, C = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { A += sh[0][k]; C += sh[1][k]; }
+    const double s = sqrt(A / (C > 1.0 ? C : 1.0));
+    scale[0] = (float)s;
+    scale[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
+  }
+}
+
+// x channel 0 = f / s (channels 1, 2 were set once)
+__global__ void prep_kernel(const float* f, const float* scale, float* x0, size_t n) {
+  const float inv = scale[1];
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    x0[k] = f[k] * inv;
+}
+
+// u = y * s * sigma * mask
+__global__ void finish_kernel(const float* y, const float* scale, const float* mask, float sigma, float* u,
+                              size_t n) {
+  const float s = scale[0] * sigma;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    u[k] = y[k] * s * mask[k];
+}
+
+}  // namespace nn
+}  // namespace fvx
+
+struct fvx_unet {
+  int h = 0, w = 0, batch_max = 0;
+  size_t n_params = 0;
+  float *wf = nullptr, *grad = nullptr, *m = nullptr, *v = nullptr;
+  __nv_bfloat16* wb = nullptr;
+  float* act[kSlots] = {};   // activations, batch_max samples
+  float* dact[kSlots] = {};  // their gradients (slots 1..8)
+  float *g = nullptr, *dxin = nullptr, *part = nullptr;
+  double* loss = nullptr;
+  // inference on one field: level mask, scale [s, 1/s], output scale sigma
+  float* mask = nullptr;
+  float* scale = nullptr;
+  float sigma = 1.f;
+  std::vector<void*> allocs;
+};
+
+static size_t slot_elems(const fvx_unet* n, int s, int batch) {
+  const int d = kSlotDiv[s];
+  return (size_t)batch * kSlotC[s] * (size_t)(n->h >> d) * (size_t)(n->w >> d);
+}
+
+static void unet_free(fvx_unet* n) {
+  for (void* p : n->allocs) cudaFree(p);
+  n->allocs.clear();
+}
+
+extern "C" long long fvx_unet_num_params(void) { return (long long)total_params(); }
+
+extern "C" int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out) {
+  if (!out) return FVX_ERR_ARG;
+  *out = nullptr;
+  if (h < 8 || w < 8 || (h % 8) || (w % 8) || batch_max < 1) return FVX_ERR_SHAPE;
+  fvx_unet* n = new fvx_unet();
+  n->h = h; n->w = w; n->batch_max = batch_max;
+  n->n_params = total_params();
+  bool ok = true;
+  auto alloc = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (cudaMalloc(&p, bytes < 16 ? 16 : bytes) != cudaSuccess) { ok = false; return nullptr; }
+    n->allocs.push_back(p);
+    cudaMemset(p, 0, bytes < 16 ? 16 : bytes);
+    return p;
+  };
+  const size_t P = n->n_params;
+  n->wf = (float*)alloc(P * 4);
+  n->grad = (float*)alloc(P * 4);
+  n->m = (float*)alloc(P * 4);
+  n->v = (float*)alloc(P * 4);
+  n->wb = (__nv_bfloat16*)alloc(P * 2);
+  for (int s = 0; s < kSlots; ++s) {
+    n->act[s] = (float*)alloc(slot_elems(n, s, batch_max) * 4);
+    if (s > 0) n->dact[s] = (float*)alloc(slot_elems(n, s, batch_max) * 4);
+  }
+  // scratch: G [B, Cout, conv grid], dXin [B, Cin, conv grid], weight partials
+  size_t gmax = 0, xmax = 0, pmax = 0;
+  for (const LayerDef& L : kNet) {
+    const int hh = h >> L.div, ww = w >> L.div;
+    gmax = std::max(gmax, (size_t)batch_max * L.cout * hh * ww);
+    xmax = std::max(xmax, (size_t)batch_max * L.cin * hh * ww);
+    const size_t nblk = (size_t)fvx_nn_conv_bwd_blocks(batch_max, hh, ww);
+    pmax = std::max(pmax, nblk * L.cout * ((size_t)L.cin * 9 + 1));
+  }
+  n->g = (float*)alloc(gmax * 4);
+  n->dxin = (float*)alloc(xmax * 4);
+  n->part = (float*)alloc(pmax * 4);
+  n->loss = (double*)alloc(8);
+  n->mask = (float*)alloc((size_t)h * w * 4);
+  n->scale = (float*)alloc(16);
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
+    unet_free(n);
+    delete n;
+    return FVX_ERR_CUDA;
+  }
+  *out = n;
+  return FVX_OK;
+}
+
+extern "C" int fvx_unet_destroy(fvx_unet* n) {
+  if (!n) return FVX_OK;
+  cudaDeviceSynchronize();
+  unet_free(n);
+  delete n;
+  return fvx_cuda_status();
+}
+
+// Copy ``count`` floats at ``offset`` of one of the network's buffers
+// (0 FP32 master parameters, 1 their gradient, 2 input x [batch_max, 3, h,
+// w], 3 output y [batch_max, 1, h, w]) from ``src`` and/or to ``dst`` (host
+// or device pointers; NULL skips that direction).
+extern "C" int fvx_unet_io(fvx_unet* n, int which, long long offset, long long count, const void* src, void* dst,
+                           void* stream) {
+  if (!n || which < 0 || which > 3 || offset < 0 || count < 0) return FVX_ERR_ARG;
+  float* buf = which == 0 ? n->wf : which == 1 ? n->grad : which == 2 ? n->act[0] : n->act[8];
+  const size_t len = which < 2 ? n->n_params : slot_elems(n, which == 2 ? 0 : 8, n->batch_max);
+  if ((size_t)(offset + count) > len) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  if (src) cudaMemcpyAsync(buf + offset, src, (size_t)count * 4, cudaMemcpyDefault, st);
+  if (dst) cudaMemcpyAsync(dst, buf + offset, (size_t)count * 4, cudaMemcpyDefault, st);
+  return fvx_cuda_status();
+}
+
+// Refresh the BF16 copy after the master parameters were written.
+extern "C" int fvx_unet_sync_params(fvx_unet* n, void* stream) {
+  if (!n) return FVX_ERR_ARG;
+  return fvx_nn_to_bf16(n->wf, n->wb, (int)n->n_params, stream);
+}
+
+static int unet_forward(fvx_unet* n, int batch, cudaStream_t st) {
+  size_t off = 0;
+  for (const LayerDef& L : kNet) {
+    const int hh = n->h >> L.div, ww = n->w >> L.div;
+    const __nv_bfloat16* W = n->wb + off;
+    const float* wf_b = n->wf + off + (size_t)L.cout * L.cin * 9;  // biases stay FP32
+    int rc = fvx_nn_conv_fwd(n->act[L.in], L.mode, batch, L.cin, W, wf_b, L.skip >= 0 ? n->act[L.skip] : nullptr,
+                             n->act[L.out], L.cout, hh, ww, L.relu, st);
+    if (rc) return rc;
+    off += layer_params(L);
+  }
+  return FVX_OK;
+}
+
+// y = net(x) on the first ``batch`` samples of the x buffer.
+extern "C" int fvx_unet_forward(fvx_unet* n, int batch, void* stream) {
+  if (!n) return FVX_ERR_ARG;
+  if (batch < 1 || batch > n->batch_max) return FVX_ERR_SHAPE;
+  return unet_forward(n, batch, fvx_stream(stream));
+}
+
+// grad = dL/dparams given dL/dy (in the y-gradient buffer, or copied from
+// ``dy`` when non-null), after a forward pass on the same batch.
+static int unet_backward(fvx_unet* n, int batch, cudaStream_t st) {
+  for (int s = 1; s < 8; ++s) cudaMemsetAsync(n->dact[s], 0, slot_elems(n, s, batch) * 4, st);
+  size_t offs[kLayers];
+  size_t off = 0;
+  for (int l = 0; l < kLayers; ++l) { offs[l] = off; off += layer_params(kNet[l]); }
+  for (int l = kLayers - 1; l >= 0; --l) {
+    const LayerDef& L = kNet[l];
+    const int hh = n->h >> L.div, ww = n->w >> L.div;
+    float* dw = n->grad + offs[l];
+    float* db = dw + (size_t)L.cout * L.cin * 9;
+    int rc = fvx_nn_conv_bwd(n->act[L.in], L.mode, batch, L.cin, n->wb + offs[l], n->dact[L.out], n->act[L.out],
+                             L.cout, hh, ww, L.relu, n->g, L.skip >= 0 ? n->dact[L.skip] : nullptr, n->dxin,
+                             L.in > 0 ? n->dact[L.in] : nullptr, dw, db, n->part, st);
+    if (rc) return rc;
+  }
+  return fvx_cuda_status();
+}
+
+extern "C" int fvx_unet_backward(fvx_unet* n, int batch, const float* dy, void* stream) {
+  if (!n) return FVX_ERR_ARG;
+  if (batch < 1 || batch > n->batch_max) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  if (dy) cudaMemcpyAsync(n->dact[8], dy, slot_elems(n, 8, batch) * 4, cudaMemcpyDeviceToDevice, st);
+  return unet_backward(n, batch, st);
+}
+
+// One Adam step on a batch already in the x buffer:
+//   L = sum_b sum_p m_b(p) (y_b(p) - target_b(p))^2 / (batch h w),
+// m_b = channel 1 of x (the level mask).  loss_out (device double, may be
+// NULL) receives L.
+extern "C" int fvx_unet_train_step(fvx_unet* n, int batch, const float* target, double lr, double beta1,
+                                   double beta2, double eps, int step, double* loss_out, void* stream) {
+  if (!n || !target || step < 1) return FVX_ERR_ARG;
+  if (batch < 1 || batch > n->batch_max) return FVX_ERR_SHAPE;
+  cudaStream_t st = fvx_stream(stream);
+  int rc = unet_forward(n, batch, st);
+  if (rc) return rc;
+  const size_t plane = (size_t)n->h * n->w;
+  cudaMemsetAsync(n->loss, 0, sizeof(double), st);
+  mse_kernel<<<blocks_for(plane * batch), 256, 0, st>>>(n->act[8], target, n->act[0] + plane, 3 * plane, plane, batch,
+                                                        n->dact[8], n->loss, (double)plane * batch);
+  if ((rc = unet_backward(n, batch, st))) return rc;
+  if ((rc = fvx_nn_adam(n->wf, n->wb, n->grad, n->m, n->v, (int)n->n_params, lr, beta1, beta2, eps, step, st)))
+    return rc;
+  if (loss_out) cudaMemcpyAsync(loss_out, n->loss, sizeof(double), cudaMemcpyDeviceToDevice, st);
+  return fvx_cuda_status();
+}
+
+// Inference set-up for one field: the mask and coefficient channels of x
+// (sample 0), the mask applied to the output, and the output scale sigma.
+extern "C" int fvx_unet_set_level(fvx_unet* n, const float* mask, const float* logc, double sigma, void* stream) {
+  if (!n || !mask || !logc) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  const size_t plane = (size_t)n->h * n->w;
+  cudaMemcpyAsync(n->mask, mask, plane * 4, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(n->act[0] + plane, mask, plane * 4, cudaMemcpyDeviceToDevice, st);
+  cudaMemcpyAsync(n->act[0] + 2 * plane, logc, plane * 4, cudaMemcpyDeviceToDevice, st);
+  n->sigma = (float)sigma;
+  return fvx_cuda_status();
+}
+
+// Coarse solver callback (fvx_precond_fn, ctx = the network): u = s sigma
+// m net([f / s, m, log c]) with s the RMS of f over wet cells.  Launches
+// only; no host synchronisation.
+extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) {
+  fvx_unet* n = (fvx_unet*)ctx;
+  if (!n || !f || !u) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  const size_t plane = (size_t)n->h * n->w;
+  rms_kernel<<<1, 1024, 0, st>>>((const float*)f, n->mask, plane, n->scale);
+  prep_kernel<<<blocks_for(plane), 256, 0, st>>>((const float*)f, n->scale, n->act[0], plane);
+  int rc = unet_forward(n, 1, st);
+  if (rc) return rc;
+  finish_kernel<<<blocks_for(plane), 256, 0, st>>>(n->act[8], n->scale, n->mask, n->sigma, (float*)u, plane);
+  return fvx_cuda_status();
+}

@@ -105,10 +105,17 @@ PRECOND_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ct
 class MaskedHelmholtzPCG:
     """Device-resident PCG on a MultigridSolver's finest operator.
 
-    ``solve(b, rtol, precond="mg"|"none"|callable, flexible=False)`` returns
-    (x FP64, info).  A callable preconditioner gets the residual tensor and
-    returns z = M r (any device computation); ``flexible`` selects the
-    Polak-Ribiere beta for preconditioners that are not a fixed linear map.
+    ``solve(b, rtol, precond=..., flexible=False, graph=False)`` returns
+    (x FP64, info).  ``precond`` is "mg" (one V-cycle, the reference's
+    make_multigrid_preconditioner), "none", a Python callable (gets the
+    residual tensor, returns z = M r), or an object with a ``c_precond()``
+    method returning (C function address, context) of an fvx_precond_fn --
+    e.g. the learned preconditioner in finitevolx_b200.learned.
+    ``flexible`` selects the Polak-Ribiere beta for preconditioners that are
+    not a fixed linear map.  ``graph=True`` captures one PCG iteration
+    (preconditioner included) in a CUDA graph and replays it, reading the
+    device convergence flag every ``chunk`` iterations; it needs a C-level
+    preconditioner ("mg", "none" or ``c_precond``).
     """
 
     def __init__(self, mg):
@@ -118,8 +125,12 @@ class MaskedHelmholtzPCG:
         self.rho = torch.empty(mg.shape, dtype=mg.dtype, device="cuda")
         self.z = torch.empty_like(self.rho)
         check(fn("fvx_pcg_bind_vectors")(self._h, P(self.rho), P(self.z)), "pcg_bind_vectors")
+        self._graphs = {}
+        self._gb = None
+        self._gx = None
 
     def __del__(self):
+        self._graphs = {}
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             try:
@@ -128,31 +139,83 @@ class MaskedHelmholtzPCG:
                 pass
             self._h = None
 
-    def solve(self, b, rtol: float = 1e-8, max_iter: int = 500, precond="mg", flexible: bool = False,
-              replace_every: int = 10, chunk: int = 4, x=None):
-        b = L.as_field(b, dtype=self.mg.dtype)
-        if tuple(b.shape) != self.mg.shape:
-            raise ValueError("rhs shape does not match the multigrid operator")
-        x = torch.empty(b.shape, dtype=torch.float64, device=b.device) if x is None else x
-        info = (ctypes.c_double * 3)()
-        cb = None
+    def _precond_args(self, precond):
+        """(kind, C function pointer, context, keep-alive) for the C entry points."""
         if isinstance(precond, str):
             if precond not in ("none", "mg"):
                 raise ValueError(f"unknown preconditioner {precond!r}")
-            kind = {"none": 0, "mg": 1}[precond]
-        else:
-            kind = 2
-            user = precond
+            return {"none": 0, "mg": 1}[precond], None, None, None
+        if hasattr(precond, "c_precond"):
+            addr, ctx = precond.c_precond()
+            return 2, ctypes.c_void_p(addr), ctypes.c_void_p(ctx), precond
+        user = precond
 
-            def _cb(ctx, rho, z, stream):
-                try:
-                    self.z.copy_(user(self.rho))
-                    return 0
-                except Exception:
-                    return 6
-            cb = PRECOND_FN(_cb)
-        st = fn("fvx_pcg_solve")(self._h, P(b), P(x), I(max_iter), D(rtol), I(kind), cb, None, I(int(flexible)),
+        def _cb(ctx, rho, z, stream):
+            try:
+                self.z.copy_(user(self.rho))
+                return 0
+            except Exception:
+                return 6
+        cb = PRECOND_FN(_cb)
+        return 2, cb, None, cb
+
+    def solve(self, b, rtol: float = 1e-8, max_iter: int = 500, precond="mg", flexible: bool = False,
+              replace_every: int = 10, chunk: int = 4, x=None, graph: bool = False):
+        b = L.as_field(b, dtype=self.mg.dtype)
+        if tuple(b.shape) != self.mg.shape:
+            raise ValueError("rhs shape does not match the multigrid operator")
+        kind, cfn, ctx, keep = self._precond_args(precond)
+        if graph:
+            if kind == 2 and isinstance(cfn, PRECOND_FN):
+                raise ValueError("graph=True needs a C-level preconditioner")
+            return self._solve_graph(b, rtol, max_iter, kind, cfn, ctx, keep, flexible, replace_every, chunk, x)
+        x = torch.empty(b.shape, dtype=torch.float64, device=b.device) if x is None else x
+        info = (ctypes.c_double * 3)()
+        st = fn("fvx_pcg_solve")(self._h, P(b), P(x), I(max_iter), D(rtol), I(kind), cfn, ctx, I(int(flexible)),
                                  I(replace_every), I(chunk), info, stream_ptr())
         if st not in (0, 5):
             check(st, "pcg_solve")
         return x, dict(iterations=int(info[0]), rel_residual=float(info[1]), converged=st == 0)
+
+    def _solve_graph(self, b, rtol, max_iter, kind, cfn, ctx, keep, flexible, replace_every, chunk, x_out):
+        if self._gb is None:
+            self._gb = torch.empty_like(self.rho)
+            self._gx = torch.empty(self.mg.shape, dtype=torch.float64, device=self.rho.device)
+        self._gb.copy_(b)
+        bb = ctypes.c_double()
+        check(fn("fvx_pcg_begin")(self._h, P(self._gb), P(self._gx), D(rtol), I(kind), cfn, ctx, ctypes.byref(bb),
+                                  stream_ptr()), "pcg_begin")
+        key = (kind, getattr(cfn, "value", None), getattr(ctx, "value", None), bool(flexible), replace_every)
+        if key not in self._graphs:
+            # one iteration per replay; the residual-replacement schedule is
+            # kept by capturing replace_every graphs (iteration i mod k)
+            per = max(replace_every, 1)
+            gs = []
+            torch.cuda.synchronize()
+            for k in range(per):
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    check(fn("fvx_pcg_iterate")(self._h, P(self._gb), P(self._gx), I(k), I(1), I(kind), cfn, ctx,
+                                                I(int(flexible)), I(replace_every), stream_ptr()), "pcg_iterate")
+                gs.append(g)
+            self._graphs[key] = (gs, keep)
+            # capture does not run the work: restart from the begin state
+            check(fn("fvx_pcg_begin")(self._h, P(self._gb), P(self._gx), D(rtol), I(kind), cfn, ctx,
+                                      ctypes.byref(bb), stream_ptr()), "pcg_begin")
+        gs = self._graphs[key][0]
+        status = (ctypes.c_double * 3)()
+        it = 0
+        conv = bb.value == 0.0
+        while not conv and it < max_iter:
+            m = min(chunk, max_iter - it)
+            for _ in range(m):
+                gs[it % len(gs)].replay()
+                it += 1
+            check(fn("fvx_pcg_status")(self._h, status, stream_ptr()), "pcg_status")
+            conv = status[0] != 0.0
+        rel = ctypes.c_double()
+        check(fn("fvx_pcg_finish")(self._h, P(self._gb), P(self._gx), D(bb.value), ctypes.byref(rel), stream_ptr()),
+              "pcg_finish")
+        x = self._gx.clone() if x_out is None else x_out.copy_(self._gx)
+        iters = int(status[1]) if bb.value != 0.0 else 0
+        return x, dict(iterations=iters, rel_residual=rel.value, converged=rel.value <= rtol)

@@ -217,6 +217,112 @@ int fvx_qg_stage_f64(const double* q_stage, const double* q_start, const double*
                      double dx, double dy, double beta, double drag, double viscosity, double a, double b,
                      double c, int method, int periodic, int write_ghost, void* stream);
 
+/* ---- masked multigrid, PCG, vertical modes -------------------------------- */
+
+/* Preconditioner / coarse-solver callback: z = M rho on ``stream``. */
+typedef int (*fvx_precond_fn)(void* ctx, const void* rho, void* z, void* stream);
+
+/* build_multigrid_solver (solvers/multigrid.py:905-1062): FP64 host build of
+ * the level hierarchy (masks mean>=0.5, face coefficients, inverse
+ * diagonals), uploaded in ``dtype`` (0 float32, 1 float64).  coeff may be
+ * NULL (c = 1); n_levels 0 = as many as halving allows (>= 8 cells). */
+typedef struct fvx_mg fvx_mg;
+int fvx_mg_create(const double* mask, const double* coeff, int ny, int nx, double dx, double dy, double lambda,
+                  int n_levels, int n_pre, int n_post, int n_coarse, double omega, int dtype, fvx_mg** out);
+int fvx_mg_destroy(fvx_mg* g);
+int fvx_mg_num_levels(fvx_mg* g);
+/* Level metadata and device arrays (mask, cx, cy, inv_diagonal). */
+int fvx_mg_level(fvx_mg* g, int level, int* ny, int* nx, double* dx2, void** mask, void** cx, void** cy,
+                 void** inv);
+/* MultigridSolver.v_cycle (multigrid.py:808-881); u_in NULL = zero guess. */
+int fvx_mg_vcycle(fvx_mg* g, const void* u_in, const void* f, void* u_out, void* stream);
+/* MultigridSolver._run_vcycles (multigrid.py:885-897). */
+int fvx_mg_solve(fvx_mg* g, const void* f, void* u, int n_cycles, void* stream);
+/* _apply_operator (multigrid.py:327-405) at a level. */
+int fvx_mg_apply(fvx_mg* g, int level, const void* u, void* out, void* stream);
+/* masked_laplacian (solvers/iterative.py:144-191). */
+int fvx_masked_laplacian_f32(const float* psi, const float* mask, float* out, int ny, int nx, double dx, double dy,
+                             double lambda, void* stream);
+int fvx_masked_laplacian_f64(const double* psi, const double* mask, double* out, int ny, int nx, double dx,
+                             double dy, double lambda, void* stream);
+
+/* Device-resident PCG on the finest MG operator (solve_cg with
+ * make_multigrid_preconditioner, iterative.py:48-136 and
+ * preconditioners.py:207-244): FP64 iterate and inner products, work vectors
+ * in the MG dtype, 2-norm relative residual checked in FP64.  precond 0 none,
+ * 1 one V-cycle, 2 the callback (fn, ctx); flexible selects Polak-Ribiere
+ * beta.  info = [iterations, relative residual, converged]. */
+typedef struct fvx_pcg fvx_pcg;
+int fvx_pcg_create(fvx_mg* g, fvx_pcg** out);
+int fvx_pcg_destroy(fvx_pcg* P);
+int fvx_pcg_bind_vectors(fvx_pcg* P, void* rho, void* z);
+int fvx_pcg_solve(fvx_pcg* P, const void* b, double* x, int max_iter, double rtol, int precond, fvx_precond_fn fn,
+                  void* ctx, int flexible, int replace_every, int chunk, double* info, void* stream);
+/* The same solve in pieces; fvx_pcg_iterate makes no host synchronisation
+ * and may be captured in a CUDA graph. */
+int fvx_pcg_begin(fvx_pcg* P, const void* b, double* x, double rtol, int precond, fvx_precond_fn fn, void* ctx,
+                  double* bb_out, void* stream);
+int fvx_pcg_iterate(fvx_pcg* P, const void* b, double* x, int it0, int niter, int precond, fvx_precond_fn fn,
+                    void* ctx, int flexible, int replace_every, void* stream);
+int fvx_pcg_status(fvx_pcg* P, double* out3, void* stream);
+int fvx_pcg_finish(fvx_pcg* P, const void* b, double* x, double bb, double* rel_out, void* stream);
+/* FP64-accumulated inner product (one device scalar). */
+int fvx_dot_f32(const float* a, const float* b, long long n, double* part, double* out_dev, void* stream);
+int fvx_dot_f64(const double* a, const double* b, long long n, double* part, double* out_dev, void* stream);
+/* layer_to_mode / mode_to_layer (vertical/vertical_modes.py:204-263). */
+int fvx_layer_mix_f32(const double* C, int nl, const float* in, float* out, long long plane, int batch,
+                      void* stream);
+int fvx_layer_mix_f64(const double* C, int nl, const double* in, double* out, long long plane, int batch,
+                      void* stream);
+
+/* ---- learned coarse-grid preconditioner (no counterpart in finitevolX) ---- */
+
+/* Hybrid cycle: the V-cycle's legs on levels 0..lvl-1 with the level-lvl
+ * correction from ``coarse`` (NULL = zero). */
+int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
+                         fvx_precond_fn coarse, void* ctx, void* stream);
+/* Downward leg only: f's restricted residual at level lvl into f_lvl. */
+int fvx_mg_restrict_residual(fvx_mg* g, const void* f, int lvl, int n_pre, void* f_lvl, void* stream);
+/* Batched MG solves at level lvl, one CTA per right-hand side. */
+long long fvx_mg_level_work(fvx_mg* g, int lvl);
+int fvx_mg_solve_level_batched(fvx_mg* g, int lvl, int batch, const void* f, void* u, int n_cycles, void* work,
+                               void* stream);
+/* The hybrid cycle as an fvx_precond_fn (ctx = the fvx_hybrid object). */
+typedef struct fvx_hybrid fvx_hybrid;
+int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, fvx_precond_fn coarse, void* ctx,
+                      fvx_hybrid** out);
+int fvx_hybrid_destroy(fvx_hybrid* h);
+int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* stream);
+
+/* 4-level U-Net (16/16/32/32 channels), BF16 weights, FP32 accumulation:
+ * create / parameter IO / forward / backward / Adam train step, and the
+ * inference callback fvx_unet_coarse (an fvx_precond_fn, ctx = the net). */
+typedef struct fvx_unet fvx_unet;
+long long fvx_unet_num_params(void);
+int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out);
+int fvx_unet_destroy(fvx_unet* n);
+int fvx_unet_io(fvx_unet* n, int which, long long offset, long long count, const void* src, void* dst,
+                void* stream);
+int fvx_unet_sync_params(fvx_unet* n, void* stream);
+int fvx_unet_forward(fvx_unet* n, int batch, void* stream);
+int fvx_unet_backward(fvx_unet* n, int batch, const float* dy, void* stream);
+int fvx_unet_train_step(fvx_unet* n, int batch, const float* target, double lr, double beta1, double beta2,
+                        double eps, int step, double* loss_out, void* stream);
+int fvx_unet_set_level(fvx_unet* n, const float* mask, const float* logc, double sigma, void* stream);
+int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream);
+/* Layer-level kernels (conv3x3 with pool/upsample input, backward, MSE, Adam). */
+int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
+                    const float* skip, float* out, int cout, int h, int w, int relu, void* stream);
+int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* dy,
+                    const float* y, int cout, int h, int w, int relu, float* g, float* dskip, float* dxin,
+                    float* dsrc, float* dw, float* db, float* part, void* stream);
+int fvx_nn_conv_bwd_blocks(int batch, int h, int w);
+int fvx_nn_mse(const float* pred, const float* target, const float* mask, long long plane, int batch, float* dpred,
+               double* loss_dev, double mask_sum, void* stream);
+int fvx_nn_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, int n, double lr, double beta1,
+                double beta2, double eps, int step, void* stream);
+int fvx_nn_to_bf16(const float* src, void* dst, int n, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

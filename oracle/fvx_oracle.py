@@ -1093,6 +1093,44 @@ def mg_solve(mg, f):
     return u
 
 
+def mg_restrict_residual(mg, f, lvl, n_pre):
+    """Downward leg of the learned preconditioner's hybrid cycle (no reference
+    counterpart; built from mg_vcycle's pieces): per level, n_pre sweeps from
+    zero, then restrict the residual.  Returns (per-level u, f) and f_lvl."""
+    us, fs = [], [f]
+    for lev in range(lvl):
+        L = mg["levels"][lev]
+        u = mg_jacobi(np.zeros_like(fs[-1]), fs[-1], L, mg["omega"], n_pre)
+        r = (fs[-1] - mg_apply(u, L)) * L["mask"]
+        C = mg["levels"][lev + 1]
+        us.append(u)
+        fs.append(mg_restrict(r, L["mask"], C["mask"]))
+    return us, fs
+
+
+def mg_hybrid(mg, f, lvl, n_pre, n_post, coarse=None):
+    """Hybrid cycle: mg_vcycle's legs on levels 0..lvl-1 with the level-lvl
+    correction e = coarse(f_lvl) (zero when coarse is None)."""
+    us, fs = mg_restrict_residual(mg, f, lvl, n_pre)
+    e = np.zeros_like(fs[lvl]) if coarse is None else coarse(fs[lvl])
+    for lev in range(lvl - 1, -1, -1):
+        L = mg["levels"][lev]
+        C = mg["levels"][lev + 1]
+        u = (us[lev] + mg_prolong(e, C["mask"], L["mask"])) * L["mask"]
+        e = mg_jacobi(u, fs[lev], L, mg["omega"], n_post)
+    return e
+
+
+def mg_level_solve(mg, lvl, f, n_cycles):
+    """u += V_lvl(f - A_lvl u) from u = 0, n_cycles times (the training targets)."""
+    L = mg["levels"][lvl]
+    u = np.zeros_like(f)
+    for _ in range(n_cycles):
+        r = (f - mg_apply(u, L)) * L["mask"]
+        u = u + mg_vcycle(mg, np.zeros_like(r), r, lvl)
+    return u
+
+
 # ---------------------------------------------------------------------------
 # Vertical modes  (vertical/vertical_modes.py:50-263)
 # ---------------------------------------------------------------------------

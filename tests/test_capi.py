@@ -15,7 +15,7 @@ LIB = ROOT / "finitevolx_b200" / "libfvx.so"
 def declared_symbols():
     text = HEADER.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\bint\s+(fvx_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(?:int|long long)\s+(fvx_\w+)\s*\(", text)))
 
 
 @pytest.fixture(scope="module")

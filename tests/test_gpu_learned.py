@@ -1,0 +1,138 @@
+"""GPU checks of the learned preconditioner.
+
+* U-Net forward, gradients (backward) and one Adam step against the FP64
+  NumPy oracle with the same BF16-rounded weights.  Tolerances: forward 2e-5
+  normwise relative (FP32 accumulation over <= 288-term sums), gradients 1e-4
+  normwise per layer, Adam 1e-6 absolute on lr = 1e-3 steps.
+* The hybrid cycle's pieces (downward leg, batched level solves, zero-
+  correction cycle) against the oracle in FP32: 1e-5 normwise.
+* Training lowers the loss; flexible PCG with the trained network reaches the
+  FP64-checked 1e-8 relative residual and needs fewer iterations than the same
+  cycle without the network.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+import finitevolx_b200 as fvx
+import oracle.fvx_oracle as O
+import oracle.unet_oracle as U
+from finitevolx_b200.learned import LearnedPreconditioner, UNet, generate_pairs
+
+from test_gpu_solvers import basin, coeff
+
+pytestmark = pytest.mark.gpu
+
+
+def nrel(a, b):
+    a = np.asarray(a, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+
+
+def _net_case(seed=0, B=2, h=32, w=32):
+    rng = np.random.default_rng(seed)
+    theta = U.init_params(seed)
+    # non-zero biases so every bias gradient path is exercised
+    off = 0
+    for ci, co, *_ in U.LAYERS:
+        off += co * ci * 9
+        theta[off:off + co] = rng.uniform(-0.1, 0.1, co)
+        off += co
+    x = rng.standard_normal((B, 3, h, w)).astype(np.float32)
+    x[:, 1] = (rng.random((B, h, w)) > 0.25).astype(np.float32)
+    t = rng.standard_normal((B, 1, h, w)).astype(np.float32)
+    return theta, x, t
+
+
+def test_unet_forward_matches_oracle(cuda_ok):
+    theta, x, _ = _net_case()
+    net = UNet(32, 32, batch_max=4)
+    net.set_params(theta)
+    y = net.forward(torch.from_numpy(x).cuda()).cpu().numpy()
+    ref = U.forward(theta.astype(np.float64), x)[8]
+    assert nrel(y, ref) < 2e-5
+
+
+def test_unet_gradients_match_oracle(cuda_ok):
+    theta, x, t = _net_case(1, B=3, h=32, w=48)
+    Lr, gref, acts = U.loss_and_grad(theta.astype(np.float64), x, t)
+    m = x[:, 1:2].astype(np.float64)
+    N = t.shape[0] * t.shape[2] * t.shape[3]
+    dy = (2.0 * (acts[8] - t) * m * m / N).astype(np.float32)
+    net = UNet(32, 48, batch_max=3)
+    net.set_params(theta)
+    g = net.backward(torch.from_numpy(x).cuda(), torch.from_numpy(dy).cuda()).cpu().numpy()
+    off = 0
+    for k, (ci, co, *_r) in enumerate(U.LAYERS):
+        n = co * ci * 9 + co
+        assert nrel(g[off:off + n], gref[off:off + n]) < 1e-4, f"layer {k}"
+        off += n
+
+
+def test_unet_train_step_loss_and_adam(cuda_ok):
+    theta, x, t = _net_case(2, B=2, h=16, w=16)
+    net = UNet(16, 16, batch_max=2)
+    net.set_params(theta)
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    net.train_step(torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda(), lr=1e-3, loss_out=loss)
+    Lr, gref, _ = U.loss_and_grad(theta.astype(np.float64), x, t)
+    assert abs(loss.item() - Lr) <= 1e-5 * Lr
+    g = net.grad().cpu().numpy().astype(np.float64)
+    th1, _, _ = U.adam(theta.astype(np.float64), g, 0.0, 0.0, 1, lr=1e-3)
+    np.testing.assert_allclose(net.params().cpu().numpy(), th1, atol=1e-6, rtol=0)
+
+
+@pytest.fixture(scope="module")
+def problem128(cuda_ok):
+    n = 128
+    m = basin(n, 21)
+    c = coeff(n, 22)
+    lam = 0.0156 * n * n  # lambda dx^2 = 0.0156 (deformation radius 8 cells)
+    mg = fvx.build_multigrid_solver(m, 1.0 / n, 1.0 / n, lambda_=lam, coeff=c, dtype=torch.float32)
+    ref = O.mg_build(m, 1.0 / n, 1.0 / n, lambda_=lam, coeff=c)
+    return n, m, c, lam, mg, ref
+
+
+def test_hybrid_pieces_match_oracle(problem128):
+    n, m, c, lam, mg, ref = problem128
+    rng = np.random.default_rng(23)
+    f = (rng.standard_normal((n, n)) * m).astype(np.float32)
+    lvl = 2
+    from finitevolx_b200._lib import I, P, check, fn, stream_ptr
+    h = n >> lvl
+    fl = torch.empty((h, h), dtype=torch.float32, device="cuda")
+    check(fn("fvx_mg_restrict_residual")(mg.handle, P(torch.from_numpy(f).cuda()), I(lvl), I(2), P(fl),
+                                         stream_ptr()), "restrict")
+    _, fs = O.mg_restrict_residual(ref, f.astype(np.float64), lvl, 2)
+    assert nrel(fl.cpu().numpy(), fs[lvl]) < 1e-5
+    F, E = generate_pairs(mg, lvl, 4, n_pre=2, seed=3, n_cycles=6)
+    for k in range(4):
+        e_ref = O.mg_level_solve(ref, lvl, F[k].double().cpu().numpy(), 6)
+        assert nrel(E[k].cpu().numpy(), e_ref) < 1e-5
+    pc0 = LearnedPreconditioner(mg, lvl=lvl, coarse=False)
+    z = pc0(torch.from_numpy(f).cuda()).cpu().numpy()
+    assert nrel(z, O.mg_hybrid(ref, f.astype(np.float64), lvl, 2, 2)) < 1e-5
+
+
+def test_learned_pcg_gain(problem128):
+    n, m, c, lam, mg, ref = problem128
+    pc = LearnedPreconditioner(mg, lvl=2, n_pre=2, n_post=2, batch_max=32, seed=0)
+    hist = pc.fit(n_pairs=1024, epochs=12, batch=32, lr=2e-3, seed=1)
+    assert hist[-1] < 0.5 * hist[0], hist
+    pcg = fvx.MaskedHelmholtzPCG(mg)
+    f = O.kminus3_field(n, n, 24) * m
+    b = torch.from_numpy(f).float().cuda()
+    x, info = pcg.solve(b, rtol=1e-8, precond=pc, flexible=True, max_iter=300)
+    assert info["converged"] and info["rel_residual"] <= 1e-8, info
+    # FP64 check of the returned iterate against the oracle operator
+    fb = b.double().cpu().numpy()
+    r = fb - O.mg_apply(x.cpu().numpy(), ref["levels"][0])
+    assert np.linalg.norm(r) <= 1.01e-8 * np.linalg.norm(fb)
+    pc0 = LearnedPreconditioner(mg, lvl=2, n_pre=2, n_post=2, coarse=False)
+    x0, info0 = pcg.solve(b, rtol=1e-8, precond=pc0, flexible=True, max_iter=300)
+    assert info0["converged"], info0
+    assert info["iterations"] < info0["iterations"], (info, info0)
+    # graph replay gives the same iterations and tolerance
+    xg, infog = pcg.solve(b, rtol=1e-8, precond=pc, flexible=True, max_iter=300, graph=True)
+    assert infog["converged"] and abs(infog["iterations"] - info["iterations"]) <= 1, (infog, info)
