@@ -238,6 +238,204 @@ coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused V-cycle legs for the host-driven (fine) levels, one launch per leg:
+//   down: u = k Jacobi sweeps from u_init (NULL = 0) on f, then the
+//         restricted residual R (f - A u) into the next level's f;
+//   up:   u = u_pre + P e_coarse, then k Jacobi sweeps, into ``out``.
+// Each CTA loads its output tile plus a halo of k (+1 for the residual) of
+// f, mask, cx, cy and inv_diag into shared memory once and runs all sweeps
+// there (the valid region shrinks by one cell per sweep); the arithmetic of
+// every cell is jacobi_at / restrict_at / prolong_at's, in the same order.
+// ---------------------------------------------------------------------------
+constexpr int kLegMaxSweeps = 16;
+
+template <typename T> struct LegTile;
+template <> struct LegTile<float> { static constexpr int TX = 64, TY = 32; };
+template <> struct LegTile<double> { static constexpr int TX = 32, TY = 16; };
+
+template <typename T>
+DEV T jac_s(const T* u, const T* f, const T* m, const T* cx, const T* cy, const T* inv, int k, int RW, T dx2,
+            T rdx2, T dy2, T rdy2, T lam, T omega) {
+  const T mc = m[k];
+  const T um = u[k] * mc;
+  const T ue = u[k + 1] * m[k + 1];
+  const T uw = u[k - 1] * m[k - 1];
+  const T un = u[k + RW] * m[k + RW];
+  const T us = u[k - RW] * m[k - RW];
+  const T lap = divd(cx[k] * (ue - um) - cx[k - 1] * (um - uw), dx2, rdx2) +
+                divd(cy[k] * (un - um) - cy[k - RW] * (um - us), dy2, rdy2);
+  const T r = f[k] - (lap - lam * um) * mc;
+  return (u[k] + omega * inv[k] * r) * mc;
+}
+
+template <typename T>
+DEV T res_s(const T* u, const T* f, const T* m, const T* cx, const T* cy, int k, int RW, T dx2, T rdx2, T dy2,
+            T rdy2, T lam) {
+  const T mc = m[k];
+  const T um = u[k] * mc;
+  const T ue = u[k + 1] * m[k + 1];
+  const T uw = u[k - 1] * m[k - 1];
+  const T un = u[k + RW] * m[k + RW];
+  const T us = u[k - RW] * m[k - RW];
+  const T lap = divd(cx[k] * (ue - um) - cx[k - 1] * (um - uw), dx2, rdx2) +
+                divd(cy[k] * (un - um) - cy[k - RW] * (um - us), dy2, rdy2);
+  return (f[k] - (lap - lam * um) * mc) * mc;
+}
+
+template <typename T>
+static size_t leg_smem(int k) {
+  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
+  const int H = k + 1;
+  const size_t RN = (size_t)(TX + 2 * H) * (TY + 2 * H);
+  const size_t CN = (size_t)((TX + 2 * H) / 2 + 3) * ((TY + 2 * H) / 2 + 3);
+  return (7 * RN + 2 * CN) * sizeof(T);
+}
+
+// L.u (tile) <- k sweeps; C.f <- restricted residual.  Halo k + 1.
+template <typename T>
+__global__ void __launch_bounds__(256)
+down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init, int k, T omega, Lev<T> C) {
+  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
+  const int H = k + 1;
+  const int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
+  extern __shared__ __align__(16) unsigned char leg_raw[];
+  T* sf = (T*)leg_raw;
+  T* sm = sf + RN;
+  T* scx = sm + RN;
+  T* scy = scx + RN;
+  T* sinv = scy + RN;
+  T* sa = sinv + RN;
+  T* sb = sa + RN;
+  const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
+  for (int q = threadIdx.x; q < RN; q += blockDim.x) {
+    const int ly = q / RW, lx = q - ly * RW;
+    const int gy = y0 + ly, gx = x0 + lx;
+    const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+    const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+    sf[q] = in ? f[c] : T(0);
+    sm[q] = in ? L.mask[c] : T(0);
+    scx[q] = in ? L.cx[c] : T(0);
+    scy[q] = in ? L.cy[c] : T(0);
+    sinv[q] = in ? L.inv[c] : T(0);
+    sa[q] = (in && u_init) ? u_init[c] : T(0);
+  }
+  __syncthreads();
+  T* a = sa;
+  T* b = sb;
+  for (int s = 1; s <= k; ++s) {
+    const int w = RW - 2 * s, h = RH - 2 * s;
+    for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+      const int ly = s + q / w, lx = s + q % w;
+      const int kk = ly * RW + lx;
+      b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
+    }
+    __syncthreads();
+    T* t = a; a = b; b = t;
+  }
+  // a is valid on the tile and one ring around it
+  for (int q = threadIdx.x; q < TX * TY; q += blockDim.x) {
+    const int ly = H + q / TX, lx = H + q % TX;
+    const int gy = y0 + ly, gx = x0 + lx;
+    if (gy < L.ny && gx < L.nx) L.u[(size_t)gy * L.nx + gx] = a[ly * RW + lx];
+  }
+  constexpr int CX = TX / 2, CY = TY / 2;
+  for (int q = threadIdx.x; q < CX * CY; q += blockDim.x) {
+    const int Jl = q / CX, Il = q % CX;
+    const int J = blockIdx.y * CY + Jl, I = blockIdx.x * CX + Il;
+    if (J >= C.ny || I >= C.nx) continue;
+    T sv[4], mv[4];
+    const int dj[4] = {0, 1, 0, 1}, di[4] = {0, 0, 1, 1};
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int kk = (H + 2 * Jl + dj[t]) * RW + (H + 2 * Il + di[t]);
+      const T mf = sm[kk];
+      const T r = res_s(a, sf, sm, scx, scy, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
+      sv[t] = r * mf;
+      mv[t] = mf;
+    }
+    const T sum4 = ((sv[0] + sv[1]) + sv[2]) + sv[3];
+    const T cnt = ((mv[0] + mv[1]) + mv[2]) + mv[3];
+    const size_t cc = (size_t)J * C.nx + I;
+    C.f[cc] = (sum4 / (cnt > T(1) ? cnt : T(1))) * C.mask[cc];
+  }
+}
+
+// out (tile) <- k sweeps from u_pre + P ec.  Halo k.
+template <typename T>
+__global__ void __launch_bounds__(256)
+up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Lev<T> C, const T* __restrict__ ec,
+              int k, T omega, T* __restrict__ out) {
+  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
+  const int H = k;
+  const int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
+  // the buffer layout of leg_smem(k) (sized for halo k + 1)
+  const int RNmax = (TX + 2 * (k + 1)) * (TY + 2 * (k + 1));
+  extern __shared__ __align__(16) unsigned char leg_raw[];
+  T* sf = (T*)leg_raw;
+  T* sm = sf + RNmax;
+  T* scx = sm + RNmax;
+  T* scy = scx + RNmax;
+  T* sinv = scy + RNmax;
+  T* sa = sinv + RNmax;
+  T* sb = sa + RNmax;
+  T* sv = sb + RNmax;  // coarse e * mask
+  const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
+  const int CX0 = (x0 >> 1) - 1, CY0 = (y0 >> 1) - 1;
+  const int CW = ((x0 + RW - 1) >> 1) + 1 - CX0 + 1, CH = ((y0 + RH - 1) >> 1) + 1 - CY0 + 1;
+  T* scm = sv + CW * CH;  // coarse mask
+  for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
+    const int J = CY0 + q / CW, I = CX0 + q % CW;
+    const bool in = J >= 0 && J < C.ny && I >= 0 && I < C.nx;
+    const size_t c = in ? (size_t)J * C.nx + I : 0;
+    const T cm = in ? C.mask[c] : T(0);
+    sv[q] = in ? ec[c] * cm : T(0);
+    scm[q] = cm;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < RN; q += blockDim.x) {
+    const int ly = q / RW, lx = q - ly * RW;
+    const int gy = y0 + ly, gx = x0 + lx;
+    const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+    const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+    const T mf = in ? L.mask[c] : T(0);
+    sf[q] = in ? f[c] : T(0);
+    sm[q] = mf;
+    scx[q] = in ? L.cx[c] : T(0);
+    scy[q] = in ? L.cy[c] : T(0);
+    sinv[q] = in ? L.inv[c] : T(0);
+    T u = T(0);
+    if (in) {
+      const int J = gy >> 1, I = gx >> 1, sj = 2 * (gy & 1) - 1, si = 2 * (gx & 1) - 1;
+      auto V = [&](int jj, int ii) -> T { return sv[(jj - CY0) * CW + (ii - CX0)]; };
+      auto M = [&](int jj, int ii) -> T { return scm[(jj - CY0) * CW + (ii - CX0)]; };
+      const T ws = ((T(9) * V(J, I) + T(3) * V(J, I + si)) + T(3) * V(J + sj, I)) + T(1) * V(J + sj, I + si);
+      const T ds = ((T(9) * M(J, I) + T(3) * M(J, I + si)) + T(3) * M(J + sj, I)) + T(1) * M(J + sj, I + si);
+      const T e = (ws / (ds > T(1) ? ds : T(1))) * mf;
+      u = (u_pre[c] + e) * mf;
+    }
+    sa[q] = u;
+  }
+  __syncthreads();
+  T* a = sa;
+  T* b = sb;
+  for (int s = 1; s <= k; ++s) {
+    const int w = RW - 2 * s, h = RH - 2 * s;
+    for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
+      const int ly = s + q / w, lx = s + q % w;
+      const int kk = ly * RW + lx;
+      b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
+    }
+    __syncthreads();
+    T* t = a; a = b; b = t;
+  }
+  for (int q = threadIdx.x; q < TX * TY; q += blockDim.x) {
+    const int ly = H + q / TX, lx = H + q % TX;
+    const int gy = y0 + ly, gx = x0 + lx;
+    if (gy < L.ny && gx < L.nx) out[(size_t)gy * L.nx + gx] = a[ly * RW + lx];
+  }
+}
+
 // masked_laplacian (iterative.py:144-191): periodic roll, (lap - lam psi_m) * m
 template <typename T>
 __global__ void masked_laplacian_kernel(const T* psi, const T* m, T* out, int ny, int nx, T dx, T dy, T lam) {
@@ -349,6 +547,7 @@ extern "C" int fvx_mg_create(const double* mask, const double* coeff, int ny, in
   if (!mask || !out) return FVX_ERR_ARG;
   *out = nullptr;
   if (ny < 1 || nx < 1 || n_pre < 0 || n_post < 0 || n_coarse < 0) return FVX_ERR_SHAPE;
+  if (n_pre > kLegMaxSweeps || n_post > kLegMaxSweeps) return FVX_ERR_ARG;  // fused legs: <= 16 sweeps
   if (dtype != 0 && dtype != 1) return FVX_ERR_DTYPE;
   if (n_levels <= 0) {  // _compute_n_levels (multigrid.py:50-76)
     int a = ny, b = nx;
@@ -435,32 +634,69 @@ extern "C" int fvx_mg_level(fvx_mg* g, int level, int* ny, int* nx, double* dx2,
 
 extern "C" int fvx_mg_num_levels(fvx_mg* g) { return g ? g->nl : -1; }
 
-// V-cycle below the finest level of a host-driven cycle.
 template <typename T>
-static int vcycle_levels(fvx_mg* g, int l, cudaStream_t st) {
+static int leg_attr() {
+  static bool done = false;
+  if (!done) {
+    const int bytes = (int)leg_smem<T>(kLegMaxSweeps);
+    if (cudaFuncSetAttribute(down_leg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(up_leg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    done = true;
+  }
+  return FVX_OK;
+}
+
+// Downward leg at host-driven level l: L.u <- k sweeps on f from u_init
+// (NULL = 0), level l+1's f <- the restricted residual.
+template <typename T>
+static int leg_down(fvx_mg* g, int l, const T* f, const T* u_init, int k, cudaStream_t st) {
+  if (k > kLegMaxSweeps) return FVX_ERR_ARG;
+  int rc = leg_attr<T>();
+  if (rc) return rc;
+  LevArray<T>& A = levs<T>(g);
+  Lev<T>& L = A.L[l];
+  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
+  dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
+  down_leg_kernel<T><<<gr, 256, leg_smem<T>(k), st>>>(L, f, u_init, k, (T)g->omega, A.L[l + 1]);
+  return fvx_cuda_status();
+}
+
+// Upward leg at host-driven level l: out <- k sweeps on f from L.u + P ec.
+template <typename T>
+static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cudaStream_t st) {
+  if (k > kLegMaxSweeps) return FVX_ERR_ARG;
+  int rc = leg_attr<T>();
+  if (rc) return rc;
+  LevArray<T>& A = levs<T>(g);
+  Lev<T>& L = A.L[l];
+  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
+  dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
+  up_leg_kernel<T><<<gr, 256, leg_smem<T>(k), st>>>(L, f, L.u, A.L[l + 1], ec, k, (T)g->omega, out);
+  return fvx_cuda_status();
+}
+
+// V-cycle below the finest level of a host-driven cycle: entered with
+// L[l].f set, zero initial guess; returns where level l's result lives
+// (L[l].u for the single-CTA coarse levels, L[l].tmp for host-driven ones).
+template <typename T>
+static int vcycle_levels(fvx_mg* g, int l, T** result, cudaStream_t st) {
   LevArray<T>& A = levs<T>(g);
   const T om = (T)g->omega;
   if (l >= g->lc) {
     coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, l, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
+    *result = A.L[l].u;
     return fvx_cuda_status();
   }
   Lev<T>& L = A.L[l];
-  const size_t n = (size_t)L.ny * L.nx;
-  const int gr = grid_for(n);
-  fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
-  T* a = L.u;
-  T* b = L.tmp;
-  for (int s = 0; s < g->n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
-  Lev<T>& C = A.L[l + 1];
-  restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
-  int rc = vcycle_levels<T>(g, l + 1, st);
+  int rc = leg_down<T>(g, l, L.f, nullptr, g->n_pre, st);
   if (rc) return rc;
-  prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
-  a = L.u; b = L.tmp;
-  for (int s = 0; s < g->n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
-  return fvx_cuda_status();
+  T* ec = nullptr;
+  if ((rc = vcycle_levels<T>(g, l + 1, &ec, st))) return rc;
+  if ((rc = leg_up<T>(g, l, L.f, ec, g->n_post, L.tmp, st))) return rc;
+  *result = L.tmp;
+  return FVX_OK;
 }
 
 // One V-cycle at level 0: u_out = V(u_in, f) (u_in NULL = zero initial
@@ -481,31 +717,17 @@ static int vcycle0(fvx_mg* g, const T* u_in, const T* f, T* u_out, cudaStream_t 
     copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
     return fvx_cuda_status();
   }
-  if (g->lc == 0) {  // whole cycle fits the single-CTA kernel
+  if (g->lc == 0 && !u_in) {  // whole cycle fits the single-CTA kernel
     copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
-    if (u_in) {
-      // a non-zero start at level 0 is run with the host-driven path below
-    } else {
-      coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, 0, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
-      copy_kernel<T><<<gr, 256, 0, st>>>(u_out, L.u, n);
-      return fvx_cuda_status();
-    }
+    coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, 0, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
+    copy_kernel<T><<<gr, 256, 0, st>>>(u_out, L.u, n);
+    return fvx_cuda_status();
   }
-  if (u_in) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, u_in, n);
-  else fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
-  copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
-  T* a = L.u; T* b = L.tmp;
-  for (int s = 0; s < g->n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-  if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
-  Lev<T>& C = A.L[1];
-  restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
-  int rc = vcycle_levels<T>(g, 1, st);
+  int rc = leg_down<T>(g, 0, f, u_in, g->n_pre, st);
   if (rc) return rc;
-  prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
-  a = L.u; b = L.tmp;
-  for (int s = 0; s < g->n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-  copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
-  return fvx_cuda_status();
+  T* ec = nullptr;
+  if ((rc = vcycle_levels<T>(g, 1, &ec, st))) return rc;
+  return leg_up<T>(g, 0, f, ec, g->n_post, u_out, st);
 }
 
 extern "C" int fvx_mg_vcycle(fvx_mg* g, const void* u_in, const void* f, void* u_out, void* stream) {
@@ -525,46 +747,28 @@ extern "C" int fvx_mg_vcycle(fvx_mg* g, const void* u_in, const void* f, void* u
 template <typename T>
 static int hybrid_down(fvx_mg* g, const T* f, int lvl, int n_pre, cudaStream_t st) {
   LevArray<T>& A = levs<T>(g);
-  const T om = (T)g->omega;
-  Lev<T>& L0 = A.L[0];
-  copy_kernel<T><<<grid_for((size_t)L0.ny * L0.nx), 256, 0, st>>>(L0.f, f, (size_t)L0.ny * L0.nx);
   for (int l = 0; l < lvl; ++l) {
-    Lev<T>& L = A.L[l];
-    const size_t n = (size_t)L.ny * L.nx;
-    const int gr = grid_for(n);
-    fill_kernel<T><<<gr, 256, 0, st>>>(L.u, n, T(0));
-    T* a = L.u;
-    T* b = L.tmp;
-    for (int s = 0; s < n_pre; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-    if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
-    Lev<T>& C = A.L[l + 1];
-    restrict_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(L, L.u, L.f, C, C.f);
+    int rc = leg_down<T>(g, l, l == 0 ? f : A.L[l].f, nullptr, n_pre, st);
+    if (rc) return rc;
   }
-  return fvx_cuda_status();
+  return FVX_OK;
 }
 
 template <typename T>
-static int hybrid_up(fvx_mg* g, T* u_out, int lvl, int n_post, cudaStream_t st) {
+static int hybrid_up(fvx_mg* g, const T* f, T* u_out, int lvl, int n_post, cudaStream_t st) {
   LevArray<T>& A = levs<T>(g);
-  const T om = (T)g->omega;
   for (int l = lvl - 1; l >= 0; --l) {
-    Lev<T>& L = A.L[l];
-    Lev<T>& C = A.L[l + 1];
-    const size_t n = (size_t)L.ny * L.nx;
-    const int gr = grid_for(n);
-    prolong_kernel<T><<<gr, 256, 0, st>>>(L, L.u, C, C.u);
-    T* a = L.u;
-    T* b = L.tmp;
-    for (int s = 0; s < n_post; ++s) { jacobi_kernel<T><<<gr, 256, 0, st>>>(L, a, L.f, b, om); T* t = a; a = b; b = t; }
-    if (l == 0) copy_kernel<T><<<gr, 256, 0, st>>>(u_out, a, n);
-    else if (a != L.u) copy_kernel<T><<<gr, 256, 0, st>>>(L.u, a, n);
+    const T* ec = l + 1 == lvl ? A.L[lvl].u : A.L[l + 1].tmp;
+    int rc = leg_up<T>(g, l, l == 0 ? f : A.L[l].f, ec, n_post, l == 0 ? u_out : A.L[l].tmp, st);
+    if (rc) return rc;
   }
-  return fvx_cuda_status();
+  return FVX_OK;
 }
 
 template <typename T>
 static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int n_post, fvx_precond_fn coarse,
                         void* ctx, cudaStream_t st) {
+  if (n_pre > kLegMaxSweeps || n_post > kLegMaxSweeps) return FVX_ERR_ARG;
   int rc = hybrid_down<T>(g, f, lvl, n_pre, st);
   if (rc) return rc;
   Lev<T>& C = levs<T>(g).L[lvl];
@@ -573,7 +777,7 @@ static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int
   } else {
     fill_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(C.u, (size_t)C.ny * C.nx, T(0));
   }
-  return hybrid_up<T>(g, u_out, lvl, n_post, st);
+  return hybrid_up<T>(g, f, u_out, lvl, n_post, st);
 }
 
 extern "C" int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
@@ -612,6 +816,43 @@ extern "C" int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* str
   fvx_hybrid* h = (fvx_hybrid*)ctx;
   if (!h) return FVX_ERR_ARG;
   return fvx_mg_vcycle_hybrid(h->g, rho, z, h->lvl, h->n_pre, h->n_post, h->coarse, h->ctx, stream);
+}
+
+// Multigrid as the level-lvl solver of the hybrid cycle (n_cycles cycles
+// from zero, one CTA): the exact-coarse-solve limit a learned coarse solver
+// is measured against.  An fvx_precond_fn with ctx = the fvx_levelsolve.
+struct fvx_levelsolve {
+  fvx_mg* g;
+  int lvl, n_cycles;
+  void* work;
+};
+
+extern "C" int fvx_mg_solve_level_batched(fvx_mg* g, int lvl, int batch, const void* f, void* u, int n_cycles,
+                                          void* work, void* stream);
+extern "C" long long fvx_mg_level_work(fvx_mg* g, int lvl);
+
+extern "C" int fvx_levelsolve_create(fvx_mg* g, int lvl, int n_cycles, fvx_levelsolve** out) {
+  if (!g || !out || n_cycles < 1) return FVX_ERR_ARG;
+  if (lvl < 0 || lvl >= g->nl) return FVX_ERR_SHAPE;
+  void* w = nullptr;
+  const size_t bytes = (size_t)fvx_mg_level_work(g, lvl) * (g->dtype == 0 ? 4 : 8);
+  if (cudaMalloc(&w, bytes) != cudaSuccess) return FVX_ERR_CUDA;
+  *out = new fvx_levelsolve{g, lvl, n_cycles, w};
+  return FVX_OK;
+}
+
+extern "C" int fvx_levelsolve_destroy(fvx_levelsolve* s) {
+  if (!s) return FVX_OK;
+  cudaDeviceSynchronize();
+  cudaFree(s->work);
+  delete s;
+  return fvx_cuda_status();
+}
+
+extern "C" int fvx_levelsolve_coarse(void* ctx, const void* f, void* u, void* stream) {
+  fvx_levelsolve* s = (fvx_levelsolve*)ctx;
+  if (!s) return FVX_ERR_ARG;
+  return fvx_mg_solve_level_batched(s->g, s->lvl, 1, f, u, s->n_cycles, s->work, stream);
 }
 
 // The downward leg only: the level-lvl restricted residual of f, copied to

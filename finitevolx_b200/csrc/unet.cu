@@ -40,53 +40,82 @@ __host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
   return mode == IN_DIRECT ? (size_t)h * w : (mode == IN_POOL ? (size_t)4 * h * w : (size_t)(h / 2) * (w / 2));
 }
 
-// y = act(W * in + b [+ skip]); one thread per output pixel, all Cout
-// accumulators in registers, input tiles and weights staged in smem.
-template <int COUT>
-__global__ void __launch_bounds__(THREADS)
-conv_fwd_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
-                const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
-                int w, int relu) {
-  __shared__ float tile[TILE + 2][TILE + 2];
-  __shared__ float ws[CMAX * 9 * COUT];
+// y = act(W * in + b [+ skip]) for one conv layer.
+// Latency-oriented: a T x T pixel tile per block with every
+// input channel staged in shared memory by one cooperative load (one
+// barrier), each thread accumulating CPT output channels of one pixel.
+// Small tiles give enough blocks for single-field inference on coarse grids.
+template <int COUT, int CPT, int T>
+__global__ void __launch_bounds__(T * T * (COUT / CPT))
+conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
+                 const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
+                 int w, int relu) {
+  constexpr int NT = T * T * (COUT / CPT);
+  constexpr int TW = T + 2;
+  extern __shared__ __align__(16) float sm[];
+  float* ws = sm;                     // [cin * 9][COUT]
+  float* tile = sm + cin * 9 * COUT;  // [cin][TW][TW]
   const int b = blockIdx.z;
-  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
-  const int tx = threadIdx.x % TILE, ty = threadIdx.x / TILE;
-  for (int k = threadIdx.x; k < cin * 9 * COUT; k += THREADS) {
-    // ws[(ci*9 + t)*COUT + co] = W[co][ci][t]
+  const int x0 = blockIdx.x * T, y0 = blockIdx.y * T;
+  const int tid = threadIdx.x;
+  for (int k = tid; k < cin * 9 * COUT; k += NT) {
     const int co = k % COUT, rest = k / COUT;
     ws[k] = __bfloat162float(wb[(size_t)co * cin * 9 + rest]);
   }
-  float acc[COUT];
-#pragma unroll
-  for (int co = 0; co < COUT; ++co) acc[co] = 0.f;
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
+  for (int k = tid; k < cin * TW * TW; k += NT) {
+    const int ci = k / (TW * TW), r = k - ci * (TW * TW);
+    const int ly = r / TW, lx = r - ly * TW;
+    tile[k] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+  }
+  __syncthreads();
+  const int p = tid % (T * T), co0 = (tid / (T * T)) * CPT;
+  const int ty = p / T, tx = p % T;
+  float acc[CPT];
+#pragma unroll
+  for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
   for (int ci = 0; ci < cin; ++ci) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < (TILE + 2) * (TILE + 2); k += THREADS) {
-      const int ly = k / (TILE + 2), lx = k % (TILE + 2);
-      tile[ly][lx] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
-    }
-    __syncthreads();
+    const float* tl = tile + ci * TW * TW + ty * TW + tx;
+    const float* wc = ws + ci * 9 * COUT + co0;
 #pragma unroll
     for (int t = 0; t < 9; ++t) {
-      const float v = tile[ty + t / 3][tx + t % 3];
-      const float* wr = ws + (ci * 9 + t) * COUT;
+      const float v = tl[(t / 3) * TW + t % 3];
+      const float* wr = wc + t * COUT;
 #pragma unroll
-      for (int co = 0; co < COUT; ++co) acc[co] = fmaf(wr[co], v, acc[co]);
+      for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
     }
   }
   const int y = y0 + ty, x = x0 + tx;
   if (y >= h || x >= w) return;
   const size_t plane = (size_t)h * w, base = (size_t)b * COUT * plane + (size_t)y * w + x;
 #pragma unroll
-  for (int co = 0; co < COUT; ++co) {
-    float v = acc[co] + bias[co];
+  for (int c = 0; c < CPT; ++c) {
+    const int co = co0 + c;
+    float v = acc[c] + bias[co];
     if (skip) v += skip[base + co * plane];
     if (relu) v = fmaxf(v, 0.f);
     out[base + co * plane] = v;
   }
+}
+
+template <int COUT, int CPT, int T>
+static int launch_conv_tile(const float* in, int mode, int batch, int cin, const __nv_bfloat16* wb,
+                            const float* bias, const float* skip, float* out, int h, int w, int relu,
+                            cudaStream_t st) {
+  constexpr int NT = T * T * (COUT / CPT);
+  const size_t smem = ((size_t)cin * 9 * COUT + (size_t)cin * (T + 2) * (T + 2)) * sizeof(float);
+  static bool attr_set = false;  // per instantiation; the largest use needs > 48 KB
+  if (!attr_set) {
+    const int max_smem = (CMAX * 9 * COUT + CMAX * (T + 2) * (T + 2)) * (int)sizeof(float);
+    if (cudaFuncSetAttribute(conv_tile_kernel<COUT, CPT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             max_smem) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    attr_set = true;
+  }
+  dim3 g((w + T - 1) / T, (h + T - 1) / T, batch);
+  conv_tile_kernel<COUT, CPT, T><<<g, NT, smem, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu);
+  return fvx_cuda_status();
 }
 
 // G = dL/d(pre-activation) = dY * (y > 0) (or dY when the layer is linear);
@@ -270,16 +299,24 @@ extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, co
   if (!in || !w_bf16 || !bias || !out) return FVX_ERR_ARG;
   if (cin < 1 || cin > CMAX || batch < 1 || h < 1 || w < 1 || mode < 0 || mode > 2) return FVX_ERR_SHAPE;
   if ((mode == IN_UP) && ((h % 2) || (w % 2))) return FVX_ERR_SHAPE;
-  dim3 g((w + TILE - 1) / TILE, (h + TILE - 1) / TILE, batch);
   cudaStream_t st = fvx_stream(stream);
   const __nv_bfloat16* wb = (const __nv_bfloat16*)w_bf16;
+  // 8 x 8 tiles with 4 or 8 output channels per thread while that gives at
+  // least one block per SM; else 4 x 4 tiles with 1 or 2 channels per
+  // thread (256 threads, 4-8x the blocks) for the coarse levels
+  const bool big = (size_t)((h + 7) / 8) * ((w + 7) / 8) * batch >= 148;
   switch (cout) {
-    case 1: conv_fwd_kernel<1><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
-    case 16: conv_fwd_kernel<16><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
-    case 32: conv_fwd_kernel<32><<<g, THREADS, 0, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu); break;
+    case 1:
+      return big ? launch_conv_tile<1, 1, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
+                 : launch_conv_tile<1, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
+    case 16:
+      return big ? launch_conv_tile<16, 4, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
+                 : launch_conv_tile<16, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
+    case 32:
+      return big ? launch_conv_tile<32, 8, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
+                 : launch_conv_tile<32, 2, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
     default: return FVX_ERR_SHAPE;
   }
-  return fvx_cuda_status();
 }
 
 // Backward of one conv layer (wb: the BF16 weights of the forward pass).
@@ -391,11 +428,17 @@ static size_t total_params() {
   return n;
 }
 
-// s = sqrt(sum(f^2 m) / max(sum m, 1)), stored as [s, 1/s] (1/s = 0 when s = 0)
-__global__ void rms_kernel(const float* f, const float* mask, size_t n, float* scale) {
+// s = sqrt(sum(f^2 m) / max(sum m, 1)), stored as [s, 1/s] (1/s = 0 when
+// s = 0).  Each block writes its partial sums; the last block to finish
+// (counted with an atomic ticket after a fence) adds them in block order
+// and resets the ticket, so the result is deterministic.
+constexpr int kRmsBlocks = 64;
+__global__ void rms_kernel(const float* f, const float* mask, size_t n, double* part, unsigned* ticket,
+                           float* scale) {
   __shared__ double sh[2][32];
+  __shared__ bool last;
   double a = 0.0, c = 0.0;
-  for (size_t k = threadIdx.x; k < n; k += blockDim.x) {
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     const double m = mask[k];
     a += (double)f[k] * f[k] * m;
     c += m;
@@ -409,9 +452,23 @@ __global__ void rms_kernel(const float* f, const float* mask, size_t n, float* s
   if (threadIdx.x == 0) {
     double A = 0.0, C = 0.0;
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { A += sh[0][k]; C += sh[1][k]; }
+    part[2 * blockIdx.x] = A;
+    part[2 * blockIdx.x + 1] = C;
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    double A = 0.0, C = 0.0;
+    for (int k = 0; k < (int)gridDim.x; ++k) {
+      A += ((volatile double*)part)[2 * k];
+      C += ((volatile double*)part)[2 * k + 1];
+    }
     const double s = sqrt(A / (C > 1.0 ? C : 1.0));
     scale[0] = (float)s;
     scale[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
+    *ticket = 0u;
   }
 }
 
@@ -445,6 +502,8 @@ struct fvx_unet {
   // inference on one field: level mask, scale [s, 1/s], output scale sigma
   float* mask = nullptr;
   float* scale = nullptr;
+  double* rms_part = nullptr;
+  unsigned* rms_ticket = nullptr;
   float sigma = 1.f;
   std::vector<void*> allocs;
 };
@@ -501,6 +560,8 @@ extern "C" int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out) {
   n->loss = (double*)alloc(8);
   n->mask = (float*)alloc((size_t)h * w * 4);
   n->scale = (float*)alloc(16);
+  n->rms_part = (double*)alloc(2 * kRmsBlocks * sizeof(double));
+  n->rms_ticket = (unsigned*)alloc(sizeof(unsigned));
   if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
     unet_free(n);
     delete n;
@@ -632,7 +693,7 @@ extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) 
   if (!n || !f || !u) return FVX_ERR_ARG;
   cudaStream_t st = fvx_stream(stream);
   const size_t plane = (size_t)n->h * n->w;
-  rms_kernel<<<1, 1024, 0, st>>>((const float*)f, n->mask, plane, n->scale);
+  rms_kernel<<<kRmsBlocks, 256, 0, st>>>((const float*)f, n->mask, plane, n->rms_part, n->rms_ticket, n->scale);
   prep_kernel<<<blocks_for(plane), 256, 0, st>>>((const float*)f, n->scale, n->act[0], plane);
   int rc = unet_forward(n, 1, st);
   if (rc) return rc;

@@ -202,11 +202,12 @@ class LearnedPreconditioner:
     pairs from ``generate_pairs``), then pass the object as ``precond`` to
     MaskedHelmholtzPCG.solve with ``flexible=True``.  ``coarse=False``
     drops the network (zero coarse correction) -- the same method without
-    the learned part.
+    the learned part; ``coarse="mg"`` solves the level-lvl problem by
+    ``mg_cycles`` multigrid cycles instead (the exact-coarse-solve limit).
     """
 
     def __init__(self, mg: MultigridSolver, lvl: int | None = None, n_pre: int = 2, n_post: int = 2,
-                 batch_max: int = 32, seed: int = 0, coarse: bool = True):
+                 batch_max: int = 32, seed: int = 0, coarse=True, mg_cycles: int = 10):
         if mg.dtype != torch.float32:
             raise ValueError("the learned preconditioner runs on a float32 MultigridSolver")
         self.mg = mg
@@ -221,7 +222,11 @@ class LearnedPreconditioner:
             raise ValueError(f"level {lvl} grid {h}x{w} is not a multiple of 8")
         self.net = UNet(h, w, batch_max, seed)
         self.sigma = 1.0
-        self.use_net = bool(coarse)
+        self.mode = "net" if coarse is True else ("mg" if coarse == "mg" else "none")
+        self._ls = ctypes.c_void_p()
+        if self.mode == "mg":
+            check(fn("fvx_levelsolve_create")(mg.handle, I(self.lvl), I(mg_cycles), ctypes.byref(self._ls)),
+                  "levelsolve_create")
         self._hy = ctypes.c_void_p()
         self._make_hybrid()
 
@@ -229,19 +234,24 @@ class LearnedPreconditioner:
         if self._hy.value:
             fn("fvx_hybrid_destroy")(self._hy)
             self._hy = ctypes.c_void_p()
-        coarse = ctypes.cast(fn("fvx_unet_coarse"), ctypes.c_void_p) if self.use_net else None
-        ctx = self.net.handle if self.use_net else None
+        if self.mode == "net":
+            coarse, ctx = ctypes.cast(fn("fvx_unet_coarse"), ctypes.c_void_p), self.net.handle
+        elif self.mode == "mg":
+            coarse, ctx = ctypes.cast(fn("fvx_levelsolve_coarse"), ctypes.c_void_p), self._ls
+        else:
+            coarse, ctx = None, None
         check(fn("fvx_hybrid_create")(self.mg.handle, I(self.lvl), I(self.n_pre), I(self.n_post), coarse, ctx,
                                       ctypes.byref(self._hy)), "hybrid_create")
 
     def __del__(self):
-        h = getattr(self, "_hy", None)
-        if h is not None and h.value:
-            try:
-                fn("fvx_hybrid_destroy")(h)
-            except Exception:
-                pass
-            self._hy = None
+        for name, dtor in (("_hy", "fvx_hybrid_destroy"), ("_ls", "fvx_levelsolve_destroy")):
+            h = getattr(self, name, None)
+            if h is not None and h.value:
+                try:
+                    fn(dtor)(h)
+                except Exception:
+                    pass
+                setattr(self, name, None)
 
     # -- training -----------------------------------------------------------
     def make_inputs(self, F, E=None):

@@ -160,7 +160,12 @@ class MaskedHelmholtzPCG:
         return 2, cb, None, cb
 
     def solve(self, b, rtol: float = 1e-8, max_iter: int = 500, precond="mg", flexible: bool = False,
-              replace_every: int = 10, chunk: int = 4, x=None, graph: bool = False):
+              replace_every: int | None = None, chunk: int = 4, x=None, graph: bool = False):
+        # float32 work vectors: the recursively updated residual drifts from
+        # b - A x by ~eps32 * cond(A) |b|, so recompute it from the FP64
+        # iterate (in FP64) every iteration; float64: every 10
+        if replace_every is None:
+            replace_every = 1 if self.mg.dtype == torch.float32 else 10
         b = L.as_field(b, dtype=self.mg.dtype)
         if tuple(b.shape) != self.mg.shape:
             raise ValueError("rhs shape does not match the multigrid operator")

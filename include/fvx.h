@@ -287,6 +287,12 @@ int fvx_mg_restrict_residual(fvx_mg* g, const void* f, int lvl, int n_pre, void*
 long long fvx_mg_level_work(fvx_mg* g, int lvl);
 int fvx_mg_solve_level_batched(fvx_mg* g, int lvl, int batch, const void* f, void* u, int n_cycles, void* work,
                                void* stream);
+/* Multigrid (n_cycles cycles) as the level-lvl solver: an fvx_precond_fn
+ * with ctx = the fvx_levelsolve (the exact-coarse-solve comparison). */
+typedef struct fvx_levelsolve fvx_levelsolve;
+int fvx_levelsolve_create(fvx_mg* g, int lvl, int n_cycles, fvx_levelsolve** out);
+int fvx_levelsolve_destroy(fvx_levelsolve* s);
+int fvx_levelsolve_coarse(void* ctx, const void* f, void* u, void* stream);
 /* The hybrid cycle as an fvx_precond_fn (ctx = the fvx_hybrid object). */
 typedef struct fvx_hybrid fvx_hybrid;
 int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, fvx_precond_fn coarse, void* ctx,
