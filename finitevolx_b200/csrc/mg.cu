@@ -33,6 +33,32 @@ struct Lev {
   T *mask, *cx, *cy, *inv, *u, *f, *tmp;
 };
 
+DEV double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+  if (w == 0)
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  return v;
+}
+
+// True in the one block that finishes last (an atomic ticket taken after a
+// fence); that block then sums the partials in block order.
+DEV bool pcg_last_block(unsigned* ticket) {
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  return last;
+}
+
 template <typename T> DEV T divd(T a, T d2, T rd2) {
   if constexpr (sizeof(T) == 8) return a / d2;
   else return a * rd2;
@@ -238,6 +264,49 @@ coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post
   }
 }
 
+// Energy-optimal scaling of a coarse correction d = C.u:
+// omega = (d . f) / (d . A d) minimises |e* - omega d| in the energy norm of
+// -A (A negative definite), so the scaled correction never increases the
+// level-lvl error; omega = 0 when d . A d = 0.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_coarse_omega(Lev<T> C, double* part, unsigned* ticket, double* omega) {
+  const size_t n = (size_t)C.ny * C.nx;
+  double df = 0.0, dad = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / C.nx), i = (int)(c - (size_t)j * C.nx);
+    const double d = (double)C.u[c];
+    df += d * (double)C.f[c];
+    dad += d * (double)apply_at(C, C.u, j, i);
+  }
+  df = block_sum(df);
+  dad = block_sum(dad);
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = df; part[2 * blockIdx.x + 1] = dad; }
+  if (pcg_last_block(ticket)) {
+    __threadfence();
+    double a = 0.0, b = 0.0;
+    for (int k = threadIdx.x; k < (int)gridDim.x; k += blockDim.x) {
+      a += ((volatile double*)part)[2 * k];
+      b += ((volatile double*)part)[2 * k + 1];
+    }
+    a = block_sum(a);
+    b = block_sum(b);
+    if (threadIdx.x == 0) {
+      *omega = b != 0.0 ? a / b : 0.0;
+      *ticket = 0u;
+    }
+  }
+}
+
+template <typename T>
+__global__ void k_scale(T* u, size_t n, const double* omega) {
+  const T w = (T)*omega;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
+    u[c] *= w;
+}
+
+constexpr int kOmegaBlocks = 64;
+
 // ---------------------------------------------------------------------------
 // Fused V-cycle legs for the host-driven (fine) levels, one launch per leg:
 //   down: u = k Jacobi sweeps from u_init (NULL = 0) on f, then the
@@ -308,17 +377,30 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
   T* sa = sinv + RN;
   T* sb = sa + RN;
   const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
-  for (int q = threadIdx.x; q < RN; q += blockDim.x) {
-    const int ly = q / RW, lx = q - ly * RW;
-    const int gy = y0 + ly, gx = x0 + lx;
-    const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-    const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-    sf[q] = in ? f[c] : T(0);
-    sm[q] = in ? L.mask[c] : T(0);
-    scx[q] = in ? L.cx[c] : T(0);
-    scy[q] = in ? L.cy[c] : T(0);
-    sinv[q] = in ? L.inv[c] : T(0);
-    sa[q] = (in && u_init) ? u_init[c] : T(0);
+  // batches of 4 cells per thread: all 24 loads in flight before any store
+  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
+    T v[4][6];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      const int ly = q / RW, lx = q - ly * RW;
+      const int gy = y0 + ly, gx = x0 + lx;
+      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+      v[u][0] = in ? f[c] : T(0);
+      v[u][1] = in ? L.mask[c] : T(0);
+      v[u][2] = in ? L.cx[c] : T(0);
+      v[u][3] = in ? L.cy[c] : T(0);
+      v[u][4] = in ? L.inv[c] : T(0);
+      v[u][5] = (in && u_init) ? u_init[c] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      if (q < RN) {
+        sf[q] = v[u][0]; sm[q] = v[u][1]; scx[q] = v[u][2]; scy[q] = v[u][3]; sinv[q] = v[u][4]; sa[q] = v[u][5];
+      }
+    }
   }
   __syncthreads();
   T* a = sa;
@@ -393,17 +475,34 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
     scm[q] = cm;
   }
   __syncthreads();
+  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
+    T v[4][6];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int q = q0 + t * blockDim.x;
+      const int ly = q / RW, lx = q - ly * RW;
+      const int gy = y0 + ly, gx = x0 + lx;
+      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+      v[t][0] = in ? f[c] : T(0);
+      v[t][1] = in ? L.mask[c] : T(0);
+      v[t][2] = in ? L.cx[c] : T(0);
+      v[t][3] = in ? L.cy[c] : T(0);
+      v[t][4] = in ? L.inv[c] : T(0);
+      v[t][5] = in ? u_pre[c] : T(0);
+    }
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+      const int q = q0 + t * blockDim.x;
+      if (q < RN) { sf[q] = v[t][0]; sm[q] = v[t][1]; scx[q] = v[t][2]; scy[q] = v[t][3]; sinv[q] = v[t][4]; sa[q] = v[t][5]; }
+    }
+  }
+  __syncthreads();
   for (int q = threadIdx.x; q < RN; q += blockDim.x) {
     const int ly = q / RW, lx = q - ly * RW;
     const int gy = y0 + ly, gx = x0 + lx;
     const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-    const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-    const T mf = in ? L.mask[c] : T(0);
-    sf[q] = in ? f[c] : T(0);
-    sm[q] = mf;
-    scx[q] = in ? L.cx[c] : T(0);
-    scy[q] = in ? L.cy[c] : T(0);
-    sinv[q] = in ? L.inv[c] : T(0);
+    const T mf = sm[q];
     T u = T(0);
     if (in) {
       const int J = gy >> 1, I = gx >> 1, sj = 2 * (gy & 1) - 1, si = 2 * (gx & 1) - 1;
@@ -412,13 +511,13 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
       const T ws = ((T(9) * V(J, I) + T(3) * V(J, I + si)) + T(3) * V(J + sj, I)) + T(1) * V(J + sj, I + si);
       const T ds = ((T(9) * M(J, I) + T(3) * M(J, I + si)) + T(3) * M(J + sj, I)) + T(1) * M(J + sj, I + si);
       const T e = (ws / (ds > T(1) ? ds : T(1))) * mf;
-      u = (u_pre[c] + e) * mf;
+      u = (sa[q] + e) * mf;
     }
-    sa[q] = u;
+    sb[q] = u;
   }
   __syncthreads();
-  T* a = sa;
-  T* b = sb;
+  T* a = sb;  // u_pre + P e
+  T* b = sa;
   for (int s = 1; s <= k; ++s) {
     const int w = RW - 2 * s, h = RH - 2 * s;
     for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
@@ -464,6 +563,7 @@ using namespace fvx::mg;
 
 struct fvx_mg {
   int nl = 0, lc = 0, n_pre = 6, n_post = 6, n_coarse = 50, dtype = 0;
+  double* omega_scratch = nullptr;  // [2 * kOmegaBlocks partials, omega], ticket after it
   double omega = 0.95, lam = 0.0;
   std::vector<void*> allocs;
   LevArray<float> A32;
@@ -765,45 +865,73 @@ static int hybrid_up(fvx_mg* g, const T* f, T* u_out, int lvl, int n_post, cudaS
   return FVX_OK;
 }
 
+// n_smooth: weighted-Jacobi sweeps on A_lvl e = f_lvl after the coarse
+// correction (they damp the high-frequency error a learned solver leaves).
+// scale: the coarse correction is first scaled by the energy-optimal omega.
 template <typename T>
-static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int n_post, fvx_precond_fn coarse,
-                        void* ctx, cudaStream_t st) {
-  if (n_pre > kLegMaxSweeps || n_post > kLegMaxSweeps) return FVX_ERR_ARG;
+static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int n_post, int n_smooth, int scale,
+                        fvx_precond_fn coarse, void* ctx, cudaStream_t st) {
+  if (n_pre > kLegMaxSweeps || n_post > kLegMaxSweeps || n_smooth < 0) return FVX_ERR_ARG;
   int rc = hybrid_down<T>(g, f, lvl, n_pre, st);
   if (rc) return rc;
   Lev<T>& C = levs<T>(g).L[lvl];
+  const size_t nc = (size_t)C.ny * C.nx;
   if (coarse) {
     if ((rc = coarse(ctx, C.f, C.u, st))) return rc;
+    if (scale) {
+      if (!g->omega_scratch) {
+        if (cudaMalloc((void**)&g->omega_scratch, (2 * kOmegaBlocks + 2) * sizeof(double)) != cudaSuccess)
+          return FVX_ERR_CUDA;
+        g->allocs.push_back(g->omega_scratch);
+        cudaMemsetAsync(g->omega_scratch, 0, (2 * kOmegaBlocks + 2) * sizeof(double), st);
+      }
+      double* part = g->omega_scratch;
+      double* om = part + 2 * kOmegaBlocks;
+      unsigned* ticket = (unsigned*)(om + 1);
+      k_coarse_omega<T><<<kOmegaBlocks, 256, 0, st>>>(C, part, ticket, om);
+      k_scale<T><<<grid_for(nc), 256, 0, st>>>(C.u, nc, om);
+    }
   } else {
-    fill_kernel<T><<<grid_for((size_t)C.ny * C.nx), 256, 0, st>>>(C.u, (size_t)C.ny * C.nx, T(0));
+    fill_kernel<T><<<grid_for(nc), 256, 0, st>>>(C.u, nc, T(0));
+  }
+  if (n_smooth > 0) {
+    T* a = C.u;
+    T* b = C.tmp;
+    for (int k = 0; k < n_smooth; ++k) {
+      jacobi_kernel<T><<<grid_for(nc), 256, 0, st>>>(C, a, C.f, b, (T)g->omega);
+      T* t = a; a = b; b = t;
+    }
+    if (a != C.u) copy_kernel<T><<<grid_for(nc), 256, 0, st>>>(C.u, a, nc);
   }
   return hybrid_up<T>(g, f, u_out, lvl, n_post, st);
 }
 
 extern "C" int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
-                                    fvx_precond_fn coarse, void* ctx, void* stream) {
+                                    int n_smooth, int scale, fvx_precond_fn coarse, void* ctx, void* stream) {
   if (!g || !f || !u_out || n_pre < 0 || n_post < 0) return FVX_ERR_ARG;
   if (lvl < 1 || lvl >= g->nl) return FVX_ERR_SHAPE;
   cudaStream_t st = fvx_stream(stream);
-  return g->dtype == 0 ? hybrid_cycle<float>(g, (const float*)f, (float*)u_out, lvl, n_pre, n_post, coarse, ctx, st)
-                       : hybrid_cycle<double>(g, (const double*)f, (double*)u_out, lvl, n_pre, n_post, coarse, ctx,
-                                              st);
+  return g->dtype == 0 ? hybrid_cycle<float>(g, (const float*)f, (float*)u_out, lvl, n_pre, n_post, n_smooth, scale,
+                                             coarse, ctx, st)
+                       : hybrid_cycle<double>(g, (const double*)f, (double*)u_out, lvl, n_pre, n_post, n_smooth,
+                                              scale, coarse, ctx, st);
 }
 
 // The hybrid cycle packaged as a preconditioner callback (ctx = the
 // fvx_hybrid object) for fvx_pcg_solve / fvx_pcg_iterate with precond 2.
 struct fvx_hybrid {
   fvx_mg* g;
-  int lvl, n_pre, n_post;
+  int lvl, n_pre, n_post, n_smooth, scale;
   fvx_precond_fn coarse;
   void* ctx;
 };
 
-extern "C" int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, fvx_precond_fn coarse, void* ctx,
-                                 fvx_hybrid** out) {
-  if (!g || !out || n_pre < 0 || n_post < 0) return FVX_ERR_ARG;
+extern "C" int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, int n_smooth, int scale,
+                                 fvx_precond_fn coarse, void* ctx, fvx_hybrid** out) {
+  if (!g || !out || n_pre < 0 || n_post < 0 || n_smooth < 0) return FVX_ERR_ARG;
+  if (n_pre > kLegMaxSweeps || n_post > kLegMaxSweeps) return FVX_ERR_ARG;
   if (lvl < 1 || lvl >= g->nl) return FVX_ERR_SHAPE;
-  *out = new fvx_hybrid{g, lvl, n_pre, n_post, coarse, ctx};
+  *out = new fvx_hybrid{g, lvl, n_pre, n_post, n_smooth, scale, coarse, ctx};
   return FVX_OK;
 }
 
@@ -815,8 +943,10 @@ extern "C" int fvx_hybrid_destroy(fvx_hybrid* h) {
 extern "C" int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* stream) {
   fvx_hybrid* h = (fvx_hybrid*)ctx;
   if (!h) return FVX_ERR_ARG;
-  return fvx_mg_vcycle_hybrid(h->g, rho, z, h->lvl, h->n_pre, h->n_post, h->coarse, h->ctx, stream);
+  return fvx_mg_vcycle_hybrid(h->g, rho, z, h->lvl, h->n_pre, h->n_post, h->n_smooth, h->scale, h->coarse, h->ctx,
+                              stream);
 }
+
 
 // Multigrid as the level-lvl solver of the hybrid cycle (n_cycles cycles
 // from zero, one CTA): the exact-coarse-solve limit a learned coarse solver
@@ -962,18 +1092,6 @@ namespace mg {
 enum Slot { S_GAMMA = 0, S_PAP, S_ALPHA, S_BETA, S_RR, S_BB, S_CONV, S_ITER, S_TOL2, S_FLEX_A, S_NSLOTS = 16 };
 constexpr int kRedBlocks = 296;  // 2 per SM
 
-DEV double block_sum(double v) {
-  __shared__ double sh[32];
-  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  v = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
-  if (w == 0)
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  __syncthreads();
-  return v;
-}
 
 template <typename T>
 __global__ void k_apply_dot(Lev<T> L, const T* p, T* Ap, double* part, const double* s) {
@@ -1086,6 +1204,149 @@ __global__ void k_zero_x(double* x, size_t n) {
   for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) x[c] = 0.0;
 }
 
+// ---- fused iteration kernels (one pass each over the level-0 arrays) ------
+constexpr int kPcgBlocks = 148 * 4;
+
+// A u at (j, i) with u given as a function of the flat index (apply_at's
+// arithmetic, in its order).
+template <typename T, typename U>
+DEV T apply_fn(const Lev<T>& L, int j, int i, U u) {
+  const int nx = L.nx, ny = L.ny;
+  const size_t c = (size_t)j * nx + i;
+  const T m = L.mask[c];
+  const T um = u(c) * m;
+  const T ue = i + 1 < nx ? u(c + 1) * L.mask[c + 1] : T(0);
+  const T uw = i > 0 ? u(c - 1) * L.mask[c - 1] : T(0);
+  const T un = j + 1 < ny ? u(c + nx) * L.mask[c + nx] : T(0);
+  const T us = j > 0 ? u(c - nx) * L.mask[c - nx] : T(0);
+  const T cxw = i > 0 ? L.cx[c - 1] : T(0);
+  const T cys = j > 0 ? L.cy[c - nx] : T(0);
+  const T lap = divd(L.cx[c] * (ue - um) - cxw * (um - uw), L.dx2, L.rdx2) +
+                divd(L.cy[c] * (un - um) - cys * (um - us), L.dy2, L.rdy2);
+  return (lap - L.lam * um) * m;
+}
+
+
+DEV double pcg_sum_parts(const double* part, int np) {
+  __threadfence();
+  double v = 0.0;
+  for (int k = threadIdx.x; k < np; k += blockDim.x) v += ((volatile const double*)part)[k];
+  return block_sum(v);
+}
+
+// p_new = z + beta p_old (recomputed at the neighbours), Ap = A p_new,
+// partial p.Ap; the last block sets alpha = gamma / p.Ap.  p ping-pongs
+// between p0 and p1 by the iteration count.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_dir_apply(Lev<T> L, const T* __restrict__ z, T* p0, T* p1, T* __restrict__ Ap, double* part, double* s,
+            unsigned* ticket) {
+  if (s[S_CONV] != 0.0) return;
+  const int it = (int)s[S_ITER];
+  const T* po = (it & 1) ? p1 : p0;
+  T* pn = (it & 1) ? p0 : p1;
+  const T beta = (T)s[S_BETA];
+  const size_t n = (size_t)L.ny * L.nx;
+  double acc = 0.0;
+  auto P = [&](size_t k) -> T { return z[k] + beta * po[k]; };
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+    const T pc = P(c);
+    const T a = apply_fn(L, j, i, P);
+    pn[c] = pc;
+    Ap[c] = a;
+    acc += (double)pc * (double)a;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (pcg_last_block(ticket)) {
+    const double v = pcg_sum_parts(part, gridDim.x);
+    if (threadIdx.x == 0) {
+      s[S_PAP] = v;
+      s[S_ALPHA] = s[S_GAMMA] / v;
+      *ticket = 0u;
+    }
+  }
+}
+
+// x_new = x + alpha p (FP64, ping-pong x0/x1), then rho: every
+// ``replace_every``-th iteration the true residual b - A x_new in FP64
+// (x_new recomputed at the neighbours, A the FP64 operator), otherwise the
+// recursion rho - alpha Ap; partial |rho|^2.  The last block counts the
+// iteration and sets the convergence flag.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_step(Lev<double> D, const T* p0, const T* p1, const T* __restrict__ Ap, double* x0, double* x1,
+       const T* __restrict__ b, T* rho, T* rho_prev, int replace_every, double* part, double* s, unsigned* ticket) {
+  if (s[S_CONV] != 0.0) return;
+  const int it = (int)s[S_ITER];
+  const T* pn = (it & 1) ? p0 : p1;
+  const double* xo = (it & 1) ? x1 : x0;
+  double* xn = (it & 1) ? x0 : x1;
+  const double a = s[S_ALPHA];
+  const bool true_res = replace_every > 0 && (it + 1) % replace_every == 0;
+  const size_t n = (size_t)D.ny * D.nx;
+  double acc = 0.0;
+  auto X = [&](size_t k) -> double { return xo[k] + a * (double)pn[k]; };
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const double xc = X(c);
+    xn[c] = xc;
+    const T ro = rho[c];
+    if (rho_prev) rho_prev[c] = ro;
+    if (true_res) {
+      const int j = (int)(c / D.nx), i = (int)(c - (size_t)j * D.nx);
+      const double r = (double)b[c] - apply_fn(D, j, i, X);
+      rho[c] = (T)r;
+      acc += r * r;
+    } else {
+      const T r = ro - (T)a * Ap[c];
+      rho[c] = r;
+      acc += (double)r * (double)r;
+    }
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) part[blockIdx.x] = acc;
+  if (pcg_last_block(ticket)) {
+    const double v = pcg_sum_parts(part, gridDim.x);
+    if (threadIdx.x == 0) {
+      s[S_RR] = v;
+      s[S_ITER] += 1.0;
+      if (v <= s[S_TOL2]) s[S_CONV] = 1.0;
+      *ticket = 0u;
+    }
+  }
+}
+
+// gamma_new = z.rho; flexible: beta = (z.rho - z.rho_prev) / gamma
+// (Polak-Ribiere), else gamma_new / gamma.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_dot_beta(const T* __restrict__ z, const T* __restrict__ rho, const T* __restrict__ rho_prev, size_t n,
+           double* part, double* part2, double* s, unsigned* ticket) {
+  if (s[S_CONV] != 0.0) return;
+  double acc = 0.0, acc2 = 0.0;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const double zc = (double)z[c];
+    acc += zc * (double)rho[c];
+    if (rho_prev) acc2 += zc * (double)rho_prev[c];
+  }
+  acc = block_sum(acc);
+  if (rho_prev) acc2 = block_sum(acc2);
+  if (threadIdx.x == 0) {
+    part[blockIdx.x] = acc;
+    if (rho_prev) part2[blockIdx.x] = acc2;
+  }
+  if (pcg_last_block(ticket)) {
+    const double v = pcg_sum_parts(part, gridDim.x);
+    const double v2 = rho_prev ? pcg_sum_parts(part2, gridDim.x) : 0.0;
+    if (threadIdx.x == 0) {
+      s[S_BETA] = (v - v2) / s[S_GAMMA];
+      s[S_GAMMA] = v;
+      *ticket = 0u;
+    }
+  }
+}
+
 }  // namespace mg
 }  // namespace fvx
 
@@ -1093,9 +1354,11 @@ struct fvx_pcg {
   fvx_mg* mg = nullptr;
   int dtype = 0;
   size_t n = 0;
-  void *rho = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *rho_prev = nullptr;
+  void *rho = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr, *rho_prev = nullptr, *p1 = nullptr;
+  double* x1 = nullptr;                       // second FP64 iterate buffer (ping-pong with the caller's x)
   void *own_rho = nullptr, *own_z = nullptr;  // allocations replaced by bound caller buffers
   double *part = nullptr, *part2 = nullptr, *s = nullptr;
+  unsigned* ticket = nullptr;
 };
 
 extern "C" int fvx_pcg_create(fvx_mg* g, fvx_pcg** out) {
@@ -1106,14 +1369,18 @@ extern "C" int fvx_pcg_create(fvx_mg* g, fvx_pcg** out) {
   P->n = g->dtype == 0 ? (size_t)g->A32.L[0].ny * g->A32.L[0].nx : (size_t)g->A64.L[0].ny * g->A64.L[0].nx;
   const size_t es = g->dtype == 0 ? 4 : 8;
   bool ok = true;
-  void** vecs[5] = {&P->rho, &P->z, &P->p, &P->Ap, &P->rho_prev};
+  void** vecs[6] = {&P->rho, &P->z, &P->p, &P->Ap, &P->rho_prev, &P->p1};
   for (void** v : vecs)
     if (ok && cudaMalloc(v, P->n * es) != cudaSuccess) ok = false;
-  if (ok && cudaMalloc((void**)&P->part, kRedBlocks * sizeof(double)) != cudaSuccess) ok = false;
-  if (ok && cudaMalloc((void**)&P->part2, kRedBlocks * sizeof(double)) != cudaSuccess) ok = false;
+  const size_t np = kPcgBlocks > kRedBlocks ? kPcgBlocks : kRedBlocks;
+  if (ok && cudaMalloc((void**)&P->x1, P->n * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->part, np * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->part2, np * sizeof(double)) != cudaSuccess) ok = false;
   if (ok && cudaMalloc((void**)&P->s, (S_NSLOTS + 2) * sizeof(double)) != cudaSuccess) ok = false;
+  if (ok && cudaMalloc((void**)&P->ticket, 4 * sizeof(unsigned)) != cudaSuccess) ok = false;
+  if (ok && cudaMemset(P->ticket, 0, 4 * sizeof(unsigned)) != cudaSuccess) ok = false;
   if (!ok) {
-    void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->part, P->part2, P->s};
+    void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->p1, P->x1, P->part, P->part2, P->s, P->ticket};
     for (void* q : ps) if (q) cudaFree(q);
     delete P;
     return FVX_ERR_CUDA;
@@ -1126,7 +1393,7 @@ extern "C" int fvx_pcg_destroy(fvx_pcg* P) {
   if (!P) return FVX_ERR_ARG;
   cudaDeviceSynchronize();
   if (P->own_rho) { P->rho = P->own_rho; P->z = P->own_z; }
-  void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->part, P->part2, P->s};
+  void* ps[] = {P->rho, P->z, P->p, P->Ap, P->rho_prev, P->p1, P->x1, P->part, P->part2, P->s, P->ticket};
   for (void* q : ps) if (q) cudaFree(q);
   delete P;
   return fvx_cuda_status();
@@ -1176,41 +1443,45 @@ static int pcg_begin_t(fvx_pcg* P, const T* b, double* x, double rtol, const Pcg
   if (bb == 0.0) return FVX_OK;
   int rc = pcg_apply_M<T>(P, c, st);
   if (rc) return rc;
-  k_copy_if<T><<<G, 256, 0, st>>>((T*)P->p, (const T*)P->z, n, s);
+  // p_old = 0 and beta = 0 (S_BETA starts at 0): the first iteration takes p = z
+  cudaMemsetAsync(P->p, 0, n * sizeof(T), st);
   k_dot<T><<<G, 256, 0, st>>>((const T*)P->rho, (const T*)P->z, nullptr, P->part, nullptr, s, n);
   k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, S_GAMMA, R_STORE, 0);
   return fvx_cuda_status();
 }
 
-// ``it0``: iterations already done (for the residual-replacement schedule).
+// ``niter`` iterations; the iteration count, the iterate/direction
+// ping-pong and the residual-replacement schedule all follow the device's
+// own counter, so the launches are the same for every call (CUDA graphs).
+// Per iteration: k_dir_apply, k_step, the preconditioner, k_dot_beta.
 template <typename T>
-static int pcg_iterate_t(fvx_pcg* P, const T* b, double* x, int it0, int niter, const PcgCall& c, cudaStream_t st) {
+static int pcg_iterate_t(fvx_pcg* P, const T* b, double* x, int niter, const PcgCall& c, cudaStream_t st) {
   fvx_mg* g = P->mg;
   Lev<T>& L = levs<T>(g).L[0];
-  const size_t n = P->n;
-  T *rho = (T*)P->rho, *z = (T*)P->z, *p = (T*)P->p, *Ap = (T*)P->Ap, *rp = (T*)P->rho_prev;
+  T *rho = (T*)P->rho, *z = (T*)P->z, *p0 = (T*)P->p, *p1 = (T*)P->p1, *Ap = (T*)P->Ap;
+  T* rp = c.flexible ? (T*)P->rho_prev : nullptr;
   double* s = P->s;
-  const int G = kRedBlocks;
+  const int G = kPcgBlocks;
   for (int k = 0; k < niter; ++k) {
-    const int it = it0 + k;
-    k_apply_dot<T><<<G, 256, 0, st>>>(L, p, Ap, P->part, s);
-    k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_ALPHA, 0);
-    k_update<T><<<G, 256, 0, st>>>(x, p, Ap, rho, c.flexible ? rp : nullptr, P->part, s, n);
-    if (c.replace_every > 0 && (it + 1) % c.replace_every == 0)
-      k_residual64<T><<<G, 256, 0, st>>>(g->L0d, x, b, rho, P->part, s, 0);
-    k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, s, 0, R_RR, 0);
+    k_dir_apply<T><<<G, 256, 0, st>>>(L, z, p0, p1, Ap, P->part, s, P->ticket);
+    k_step<T><<<G, 256, 0, st>>>(g->L0d, p0, p1, Ap, x, P->x1, b, rho, rp, c.replace_every, P->part, s,
+                                 P->ticket + 1);
     int rc = pcg_apply_M<T>(P, c, st);
     if (rc) return rc;
-    k_dot<T><<<G, 256, 0, st>>>(z, rho, c.flexible ? rp : nullptr, P->part, P->part2, s, n);
-    k_reduce<<<1, 256, 0, st>>>(P->part, c.flexible ? P->part2 : nullptr, G, s, 0,
-                                c.flexible ? R_BETA_FLEX : R_BETA, 0);
-    k_pupdate<T><<<G, 256, 0, st>>>(p, z, s, n);
+    k_dot_beta<T><<<G, 256, 0, st>>>(z, rho, rp, P->n, P->part, P->part2, s, P->ticket + 2);
   }
   return fvx_cuda_status();
 }
 
+// Final iterate into x (odd iteration counts leave it in the second
+// buffer) and its FP64 true relative residual.
 template <typename T>
 static int pcg_finish_t(fvx_pcg* P, const T* b, double* x, double bb, double* rel_out, cudaStream_t st) {
+  double iters = 0;
+  cudaMemcpyAsync(&iters, P->s + S_ITER, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
+  if (((long long)iters) & 1)
+    cudaMemcpyAsync(x, P->x1, P->n * sizeof(double), cudaMemcpyDeviceToDevice, st);
   const int G = kRedBlocks;
   k_residual64<T><<<G, 256, 0, st>>>(P->mg->L0d, x, b, (T*)nullptr, P->part, P->s, 1);
   k_reduce<<<1, 256, 0, st>>>(P->part, nullptr, G, P->s, S_RR, R_STORE, 1);
@@ -1235,8 +1506,9 @@ extern "C" int fvx_pcg_iterate(fvx_pcg* P, const void* b, double* x, int it0, in
   if (!P || !b || !x || niter < 0 || (precond == 2 && !fn)) return FVX_ERR_ARG;
   PcgCall c{precond, fn, ctx, flexible, replace_every};
   cudaStream_t st = fvx_stream(stream);
-  return P->dtype == 0 ? pcg_iterate_t<float>(P, (const float*)b, x, it0, niter, c, st)
-                       : pcg_iterate_t<double>(P, (const double*)b, x, it0, niter, c, st);
+  (void)it0;  // the schedule follows the device iteration counter
+  return P->dtype == 0 ? pcg_iterate_t<float>(P, (const float*)b, x, niter, c, st)
+                       : pcg_iterate_t<double>(P, (const double*)b, x, niter, c, st);
 }
 
 // Reads [converged flag, iterations, last |rho|^2]; synchronises the stream.
@@ -1260,6 +1532,17 @@ extern "C" int fvx_pcg_finish(fvx_pcg* P, const void* b, double* x, double bb, d
                        : pcg_finish_t<double>(P, (const double*)b, x, bb, rel_out, st);
 }
 
+// Iterations to run before the next read of the convergence flag: the
+// number the last chunk's residual reduction predicts to reach tol2 (so
+// few iterations run after convergence), between 1 and chunk_max.
+static int pcg_next_chunk(double rr_prev, double rr, int done, double tol2, int chunk_max) {
+  if (!(rr > 0.0) || !(rr_prev > 0.0) || rr >= rr_prev || done < 1) return chunk_max;
+  const double per_it = log(rr / rr_prev) / done;  // < 0
+  const double need = log(tol2 / rr) / per_it;
+  int m = need <= 1.0 ? 1 : (int)ceil(need);
+  return m < 1 ? 1 : (m > chunk_max ? chunk_max : m);
+}
+
 template <typename T>
 static int pcg_run(fvx_pcg* P, const T* b, double* x, int max_iter, double rtol, int precond, fvx_precond_fn fn,
                    void* ctx, int flexible, int replace_every, int chunk, double* info, cudaStream_t st) {
@@ -1273,11 +1556,15 @@ static int pcg_run(fvx_pcg* P, const T* b, double* x, int max_iter, double rtol,
   }
   int it = 0;
   double hs[3] = {0, 0, 0};
+  double rr_prev = bb;
+  int m = chunk < 2 ? chunk : 2;
   while (it < max_iter && hs[0] == 0.0) {
-    const int m = chunk < max_iter - it ? chunk : max_iter - it;
-    if ((rc = pcg_iterate_t<T>(P, b, x, it, m, c, st))) return rc;
+    if (m > max_iter - it) m = max_iter - it;
+    if ((rc = pcg_iterate_t<T>(P, b, x, m, c, st))) return rc;
     it += m;
     if ((rc = fvx_pcg_status(P, hs, st))) return rc;
+    m = pcg_next_chunk(rr_prev, hs[2], m, rtol * rtol * bb, chunk);
+    rr_prev = hs[2];
   }
   double rel = 0;
   if ((rc = pcg_finish_t<T>(P, b, x, bb, &rel, st))) return rc;

@@ -58,16 +58,35 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const int b = blockIdx.z;
   const int x0 = blockIdx.x * T, y0 = blockIdx.y * T;
   const int tid = threadIdx.x;
-  for (int k = tid; k < cin * 9 * COUT; k += NT) {
-    const int co = k % COUT, rest = k / COUT;
-    ws[k] = __bfloat162float(wb[(size_t)co * cin * 9 + rest]);
+  // staging in batches of 8 per thread so the loads overlap
+  const int nw = cin * 9 * COUT;
+  for (int k0 = tid; k0 < nw; k0 += 8 * NT) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k0 + u * NT;
+      const int co = k % COUT, rest = k / COUT;
+      v[u] = k < nw ? __bfloat162float(wb[(size_t)co * cin * 9 + rest]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + u * NT < nw) ws[k0 + u * NT] = v[u];
   }
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
-  for (int k = tid; k < cin * TW * TW; k += NT) {
-    const int ci = k / (TW * TW), r = k - ci * (TW * TW);
-    const int ly = r / TW, lx = r - ly * TW;
-    tile[k] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+  const int nt = cin * TW * TW;
+  for (int k0 = tid; k0 < nt; k0 += 4 * NT) {
+    float v[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = k0 + u * NT;
+      const int ci = k / (TW * TW), r = k - ci * (TW * TW);
+      const int ly = r / TW, lx = r - ly * TW;
+      v[u] = k < nt ? in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (k0 + u * NT < nt) tile[k0 + u * NT] = v[u];
   }
   __syncthreads();
   const int p = tid % (T * T), co0 = (tid / (T * T)) * CPT;

@@ -204,10 +204,15 @@ class LearnedPreconditioner:
     drops the network (zero coarse correction) -- the same method without
     the learned part; ``coarse="mg"`` solves the level-lvl problem by
     ``mg_cycles`` multigrid cycles instead (the exact-coarse-solve limit).
+    ``scale`` multiplies the coarse correction d by the energy-optimal
+    omega = (d . f) / (d . A d), so it never increases the level-lvl error;
+    ``n_smooth`` Jacobi sweeps at level lvl follow it.  Changing these
+    attributes takes effect after ``rebuild()``.
     """
 
     def __init__(self, mg: MultigridSolver, lvl: int | None = None, n_pre: int = 2, n_post: int = 2,
-                 batch_max: int = 32, seed: int = 0, coarse=True, mg_cycles: int = 10):
+                 batch_max: int = 32, seed: int = 0, coarse=True, mg_cycles: int = 10, n_smooth: int = 0,
+                 scale: bool = True):
         if mg.dtype != torch.float32:
             raise ValueError("the learned preconditioner runs on a float32 MultigridSolver")
         self.mg = mg
@@ -215,7 +220,9 @@ class LearnedPreconditioner:
             lvl = max(1, next(k for k in range(mg.n_levels) if mg.level(k)["mask"].numel() <= 128 * 128))
         if not 1 <= lvl < mg.n_levels:
             raise ValueError(f"level {lvl} outside 1 .. {mg.n_levels - 1}")
-        self.lvl, self.n_pre, self.n_post = int(lvl), int(n_pre), int(n_post)
+        self.lvl, self.n_pre, self.n_post, self.n_smooth = int(lvl), int(n_pre), int(n_post), int(n_smooth)
+        self.scale = bool(scale)
+        self._version = 0
         self.m_lvl, self.logc = _level_features(mg, self.lvl)
         h, w = self.m_lvl.shape
         if h % 8 or w % 8:
@@ -240,8 +247,14 @@ class LearnedPreconditioner:
             coarse, ctx = ctypes.cast(fn("fvx_levelsolve_coarse"), ctypes.c_void_p), self._ls
         else:
             coarse, ctx = None, None
-        check(fn("fvx_hybrid_create")(self.mg.handle, I(self.lvl), I(self.n_pre), I(self.n_post), coarse, ctx,
+        check(fn("fvx_hybrid_create")(self.mg.handle, I(self.lvl), I(self.n_pre), I(self.n_post), I(self.n_smooth),
+                                      I(int(self.scale and self.mode != "none")), coarse, ctx,
                                       ctypes.byref(self._hy)), "hybrid_create")
+        self._version += 1
+
+    def rebuild(self):
+        """Apply changed n_pre / n_post / n_smooth / scale."""
+        self._make_hybrid()
 
     def __del__(self):
         for name, dtor in (("_hy", "fvx_hybrid_destroy"), ("_ls", "fvx_levelsolve_destroy")):

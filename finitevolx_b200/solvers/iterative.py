@@ -99,6 +99,17 @@ def masked_laplacian(psi, mask, dx: float, dy: float, lambda_: float = 0.0) -> t
     return out
 
 
+def _next_chunk(rr_prev, rr, done, tol2, chunk_max):
+    """Iterations the last chunk's residual reduction predicts are still
+    needed (1 .. chunk_max), so few iterations run after convergence."""
+    import math
+    if not (rr > 0.0 and rr_prev > 0.0) or rr >= rr_prev or done < 1:
+        return chunk_max
+    per_it = math.log(rr / rr_prev) / done
+    need = math.log(tol2 / rr) / per_it
+    return max(1, min(chunk_max, 1 if need <= 1.0 else math.ceil(need)))
+
+
 PRECOND_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p)
 
 
@@ -160,7 +171,7 @@ class MaskedHelmholtzPCG:
         return 2, cb, None, cb
 
     def solve(self, b, rtol: float = 1e-8, max_iter: int = 500, precond="mg", flexible: bool = False,
-              replace_every: int | None = None, chunk: int = 4, x=None, graph: bool = False):
+              replace_every: int | None = None, chunk: int = 8, x=None, graph: bool = False):
         # float32 work vectors: the recursively updated residual drifts from
         # b - A x by ~eps32 * cond(A) |b|, so recompute it from the FP64
         # iterate (in FP64) every iteration; float64: every 10
@@ -190,20 +201,20 @@ class MaskedHelmholtzPCG:
         bb = ctypes.c_double()
         check(fn("fvx_pcg_begin")(self._h, P(self._gb), P(self._gx), D(rtol), I(kind), cfn, ctx, ctypes.byref(bb),
                                   stream_ptr()), "pcg_begin")
-        key = (kind, getattr(cfn, "value", None), getattr(ctx, "value", None), bool(flexible), replace_every)
+        # the preconditioner object (kept alive by the cache) and its version
+        # identify what the graph captured
+        key = (kind, id(keep) if keep is not None else None, getattr(keep, "_version", 0), bool(flexible),
+               replace_every)
         if key not in self._graphs:
-            # one iteration per replay; the residual-replacement schedule is
-            # kept by capturing replace_every graphs (iteration i mod k)
-            per = max(replace_every, 1)
-            gs = []
+            # one iteration per replay: the iteration counter, the buffer
+            # ping-pong and the residual-replacement schedule live on the
+            # device, so the same launches serve every iteration
             torch.cuda.synchronize()
-            for k in range(per):
-                g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g):
-                    check(fn("fvx_pcg_iterate")(self._h, P(self._gb), P(self._gx), I(k), I(1), I(kind), cfn, ctx,
-                                                I(int(flexible)), I(replace_every), stream_ptr()), "pcg_iterate")
-                gs.append(g)
-            self._graphs[key] = (gs, keep)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                check(fn("fvx_pcg_iterate")(self._h, P(self._gb), P(self._gx), I(0), I(1), I(kind), cfn, ctx,
+                                            I(int(flexible)), I(replace_every), stream_ptr()), "pcg_iterate")
+            self._graphs[key] = ([g], keep)
             # capture does not run the work: restart from the begin state
             check(fn("fvx_pcg_begin")(self._h, P(self._gb), P(self._gx), D(rtol), I(kind), cfn, ctx,
                                       ctypes.byref(bb), stream_ptr()), "pcg_begin")
@@ -211,13 +222,18 @@ class MaskedHelmholtzPCG:
         status = (ctypes.c_double * 3)()
         it = 0
         conv = bb.value == 0.0
+        rr_prev = bb.value
+        tol2 = rtol * rtol * bb.value
+        m = min(chunk, 2)
         while not conv and it < max_iter:
-            m = min(chunk, max_iter - it)
+            m = min(m, max_iter - it)
             for _ in range(m):
-                gs[it % len(gs)].replay()
+                gs[0].replay()
                 it += 1
             check(fn("fvx_pcg_status")(self._h, status, stream_ptr()), "pcg_status")
             conv = status[0] != 0.0
+            m = _next_chunk(rr_prev, status[2], m, tol2, chunk)
+            rr_prev = status[2]
         rel = ctypes.c_double()
         check(fn("fvx_pcg_finish")(self._h, P(self._gb), P(self._gx), D(bb.value), ctypes.byref(rel), stream_ptr()),
               "pcg_finish")

@@ -277,10 +277,12 @@ int fvx_layer_mix_f64(const double* C, int nl, const double* in, double* out, lo
 
 /* ---- learned coarse-grid preconditioner (no counterpart in finitevolX) ---- */
 
-/* Hybrid cycle: the V-cycle's legs on levels 0..lvl-1 with the level-lvl
- * correction from ``coarse`` (NULL = zero). */
-int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
-                         fvx_precond_fn coarse, void* ctx, void* stream);
+/* Hybrid cycle: the V-cycle's legs on levels 0..lvl-1 (fused kernels,
+ * n_pre, n_post <= 16) with the level-lvl correction from ``coarse`` (NULL =
+ * zero), scaled by the energy-optimal omega if ``scale``, followed by
+ * n_smooth Jacobi sweeps at level lvl. */
+int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post, int n_smooth,
+                         int scale, fvx_precond_fn coarse, void* ctx, void* stream);
 /* Downward leg only: f's restricted residual at level lvl into f_lvl. */
 int fvx_mg_restrict_residual(fvx_mg* g, const void* f, int lvl, int n_pre, void* f_lvl, void* stream);
 /* Batched MG solves at level lvl, one CTA per right-hand side. */
@@ -295,8 +297,8 @@ int fvx_levelsolve_destroy(fvx_levelsolve* s);
 int fvx_levelsolve_coarse(void* ctx, const void* f, void* u, void* stream);
 /* The hybrid cycle as an fvx_precond_fn (ctx = the fvx_hybrid object). */
 typedef struct fvx_hybrid fvx_hybrid;
-int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, fvx_precond_fn coarse, void* ctx,
-                      fvx_hybrid** out);
+int fvx_hybrid_create(fvx_mg* g, int lvl, int n_pre, int n_post, int n_smooth, int scale, fvx_precond_fn coarse,
+                      void* ctx, fvx_hybrid** out);
 int fvx_hybrid_destroy(fvx_hybrid* h);
 int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* stream);
 
