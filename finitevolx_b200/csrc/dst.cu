@@ -58,6 +58,7 @@ struct Epi {
   const double* inv_eig64;
   int n_eig;               // batch b uses grid b % n_eig
   int* err;
+  int perm_r = 0;          // store r at its even/odd de-interleaved position (the next product's layout)
 };
 
 // ---- PTX helpers ----------------------------------------------------------
@@ -138,8 +139,13 @@ constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN 
                             ((uint32_t)(BM >> 4) << 24);
 
 // ---- epilogue store ---------------------------------------------------------
+// Position of index r in the even/odd de-interleaved layout of a length-R
+// axis: evens first (r / 2), then odds (R / 2 + r / 2).
+DEV int deinterleave(int r, int R) { return (r & 1) ? (R >> 1) + (r >> 1) : (r >> 1); }
+
 DEV void epi_store(const Epi& ep, int b, int r, int n, float acc) {
-  long long idx = (long long)b * ep.batch_stride + (long long)(n + ep.off_n) * ep.ld + (r + ep.off_r);
+  const int rs = ep.perm_r ? deinterleave(r, ep.rows_per_batch) : r;
+  long long idx = (long long)b * ep.batch_stride + (long long)(n + ep.off_n) * ep.ld + (rs + ep.off_r);
   switch (ep.mode) {
     case EPI_SPLIT: {
       float x = acc * (float)ep.alpha;
@@ -266,6 +272,134 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
   }
 }
 
+// ---- even/odd DST-I product ---------------------------------------------------
+// S[N-1-j][k] = (-1)^k S[j][k] and S is symmetric, so for C = X S (N even)
+//   P[:, k] = sum_{j even} X[:, j] S[j, k],  Q[:, k] = sum_{j odd} X[:, j] S[j, k]
+//   C[:, k] = P + Q,  C[:, N-1-k] = P - Q      (k < N/2)
+// which halves the multiply work.  X arrives with its columns de-interleaved
+// (evens then odds), so the even and odd halves are plain column ranges of
+// one TMA tensor; B_P[k][j'] = S[2j'][k] and B_Q[k][j'] = S[2j'+1][k] are
+// N/2 x N/2 K-major tables.  Each CTA owns a 128-row x 128-k tile of P and
+// of Q (TMEM columns 0-127 and 128-255); the k loop alternates P and Q
+// blocks through a 3-stage TMA ring of 64 KiB stages.
+constexpr int SBN = 128, SSTAGES = 3;
+constexpr int S_A_TILE = BM * BK * 2;                       // 16 KiB
+constexpr int S_B_TILE = SBN * BK * 2;                      // 16 KiB
+constexpr int S_STAGE = 2 * S_A_TILE + 2 * S_B_TILE;        // 64 KiB
+constexpr int S_SMEM = SSTAGES * S_STAGE + 1024 + 256;
+constexpr uint32_t kIdesc128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SBN >> 3) << 17) |
+                               ((uint32_t)(BM >> 4) << 24);
+
+__global__ void __launch_bounds__(THREADS, 1)
+gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                     const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
+                     const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl, int K,
+                     Epi ep) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + SSTAGES * S_STAGE);  // full[S], empty[S], acc
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * SSTAGES + 1);
+  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * SBN;
+  const int KH = K >> 1;
+  const int KT = 2 * ((KH + BK - 1) / BK);  // P and Q blocks alternate
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[SSTAGES + s]); };
+  const uint32_t accb = smem_u32(&bars[2 * SSTAGES]);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < SSTAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
+    mbar_init(accb, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * SBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0 && lane == 0) {
+    for (int kt = 0; kt < KT; ++kt) {
+      const int s = kt % SSTAGES;
+      if (kt >= SSTAGES && !mbar_wait(empty(s), ((kt / SSTAGES) - 1) & 1, abort_flag, ep.err)) break;
+      mbar_expect_tx(full(s), S_STAGE);
+      const uint32_t base = smem_u32(smem + s * S_STAGE);
+      const int kb = kt >> 1;
+      const bool odd = kt & 1;
+      const int ac = (odd ? KH : 0) + kb * BK;
+      tma_load_2d(base, &mAh, full(s), ac, m0);
+      tma_load_2d(base + S_A_TILE, &mAl, full(s), ac, m0);
+      tma_load_2d(base + 2 * S_A_TILE, odd ? &mQh : &mPh, full(s), kb * BK, n0);
+      tma_load_2d(base + 2 * S_A_TILE + S_B_TILE, odd ? &mQl : &mPl, full(s), kb * BK, n0);
+    }
+  } else if (warp == 1 && lane == 0) {
+    bool ok = true;
+    for (int kt = 0; kt < KT && ok; ++kt) {
+      const int s = kt % SSTAGES;
+      ok = mbar_wait(full(s), (kt / SSTAGES) & 1, abort_flag, ep.err);
+      if (!ok) break;
+      tc_fence_after();
+      const uint32_t base = smem_u32(smem + s * S_STAGE);
+      const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + S_A_TILE);
+      const uint64_t bh = sdesc_sw128(base + 2 * S_A_TILE), bl = sdesc_sw128(base + 2 * S_A_TILE + S_B_TILE);
+      const int kb = kt >> 1;
+      const uint32_t d = tmem + ((kt & 1) ? (uint32_t)SBN : 0u);
+#pragma unroll
+      for (int kk = 0; kk < BK / 16; ++kk) {
+        const uint64_t o = (uint64_t)(kk * 32 >> 4);
+        umma_bf16(d, ah + o, bh + o, kIdesc128, (kb | kk) != 0);
+        umma_bf16(d, ah + o, bl + o, kIdesc128, 1u);
+        umma_bf16(d, al + o, bh + o, kIdesc128, 1u);
+      }
+      umma_commit(empty(s));
+    }
+    umma_commit(accb);
+  } else if (warp >= 2) {
+    const int wq = warp & 3;
+    const int row = wq * 32 + lane;
+    const int m = m0 + row;
+    const bool mvalid = m < ep.m_total;
+    const int b = mvalid ? m / ep.rows_per_batch : 0;
+    const int r = mvalid ? m - b * ep.rows_per_batch : 0;
+    if (mbar_wait(accb, 0, abort_flag, ep.err)) {
+      tc_fence_after();
+      if (!*abort_flag) {
+#pragma unroll 1
+        for (int c0 = 0; c0 < SBN; c0 += 32) {
+          uint32_t vp[32], vq[32];
+          const uint32_t lanes = (uint32_t)(wq * 32) << 16;
+          tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
+          tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+          tmem_wait_ld();
+          if (mvalid) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int k = n0 + c0 + j;
+              if (k < KH) {
+                const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
+                epi_store(ep, b, r, k, P + Q);
+                epi_store(ep, b, r, K - 1 - k, P - Q);
+              }
+            }
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * SBN));
+  }
+}
+
 // ---- FP64 SIMT GEMM with the same transposed-store epilogue (correctness path)
 constexpr int DT = 64, DK = 16;
 __global__ void __launch_bounds__(256)
@@ -318,9 +452,12 @@ gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict_
 }
 
 // ---- input split / copy / residual kernels ---------------------------------
+// perm: store x at its de-interleaved position (the even/odd product's
+// operand layout).
 template <typename T>
 __global__ void split_input_kernel(const T* __restrict__ in, long long bstride, long long ld, int ny, int nx,
-                                   int batch, bf16* __restrict__ hi, bf16* __restrict__ lo, double scale) {
+                                   int batch, bf16* __restrict__ hi, bf16* __restrict__ lo, double scale,
+                                   int perm = 0) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = (long long)batch * ny * nx;
   for (; k < n; k += (long long)gridDim.x * blockDim.x) {
@@ -329,8 +466,9 @@ __global__ void split_input_kernel(const T* __restrict__ in, long long bstride, 
     int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
     float v = (float)((double)in[b * bstride + (long long)y * ld + x] * scale);
     bf16 h = __float2bfloat16_rn(v);
-    hi[k] = h;
-    lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+    const long long o = perm ? k - x + deinterleave(x, nx) : k;
+    hi[o] = h;
+    lo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
   }
 }
 
@@ -371,7 +509,7 @@ template <typename T>
 __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long fld, const double* __restrict__ psi,
                                 long long pb, long long pld, int ny, int nx, int batch, double dx, double dy,
                                 const double* __restrict__ lam, int nlam, bf16* __restrict__ hi,
-                                bf16* __restrict__ lo, double* norms) {
+                                bf16* __restrict__ lo, double* norms, int perm) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long n = (long long)batch * ny * nx;
   double s_r = 0, s_f = 0, s_p = 0;
@@ -389,8 +527,9 @@ __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long
     double r = fv - (lap - lam[b % nlam] * c);
     float rv = (float)r;
     bf16 h = __float2bfloat16_rn(rv);
-    hi[k] = h;
-    lo[k] = __float2bfloat16_rn(rv - __bfloat162float(h));
+    const long long o = perm ? k - x + deinterleave(x, nx) : k;
+    hi[o] = h;
+    lo[o] = __float2bfloat16_rn(rv - __bfloat162float(h));
     s_r += r * r;
     s_f += fv * fv;
     s_p += c * c;
@@ -454,6 +593,29 @@ static int gemm_split(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* 
   return fvx_cuda_status();
 }
 
+// C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns
+// de-interleaved; P/Q: the [K/2][K/2] hi/lo tables.  Needs K % 256 == 0.
+static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph, const bf16* Pl, const bf16* Qh,
+                    const bf16* Ql, const Epi& ep, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    if (cudaFuncSetAttribute(gemm_sym_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S_SMEM) !=
+        cudaSuccess)
+      return FVX_ERR_CUDA;
+    attr_set = true;
+  }
+  if (K % (2 * SBN) != 0) return FVX_ERR_SHAPE;
+  const int KH = K / 2;
+  CUtensorMap a_h, a_l, p_h, p_l, q_h, q_l;
+  if (!make_map(&a_h, Xh, K, M, BM) || !make_map(&a_l, Xl, K, M, BM) || !make_map(&p_h, Ph, KH, KH, SBN) ||
+      !make_map(&p_l, Pl, KH, KH, SBN) || !make_map(&q_h, Qh, KH, KH, SBN) || !make_map(&q_l, Ql, KH, KH, SBN))
+    return FVX_ERR_ARG;
+  dim3 grid(KH / SBN, (M + BM - 1) / BM);
+  if (grid.y > 65535) return FVX_ERR_SHAPE;
+  gemm_sym_bf16_kernel<<<grid, THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, K, ep);
+  return fvx_cuda_status();
+}
+
 static int gemm_f64(const double* A, int lda, int M, int K, const double* S, int N, const Epi& ep, cudaStream_t st) {
   dim3 grid((N + DT - 1) / DT, (M + DT - 1) / DT);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
@@ -479,6 +641,9 @@ struct fvx_dst_plan {
   std::vector<double> lam_host;
   double* lam_dev = nullptr;
   bf16 *Sxh = nullptr, *Sxl = nullptr, *Syh = nullptr, *Syl = nullptr;
+  bool sym = false;  // even/odd products (nx, ny multiples of 256); operands x/y de-interleaved
+  bf16 *xPh = nullptr, *xPl = nullptr, *xQh = nullptr, *xQl = nullptr;  // [nx/2][nx/2]
+  bf16 *yPh = nullptr, *yPl = nullptr, *yQh = nullptr, *yQl = nullptr;  // [ny/2][ny/2]
   double *Sx64 = nullptr, *Sy64 = nullptr;
   float* inv32 = nullptr;   // [n_lam][ny][nx]
   double* inv64 = nullptr;  // [n_lam][ny][nx]
@@ -490,7 +655,8 @@ struct fvx_dst_plan {
 
 static void dst_free(fvx_dst_plan* p) {
   void* ptrs[] = {p->lam_dev, p->Sxh, p->Sxl, p->Syh, p->Syl, p->Sx64, p->Sy64, p->inv32, p->inv64,
-                  p->W1h,     p->W1l, p->W2h, p->W2l, p->V1,  p->V2,  p->norms, p->err};
+                  p->W1h,     p->W1l, p->W2h, p->W2l, p->V1,  p->V2,  p->norms, p->err,
+                  p->xPh,     p->xPl, p->xQh, p->xQl, p->yPh, p->yPl, p->yQh,   p->yQl};
   for (void* q : ptrs)
     if (q) cudaFree(q);
 }
@@ -504,6 +670,7 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
   p->ny = ny; p->nx = nx; p->dx = dx; p->dy = dy; p->batch_max = batch_max; p->n_lam = n_lambda;
   p->lam_host.assign(lambdas, lambdas + n_lambda);
   p->split_ok = (nx % 8 == 0) && (ny % 8 == 0);
+  p->sym = p->split_ok && nx % (2 * SBN) == 0 && ny % (2 * SBN) == 0;
   const size_t plane = (size_t)ny * nx, work = plane * batch_max;
   bool ok = true;
   auto A = [&](void** q, size_t bytes) { if (ok && cudaMalloc(q, bytes) != cudaSuccess) ok = false; };
@@ -519,6 +686,13 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
     A((void**)&p->Syh, sizeof(bf16) * ny * ny); A((void**)&p->Syl, sizeof(bf16) * ny * ny);
     A((void**)&p->W1h, sizeof(bf16) * work); A((void**)&p->W1l, sizeof(bf16) * work);
     A((void**)&p->W2h, sizeof(bf16) * work); A((void**)&p->W2l, sizeof(bf16) * work);
+  }
+  if (p->sym) {
+    const size_t hx = (size_t)(nx / 2) * (nx / 2), hy = (size_t)(ny / 2) * (ny / 2);
+    A((void**)&p->xPh, sizeof(bf16) * hx); A((void**)&p->xPl, sizeof(bf16) * hx);
+    A((void**)&p->xQh, sizeof(bf16) * hx); A((void**)&p->xQl, sizeof(bf16) * hx);
+    A((void**)&p->yPh, sizeof(bf16) * hy); A((void**)&p->yPl, sizeof(bf16) * hy);
+    A((void**)&p->yQh, sizeof(bf16) * hy); A((void**)&p->yQl, sizeof(bf16) * hy);
   }
   if (want_fp64 || !p->split_ok) {
     A((void**)&p->V1, sizeof(double) * work);
@@ -571,6 +745,27 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
     split(Sy, h, l);
     cudaMemcpy(p->Syh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(p->Syl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+    if (p->sym) {
+      // B_P[k][j'] = S[2j'][k], B_Q[k][j'] = S[2j'+1][k] for k, j' < n/2
+      auto halves = [&](const std::vector<double>& S, int n, bf16* Ph, bf16* Pl, bf16* Qh, bf16* Ql) {
+        const int hn = n / 2;
+        std::vector<double> P((size_t)hn * hn), Q((size_t)hn * hn);
+        for (int k = 0; k < hn; ++k)
+          for (int j = 0; j < hn; ++j) {
+            P[(size_t)k * hn + j] = S[(size_t)(2 * j) * n + k];
+            Q[(size_t)k * hn + j] = S[(size_t)(2 * j + 1) * n + k];
+          }
+        std::vector<bf16> hh, ll;
+        split(P, hh, ll);
+        cudaMemcpy(Ph, hh.data(), sizeof(bf16) * hh.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(Pl, ll.data(), sizeof(bf16) * ll.size(), cudaMemcpyHostToDevice);
+        split(Q, hh, ll);
+        cudaMemcpy(Qh, hh.data(), sizeof(bf16) * hh.size(), cudaMemcpyHostToDevice);
+        cudaMemcpy(Ql, ll.data(), sizeof(bf16) * ll.size(), cudaMemcpyHostToDevice);
+      };
+      halves(Sx, nx, p->xPh, p->xPl, p->xQh, p->xQl);
+      halves(Sy, ny, p->yPh, p->yPl, p->yQh, p->yQl);
+    }
   }
   cudaMemset(p->err, 0, sizeof(int));
   if (cudaDeviceSynchronize() != cudaSuccess) { dst_free(p); delete p; return FVX_ERR_CUDA; }
@@ -615,6 +810,19 @@ static int chain_split(fvx_dst_plan* p, int B, int out_mode, void* out, long lon
   const int ny = p->ny, nx = p->nx;
   const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
   int rc;
+  if (p->sym) {
+    // even/odd products; every intermediate is stored de-interleaved along
+    // the next product's contraction axis, the result in natural order
+    Epi e1 = make_epi(p, EPI_SPLIT, ny, B * ny, nx, p->W2h, p->W2l, (long long)nx * ny, ny, 0, 0, 1.0, false);
+    e1.perm_r = 1;
+    if ((rc = gemm_sym(p->W1h, p->W1l, B * ny, nx, p->xPh, p->xPl, p->xQh, p->xQl, e1, st))) return rc;
+    Epi e2 = make_epi(p, EPI_SPLIT, nx, B * nx, ny, p->W1h, p->W1l, (long long)ny * nx, nx, 0, 0, 1.0, true);
+    e2.perm_r = 1;
+    if ((rc = gemm_sym(p->W2h, p->W2l, B * nx, ny, p->yPh, p->yPl, p->yQh, p->yQl, e2, st))) return rc;
+    if ((rc = gemm_sym(p->W1h, p->W1l, B * ny, nx, p->xPh, p->xPl, p->xQh, p->xQl, e1, st))) return rc;
+    Epi e4 = make_epi(p, out_mode, nx, B * nx, ny, out, nullptr, ob, old, 0, 0, c, false);
+    return gemm_sym(p->W2h, p->W2l, B * nx, ny, p->yPh, p->yPl, p->yQh, p->yQl, e4, st);
+  }
   // 1: (Q S_x)^T -> W2 [B][nx][ny]
   Epi e1 = make_epi(p, EPI_SPLIT, ny, B * ny, nx, p->W2h, p->W2l, (long long)nx * ny, ny, 0, 0, 1.0, false);
   if ((rc = gemm_split(p->W1h, p->W1l, B * ny, nx, p->Sxh, p->Sxl, nx, e1, st))) return rc;
@@ -657,7 +865,7 @@ extern "C" int fvx_dst_solve_f32(fvx_dst_plan* p, const float* rhs, long long rh
     return chain_f64(p, batch, EPI_F32, psi, psi_bstride, psi_ld, st);
   }
   split_input_kernel<float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, p->ny, p->nx, batch, p->W1h,
-                                                        p->W1l, 1.0);
+                                                        p->W1l, 1.0, p->sym ? 1 : 0);
   int rc = fvx_cuda_status();
   if (rc) return rc;
   return chain_split(p, batch, EPI_F32, psi, psi_bstride, psi_ld, st);
@@ -671,6 +879,12 @@ extern "C" int fvx_dst_solve_presplit_f32(fvx_dst_plan* p, float* psi, long long
   if (batch < 1 || batch > p->batch_max || !p->split_ok) return FVX_ERR_SHAPE;
   return chain_split(p, batch, EPI_F32, psi, psi_bstride, psi_ld, fvx_stream(stream));
 }
+
+// Layout of the chain's first operand (the fvx_dst_workspace buffers): 0
+// natural [b][y][x]; 1 x de-interleaved, x stored at x / 2 (even x) or
+// nx / 2 + x / 2 (odd x) -- the even/odd products of plans whose ny and nx
+// are multiples of 256.
+extern "C" int fvx_dst_operand_layout(fvx_dst_plan* p) { return p ? (p->sym ? 1 : 0) : -1; }
 
 extern "C" int fvx_dst_workspace(fvx_dst_plan* p, void** w1_hi, void** w1_lo) {
   if (!p || !w1_hi || !w1_lo) return FVX_ERR_ARG;
@@ -705,7 +919,8 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
   for (double l : p->lam_host) lam_max = fmax(lam_max, fabs(l));
   const double anorm = 4.0 / (p->dx * p->dx) + 4.0 / (p->dy * p->dy) + lam_max;
   zero_f64_kernel<<<grid1d(n), 256, 0, st>>>(psi, psi_bstride, psi_ld, ny, nx, batch);
-  split_input_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->W1h, p->W1l, 1.0);
+  split_input_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->W1h, p->W1l, 1.0,
+                                                         p->sym ? 1 : 0);
   if ((rc = fvx_cuda_status())) return rc;
   double be = 1, rr = 1;
   int it = 0;
@@ -714,7 +929,7 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
     cudaMemsetAsync(p->norms, 0, sizeof(double) * 4, st);
     residual_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
                                                         batch, p->dx, p->dy, p->lam_dev, p->n_lam, p->W1h, p->W1l,
-                                                        p->norms);
+                                                        p->norms, p->sym ? 1 : 0);
     double h[4];
     if (cudaMemcpyAsync(h, p->norms, sizeof(h), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
@@ -738,10 +953,18 @@ extern "C" int fvx_dst_gemm_step(fvx_dst_plan* p, int which, int batch, void* st
   cudaStream_t st = fvx_stream(stream);
   if (which == 0) {
     Epi e1 = make_epi(p, EPI_SPLIT, ny, batch * ny, nx, p->W2h, p->W2l, (long long)nx * ny, ny, 0, 0, 1.0, false);
+    if (p->sym) {
+      e1.perm_r = 1;
+      return gemm_sym(p->W1h, p->W1l, batch * ny, nx, p->xPh, p->xPl, p->xQh, p->xQl, e1, st);
+    }
     return gemm_split(p->W1h, p->W1l, batch * ny, nx, p->Sxh, p->Sxl, nx, e1, st);
   }
   if (which == 1) {
     Epi e2 = make_epi(p, EPI_SPLIT, nx, batch * nx, ny, p->W1h, p->W1l, (long long)ny * nx, nx, 0, 0, 1.0, true);
+    if (p->sym) {
+      e2.perm_r = 1;
+      return gemm_sym(p->W2h, p->W2l, batch * nx, ny, p->yPh, p->yPl, p->yQh, p->yQl, e2, st);
+    }
     return gemm_split(p->W2h, p->W2l, batch * nx, ny, p->Syh, p->Syl, ny, e2, st);
   }
   return FVX_ERR_ARG;

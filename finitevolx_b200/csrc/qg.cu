@@ -37,6 +37,7 @@ struct StageArgs {
   void* out;           // [Ny][Nx]
   __nv_bfloat16* split_hi;  // [Ny-2][Nx-2] or null
   __nv_bfloat16* split_lo;
+  int split_layout;         // 1: x de-interleaved (the even/odd DST operand layout)
   int ny, nx;
   double a, b, c;      // out = a*qn + b*qs + c*rhs
   double dx, dy, beta, drag, visc;
@@ -167,7 +168,8 @@ stage_kernel(StageArgs A) {
     r = r + cc * rhs;
     out[g] = r;
     if (A.split_hi) {
-      size_t s = (size_t)(gj - 1) * nxi + (gi - 1);
+      const int xi = gi - 1;
+      size_t s = (size_t)(gj - 1) * nxi + (A.split_layout ? ((xi & 1) ? (nxi >> 1) + (xi >> 1) : (xi >> 1)) : xi);
       float fv = (float)r;
       __nv_bfloat16 h = __float2bfloat16_rn(fv);
       A.split_hi[s] = h;
@@ -239,7 +241,8 @@ using namespace fvx;
 
 #define FVX_DEF_QG(SFX, T)                                                                                   \
   extern "C" int fvx_qg_stage_##SFX(const T* q_stage, const T* q_start, const T* psi_interior,             \
-                                    const T* forcing, T* q_out, void* split_hi, void* split_lo, int ny, int nx, \
+                                    const T* forcing, T* q_out, void* split_hi, void* split_lo,              \
+                                    int split_layout, int ny, int nx,                                        \
                                     double dx, double dy, double beta, double drag, double viscosity,       \
                                     double a, double b, double c, int method, int periodic, int write_ghost, \
                                     void* stream) {                                                          \
@@ -249,6 +252,7 @@ using namespace fvx;
     qg::StageArgs A;                                                                                         \
     A.qs = q_stage; A.qn = q_start; A.psi = psi_interior; A.forcing = forcing; A.out = q_out;              \
     A.split_hi = (__nv_bfloat16*)split_hi; A.split_lo = (__nv_bfloat16*)split_lo;                          \
+    A.split_layout = split_layout;                                                                           \
     A.ny = ny; A.nx = nx; A.a = a; A.b = b; A.c = c; A.dx = dx; A.dy = dy; A.beta = beta;                    \
     A.drag = drag; A.visc = viscosity; A.periodic = periodic; A.write_ghost = write_ghost;                   \
     return qg::dispatch<T>(method, A, fvx_stream(stream));                                                   \

@@ -53,8 +53,10 @@ class QGModel:
         self.forcing = None if forcing is None else L.as_field(forcing, dtype=dtype)
         hi, lo = ctypes.c_void_p(), ctypes.c_void_p()
         self._fused_split = dtype == torch.float32 and self.plan.split_ok
+        self._layout = 0
         if self._fused_split:
             check(fn("fvx_dst_workspace")(self.plan.handle, ctypes.byref(hi), ctypes.byref(lo)), "workspace")
+            self._layout = fn("fvx_dst_operand_layout")(self.plan.handle)
         self._w1 = (hi, lo)
         self.kernel_launches = 0
 
@@ -80,7 +82,8 @@ class QGModel:
     def _stage(self, qs, qn, out, a, b, c, split, write_ghost):
         g = self.grid
         hi, lo = self._w1 if split else (ctypes.c_void_p(0), ctypes.c_void_p(0))
-        check(fn(f"fvx_qg_stage_{sfx(qs)}")(P(qs), P(qn), P(self.psi), P(self.forcing), P(out), hi, lo, I(g.Ny),
+        check(fn(f"fvx_qg_stage_{sfx(qs)}")(P(qs), P(qn), P(self.psi), P(self.forcing), P(out), hi, lo,
+                                            I(self._layout if split else 0), I(g.Ny),
                                             I(g.Nx), D(g.dx), D(g.dy), D(self.beta), D(self.drag), D(self.visc),
                                             D(a), D(b), D(c), I(SCHEMES[self.method]),
                                             I(1 if self.bc == "periodic" else 0), I(int(write_ghost)),

@@ -175,10 +175,13 @@ int fvx_dst_solve_f64(fvx_dst_plan* plan, const double* rhs, long long rhs_bstri
                       long long psi_bstride, long long psi_ld, int batch, int method, double tol, int max_iter,
                       double* info, void* stream);
 /* Same chain on an operand already split into the plan workspace (written
- * by fvx_qg_stage_f32's split outputs); fvx_dst_workspace returns it. */
+ * by fvx_qg_stage_f32's split outputs); fvx_dst_workspace returns it and
+ * fvx_dst_operand_layout its layout (0 natural, 1 x de-interleaved: the
+ * even/odd products of plans with ny, nx multiples of 256). */
 int fvx_dst_solve_presplit_f32(fvx_dst_plan* plan, float* psi, long long psi_bstride, long long psi_ld, int batch,
                                void* stream);
 int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
+int fvx_dst_operand_layout(fvx_dst_plan* plan);
 /* One product of the chain on the current workspaces (timing only). */
 int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
 
@@ -205,15 +208,17 @@ int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, float* psi, lo
  * - drag*laplacian(psi) + viscosity*laplacian(BC(q_stage)), (u, v) the
  * geostrophic velocity of psi_interior (zero outside).  periodic: 1 periodic
  * ghost ring, 0 zero ring.  write_ghost refills q_out's ring.  split_hi/lo
- * (bf16 [ny-2][nx-2], may be NULL) receive q_out's interior for the next DST.
+ * (bf16 [ny-2][nx-2], may be NULL) receive q_out's interior for the next DST,
+ * in the layout split_layout (fvx_dst_operand_layout of the plan).
  * method: 1 upwind1, 3 upwind3, 4 weno3, 5 weno5, 6 wenoz5, 7 weno7,
  * 8 weno9, 9 minmod, 10 van_leer. */
 int fvx_qg_stage_f32(const float* q_stage, const float* q_start, const float* psi_interior, const float* forcing,
-                     float* q_out, void* split_hi, void* split_lo, int ny, int nx, double dx, double dy,
+                     float* q_out, void* split_hi, void* split_lo, int split_layout, int ny, int nx, double dx,
+                     double dy,
                      double beta, double drag, double viscosity, double a, double b, double c, int method,
                      int periodic, int write_ghost, void* stream);
 int fvx_qg_stage_f64(const double* q_stage, const double* q_start, const double* psi_interior,
-                     const double* forcing, double* q_out, void* split_hi, void* split_lo, int ny, int nx,
+                     const double* forcing, double* q_out, void* split_hi, void* split_lo, int split_layout, int ny, int nx,
                      double dx, double dy, double beta, double drag, double viscosity, double a, double b,
                      double c, int method, int periodic, int write_ghost, void* stream);
 

@@ -31,7 +31,9 @@ def rel_err(a, b):
     return np.abs(np.asarray(a, np.float64) - b).max() / max(np.abs(b).max(), 1e-300)
 
 
-@pytest.mark.parametrize("shape,lam", [((128, 128), 0.0), ((256, 128), 3.0), ((64, 192), 50.0)])
+# (256, 512), (512, 256): multiples of 256, the even/odd (half-work) products
+@pytest.mark.parametrize("shape,lam", [((128, 128), 0.0), ((256, 128), 3.0), ((64, 192), 50.0),
+                                       ((256, 512), 2.0), ((512, 256), 0.0)])
 def test_dst_split_bf16_chain(cuda_ok, shape, lam):
     ny, nx = shape
     f = O.kminus3_field(ny, nx, 3)
@@ -39,6 +41,8 @@ def test_dst_split_bf16_chain(cuda_ok, shape, lam):
     got = solve_helmholtz_dst(dev(f, torch.float32), 0.05, 0.07, lam)
     plan = DSTHelmholtzPlan(ny, nx, 0.05, 0.07, (lam,))
     plan.check_device()
+    from finitevolx_b200._lib import fn
+    assert fn("fvx_dst_operand_layout")(plan.handle) == int(ny % 256 == 0 and nx % 256 == 0)
     e = rel_err(host(got), ref)
     assert e < 1e-4, e
 
