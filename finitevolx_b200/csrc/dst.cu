@@ -25,6 +25,7 @@
 #include <cuda_bf16.h>
 
 #include <cmath>
+#include <cstring>
 #include <cstdio>
 #include <vector>
 
@@ -59,6 +60,7 @@ struct Epi {
   int n_eig;               // batch b uses grid b % n_eig
   int* err;
   int perm_r = 0;          // store r at its even/odd de-interleaved position (the next product's layout)
+  int tma_out = 0;         // even/odd kernel: stage the tile in shared memory, TMA bulk-tensor stores
 };
 
 // ---- PTX helpers ----------------------------------------------------------
@@ -101,6 +103,16 @@ DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0,
           dst),
       "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1)
       : "memory");
+}
+DEV void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1, int c2) {
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                   (uint64_t)map),
+               "r"(src), "r"(c0), "r"(c1), "r"(c2)
+               : "memory");
+}
+DEV void tma_store_commit_wait() {
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
 DEV void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
   asm volatile(
@@ -204,6 +216,9 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  // CTAs start their K loop at different blocks so the ones that share an
+  // A or B tile do not all read the same L2 lines at the same time
+  const int kshift = (int)((blockIdx.x * 5u + blockIdx.y * 3u) % (unsigned)KT);
   if (warp == 0 && lane == 0) {
     // TMA producer
     for (int kt = 0; kt < KT; ++kt) {
@@ -211,10 +226,11 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
       if (kt >= STAGES && !mbar_wait(empty(s), ((kt / STAGES) - 1) & 1, abort_flag, ep.err)) break;
       mbar_expect_tx(full(s), STAGE_BYTES);
       const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
-      tma_load_2d(base, &mAh, full(s), kt * BK, m0);
-      tma_load_2d(base + A_TILE, &mAl, full(s), kt * BK, m0);
-      tma_load_2d(base + 2 * A_TILE, &mBh, full(s), kt * BK, n0);
-      tma_load_2d(base + 2 * A_TILE + B_TILE, &mBl, full(s), kt * BK, n0);
+      const int kc = ((kt + kshift) % KT) * BK;
+      tma_load_2d(base, &mAh, full(s), kc, m0);
+      tma_load_2d(base + A_TILE, &mAl, full(s), kc, m0);
+      tma_load_2d(base + 2 * A_TILE, &mBh, full(s), kc, n0);
+      tma_load_2d(base + 2 * A_TILE + B_TILE, &mBl, full(s), kc, n0);
     }
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: three split products per 16-wide K step
@@ -293,7 +309,8 @@ constexpr uint32_t kIdesc128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(
 __global__ void __launch_bounds__(THREADS, 1)
 gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                      const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
-                     const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl, int K,
+                     const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl,
+                     const __grid_constant__ CUtensorMap mO0, const __grid_constant__ CUtensorMap mO1, int K,
                      Epi ep) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -324,12 +341,15 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
+  // staggered start (an even shift keeps the P / Q alternation)
+  const int kshift = 2 * (int)((blockIdx.x * 5u + blockIdx.y * 3u) % (unsigned)(KT / 2));
   if (warp == 0 && lane == 0) {
-    for (int kt = 0; kt < KT; ++kt) {
-      const int s = kt % SSTAGES;
-      if (kt >= SSTAGES && !mbar_wait(empty(s), ((kt / SSTAGES) - 1) & 1, abort_flag, ep.err)) break;
+    for (int kt0 = 0; kt0 < KT; ++kt0) {
+      const int s = kt0 % SSTAGES;
+      if (kt0 >= SSTAGES && !mbar_wait(empty(s), ((kt0 / SSTAGES) - 1) & 1, abort_flag, ep.err)) break;
       mbar_expect_tx(full(s), S_STAGE);
       const uint32_t base = smem_u32(smem + s * S_STAGE);
+      const int kt = (kt0 + kshift) % KT;
       const int kb = kt >> 1;
       const bool odd = kt & 1;
       const int ac = (odd ? KH : 0) + kb * BK;
@@ -340,20 +360,21 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
-    for (int kt = 0; kt < KT && ok; ++kt) {
-      const int s = kt % SSTAGES;
-      ok = mbar_wait(full(s), (kt / SSTAGES) & 1, abort_flag, ep.err);
+    for (int kt0 = 0; kt0 < KT && ok; ++kt0) {
+      const int s = kt0 % SSTAGES;
+      ok = mbar_wait(full(s), (kt0 / SSTAGES) & 1, abort_flag, ep.err);
       if (!ok) break;
       tc_fence_after();
       const uint32_t base = smem_u32(smem + s * S_STAGE);
       const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + S_A_TILE);
       const uint64_t bh = sdesc_sw128(base + 2 * S_A_TILE), bl = sdesc_sw128(base + 2 * S_A_TILE + S_B_TILE);
-      const int kb = kt >> 1;
+      const int kt = (kt0 + kshift) % KT;
       const uint32_t d = tmem + ((kt & 1) ? (uint32_t)SBN : 0u);
+      const bool first = kt0 < 2;  // the first P block and the first Q block overwrite
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk) {
         const uint64_t o = (uint64_t)(kk * 32 >> 4);
-        umma_bf16(d, ah + o, bh + o, kIdesc128, (kb | kk) != 0);
+        umma_bf16(d, ah + o, bh + o, kIdesc128, !(first && kk == 0));
         umma_bf16(d, ah + o, bl + o, kIdesc128, 1u);
         umma_bf16(d, al + o, bh + o, kIdesc128, 1u);
       }
@@ -367,8 +388,77 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
     const bool mvalid = m < ep.m_total;
     const int b = mvalid ? m / ep.rows_per_batch : 0;
     const int r = mvalid ? m - b * ep.rows_per_batch : 0;
-    if (mbar_wait(accb, 0, abort_flag, ep.err)) {
-      tc_fence_after();
+    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+    if (ok) tc_fence_after();
+    if (ep.tma_out) {
+      // Tile staged in the idle operand ring (all MMAs have completed), then
+      // written by TMA bulk-tensor stores.  The host enables this only when
+      // R is a multiple of 128 and the outputs satisfy TMA's alignment, so
+      // the tile has one batch index b and starts at an even r0.
+      const int R = ep.rows_per_batch;
+      const int bb = m0 / R, r0 = m0 - bb * R;
+      const int be = bb % ep.n_eig;
+      const bool go = ok && !*abort_flag;
+      if (go) {
+        const float alpha = (float)ep.alpha;
+        const int half = row & 1, rl = row >> 1;
+#pragma unroll 1
+        for (int c0 = 0; c0 < SBN; c0 += 32) {
+          uint32_t vp[32], vq[32];
+          const uint32_t lanes = (uint32_t)(wq * 32) << 16;
+          tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
+          tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int kl = c0 + j, k = n0 + kl;
+            const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
+            float xp = (P + Q) * alpha, xm = (P - Q) * alpha;
+            if (ep.inv_eig) {
+              const float* ie = ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row);
+              xp *= ie[(long long)k * R];
+              xm *= ie[(long long)(K - 1 - k) * R];
+            }
+            if (ep.mode == EPI_SPLIT) {
+              // boxes [which][half][hi/lo][128 n][64 r] bf16
+              bf16* box = (bf16*)smem;
+              const bf16 hp = __float2bfloat16_rn(xp), hm = __float2bfloat16_rn(xm);
+              const bf16 lp = __float2bfloat16_rn(xp - __bfloat162float(hp));
+              const bf16 lm = __float2bfloat16_rn(xm - __bfloat162float(hm));
+              const int op = kl * 64 + rl, om = (127 - kl) * 64 + rl;
+              box[((0 * 2 + half) * 2 + 0) * 8192 + op] = hp;
+              box[((0 * 2 + half) * 2 + 1) * 8192 + op] = lp;
+              box[((1 * 2 + half) * 2 + 0) * 8192 + om] = hm;
+              box[((1 * 2 + half) * 2 + 1) * 8192 + om] = lm;
+            } else {
+              // boxes [which][128 n][128 r] fp32
+              float* box = (float*)smem;
+              box[kl * 128 + row] = xp;
+              box[16384 + (127 - kl) * 128 + row] = xm;
+            }
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (go && warp == 2 && lane == 0) {
+        const uint32_t sb = smem_u32(smem);
+        if (ep.mode == EPI_SPLIT) {
+          for (int which = 0; which < 2; ++which)
+            for (int hf = 0; hf < 2; ++hf)
+              for (int hl = 0; hl < 2; ++hl) {
+                const uint32_t src = sb + (uint32_t)(((which * 2 + hf) * 2 + hl) * 8192 * 2);
+                const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
+                const int y = which ? K - n0 - SBN : n0;
+                tma_store_3d(hl ? &mO1 : &mO0, src, x, y, bb);
+              }
+        } else {
+          tma_store_3d(&mO0, sb, r0, n0, bb);
+          tma_store_3d(&mO0, sb + 16384 * 4, r0, K - n0 - SBN, bb);
+        }
+        tma_store_commit_wait();
+      }
+    } else if (ok) {
       if (!*abort_flag) {
 #pragma unroll 1
         for (int c0 = 0; c0 < SBN; c0 += 32) {
@@ -593,10 +683,29 @@ static int gemm_split(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* 
   return fvx_cuda_status();
 }
 
+// 3-D tensor map over an epilogue output [B][N][R] (R innermost, row pitch
+// ld, batch pitch bs, in elements), box {box_r, 128, 1}, no swizzle.
+static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uint64_t N, uint64_t B, long long ld,
+                         long long bs, uint32_t box_r) {
+  auto enc = encode_fn();
+  if (!enc) return false;
+  const uint64_t es = f32 ? 4 : 2;
+  if (((uintptr_t)base & 15) != 0 || ((uint64_t)ld * es) % 16 != 0 || (B > 1 && ((uint64_t)bs * es) % 16 != 0))
+    return false;
+  cuuint64_t dims[3] = {R, N, B};
+  cuuint64_t strides[2] = {(cuuint64_t)ld * es, (cuuint64_t)(B > 1 ? bs : ld * (long long)N) * es};
+  cuuint32_t box[3] = {box_r, (cuuint32_t)SBN, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides,
+             box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 // C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns
 // de-interleaved; P/Q: the [K/2][K/2] hi/lo tables.  Needs K % 256 == 0.
 static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph, const bf16* Pl, const bf16* Qh,
-                    const bf16* Ql, const Epi& ep, cudaStream_t st) {
+                    const bf16* Ql, const Epi& ep_in, cudaStream_t st) {
+  Epi ep = ep_in;
   static bool attr_set = false;
   if (!attr_set) {
     if (cudaFuncSetAttribute(gemm_sym_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S_SMEM) !=
@@ -610,9 +719,24 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
   if (!make_map(&a_h, Xh, K, M, BM) || !make_map(&a_l, Xl, K, M, BM) || !make_map(&p_h, Ph, KH, KH, SBN) ||
       !make_map(&p_l, Pl, KH, KH, SBN) || !make_map(&q_h, Qh, KH, KH, SBN) || !make_map(&q_l, Ql, KH, KH, SBN))
     return FVX_ERR_ARG;
+  // staged TMA stores for the split and FP32 outputs when their layout allows
+  CUtensorMap o0, o1;
+  memset(&o0, 0, sizeof(o0));
+  memset(&o1, 0, sizeof(o1));
+  ep.tma_out = 0;
+  const int R = ep.rows_per_batch;
+  if ((ep.mode == EPI_SPLIT || ep.mode == EPI_F32) && R % BM == 0 && M % R == 0 && ep.off_n == 0 &&
+      ep.off_r == 0 && ep.n_cols == K && (ep.mode == EPI_F32 || ep.perm_r)) {
+    const uint64_t B = (uint64_t)(M / R);
+    bool okm = ep.mode == EPI_SPLIT
+                   ? make_out_map(&o0, ep.out0, false, R, K, B, ep.ld, ep.batch_stride, 64) &&
+                         make_out_map(&o1, ep.out1, false, R, K, B, ep.ld, ep.batch_stride, 64)
+                   : make_out_map(&o0, ep.out0, true, R, K, B, ep.ld, ep.batch_stride, 128);
+    ep.tma_out = okm ? 1 : 0;
+  }
   dim3 grid(KH / SBN, (M + BM - 1) / BM);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  gemm_sym_bf16_kernel<<<grid, THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, K, ep);
+  gemm_sym_bf16_kernel<<<grid, THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
   return fvx_cuda_status();
 }
 
