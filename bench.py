@@ -359,9 +359,52 @@ def main():
     e2e = world * cells * args.steps / (e2e_ms * 1e-3) / 1e6
     nbytes = host_in.numel() * host_in.element_size()
 
+    # fused vs unfused: the same step as the reference's operator sequence,
+    # one kernel (or torch copy) per operator, through the same library
+    for _ in range(3):
+        model.step_unfused(qa, dt)
+    torch.cuda.synchronize()
+    unf_ms = 0.0
+    n_unf = max(5, min(20, args.steps))
+    for k in range(n_unf):
+        flush.fill_(float(k))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        model.step_unfused(qa, dt)
+        e1.record()
+        e1.synchronize()
+        unf_ms += e0.elapsed_time(e1)
+    unf_ms /= n_unf
+
+    # the fused stage kernel alone (HBM roofline): stage 2's form (reads
+    # q_stage, q_n, psi; writes q_next and the split DST operand)
+    st_ms = []
+    for k in range(20):
+        flush.fill_(float(k))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        model._stage(qa, qb, qb, 0.75, 0.25, 0.25 * dt, True, False)
+        e1.record()
+        e1.synchronize()
+        st_ms.append(e0.elapsed_time(e1))
+    stage_ms = statistics.mean(st_ms)
+    # algorithmic bytes: q_stage, q_n, psi read, q_next written (FP32, one
+    # pass each) = 16 B/cell, plus the DST operand written as bf16 hi/lo
+    # (4 B/cell)
+    stage_bytes = 20.0 * n * n
+    hbm_peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hbm_peak = json.load(f).get("hbm_gbs")
+    except Exception:
+        pass
+
     # dominant kernel: one tcgen05 DST GEMM (2048 x 2048 x 2048, 3xBF16)
     from finitevolx_b200._lib import I, fn, stream_ptr
     h = model.plan.handle
+    sym = fn("fvx_dst_operand_layout")(h) == 1
     gemm = fn("fvx_dst_gemm_step")
     for _ in range(5):
         gemm(h, I(0), I(1), stream_ptr())
@@ -398,10 +441,23 @@ def main():
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": per_step_launches * args.steps,
-            "roofline": {"bound": "tensor", "kernel": "gemm_split_bf16_kernel (DST product, 3xBF16)",
+            "roofline": {"bound": "tensor",
+                         "kernel": ("gemm_sym_bf16_kernel (even/odd DST-I product, 3xBF16)" if sym
+                                    else "gemm_split_bf16_kernel (DST product, 3xBF16)"),
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": peak_src, "traffic": None,
-                         "per_launch_ms": gemm_ms, "algorithmic_flops_per_launch": flops},
+                         "per_launch_ms": gemm_ms, "algorithmic_flops_per_launch": flops,
+                         "executed_tensor_flops_per_launch": (3.0 if sym else 6.0) * n ** 3,
+                         "executed_frac": (3.0 if sym else 6.0) * n ** 3 / (gemm_ms * 1e-3) / 1e12 / peak},
+            "stage_kernel": {"bound": "hbm", "kernel": "qg stage_kernel<float, WENO5>",
+                             "per_launch_ms": stage_ms, "algorithmic_bytes_per_launch": stage_bytes,
+                             "achieved": stage_bytes / (stage_ms * 1e-3) / 1e9, "unit": "GB/s",
+                             "peak": hbm_peak,
+                             "frac": (stage_bytes / (stage_ms * 1e-3) / 1e9 / hbm_peak) if hbm_peak else None},
+            "fused_vs_unfused": {"fused_ms_per_step": t_max / args.steps, "unfused_ms_per_step": unf_ms,
+                                 "speedup": unf_ms / (t_max / args.steps),
+                                 "unfused": "the reference operator sequence, one library kernel or torch copy per "
+                                            "operator (QGModel.step_unfused)"},
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -401,6 +401,7 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
       const bool go = ok && !*abort_flag;
       if (go) {
         const float alpha = (float)ep.alpha;
+        const bool scaled = ep.alpha != 1.0;
         const int half = row & 1, rl = row >> 1;
 #pragma unroll 1
         for (int c0 = 0; c0 < SBN; c0 += 32) {
@@ -413,7 +414,8 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
           for (int j = 0; j < 32; ++j) {
             const int kl = c0 + j, k = n0 + kl;
             const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
-            float xp = (P + Q) * alpha, xm = (P - Q) * alpha;
+            float xp = P + Q, xm = P - Q;
+            if (scaled) { xp *= alpha; xm *= alpha; }
             if (ep.inv_eig) {
               const float* ie = ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row);
               xp *= ie[(long long)k * R];
@@ -422,14 +424,14 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
             if (ep.mode == EPI_SPLIT) {
               // boxes [which][half][hi/lo][128 n][64 r] bf16
               bf16* box = (bf16*)smem;
-              const bf16 hp = __float2bfloat16_rn(xp), hm = __float2bfloat16_rn(xm);
-              const bf16 lp = __float2bfloat16_rn(xp - __bfloat162float(hp));
-              const bf16 lm = __float2bfloat16_rn(xm - __bfloat162float(hm));
+              // both values of the pair converted by one packed cvt
+              const __nv_bfloat162 h2 = __floats2bfloat162_rn(xp, xm);
+              const __nv_bfloat162 l2 = __floats2bfloat162_rn(xp - __low2float(h2), xm - __high2float(h2));
               const int op = kl * 64 + rl, om = (127 - kl) * 64 + rl;
-              box[((0 * 2 + half) * 2 + 0) * 8192 + op] = hp;
-              box[((0 * 2 + half) * 2 + 1) * 8192 + op] = lp;
-              box[((1 * 2 + half) * 2 + 0) * 8192 + om] = hm;
-              box[((1 * 2 + half) * 2 + 1) * 8192 + om] = lm;
+              box[((0 * 2 + half) * 2 + 0) * 8192 + op] = h2.x;
+              box[((0 * 2 + half) * 2 + 1) * 8192 + op] = l2.x;
+              box[((1 * 2 + half) * 2 + 0) * 8192 + om] = h2.y;
+              box[((1 * 2 + half) * 2 + 1) * 8192 + om] = l2.y;
             } else {
               // boxes [which][128 n][128 r] fp32
               float* box = (float*)smem;

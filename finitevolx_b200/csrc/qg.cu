@@ -45,12 +45,44 @@ struct StageArgs {
   int write_ghost;
 };
 
+// Face value on a line segment far from both ends: a WENO scheme at its full
+// reach (what face_value's boundary ladder picks when d >= reach), other
+// schemes through face_value itself.
 template <typename T, int S>
-__global__ void __launch_bounds__(THREADS)
-stage_kernel(StageArgs A) {
+DEV T face_value_full(const T* p, int st, int i, int N, bool pos) {
+  if constexpr (SchemeInfo<S>::is_weno) {
+    constexpr bool Z = SchemeInfo<S>::zfam;
+    constexpr int R = SchemeInfo<S>::reach;
+    const T* b = pos ? p : p + st;
+    const int s = pos ? st : -st;
+    auto e = [&](int k) -> T { return b[k * s]; };
+    if constexpr (R >= 4) {
+      T v[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) v[k] = e(k - 4);
+      return weno_generic<T, 5>(v);
+    } else if constexpr (R == 3) {
+      T v[7];
+#pragma unroll
+      for (int k = 0; k < 7; ++k) v[k] = e(k - 3);
+      return weno_generic<T, 4>(v);
+    } else if constexpr (R == 2) {
+      return weno5<T, Z>(e(-2), e(-1), e(0), e(1), e(2));
+    } else {
+      return Z ? wenoz3(e(-1), e(0), e(1)) : weno3(e(-1), e(0), e(1));
+    }
+  } else {
+    return face_value<T, S>(p, st, i, N, pos);
+  }
+}
+
+// IN: the tile and its halo lie inside the interior and every face is at
+// least the scheme's reach from both ends (the kernel decides per block):
+// no bounds tests, wrap-around loads, ghost writes or boundary ladder.
+template <typename T, int S, bool IN>
+DEV void stage_body(const StageArgs& A, uint8_t* sm) {
   constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
   constexpr int QW = TX + 2 * H, QH = TY + 2 * H;
-  extern __shared__ __align__(16) uint8_t sm[];
   T* qt = (T*)sm;                          // [QH][QW]
   T* pt = qt + QH * QW;                    // psi [TY+2][TX+2], origin (y0-1, x0-1)
   T* xt = pt + (TY + 2) * (TX + 2);        // X [TY+1][TX+1], origin (y0-1, x0-1)
@@ -68,7 +100,9 @@ stage_kernel(StageArgs A) {
     int ly = k / QW, lx = k - ly * QW;
     int gy = y0 - H + ly, gx = x0 - H + lx;
     T val = T(0);
-    if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
+    if (IN) {
+      val = qs[(size_t)gy * nx + gx];
+    } else if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
       bool gh = gy == 0 || gy == ny - 1 || gx == 0 || gx == nx - 1;
       if (!gh) val = qs[(size_t)gy * nx + gx];
       else if (A.periodic) {
@@ -82,7 +116,8 @@ stage_kernel(StageArgs A) {
   for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
     int ly = k / (TX + 2), lx = k - ly * (TX + 2);
     int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
-    pt[k] = (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2) ? psi[(size_t)(gy - 1) * nxi + (gx - 1)] : T(0);
+    pt[k] = (IN || (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2)) ? psi[(size_t)(gy - 1) * nxi + (gx - 1)]
+                                                                         : T(0);
   }
   __syncthreads();
   // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
@@ -90,7 +125,7 @@ stage_kernel(StageArgs A) {
     int ly = k / (TX + 1), lx = k - ly * (TX + 1);
     int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
     T val = T(0);
-    if (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2) {
+    if (IN || (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2)) {
       const T* p = pt + ly * (TX + 2) + lx;  // psi at (gy, gx)
       val = T(0.25) * (p[0] + p[1] + p[TX + 2] + p[TX + 3]);
     }
@@ -101,12 +136,12 @@ stage_kernel(StageArgs A) {
   const T rdx = T(1.0 / A.dx), rdy = T(1.0 / A.dy);
   // u at U-point (j, i) = -(X[j,i] - X[j-1,i]) / dy on [1, N-2]^2
   auto uvel = [&](int gy, int gx) -> T {
-    if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
+    if (!IN && (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2)) return T(0);
     const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
     return -divr(p[0] - p[-(TX + 1)], dy, rdy);
   };
   auto vvel = [&](int gy, int gx) -> T {
-    if (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2) return T(0);
+    if (!IN && (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2)) return T(0);
     const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
     return divr(p[0] - p[-1], dx, rdx);
   };
@@ -115,7 +150,10 @@ stage_kernel(StageArgs A) {
     int ly = k / (TX + 1), lf = k - ly * (TX + 1);
     int gj = y0 + ly, gi = x0 - 1 + lf;
     T f = T(0);
-    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
+    if (IN) {
+      T uu = uvel(gj, gi);
+      f = face_value_full<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
+    } else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
       T uu = uvel(gj, gi);
       f = face_value<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
     }
@@ -126,7 +164,9 @@ stage_kernel(StageArgs A) {
     int gj = y0 - 1 + lf, gi = x0 + lx;
     T f = T(0);
     T vv = vvel(gj, gi);
-    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)
+    if (IN)
+      f = face_value_full<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+    else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)
       f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
     fn[k] = f;
     vs[k] = vv;
@@ -141,9 +181,9 @@ stage_kernel(StageArgs A) {
   for (int k = tid; k < TY * TX; k += THREADS) {
     int ly = k / TX, lx = k - ly * TX;
     int gj = y0 + ly, gi = x0 + lx;
-    if (gj < 1 || gj > ny - 2 || gi < 1 || gi > nx - 2) continue;  // ghost ring written below
+    if (!IN && (gj < 1 || gj > ny - 2 || gi < 1 || gi > nx - 2)) continue;  // ghost ring written below
     T rhs = T(0);
-    if (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3)
+    if (IN || (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3))
       rhs = -(divr(fe[ly * (TX + 1) + lx + 1] - fe[ly * (TX + 1) + lx], dx, rdx) +
               divr(fn[(ly + 1) * TX + lx] - fn[ly * TX + lx], dy, rdy));
     T vc = T(0.5) * (vs[(ly + 1) * TX + lx] + vs[ly * TX + lx]);
@@ -175,7 +215,7 @@ stage_kernel(StageArgs A) {
       A.split_hi[s] = h;
       A.split_lo[s] = __float2bfloat16_rn(fv - __bfloat162float(h));
     }
-    if (A.write_ghost && A.periodic) {
+    if (!IN && A.write_ghost && A.periodic) {
       // copies of this interior cell into the ghost ring (S, N, W, E fill)
       int ys[2] = {gj, gj == ny - 2 ? 0 : (gj == 1 ? ny - 1 : -1)};
       int xs[2] = {gi, gi == nx - 2 ? 0 : (gi == 1 ? nx - 1 : -1)};
@@ -186,7 +226,7 @@ stage_kernel(StageArgs A) {
         }
     }
   }
-  if (A.write_ghost && !A.periodic) {
+  if (!IN && A.write_ghost && !A.periodic) {
     for (int k = tid; k < TY * TX; k += THREADS) {
       int ly = k / TX, lx = k - ly * TX;
       int gj = y0 + ly, gi = x0 + lx;
@@ -194,6 +234,20 @@ stage_kernel(StageArgs A) {
         out[(size_t)gj * nx + gi] = T(0);
     }
   }
+}
+
+template <typename T, int S>
+__global__ void __launch_bounds__(THREADS)
+stage_kernel(StageArgs A) {
+  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
+  constexpr int R = SchemeInfo<S>::reach;
+  extern __shared__ __align__(16) uint8_t sm[];
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  // loads inside [1, N-2] and every upwind cell c with reach <= min(c, N-1-c)
+  const bool in = x0 - H >= 1 && x0 + TX + H - 1 <= A.nx - 2 && y0 - H >= 1 && y0 + TY + H - 1 <= A.ny - 2 &&
+                  x0 - 1 >= R && x0 + TX <= A.nx - 1 - R && y0 - 1 >= R && y0 + TY <= A.ny - 1 - R;
+  if (in) stage_body<T, S, true>(A, sm);
+  else stage_body<T, S, false>(A, sm);
 }
 
 template <typename T, int S>

@@ -97,9 +97,11 @@ def qg_setup(n, dtype, seed=0):
     return grid, q
 
 
-@pytest.mark.parametrize("method", ("weno5", "upwind1", "weno7", "van_leer"))
-def test_qg_tendency_fp64(cuda_ok, method):
-    n = 64
+# 64^2: every tile touches the boundary; 256^2 (and 320 x 256) also has
+# interior tiles, which the stage kernel runs without boundary handling
+@pytest.mark.parametrize("method,n", [("weno5", 64), ("upwind1", 64), ("weno7", 64), ("van_leer", 64),
+                                      ("weno5", 256), ("weno9", 256), ("van_leer", 256), ("wenoz5", 256)])
+def test_qg_tendency_fp64(cuda_ok, method, n):
     grid, q = qg_setup(n, torch.float64)
     lam = 1.0 / 4e4 ** 2
     m = QGModel(grid, 1.7e-11, lam, method=method, dtype=torch.float64, drag=1e-7, viscosity=50.0)
