@@ -403,8 +403,19 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
         const float alpha = (float)ep.alpha;
         const bool scaled = ep.alpha != 1.0;
         const int half = row & 1, rl = row >> 1;
+        const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
 #pragma unroll 1
         for (int c0 = 0; c0 < SBN; c0 += 32) {
+          // 1/Lambda of the chunk's 64 outputs, all loads in flight before use
+          float ivp[32], ivm[32];
+          if (ie) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+              const int k = n0 + c0 + j;
+              ivp[j] = __ldg(ie + (long long)k * R);
+              ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
+            }
+          }
           uint32_t vp[32], vq[32];
           const uint32_t lanes = (uint32_t)(wq * 32) << 16;
           tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
@@ -412,14 +423,13 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
           tmem_wait_ld();
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            const int kl = c0 + j, k = n0 + kl;
+            const int kl = c0 + j;
             const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
             float xp = P + Q, xm = P - Q;
             if (scaled) { xp *= alpha; xm *= alpha; }
-            if (ep.inv_eig) {
-              const float* ie = ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row);
-              xp *= ie[(long long)k * R];
-              xm *= ie[(long long)(K - 1 - k) * R];
+            if (ie) {
+              xp *= ivp[j];
+              xm *= ivm[j];
             }
             if (ep.mode == EPI_SPLIT) {
               // boxes [which][half][hi/lo][128 n][64 r] bf16
