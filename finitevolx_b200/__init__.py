@@ -51,6 +51,7 @@ from finitevolx_b200.vertical import (
     mode_to_layer,
 )
 from finitevolx_b200.qg import QGModel
+from finitevolx_b200.ensemble import QGEnsemble
 
 __all__ = [
     "ArakawaCGrid2D", "CartesianGrid2D", "Mask2D", "StencilCapability2D", "count_contiguous",
@@ -61,5 +62,5 @@ __all__ = [
     "DSTHelmholtzPlan", "MaskedHelmholtzPCG", "MultigridSolver", "build_multigrid_solver",
     "make_multigrid_preconditioner", "masked_laplacian", "pv_inversion", "solve_cg", "solve_helmholtz_dst",
     "solve_poisson_dst", "streamfunction_from_vorticity", "build_coupling_matrix",
-    "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel",
+    "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel", "QGEnsemble",
 ]

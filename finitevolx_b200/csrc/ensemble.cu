@@ -1,0 +1,417 @@
+// Ensemble of multi-layer QG models with uneven grid sizes and layer
+// counts, one RK3-SSP step for every member per call.
+//
+// Member model (built from finitevolX's pieces; the reference has no
+// multi-layer time stepper): layers k = 1..nl of PV q_k on an (n+2)^2 grid
+// with one ghost ring (periodic q, Dirichlet psi), inverted through vertical
+// modes -- q_m = sum_l L2M[m][l] q_l (vertical_modes.py:193-227), one DST-I
+// Helmholtz solve per mode with lambda_m = 1/Rd_m^2 (elliptic.py:390-542),
+// psi_k = sum_m M2L[k][m] psi_m (:230-263) -- and each layer stepped with the
+// 1.5-layer tendency (advection of q_k by its geostrophic velocity plus
+// beta v_k, scripts/qg_1p5_layer.py:454-487) in rk3_ssp_step
+// (timestepping/explicit_rk.py:74-121).
+//
+// Per RK stage: for each grid-size group, one kernel mixes the layers of
+// every member into modes and writes them as the split DST operand, one
+// batched tensor-core DST chain solves all modes of the group (per-mode
+// lambda), one kernel mixes modes back into layer streamfunctions; then ONE
+// persistent launch runs the fused stage on every tile of every layer of
+// every member, CTAs pulling (field, tile) items from an atomic work queue
+// (largest fields first).  All launches are stream-ordered with no host
+// synchronisation, so a host can capture whole steps in a CUDA graph.
+#include "qg_stage.cuh"
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+struct fvx_dst_plan;
+extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int batch_max, const double* lambdas,
+                                   int n_lambda, int want_fp64, fvx_dst_plan** out);
+extern "C" int fvx_dst_plan_destroy(fvx_dst_plan* p);
+extern "C" int fvx_dst_solve_presplit_f32(fvx_dst_plan* p, float* psi, long long psi_bstride, long long psi_ld,
+                                          int batch, void* stream);
+extern "C" int fvx_dst_workspace(fvx_dst_plan* p, void** w1_hi, void** w1_lo);
+extern "C" int fvx_dst_operand_layout(fvx_dst_plan* p);
+
+namespace fvx {
+namespace ens {
+
+constexpr int TXE = 64, TYE = 16;
+constexpr int kMaxLayers = 3;
+
+struct FieldDesc {
+  qg::StageArgs a[3];  // the three RK stages
+  int tiles_x, tile0;  // tiles per row, first queue index
+};
+
+struct ModeDesc {      // batch entry: sum_l c[l] q_l (interior of a [n+2]^2 field)
+  const float* q[kMaxLayers];
+  float c[kMaxLayers];
+  int nl;
+};
+
+struct LayerDesc {     // psi_k = sum_m c[m] psi_mode[b[m]]
+  float* psi;
+  int b[kMaxLayers];
+  float c[kMaxLayers];
+  int nl;
+};
+
+// Persistent fused-stage kernel over every tile of every field.
+template <int S>
+__global__ void __launch_bounds__(qg::THREADS)
+ens_stage_kernel(const FieldDesc* __restrict__ fields, int nfields, int stage, int total, unsigned* counter) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  __shared__ int item;
+  for (;;) {
+    if (threadIdx.x == 0) item = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int t = item;
+    __syncthreads();
+    if (t >= total) break;
+    int lo = 0, hi = nfields - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (fields[mid].tile0 <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const qg::StageArgs A = fields[lo].a[stage];
+    const int lt = t - fields[lo].tile0;
+    const int ty = lt / fields[lo].tiles_x, tx = lt - ty * fields[lo].tiles_x;
+    qg::stage_tile<float, S, TXE, TYE>(A, sm, tx * TXE, ty * TYE);
+    __syncthreads();
+  }
+}
+
+// Layers -> modes, written split into bf16 hi/lo (x de-interleaved when perm).
+__global__ void ens_mode_split_kernel(const ModeDesc* __restrict__ md, int B, int n, __nv_bfloat16* hi,
+                                      __nv_bfloat16* lo, int perm) {
+  const size_t plane = (size_t)n * n, total = plane * B;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+    const int b = (int)(k / plane);
+    const size_t r = k - (size_t)b * plane;
+    const int y = (int)(r / n), x = (int)(r - (size_t)y * n);
+    const ModeDesc& d = md[b];
+    const size_t g = (size_t)(y + 1) * (n + 2) + (x + 1);
+    float v = d.c[0] * d.q[0][g];
+    for (int l = 1; l < d.nl; ++l) v += d.c[l] * d.q[l][g];
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    const int xs = perm ? ((x & 1) ? (n >> 1) + (x >> 1) : (x >> 1)) : x;
+    const size_t o = (size_t)b * plane + (size_t)y * n + xs;
+    hi[o] = h;
+    lo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+  }
+}
+
+__global__ void ens_layer_mix_kernel(const LayerDesc* __restrict__ ld, int nlay, int n,
+                                     const float* __restrict__ psim) {
+  const size_t plane = (size_t)n * n, total = plane * nlay;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(k / plane);
+    const size_t r = k - (size_t)f * plane;
+    const LayerDesc& d = ld[f];
+    float v = d.c[0] * psim[(size_t)d.b[0] * plane + r];
+    for (int m = 1; m < d.nl; ++m) v += d.c[m] * psim[(size_t)d.b[m] * plane + r];
+    d.psi[r] = v;
+  }
+}
+
+static int grid_blocks(size_t n) {
+  size_t b = (n + 255) / 256;
+  return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
+}
+
+}  // namespace ens
+}  // namespace fvx
+
+using namespace fvx;
+using namespace fvx::ens;
+
+struct fvx_ens {
+  int method = 5;
+  int nm = 0, nfields = 0, total_tiles = 0, blocks = 0, grid = 0;
+  size_t smem = 0;
+  std::vector<int> n, nl;
+  std::vector<float*> q, y1, y2, psi;  // per field (member-major, layer-minor)
+  std::vector<int> field0;             // first field of each member
+  struct Group {
+    int n = 0, B = 0, nlay = 0;
+    fvx_dst_plan* plan = nullptr;
+    float* psim = nullptr;
+    ModeDesc* md[3] = {nullptr, nullptr, nullptr};
+    LayerDesc* ld = nullptr;
+    __nv_bfloat16 *hi = nullptr, *lo = nullptr;
+    int perm = 0;
+  };
+  std::vector<Group> groups;
+  FieldDesc* fd = nullptr;
+  unsigned* counter = nullptr;
+  std::vector<void*> allocs;
+};
+
+static void ens_free(fvx_ens* e) {
+  for (auto& g : e->groups)
+    if (g.plan) fvx_dst_plan_destroy(g.plan);
+  for (void* p : e->allocs) cudaFree(p);
+  e->allocs.clear();
+}
+
+template <int S>
+static int ens_stage_smem_and_blocks(int blocks_per_sm, int* blocks, size_t* smem) {
+  *smem = qg::smem_bytes<float, S, TXE, TYE>();
+  static bool set = false;
+  if (!set) {
+    if (cudaFuncSetAttribute(ens_stage_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
+        cudaSuccess)
+      return FVX_ERR_CUDA;
+    set = true;
+  }
+  int occ = 0, dev = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_stage_kernel<S>, qg::THREADS, *smem) != cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                 cudaSuccess)
+    return FVX_ERR_CUDA;
+  const int per = blocks_per_sm > 0 ? std::min(blocks_per_sm, std::max(occ, 1)) : std::max(occ, 1);
+  *blocks = per * sms;
+  return FVX_OK;
+}
+
+template <int S>
+static int ens_stage_launch(fvx_ens* e, int stage, cudaStream_t st) {
+  if (e->grid <= 0) {  // resolved once (occupancy query) per object and setting
+    int rc = ens_stage_smem_and_blocks<S>(e->blocks, &e->grid, &e->smem);
+    if (rc) return rc;
+  }
+  const int blocks = e->grid;
+  const size_t smem = e->smem;
+  cudaMemsetAsync(e->counter, 0, sizeof(unsigned), st);
+  ens_stage_kernel<S><<<blocks, qg::THREADS, smem, st>>>(e->fd, e->nfields, stage, e->total_tiles, e->counter);
+  return fvx_cuda_status();
+}
+
+static int ens_stage_dispatch(fvx_ens* e, int stage, cudaStream_t st) {
+  switch (e->method) {
+    case FVX_UPWIND1: return ens_stage_launch<FVX_UPWIND1>(e, stage, st);
+    case FVX_WENO3: return ens_stage_launch<FVX_WENO3>(e, stage, st);
+    case FVX_WENO5: return ens_stage_launch<FVX_WENO5>(e, stage, st);
+    case FVX_WENOZ5: return ens_stage_launch<FVX_WENOZ5>(e, stage, st);
+    case FVX_VAN_LEER: return ens_stage_launch<FVX_VAN_LEER>(e, stage, st);
+    default: return FVX_ERR_METHOD;
+  }
+}
+
+// n, nl: per member; l2m, m2l: per member nl*nl row-major, concatenated;
+// lam: per member nl (mode lambdas); dx, dy, dt: per member.  n must be a
+// multiple of 8 (the tensor-core DST).  method: 1 upwind1, 4 weno3, 5 weno5,
+// 6 wenoz5, 10 van_leer.
+extern "C" int fvx_ens_create(int n_members, const int* n, const int* nl, const double* l2m, const double* m2l,
+                              const double* lam, const double* dx, const double* dy, const double* dt, double beta,
+                              int method, fvx_ens** out) {
+  if (!out || !n || !nl || !l2m || !m2l || !lam || !dx || !dy || !dt || n_members < 1) return FVX_ERR_ARG;
+  *out = nullptr;
+  if (method != FVX_UPWIND1 && method != FVX_WENO3 && method != FVX_WENO5 && method != FVX_WENOZ5 &&
+      method != FVX_VAN_LEER)
+    return FVX_ERR_METHOD;
+  for (int m = 0; m < n_members; ++m)
+    if (n[m] < 8 || n[m] % 8 || nl[m] < 1 || nl[m] > kMaxLayers) return FVX_ERR_SHAPE;
+  fvx_ens* e = new fvx_ens();
+  e->method = method;
+  e->nm = n_members;
+  e->n.assign(n, n + n_members);
+  e->nl.assign(nl, nl + n_members);
+  bool ok = true;
+  auto A = [&](size_t bytes) -> void* {
+    void* p = nullptr;
+    if (ok && cudaMalloc(&p, bytes) == cudaSuccess) {
+      e->allocs.push_back(p);
+      cudaMemset(p, 0, bytes);
+      return p;
+    }
+    ok = false;
+    return nullptr;
+  };
+  // fields
+  std::vector<int> coff(n_members + 1, 0);  // offsets into the concatenated nl*nl matrices
+  for (int m = 0; m < n_members; ++m) coff[m + 1] = coff[m] + nl[m] * nl[m];
+  std::vector<int> loff(n_members + 1, 0);
+  for (int m = 0; m < n_members; ++m) loff[m + 1] = loff[m] + nl[m];
+  for (int m = 0; m < n_members; ++m) {
+    e->field0.push_back((int)e->q.size());
+    const size_t full = (size_t)(n[m] + 2) * (n[m] + 2), inter = (size_t)n[m] * n[m];
+    for (int k = 0; k < nl[m]; ++k) {
+      e->q.push_back((float*)A(full * 4));
+      e->y1.push_back((float*)A(full * 4));
+      e->y2.push_back((float*)A(full * 4));
+      e->psi.push_back((float*)A(inter * 4));
+    }
+  }
+  e->nfields = (int)e->q.size();
+  if (!ok) { ens_free(e); delete e; return FVX_ERR_CUDA; }
+  // size groups: modes batched per grid size
+  std::vector<int> sizes(e->n);
+  std::sort(sizes.begin(), sizes.end());
+  sizes.erase(std::unique(sizes.begin(), sizes.end()), sizes.end());
+  std::vector<std::vector<int>> batch_of(n_members);  // batch index of each member mode within its group
+  for (int sz : sizes) {
+    fvx_ens::Group g;
+    g.n = sz;
+    std::vector<double> lams;
+    std::vector<ModeDesc> md[3];
+    std::vector<LayerDesc> ld;
+    double gdx = 0, gdy = 0;
+    for (int m = 0; m < n_members; ++m) {
+      if (n[m] != sz) continue;
+      if (gdx == 0) { gdx = dx[m]; gdy = dy[m]; }
+      if (dx[m] != gdx || dy[m] != gdy) { ens_free(e); delete e; return FVX_ERR_ARG; }  // one spacing per size
+      for (int mo = 0; mo < nl[m]; ++mo) {
+        batch_of[m].push_back(g.B++);
+        lams.push_back(lam[loff[m] + mo]);
+        for (int s = 0; s < 3; ++s) {
+          ModeDesc d{};
+          d.nl = nl[m];
+          for (int l = 0; l < nl[m]; ++l) {
+            const int f = e->field0[m] + l;
+            d.q[l] = s == 0 ? e->q[f] : (s == 1 ? e->y1[f] : e->y2[f]);
+            d.c[l] = (float)l2m[coff[m] + mo * nl[m] + l];
+          }
+          md[s].push_back(d);
+        }
+      }
+    }
+    for (int m = 0; m < n_members; ++m) {
+      if (n[m] != sz) continue;
+      for (int k = 0; k < nl[m]; ++k) {
+        LayerDesc d{};
+        d.psi = e->psi[e->field0[m] + k];
+        d.nl = nl[m];
+        for (int mo = 0; mo < nl[m]; ++mo) {
+          d.b[mo] = batch_of[m][mo];
+          d.c[mo] = (float)m2l[coff[m] + k * nl[m] + mo];
+        }
+        ld.push_back(d);
+      }
+    }
+    g.nlay = (int)ld.size();
+    int rc = fvx_dst_plan_create(sz, sz, gdx, gdy, g.B, lams.data(), (int)lams.size(), 0, &g.plan);
+    if (rc) { ens_free(e); delete e; return rc; }
+    void *hi = nullptr, *lo = nullptr;
+    if ((rc = fvx_dst_workspace(g.plan, &hi, &lo))) {
+      fvx_dst_plan_destroy(g.plan);
+      ens_free(e); delete e; return rc;
+    }
+    g.hi = (__nv_bfloat16*)hi;
+    g.lo = (__nv_bfloat16*)lo;
+    g.perm = fvx_dst_operand_layout(g.plan);
+    g.psim = (float*)A((size_t)g.B * sz * sz * 4);
+    for (int s = 0; s < 3; ++s) {
+      g.md[s] = (ModeDesc*)A(md[s].size() * sizeof(ModeDesc));
+      if (ok) cudaMemcpy(g.md[s], md[s].data(), md[s].size() * sizeof(ModeDesc), cudaMemcpyHostToDevice);
+    }
+    g.ld = (LayerDesc*)A(ld.size() * sizeof(LayerDesc));
+    if (ok) cudaMemcpy(g.ld, ld.data(), ld.size() * sizeof(LayerDesc), cudaMemcpyHostToDevice);
+    e->groups.push_back(g);
+    if (!ok) { ens_free(e); delete e; return FVX_ERR_CUDA; }
+  }
+  // work queue: fields ordered by size (largest first), tiles numbered consecutively
+  std::vector<int> order(e->nfields);
+  std::iota(order.begin(), order.end(), 0);
+  std::vector<int> fmember(e->nfields);
+  for (int m = 0; m < n_members; ++m)
+    for (int k = 0; k < nl[m]; ++k) fmember[e->field0[m] + k] = m;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return n[fmember[a]] > n[fmember[b]]; });
+  std::vector<FieldDesc> fd(e->nfields);
+  int t0 = 0;
+  for (int i = 0; i < e->nfields; ++i) {
+    const int f = order[i], m = fmember[f];
+    const int N = n[m] + 2;
+    FieldDesc d{};
+    d.tiles_x = (N + TXE - 1) / TXE;
+    d.tile0 = t0;
+    t0 += d.tiles_x * ((N + TYE - 1) / TYE);
+    const double a[3] = {0.0, 0.75, 1.0 / 3.0}, b[3] = {1.0, 0.25, 2.0 / 3.0}, c[3] = {1.0, 0.25, 2.0 / 3.0};
+    const float* qs[3] = {e->q[f], e->y1[f], e->y2[f]};
+    float* outp[3] = {e->y1[f], e->y2[f], e->q[f]};
+    for (int s = 0; s < 3; ++s) {
+      qg::StageArgs& A2 = d.a[s];
+      A2 = qg::StageArgs{};
+      A2.qs = qs[s];
+      A2.qn = s == 0 ? nullptr : e->q[f];
+      A2.psi = e->psi[f];
+      A2.forcing = nullptr;
+      A2.out = outp[s];
+      A2.split_hi = nullptr;
+      A2.split_lo = nullptr;
+      A2.split_layout = 0;
+      A2.ny = N; A2.nx = N;
+      A2.a = a[s]; A2.b = b[s]; A2.c = c[s] * dt[m];
+      A2.dx = dx[m]; A2.dy = dy[m]; A2.beta = beta;
+      A2.drag = 0.0; A2.visc = 0.0;
+      A2.periodic = 1;
+      A2.write_ghost = s == 2 ? 1 : 0;
+    }
+    fd[i] = d;
+  }
+  e->total_tiles = t0;
+  e->fd = (FieldDesc*)A(fd.size() * sizeof(FieldDesc));
+  e->counter = (unsigned*)A(sizeof(unsigned));
+  if (ok) cudaMemcpy(e->fd, fd.data(), fd.size() * sizeof(FieldDesc), cudaMemcpyHostToDevice);
+  if (!ok || cudaDeviceSynchronize() != cudaSuccess) { ens_free(e); delete e; return FVX_ERR_CUDA; }
+  *out = e;
+  return FVX_OK;
+}
+
+extern "C" int fvx_ens_destroy(fvx_ens* e) {
+  if (!e) return FVX_OK;
+  cudaDeviceSynchronize();
+  ens_free(e);
+  delete e;
+  return fvx_cuda_status();
+}
+
+// Copy layer ``layer`` of member ``member`` ([n+2][n+2] FP32, ghost ring
+// included) from ``src`` and/or to ``dst`` (host or device pointers).
+extern "C" int fvx_ens_io(fvx_ens* e, int member, int layer, const void* src, void* dst, void* stream) {
+  if (!e || member < 0 || member >= e->nm || layer < 0 || layer >= e->nl[member]) return FVX_ERR_ARG;
+  float* q = e->q[e->field0[member] + layer];
+  const size_t bytes = (size_t)(e->n[member] + 2) * (e->n[member] + 2) * sizeof(float);
+  cudaStream_t st = fvx_stream(stream);
+  if (src) cudaMemcpyAsync(q, src, bytes, cudaMemcpyDefault, st);
+  if (dst) cudaMemcpyAsync(dst, q, bytes, cudaMemcpyDefault, st);
+  return fvx_cuda_status();
+}
+
+// Persistent stage grid: CTAs per SM (0 = as many as fit).
+extern "C" int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm) {
+  if (!e || blocks_per_sm < 0) return FVX_ERR_ARG;
+  e->blocks = blocks_per_sm;
+  e->grid = 0;
+  return FVX_OK;
+}
+
+// Launches of one step (for the caller's launch count).
+extern "C" int fvx_ens_launches_per_step(fvx_ens* e) {
+  if (!e) return -1;
+  // per stage: per group (mode split + 4 DST products + layer mix) + counter reset + stage kernel
+  return 3 * ((int)e->groups.size() * 6 + 2);
+}
+
+// n_steps RK3-SSP steps of every member.
+extern "C" int fvx_ens_step(fvx_ens* e, int n_steps, void* stream) {
+  if (!e || n_steps < 0) return FVX_ERR_ARG;
+  cudaStream_t st = fvx_stream(stream);
+  for (int it = 0; it < n_steps; ++it)
+    for (int s = 0; s < 3; ++s) {
+      for (auto& g : e->groups) {
+        const size_t tot = (size_t)g.B * g.n * g.n;
+        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, st>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm);
+        int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, (long long)g.n * g.n, g.n, g.B, st);
+        if (rc) return rc;
+        const size_t tl = (size_t)g.nlay * g.n * g.n;
+        ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, st>>>(g.ld, g.nlay, g.n, g.psim);
+      }
+      int rc = ens_stage_dispatch(e, s, st);
+      if (rc) return rc;
+    }
+  return fvx_cuda_status();
+}

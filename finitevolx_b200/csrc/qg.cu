@@ -13,263 +13,36 @@
 // face fluxes and velocities stay in shared memory, and the kernel writes
 // q_out (interior, plus the ghost ring on the last stage) and optionally the
 // bf16 hi/lo split of q_out's interior that the next DST product reads.
-#include "recon.cuh"
-
-#include <cuda_bf16.h>
+#include "qg_stage.cuh"
 
 namespace fvx {
 namespace qg {
 
-constexpr int TX = 64, TY = 16, THREADS = 256;
-
-// a / d: exact division in FP64; multiplication by the rounded reciprocal in
-// FP32 (<= 1 ulp from the quotient).
-template <typename T> DEV T divr(T a, T d, T rd) {
-  if constexpr (sizeof(T) == 8) return a / d;
-  else return a * rd;
-}
-
-struct StageArgs {
-  const void* qs;      // stage state [Ny][Nx]
-  const void* qn;      // step-start state (null on stage 1)
-  const void* psi;     // interior-only [Ny-2][Nx-2]
-  const void* forcing; // [Ny][Nx] or null
-  void* out;           // [Ny][Nx]
-  __nv_bfloat16* split_hi;  // [Ny-2][Nx-2] or null
-  __nv_bfloat16* split_lo;
-  int split_layout;         // 1: x de-interleaved (the even/odd DST operand layout)
-  int ny, nx;
-  double a, b, c;      // out = a*qn + b*qs + c*rhs
-  double dx, dy, beta, drag, visc;
-  int periodic;        // 1: periodic ghost ring, 0: zero (wall) ghost ring
-  int write_ghost;
-};
-
-// Face value on a line segment far from both ends: a WENO scheme at its full
-// reach (what face_value's boundary ladder picks when d >= reach), other
-// schemes through face_value itself.
-template <typename T, int S>
-DEV T face_value_full(const T* p, int st, int i, int N, bool pos) {
-  if constexpr (SchemeInfo<S>::is_weno) {
-    constexpr bool Z = SchemeInfo<S>::zfam;
-    constexpr int R = SchemeInfo<S>::reach;
-    const T* b = pos ? p : p + st;
-    const int s = pos ? st : -st;
-    auto e = [&](int k) -> T { return b[k * s]; };
-    if constexpr (R >= 4) {
-      T v[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) v[k] = e(k - 4);
-      return weno_generic<T, 5>(v);
-    } else if constexpr (R == 3) {
-      T v[7];
-#pragma unroll
-      for (int k = 0; k < 7; ++k) v[k] = e(k - 3);
-      return weno_generic<T, 4>(v);
-    } else if constexpr (R == 2) {
-      return weno5<T, Z>(e(-2), e(-1), e(0), e(1), e(2));
-    } else {
-      return Z ? wenoz3(e(-1), e(0), e(1)) : weno3(e(-1), e(0), e(1));
-    }
-  } else {
-    return face_value<T, S>(p, st, i, N, pos);
-  }
-}
-
-// IN: the tile and its halo lie inside the interior and every face is at
-// least the scheme's reach from both ends (the kernel decides per block):
-// no bounds tests, wrap-around loads, ghost writes or boundary ladder.
-template <typename T, int S, bool IN>
-DEV void stage_body(const StageArgs& A, uint8_t* sm) {
-  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
-  constexpr int QW = TX + 2 * H, QH = TY + 2 * H;
-  T* qt = (T*)sm;                          // [QH][QW]
-  T* pt = qt + QH * QW;                    // psi [TY+2][TX+2], origin (y0-1, x0-1)
-  T* xt = pt + (TY + 2) * (TX + 2);        // X [TY+1][TX+1], origin (y0-1, x0-1)
-  T* fe = xt + (TY + 1) * (TX + 1);        // [TY][TX+1]
-  T* fn = fe + TY * (TX + 1);              // [TY+1][TX]
-  T* vs = fn + (TY + 1) * TX;              // v on north faces [TY+1][TX], origin (y0-1, x0)
-  const int ny = A.ny, nx = A.nx;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int tid = threadIdx.x;
-  const T* qs = (const T*)A.qs;
-  const T* psi = (const T*)A.psi;
-  const int nxi = nx - 2;
-  // ---- loads: q with BC applied on the fly, psi with zero outside --------
-  for (int k = tid; k < QH * QW; k += THREADS) {
-    int ly = k / QW, lx = k - ly * QW;
-    int gy = y0 - H + ly, gx = x0 - H + lx;
-    T val = T(0);
-    if (IN) {
-      val = qs[(size_t)gy * nx + gx];
-    } else if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
-      bool gh = gy == 0 || gy == ny - 1 || gx == 0 || gx == nx - 1;
-      if (!gh) val = qs[(size_t)gy * nx + gx];
-      else if (A.periodic) {
-        int sy = gy == 0 ? ny - 2 : (gy == ny - 1 ? 1 : gy);
-        int sx = gx == 0 ? nx - 2 : (gx == nx - 1 ? 1 : gx);
-        val = qs[(size_t)sy * nx + sx];
-      }
-    }
-    qt[k] = val;
-  }
-  for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
-    int ly = k / (TX + 2), lx = k - ly * (TX + 2);
-    int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
-    pt[k] = (IN || (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2)) ? psi[(size_t)(gy - 1) * nxi + (gx - 1)]
-                                                                         : T(0);
-  }
-  __syncthreads();
-  // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
-  for (int k = tid; k < (TY + 1) * (TX + 1); k += THREADS) {
-    int ly = k / (TX + 1), lx = k - ly * (TX + 1);
-    int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
-    T val = T(0);
-    if (IN || (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2)) {
-      const T* p = pt + ly * (TX + 2) + lx;  // psi at (gy, gx)
-      val = T(0.25) * (p[0] + p[1] + p[TX + 2] + p[TX + 3]);
-    }
-    xt[k] = val;
-  }
-  __syncthreads();
-  const T dx = T(A.dx), dy = T(A.dy);
-  const T rdx = T(1.0 / A.dx), rdy = T(1.0 / A.dy);
-  // u at U-point (j, i) = -(X[j,i] - X[j-1,i]) / dy on [1, N-2]^2
-  auto uvel = [&](int gy, int gx) -> T {
-    if (!IN && (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2)) return T(0);
-    const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
-    return -divr(p[0] - p[-(TX + 1)], dy, rdy);
-  };
-  auto vvel = [&](int gy, int gx) -> T {
-    if (!IN && (gy < 1 || gy > ny - 2 || gx < 1 || gx > nx - 2)) return T(0);
-    const T* p = xt + (gy - (y0 - 1)) * (TX + 1) + (gx - (x0 - 1));
-    return divr(p[0] - p[-1], dx, rdx);
-  };
-  // ---- face fluxes --------------------------------------------------------
-  for (int k = tid; k < TY * (TX + 1); k += THREADS) {
-    int ly = k / (TX + 1), lf = k - ly * (TX + 1);
-    int gj = y0 + ly, gi = x0 - 1 + lf;
-    T f = T(0);
-    if (IN) {
-      T uu = uvel(gj, gi);
-      f = face_value_full<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
-    } else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T uu = uvel(gj, gi);
-      f = face_value<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
-    }
-    fe[k] = f;
-  }
-  for (int k = tid; k < (TY + 1) * TX; k += THREADS) {
-    int lf = k / TX, lx = k - lf * TX;
-    int gj = y0 - 1 + lf, gi = x0 + lx;
-    T f = T(0);
-    T vv = vvel(gj, gi);
-    if (IN)
-      f = face_value_full<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
-    else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)
-      f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
-    fn[k] = f;
-    vs[k] = vv;
-  }
-  __syncthreads();
-  // ---- tendency, RK combination, stores ------------------------------------
-  const T* qn = (const T*)A.qn;
-  const T* F = (const T*)A.forcing;
-  T* out = (T*)A.out;
-  const T beta = T(A.beta), drag = T(A.drag), visc = T(A.visc);
-  const T ca = T(A.a), cb = T(A.b), cc = T(A.c);
-  for (int k = tid; k < TY * TX; k += THREADS) {
-    int ly = k / TX, lx = k - ly * TX;
-    int gj = y0 + ly, gi = x0 + lx;
-    if (!IN && (gj < 1 || gj > ny - 2 || gi < 1 || gi > nx - 2)) continue;  // ghost ring written below
-    T rhs = T(0);
-    if (IN || (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3))
-      rhs = -(divr(fe[ly * (TX + 1) + lx + 1] - fe[ly * (TX + 1) + lx], dx, rdx) +
-              divr(fn[(ly + 1) * TX + lx] - fn[ly * TX + lx], dy, rdy));
-    T vc = T(0.5) * (vs[(ly + 1) * TX + lx] + vs[ly * TX + lx]);
-    rhs = rhs + (-beta * vc);
-    size_t g = (size_t)gj * nx + gi;
-    if (F) rhs = rhs + F[g];
-    if (A.drag != 0.0) {
-      const T* p = pt + (ly + 1) * (TX + 2) + (lx + 1);
-      T d2x = divr((p[1] - p[0]) - (p[0] - p[-1]), dx * dx, rdx * rdx);
-      T d2y = divr((p[TX + 2] - p[0]) - (p[0] - p[-(TX + 2)]), dy * dy, rdy * rdy);
-      rhs = rhs - drag * (d2x + d2y);
-    }
-    if (A.visc != 0.0) {
-      const T* q = qt + (ly + H) * QW + (lx + H);
-      T d2x = divr((q[1] - q[0]) - (q[0] - q[-1]), dx * dx, rdx * rdx);
-      T d2y = divr((q[QW] - q[0]) - (q[0] - q[-QW]), dy * dy, rdy * rdy);
-      rhs = rhs + visc * (d2x + d2y);
-    }
-    T qsv = qt[(ly + H) * QW + (lx + H)];
-    T r = cb * qsv;
-    if (qn) r = ca * qn[g] + r;
-    r = r + cc * rhs;
-    out[g] = r;
-    if (A.split_hi) {
-      const int xi = gi - 1;
-      size_t s = (size_t)(gj - 1) * nxi + (A.split_layout ? ((xi & 1) ? (nxi >> 1) + (xi >> 1) : (xi >> 1)) : xi);
-      float fv = (float)r;
-      __nv_bfloat16 h = __float2bfloat16_rn(fv);
-      A.split_hi[s] = h;
-      A.split_lo[s] = __float2bfloat16_rn(fv - __bfloat162float(h));
-    }
-    if (!IN && A.write_ghost && A.periodic) {
-      // copies of this interior cell into the ghost ring (S, N, W, E fill)
-      int ys[2] = {gj, gj == ny - 2 ? 0 : (gj == 1 ? ny - 1 : -1)};
-      int xs[2] = {gi, gi == nx - 2 ? 0 : (gi == 1 ? nx - 1 : -1)};
-      for (int a2 = 0; a2 < 2; ++a2)
-        for (int b2 = 0; b2 < 2; ++b2) {
-          if ((a2 == 0 && b2 == 0) || ys[a2] < 0 || xs[b2] < 0) continue;
-          out[(size_t)ys[a2] * nx + xs[b2]] = r;
-        }
-    }
-  }
-  if (!IN && A.write_ghost && !A.periodic) {
-    for (int k = tid; k < TY * TX; k += THREADS) {
-      int ly = k / TX, lx = k - ly * TX;
-      int gj = y0 + ly, gi = x0 + lx;
-      if (gj < ny && gi < nx && (gj == 0 || gj == ny - 1 || gi == 0 || gi == nx - 1))
-        out[(size_t)gj * nx + gi] = T(0);
-    }
-  }
-}
-
-template <typename T, int S>
-__global__ void __launch_bounds__(THREADS)
-stage_kernel(StageArgs A) {
-  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
-  constexpr int R = SchemeInfo<S>::reach;
-  extern __shared__ __align__(16) uint8_t sm[];
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  // loads inside [1, N-2] and every upwind cell c with reach <= min(c, N-1-c)
-  const bool in = x0 - H >= 1 && x0 + TX + H - 1 <= A.nx - 2 && y0 - H >= 1 && y0 + TY + H - 1 <= A.ny - 2 &&
-                  x0 - 1 >= R && x0 + TX <= A.nx - 1 - R && y0 - 1 >= R && y0 + TY <= A.ny - 1 - R;
-  if (in) stage_body<T, S, true>(A, sm);
-  else stage_body<T, S, false>(A, sm);
-}
-
-template <typename T, int S>
-static size_t smem_bytes() {
-  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
-  size_t n = (size_t)(TY + 2 * H) * (TX + 2 * H) + (TY + 2) * (TX + 2) + (TY + 1) * (TX + 1) + TY * (TX + 1) +
-             2 * (TY + 1) * TX;
-  return n * sizeof(T);
-}
-
-template <typename T, int S>
-static int launch(const StageArgs& a, cudaStream_t st) {
-  size_t sm = smem_bytes<T, S>();
+template <typename T, int S, int TX, int TY>
+static int launch_t(const StageArgs& a, cudaStream_t st) {
+  size_t sm = smem_bytes<T, S, TX, TY>();
   static bool set = false;
   if (!set) {
-    if (cudaFuncSetAttribute(stage_kernel<T, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) != cudaSuccess)
+    if (cudaFuncSetAttribute(stage_kernel<T, S, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
+        cudaSuccess)
       return FVX_ERR_CUDA;
     set = true;
   }
   dim3 g((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
-  stage_kernel<T, S><<<g, THREADS, sm, st>>>(a);
+  stage_kernel<T, S, TX, TY><<<g, THREADS, sm, st>>>(a);
   return fvx_cuda_status();
+}
+
+// Tile configuration per (scheme, dtype), set by the autotuner.
+static int g_tile_cfg[32][2] = {};
+
+template <typename T, int S>
+static int launch(const StageArgs& a, cudaStream_t st) {
+  switch (g_tile_cfg[S][sizeof(T) == 8]) {
+    case 1: return launch_t<T, S, kTileTX[1], kTileTY[1]>(a, st);
+    case 2: return launch_t<T, S, kTileTX[2], kTileTY[2]>(a, st);
+    default: return launch_t<T, S, kTileTX[0], kTileTY[0]>(a, st);
+  }
 }
 
 template <typename T>
@@ -314,3 +87,13 @@ using namespace fvx;
 
 FVX_DEF_QG(f32, float)
 FVX_DEF_QG(f64, double)
+
+// Tile shape of the fused stage kernel for one scheme and dtype (0 FP32, 1
+// FP64): cfg 0 = 64x16, 1 = 32x16, 2 = 128x8 cells.  Returns the number of
+// configurations when cfg < 0 (and changes nothing).
+extern "C" int fvx_qg_tile_config(int method, int dtype, int cfg) {
+  if (cfg < 0) return qg::kTileConfigs;
+  if (method < 0 || method >= 32 || dtype < 0 || dtype > 1 || cfg >= qg::kTileConfigs) return FVX_ERR_ARG;
+  qg::g_tile_cfg[method][dtype] = cfg;
+  return FVX_OK;
+}

@@ -1182,6 +1182,11 @@ def qg_tendency(q, dx, dy, beta, lam, method="weno5", bc="periodic", forcing=Non
     qb = enforce_periodic(q) if bc == "periodic" else pad_interior_constant(q)
     psi = np.zeros_like(qb)
     psi[1:-1, 1:-1] = solve_helmholtz_dst(qb[1:-1, 1:-1], dx, dy, lam)
+    return qg_tendency_psi(qb, psi, dx, dy, beta, method, forcing, drag, viscosity)
+
+
+def qg_tendency_psi(qb, psi, dx, dy, beta, method="weno5", forcing=None, drag=0.0, viscosity=0.0):
+    """The same tendency for a given (BC-filled) q and streamfunction psi."""
     u, v = qg_velocity(psi, dx, dy)
     rhs = advection2d(qb, u, v, dx, dy, method)
     vc = interp2d("V_to_T", v)
@@ -1193,6 +1198,31 @@ def qg_tendency(q, dx, dy, beta, lam, method="weno5", bc="periodic", forcing=Non
     if viscosity:
         rhs = rhs + viscosity * diff2d("laplacian", qb, dx, dy)
     return rhs
+
+
+def mlqg_tendency(q, l2m, m2l, lams, dx, dy, beta, method="weno5"):
+    """Multi-layer QG tendency, q [nl, Ny, Nx]: modes (layer_to_mode,
+    vertical_modes.py:193-227), one DST Helmholtz per mode (pv_inversion,
+    elliptic.py:390-542), back to layers (mode_to_layer, :230-263), then each
+    layer's 1.5-layer tendency with its own psi (periodic q)."""
+    nl = q.shape[0]
+    qb = np.stack([enforce_periodic(q[k]) for k in range(nl)])
+    qm = np.einsum("kl,lyx->kyx", l2m, qb[:, 1:-1, 1:-1])
+    psim = np.stack([solve_helmholtz_dst(qm[k], dx, dy, lams[k]) for k in range(nl)])
+    psil = np.einsum("kl,lyx->kyx", m2l, psim)
+    out = np.zeros_like(qb)
+    for k in range(nl):
+        psi = np.zeros_like(qb[k])
+        psi[1:-1, 1:-1] = psil[k]
+        out[k] = qg_tendency_psi(qb[k], psi, dx, dy, beta, method)
+    return out
+
+
+def mlqg_step(q, l2m, m2l, lams, dx, dy, beta, dt, method="weno5"):
+    """One rk3_ssp_step of the multi-layer tendency, ghost rings refilled."""
+    f = lambda y: mlqg_tendency(y, l2m, m2l, lams, dx, dy, beta, method)  # noqa: E731
+    out = rk3_ssp_step(q, f, dt)
+    return np.stack([enforce_periodic(out[k]) for k in range(q.shape[0])])
 
 
 def qg_step(q, dx, dy, beta, lam, dt, method="weno5", bc="periodic", **kw):
