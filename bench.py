@@ -307,7 +307,7 @@ def ensemble_section(members, n_steps, rank=0):
             "launches_per_step": ens.launches_per_step}
 
 
-def main():def main():
+def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
