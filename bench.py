@@ -289,6 +289,8 @@ def ensemble_section(members, n_steps, rank=0):
             q = torch.zeros((n + 2, n + 2), device="cuda")
             q[1:-1, 1:-1] = torch.randn((n, n), device="cuda", generator=g) * 1e-5
             ens.set_layer(m, k, q)
+    from finitevolx_b200 import autotune
+    tuned = autotune.tune_ensemble(ens)
     g = ens.capture(n_steps)
     g.replay()  # warm-up run of the graph
     torch.cuda.synchronize()
@@ -304,7 +306,7 @@ def ensemble_section(members, n_steps, rank=0):
                         f"WENO5, FP32, {n_steps} RK3 steps in one CUDA graph",
             "members": len(members), "layer_cells_per_step": cells, "steps": n_steps, "ms": ms,
             "ms_per_step": ms / n_steps, "value": cells * n_steps / (ms * 1e-3) / 1e6, "unit": "Mcell-steps/s",
-            "launches_per_step": ens.launches_per_step}
+            "launches_per_step": ens.launches_per_step, "autotuned_blocks_per_sm": tuned["blocks_per_sm"]}
 
 
 def main():
@@ -333,6 +335,12 @@ def main():
     q0 = torch.as_tensor(initial_q(n, seed=rank), dtype=torch.float32, device="cuda")
     qa, qb = q0.clone(), torch.empty_like(q0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # autotuned launch choices (stage tile shape; fused or separate DST split)
+    from finitevolx_b200 import autotune
+    tuned = {"stage_tile": autotune.tune_qg_stage(model, qa, dt)["tile"],
+             "fused_split": autotune.tune_qg_split(model, qa, dt)["fused"]}
+    qa.copy_(q0)
 
     # warm-up (eager), leaves split(qb) in the DST workspace for the graphs
     for _ in range(max(args.warmup, 3)):
@@ -483,7 +491,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config(n, args.method),
+            "config": dict(config(n, args.method), autotuned=tuned),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "ms_per_step": e2e_ms / args.steps},
             "gpu_launches": per_step_launches * args.steps,

@@ -59,6 +59,9 @@ class QGModel:
             self._layout = fn("fvx_dst_operand_layout")(self.plan.handle)
         self._w1 = (hi, lo)
         self.kernel_launches = 0
+        # the stage kernel writes the next DST operand split (False: a
+        # separate split pass per solve); finitevolx_b200.autotune picks it
+        self.fuse_split = True
 
     # -- pieces --------------------------------------------------------------
     def _dst_from(self, q):
@@ -109,7 +112,8 @@ class QGModel:
         """
         q = L.as_field(q, dtype=self.dtype)
         out = torch.empty_like(q) if out is None else out
-        split = self._fused_split
+        split = self._fused_split and self.fuse_split
+        presplit = presplit and split
         stages = ((q, self.y1), (self.y1, self.y2), (self.y2, out))
         for s, ((a, b, c), (qs, qo)) in enumerate(zip(RK3, stages)):
             # the stage kernel before this one left qs's interior split in the workspace

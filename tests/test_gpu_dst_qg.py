@@ -140,3 +140,31 @@ def test_qg_step_fp32_within_1e5(cuda_ok):
     q2b = m.step(q1.clone(), dt, presplit=False)
     np.testing.assert_array_equal(host(q2a), host(q2b))
     m.plan.check_device()
+
+
+def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
+    # every tile shape and both split placements give the same step (FP32,
+    # 1e-6 relative: only accumulation order may differ), and the tuner
+    # caches its choice
+    from finitevolx_b200 import autotune
+    monkeypatch.setenv("FVX_AUTOTUNE_CACHE", str(tmp_path / "tune.json"))
+    n = 256
+    grid, q = qg_setup(n, torch.float32, 5)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method="weno5", dtype=torch.float32)
+    qd = dev(q, torch.float32)
+    outs = []
+    for cfg in range(3):
+        autotune.set_stage_tile("weno5", torch.float32, cfg)
+        outs.append(host(m.step(qd, dt)))
+    m.fuse_split = False
+    outs.append(host(m.step(qd, dt)))
+    m.fuse_split = True
+    for o in outs[1:]:
+        assert rel_err(o, outs[0]) < 1e-6
+    r1 = autotune.tune_qg_stage(m, qd, dt)
+    assert r1["tile"] in ("64x16", "32x16", "128x8") and len(r1["ms"]) == 3
+    r2 = autotune.tune_qg_split(m, qd, dt)
+    assert set(r2["ms"]) == {"fused", "unfused"}
+    assert autotune.tune_qg_stage(m, qd, dt) == r1  # from the cache
+    autotune.set_stage_tile("weno5", torch.float32, 0)
