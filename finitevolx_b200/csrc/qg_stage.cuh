@@ -68,6 +68,77 @@ DEV T face_value_full(const T* p, int st, int i, int N, bool pos) {
   }
 }
 
+// ---- packed FP32 pairs (Blackwell f32x2 arithmetic) -----------------------
+// Two independent values per instruction; each lane is an IEEE round-to-
+// nearest FP32 operation, the same as its scalar form.
+DEV unsigned long long f2pack(float2 a) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a.x), "f"(a.y));
+  return r;
+}
+DEV float2 f2unpack(unsigned long long r) {
+  float2 d;
+  asm("mov.b64 {%0,%1}, %2;" : "=f"(d.x), "=f"(d.y) : "l"(r));
+  return d;
+}
+DEV float2 f2fma(float2 a, float2 b, float2 c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)), "l"(f2pack(c)));
+  return f2unpack(d);
+}
+DEV float2 f2add(float2 a, float2 b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(d);
+}
+DEV float2 f2mul(float2 a, float2 b) {
+  unsigned long long d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(f2pack(a)), "l"(f2pack(b)));
+  return f2unpack(d);
+}
+DEV float2 f2s(float c) { return make_float2(c, c); }
+
+// WENO5 / WENO-Z5 (weno5<float, Z> in recon.cuh, same formulas and order)
+// on two stencils at once; divisions stay scalar (__fdividef per lane).
+template <bool Z>
+DEV float2 weno5_x2(float2 qmm, float2 qm, float2 q0, float2 qp, float2 qpp) {
+  const float2 qi1 = f2fma(f2s(11.f / 6.f), q0, f2fma(f2s(-7.f / 6.f), qm, f2mul(f2s(1.f / 3.f), qmm)));
+  const float2 qi2 = f2fma(f2s(1.f / 3.f), qp, f2fma(f2s(5.f / 6.f), q0, f2mul(f2s(-1.f / 6.f), qm)));
+  const float2 qi3 = f2fma(f2s(-1.f / 6.f), qpp, f2fma(f2s(5.f / 6.f), qp, f2mul(f2s(1.f / 3.f), q0)));
+  const float2 k1 = f2s(13.f / 12.f), k2 = f2s(0.25f);
+  const float2 a1 = f2add(f2fma(f2s(-2.f), qm, qmm), q0);
+  const float2 c1 = f2fma(f2s(3.f), q0, f2fma(f2s(-4.f), qm, qmm));
+  const float2 b1 = f2fma(k2, f2mul(c1, c1), f2mul(k1, f2mul(a1, a1)));
+  const float2 a2 = f2add(f2fma(f2s(-2.f), q0, qm), qp);
+  const float2 c2 = f2add(qm, f2mul(f2s(-1.f), qp));
+  const float2 b2 = f2fma(k2, f2mul(c2, c2), f2mul(k1, f2mul(a2, a2)));
+  const float2 a3 = f2add(f2fma(f2s(-2.f), qp, q0), qpp);
+  const float2 c3 = f2add(f2fma(f2s(-4.f), qp, f2mul(f2s(3.f), q0)), qpp);
+  const float2 b3 = f2fma(k2, f2mul(c3, c3), f2mul(k1, f2mul(a3, a3)));
+  float2 w1, w2, w3;
+  if (Z) {
+    const float2 eps = f2s(1e-16f);
+    const float2 tau = make_float2(fabsf(b1.x - b3.x), fabsf(b1.y - b3.y));
+    const float2 d1 = f2add(b1, eps), d2 = f2add(b2, eps), d3 = f2add(b3, eps);
+    const float2 r1 = make_float2(__fdividef(tau.x, d1.x), __fdividef(tau.y, d1.y));
+    const float2 r2 = make_float2(__fdividef(tau.x, d2.x), __fdividef(tau.y, d2.y));
+    const float2 r3 = make_float2(__fdividef(tau.x, d3.x), __fdividef(tau.y, d3.y));
+    w1 = f2mul(f2s(0.1f), f2add(f2s(1.f), r1));
+    w2 = f2mul(f2s(0.6f), f2add(f2s(1.f), r2));
+    w3 = f2mul(f2s(0.3f), f2add(f2s(1.f), r3));
+  } else {
+    const float2 eps = f2s(1e-8f);
+    const float2 d1 = f2add(b1, eps), d2 = f2add(b2, eps), d3 = f2add(b3, eps);
+    const float2 s1 = f2mul(d1, d1), s2 = f2mul(d2, d2), s3 = f2mul(d3, d3);
+    w1 = make_float2(__fdividef(0.1f, s1.x), __fdividef(0.1f, s1.y));
+    w2 = make_float2(__fdividef(0.6f, s2.x), __fdividef(0.6f, s2.y));
+    w3 = make_float2(__fdividef(0.3f, s3.x), __fdividef(0.3f, s3.y));
+  }
+  const float2 num = f2fma(w3, qi3, f2fma(w2, qi2, f2mul(w1, qi1)));
+  const float2 den = f2add(f2add(w1, w2), w3);
+  return make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
+}
+
 // IN: the tile and its halo lie inside the interior and every face is at
 // least the scheme's reach from both ends (the kernel decides per block):
 // no bounds tests, wrap-around loads, ghost writes or boundary ladder.
@@ -137,6 +208,43 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     return divr(p[0] - p[-1], dx, rdx);
   };
   // ---- face fluxes --------------------------------------------------------
+  constexpr bool PACK =
+      IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
+  if constexpr (PACK) {
+    // each cell's east and north faces as one packed pair of reconstructions
+    for (int k = tid; k < TY * TX; k += THREADS) {
+      const int ly = k / TX, lx = k % TX;
+      const int gj = y0 + ly, gi = x0 + lx;
+      const float uu = (float)uvel(gj, gi), vv = (float)vvel(gj, gi);
+      const float* p = (const float*)qt + (ly + H) * QW + (lx + H);
+      const bool px = uu >= 0.f, py = vv >= 0.f;
+      // oriented stencils (face_value_full): pos e(k) = p[k], neg e(k) = p[1-k]
+      float2 e[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const float xa = p[j - 2], xb = p[3 - j];
+        const float ya = p[(j - 2) * QW], yb = p[(3 - j) * QW];
+        e[j] = make_float2(px ? xa : xb, py ? ya : yb);
+      }
+      const float2 f = weno5_x2<SchemeInfo<S>::zfam>(e[0], e[1], e[2], e[3], e[4]);
+      fe[ly * (TX + 1) + lx + 1] = (T)(f.x * uu);
+      fn[(ly + 1) * TX + lx] = (T)(f.y * vv);
+      vs[(ly + 1) * TX + lx] = (T)vv;
+    }
+    // the tile's west-most east faces and south-most north faces
+    for (int k = tid; k < TY + TX; k += THREADS) {
+      if (k < TY) {
+        const int ly = k, gj = y0 + ly, gi = x0 - 1;
+        const T uu = uvel(gj, gi);
+        fe[ly * (TX + 1)] = face_value_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
+      } else {
+        const int lx = k - TY, gj = y0 - 1, gi = x0 + lx;
+        const T vv = vvel(gj, gi);
+        fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+        vs[lx] = vv;
+      }
+    }
+  } else {
   for (int k = tid; k < TY * (TX + 1); k += THREADS) {
     int ly = k / (TX + 1), lf = k - ly * (TX + 1);
     int gj = y0 + ly, gi = x0 - 1 + lf;
@@ -161,6 +269,7 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
       f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
     fn[k] = f;
     vs[k] = vv;
+  }
   }
   __syncthreads();
   // ---- tendency, RK combination, stores ------------------------------------

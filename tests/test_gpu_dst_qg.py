@@ -168,3 +168,15 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     assert set(r2["ms"]) == {"fused", "unfused"}
     assert autotune.tune_qg_stage(m, qd, dt) == r1  # from the cache
     autotune.set_stage_tile("weno5", torch.float32, 0)
+
+
+@pytest.mark.parametrize("method", ("wenoz5", "weno5"))
+def test_qg_step_fp32_packed_interior(cuda_ok, method):
+    # 320^2: interior tiles take the packed (f32x2) two-face WENO path, edge
+    # tiles the scalar one; both must sit within the FP32 bar of the oracle
+    n = 320
+    grid, q = qg_setup(n, torch.float32, 6)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method=method, dtype=torch.float32)
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method)
+    assert rel_err(host(m.step(dev(q, torch.float32), dt)), ref) < 1e-5
