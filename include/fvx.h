@@ -336,6 +336,47 @@ int fvx_nn_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, i
                 double beta2, double eps, int step, void* stream);
 int fvx_nn_to_bf16(const float* src, void* dst, int n, void* stream);
 
+/* ---- QG fused-stage tile shape (autotuner) -------------------------------- */
+/* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8 cells for (method, dtype 0 FP32 / 1
+ * FP64); cfg < 0 returns the number of configurations.  No counterpart in
+ * finitevolX (launch configuration). */
+int fvx_qg_tile_config(int method, int dtype, int cfg);
+
+/* ---- ensemble of multi-layer QG members ------------------------------------ */
+/* Members (n[m]^2 interior, nl[m] <= 3 layers; l2m/m2l row-major nl x nl per
+ * member, concatenated; lam: per-mode 1/Rd^2) stepped with rk3_ssp_step
+ * (timestepping/explicit_rk.py:74-121) of the per-layer 1.5-layer tendency
+ * (scripts/qg_1p5_layer.py:454-487) with psi from the vertical modes
+ * (vertical_modes.py:193-263, elliptic.py:390-542).  One persistent
+ * work-queue launch per RK stage over every tile of every layer. */
+typedef struct fvx_ens fvx_ens;
+int fvx_ens_create(int n_members, const int* n, const int* nl, const double* l2m, const double* m2l,
+                   const double* lam, const double* dx, const double* dy, const double* dt, double beta, int method,
+                   fvx_ens** out);
+int fvx_ens_destroy(fvx_ens* e);
+int fvx_ens_io(fvx_ens* e, int member, int layer, const void* src, void* dst, void* stream);
+int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm);
+int fvx_ens_launches_per_step(fvx_ens* e);
+int fvx_ens_step(fvx_ens* e, int n_steps, void* stream);
+
+/* ---- diagnostics (operators/diagnostics.py) -------------------------------- */
+/* op: 0 kinetic_energy(u,v) :35-73, 1 bernoulli_potential(h,u,v; p0 = g)
+ * :76-112, 2 shear_strain(u,v; dx,dy) :184-213, 3 tensor_strain :216-245,
+ * 4 qg_potential_vorticity(psi, y; f0, beta, dx, dy, y0) :395-452,
+ * 5 potential_vorticity(omega, f, h) :150-181, 6 enstrophy :308-329,
+ * 7 potential_enstrophy :332-360, 8 strain_magnitude_squared :248-271,
+ * 9 okubo_weiss :274-305, 10 available_potential_energy(h, H; g') :363-392. */
+int fvx_diag2d_f32(int op, const float* a, const float* b, const float* c, float* out, int ny, int nx, double p0,
+                   double p1, double p2, double p3, double p4, void* stream);
+int fvx_diag2d_f64(int op, const double* a, const double* b, const double* c, double* out, int ny, int nx,
+                   double p0, double p1, double p2, double p3, double p4, void* stream);
+/* total_energy / total_enstrophy (:498-555): scale * sum over the interior
+ * of (a + b) (b may be NULL) into a device double, deterministic. */
+int fvx_interior_sum_f32(const float* a, const float* b, int ny, int nx, double scale, double* part,
+                         unsigned* ticket, double* out_dev, void* stream);
+int fvx_interior_sum_f64(const double* a, const double* b, int ny, int nx, double scale, double* part,
+                         unsigned* ticket, double* out_dev, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

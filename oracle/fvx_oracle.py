@@ -1267,3 +1267,86 @@ def fourier_streamfunction(ny, nx, dx, dy, seed, n_modes=8, umax=1.0):
     u, v = diff2d("grad_perp", full, dx, dy)
     s = max(np.abs(u).max(), np.abs(v).max())
     return full * (umax / s)
+
+
+# ---------------------------------------------------------------------------
+# Diagnostics (operators/diagnostics.py)
+# ---------------------------------------------------------------------------
+
+
+def _ring0(x):
+    out = np.zeros_like(x)
+    out[1:-1, 1:-1] = x[1:-1, 1:-1]
+    return out
+
+
+def kinetic_energy(u, v):
+    """diagnostics.py:35-73: 0.5 (avg_x_bwd(u^2) + avg_y_bwd(v^2)), zero ring."""
+    u2, v2 = u ** 2, v ** 2
+    ke = np.zeros_like(u)
+    ke[1:-1, 1:-1] = 0.5 * (0.5 * (u2[1:-1, 1:-1] + u2[1:-1, :-2]) + 0.5 * (v2[1:-1, 1:-1] + v2[:-2, 1:-1]))
+    return ke
+
+
+def bernoulli_potential(h, u, v, gravity=9.81):
+    """diagnostics.py:76-112."""
+    return _ring0(kinetic_energy(u, v) + gravity * h)
+
+
+def shear_strain(u, v, dx, dy):
+    """diagnostics.py:184-213: diff_x_fwd(v)/dx + diff_y_fwd(u)/dy."""
+    out = np.zeros_like(u)
+    out[1:-1, 1:-1] = (v[1:-1, 2:] - v[1:-1, 1:-1]) / dx + (u[2:, 1:-1] - u[1:-1, 1:-1]) / dy
+    return out
+
+
+def tensor_strain(u, v, dx, dy):
+    """diagnostics.py:216-245: diff_x_bwd(u)/dx - diff_y_bwd(v)/dy."""
+    out = np.zeros_like(u)
+    out[1:-1, 1:-1] = (u[1:-1, 1:-1] - u[1:-1, :-2]) / dx - (v[1:-1, 1:-1] - v[:-2, 1:-1]) / dy
+    return out
+
+
+def qg_potential_vorticity(psi, f0, beta, dx, dy, y, y0):
+    """diagnostics.py:395-452."""
+    d2x = ((psi[1:-1, 2:] - psi[1:-1, 1:-1]) - (psi[1:-1, 1:-1] - psi[1:-1, :-2])) / dx ** 2
+    d2y = ((psi[2:, 1:-1] - psi[1:-1, 1:-1]) - (psi[1:-1, 1:-1] - psi[:-2, 1:-1])) / dy ** 2
+    out = np.zeros_like(psi)
+    out[1:-1, 1:-1] = (d2x + d2y) / f0 + beta * (y[1:-1, 1:-1] - y0) / f0
+    return out
+
+
+def potential_vorticity(omega, f, h):
+    """diagnostics.py:150-181."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(h == 0, np.nan, (omega + f) / h)
+
+
+def enstrophy(omega):
+    return 0.5 * omega ** 2
+
+
+def potential_enstrophy(q, h):
+    return 0.5 * q ** 2 * h
+
+
+def strain_magnitude_squared(sn, ss):
+    return sn ** 2 + ss ** 2
+
+
+def okubo_weiss(sn, ss, omega):
+    return sn ** 2 + ss ** 2 - omega ** 2
+
+
+def available_potential_energy(h, H, g_prime):
+    return 0.5 * g_prime * (h - H) ** 2
+
+
+def total_energy(ke, ape, dx, dy):
+    """diagnostics.py:498-524."""
+    return np.sum(ke[1:-1, 1:-1] + ape[1:-1, 1:-1]) * dx * dy
+
+
+def total_enstrophy(ens, dx, dy):
+    """diagnostics.py:527-555."""
+    return np.sum(ens[1:-1, 1:-1]) * dx * dy
