@@ -52,6 +52,8 @@ from finitevolx_b200.vertical import (
 )
 from finitevolx_b200.qg import QGModel
 from finitevolx_b200.ensemble import QGEnsemble
+from finitevolx_b200.swm import Coriolis2D, MomentumAdvection2D, Vorticity2D
+from finitevolx_b200 import diagnostics
 
 __all__ = [
     "ArakawaCGrid2D", "CartesianGrid2D", "Mask2D", "StencilCapability2D", "count_contiguous",
@@ -63,4 +65,5 @@ __all__ = [
     "make_multigrid_preconditioner", "masked_laplacian", "pv_inversion", "solve_cg", "solve_helmholtz_dst",
     "solve_poisson_dst", "streamfunction_from_vorticity", "build_coupling_matrix",
     "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel", "QGEnsemble",
+    "Coriolis2D", "MomentumAdvection2D", "Vorticity2D", "diagnostics",
 ]

@@ -377,6 +377,20 @@ int fvx_interior_sum_f32(const float* a, const float* b, int ny, int nx, double 
 int fvx_interior_sum_f64(const double* a, const double* b, int ny, int nx, double scale, double* part,
                          unsigned* ticket, double* out_dev, void* stream);
 
+/* ---- shallow-water operators ----------------------------------------------- */
+/* op 0 Coriolis2D (u, v, f) -> (du, dv) (operators/coriolis.py:34-133);
+ * 1-3 Vorticity2D.pv_flux_{energy,enstrophy}_conserving / _arakawa_lamb
+ * (q, u, v; alpha) -> (qu, qv) (operators/vorticity.py:120-235);
+ * 4-6 MomentumAdvection2D energy / enstrophy / al (u, v) -> (du, dv)
+ * (diffusion/momentum.py:108-216); 7 Vorticity2D.potential_vorticity
+ * (u, v, h, f) -> q (vorticity.py:60-118).  Masks (bool [Ny][Nx]) may be NULL. */
+int fvx_sw2d_f32(int op, const float* a, const float* b, const float* c, const float* d, float* out1, float* out2,
+                 int ny, int nx, double dx, double dy, double alpha, const uint8_t* mask_h, const uint8_t* mask_u,
+                 const uint8_t* mask_v, const uint8_t* mask_xy, void* stream);
+int fvx_sw2d_f64(int op, const double* a, const double* b, const double* c, const double* d, double* out1,
+                 double* out2, int ny, int nx, double dx, double dy, double alpha, const uint8_t* mask_h,
+                 const uint8_t* mask_u, const uint8_t* mask_v, const uint8_t* mask_xy, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

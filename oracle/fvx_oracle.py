@@ -1350,3 +1350,95 @@ def total_energy(ke, ape, dx, dy):
 def total_enstrophy(ens, dx, dy):
     """diagnostics.py:527-555."""
     return np.sum(ens[1:-1, 1:-1]) * dx * dy
+
+
+# ---------------------------------------------------------------------------
+# Shallow-water operators: Coriolis2D (operators/coriolis.py:34-133),
+# Vorticity2D (operators/vorticity.py:60-235), MomentumAdvection2D
+# (diffusion/momentum.py:35-216) -- composed from interp2d / diff2d exactly as
+# the reference composes Interpolation2D / Difference2D.
+# ---------------------------------------------------------------------------
+
+
+def coriolis2d(u, v, f, mask=None):
+    """coriolis.py:86-133 (unmasked interpolation, masked outputs)."""
+    f_on_u, f_on_v = interp2d("T_to_U", f), interp2d("T_to_V", f)
+    v_on_u, u_on_v = interp2d("V_to_U", v), interp2d("U_to_V", u)
+    du = _interior(f_on_u[1:-1, 1:-1] * v_on_u[1:-1, 1:-1], u)
+    dv = _interior(-f_on_v[1:-1, 1:-1] * u_on_v[1:-1, 1:-1], v)
+    if mask is not None:
+        du, dv = du * mask["u"], dv * mask["v"]
+    return du, dv
+
+
+def potential_vorticity_x(u, v, h, f, dx, dy, mask=None):
+    """Vorticity2D.potential_vorticity (vorticity.py:60-118)."""
+    zeta = diff2d("curl", u, dx, dy, mask, v)
+    f_on_q, h_on_q = interp2d("T_to_X", f, mask), interp2d("T_to_X", h, mask)
+    num = zeta[1:-1, 1:-1] + f_on_q[1:-1, 1:-1]
+    den = h_on_q[1:-1, 1:-1]
+    with np.errstate(divide="ignore", invalid="ignore"):
+        pv = np.where(den == 0, np.nan, num / den)
+    out = _interior(pv, h)
+    if mask is not None:
+        out = np.where(mask["xy_corner_strict"] != 0, out, 0.0)
+    return out
+
+
+def pv_flux(q, u, v, scheme, alpha=1.0 / 3.0, mask=None):
+    """Vorticity2D.pv_flux_{energy,enstrophy}_conserving / _arakawa_lamb
+    (vorticity.py:120-235)."""
+    def energy():
+        q_on_u, q_on_v = interp2d("X_to_U", q, mask), interp2d("X_to_V", q, mask)
+        return (_interior(q_on_u[1:-1, 1:-1] * u[1:-1, 1:-1], u),
+                _interior(q_on_v[1:-1, 1:-1] * v[1:-1, 1:-1], v))
+
+    def enstrophy():
+        u_on_q, v_on_q = interp2d("U_to_X", u, mask), interp2d("V_to_X", v, mask)
+        qu_at_q = _interior(q[1:-1, 1:-1] * u_on_q[1:-1, 1:-1], q)
+        qv_at_q = _interior(q[1:-1, 1:-1] * v_on_q[1:-1, 1:-1], q)
+        return interp2d("X_to_U", qu_at_q, mask), interp2d("X_to_V", qv_at_q, mask)
+
+    if scheme == "energy":
+        return energy()
+    if scheme == "enstrophy":
+        return enstrophy()
+    (ue, ve), (us, vs) = energy(), enstrophy()
+    return alpha * ue + (1.0 - alpha) * us, alpha * ve + (1.0 - alpha) * vs
+
+
+def momentum_advection(u, v, dx, dy, scheme="energy", mask=None):
+    """MomentumAdvection2D.__call__ (momentum.py:108-216)."""
+    zeta = diff2d("curl", u, dx, dy, mask, v)
+    u_on_T, v_on_T = interp2d("U_to_T", u, mask), interp2d("V_to_T", v, mask)
+    K = _interior(0.5 * (u_on_T[1:-1, 1:-1] ** 2 + v_on_T[1:-1, 1:-1] ** 2), u)
+    dK_dx, dK_dy = diff2d("diff_x_T_to_U", K, dx, dy, mask), diff2d("diff_y_T_to_V", K, dx, dy, mask)
+
+    def e_scheme():
+        zeta_on_u, zeta_on_v = interp2d("X_to_U", zeta, mask), interp2d("X_to_V", zeta, mask)
+        v_on_u, u_on_v = interp2d("V_to_U", v, mask), interp2d("U_to_V", u, mask)
+        return (_interior(zeta_on_u[1:-1, 1:-1] * v_on_u[1:-1, 1:-1], u),
+                _interior(zeta_on_v[1:-1, 1:-1] * u_on_v[1:-1, 1:-1], v))
+
+    def z_scheme():
+        v_on_q, u_on_q = interp2d("V_to_X", v, mask), interp2d("U_to_X", u, mask)
+        zv_at_q = _interior(zeta[1:-1, 1:-1] * v_on_q[1:-1, 1:-1], u)
+        zu_at_q = _interior(zeta[1:-1, 1:-1] * u_on_q[1:-1, 1:-1], v)
+        return interp2d("X_to_U", zv_at_q, mask), interp2d("X_to_V", zu_at_q, mask)
+
+    if scheme == "energy":
+        zv_u, zu_v = e_scheme()
+    elif scheme == "enstrophy":
+        zv_u, zu_v = z_scheme()
+    elif scheme == "al":
+        a = 1.0 / 3.0
+        (e1, e2), (s1, s2) = e_scheme(), z_scheme()
+        zv_u = _interior(a * e1[1:-1, 1:-1] + (1.0 - a) * s1[1:-1, 1:-1], u)
+        zu_v = _interior(a * e2[1:-1, 1:-1] + (1.0 - a) * s2[1:-1, 1:-1], v)
+    else:
+        raise ValueError(f"Unknown scheme: {scheme!r}.  Choose 'energy', 'enstrophy', or 'al'.")
+    du = _interior(zv_u[2:-2, 2:-2] - dK_dx[2:-2, 2:-2], u, ghost=2)
+    dv = _interior(-zu_v[2:-2, 2:-2] - dK_dy[2:-2, 2:-2], v, ghost=2)
+    if mask is not None:
+        du, dv = du * mask["u"], dv * mask["v"]
+    return du, dv
