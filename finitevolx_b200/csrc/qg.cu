@@ -28,8 +28,8 @@ static int launch_t(const StageArgs& a, cudaStream_t st) {
       return FVX_ERR_CUDA;
     set = true;
   }
-  dim3 g((a.nx + TX - 1) / TX, (a.ny + TY - 1) / TY);
-  stage_kernel<T, S, TX, TY><<<g, THREADS, sm, st>>>(a);
+  const TileSplit ts = tile_split<S, TX, TY>(a.ny, a.nx);
+  stage_kernel<T, S, TX, TY><<<ts.ntx * ts.nty, THREADS, sm, st>>>(a, ts);
   return fvx_cuda_status();
 }
 

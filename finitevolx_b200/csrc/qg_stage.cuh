@@ -68,6 +68,21 @@ DEV T face_value_full(const T* p, int st, int i, int N, bool pos) {
   }
 }
 
+// ---- asynchronous global -> shared copies (cp.async, no register staging) --
+// Interior tiles' loads are plain copies: issue them all, then wait once, so
+// the tile load costs one memory latency instead of one per loop iteration.
+// (The q rows' pitch, Nx elements, is not 16-byte aligned in general, which
+// rules out TMA tiles here.)
+template <typename T>
+DEV void cp_async_elem(T* dst, const T* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // ---- packed FP32 pairs (Blackwell f32x2 arithmetic) -----------------------
 // Two independent values per instruction; each lane is an IEEE round-to-
 // nearest FP32 operation, the same as its scalar form.
@@ -158,28 +173,42 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   const T* psi = (const T*)A.psi;
   const int nxi = nx - 2;
   // ---- loads: q with BC applied on the fly, psi with zero outside --------
+  if constexpr (IN) {
+    for (int k = tid; k < QH * QW; k += THREADS) {
+      const int ly = k / QW, lx = k - ly * QW;
+      cp_async_elem(qt + k, qs + (size_t)(y0 - H + ly) * nx + (x0 - H + lx));
+    }
+    for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
+      const int ly = k / (TX + 2), lx = k - ly * (TX + 2);
+      cp_async_elem(pt + k, psi + (size_t)(y0 - 2 + ly) * nxi + (x0 - 2 + lx));
+    }
+    cp_async_wait_all();
+  } else {
+  // general tiles: wrap-around / zero-ring sources resolved per element, the
+  // copies themselves asynchronous (one wait for the whole tile)
   for (int k = tid; k < QH * QW; k += THREADS) {
     int ly = k / QW, lx = k - ly * QW;
     int gy = y0 - H + ly, gx = x0 - H + lx;
-    T val = T(0);
-    if (IN) {
-      val = qs[(size_t)gy * nx + gx];
-    } else if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
+    const T* src = nullptr;
+    if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
       bool gh = gy == 0 || gy == ny - 1 || gx == 0 || gx == nx - 1;
-      if (!gh) val = qs[(size_t)gy * nx + gx];
+      if (!gh) src = qs + (size_t)gy * nx + gx;
       else if (A.periodic) {
         int sy = gy == 0 ? ny - 2 : (gy == ny - 1 ? 1 : gy);
         int sx = gx == 0 ? nx - 2 : (gx == nx - 1 ? 1 : gx);
-        val = qs[(size_t)sy * nx + sx];
+        src = qs + (size_t)sy * nx + sx;
       }
     }
-    qt[k] = val;
+    if (src) cp_async_elem(qt + k, src);
+    else qt[k] = T(0);
   }
   for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
     int ly = k / (TX + 2), lx = k - ly * (TX + 2);
     int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
-    pt[k] = (IN || (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2)) ? psi[(size_t)(gy - 1) * nxi + (gx - 1)]
-                                                                         : T(0);
+    if (gy >= 1 && gy <= ny - 2 && gx >= 1 && gx <= nx - 2) cp_async_elem(pt + k, psi + (size_t)(gy - 1) * nxi + (gx - 1));
+    else pt[k] = T(0);
+  }
+  cp_async_wait_all();
   }
   __syncthreads();
   // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
@@ -348,11 +377,71 @@ DEV void stage_tile(const StageArgs& A, uint8_t* sm, int x0, int y0) {
   else stage_body<T, S, false, TX, TY>(A, sm, x0, y0);
 }
 
+// Interior tile rectangle [txa, txb] x [tya, tyb] (empty when txa > txb or
+// tya > tyb): the tiles stage_tile runs with the interior body.  The same
+// bounds as stage_tile's test, solved for the tile index.
+struct TileSplit {
+  int ntx, nty, txa, txb, tya, tyb;
+};
+
+template <int S, int TX, int TY>
+static TileSplit tile_split(int ny, int nx) {
+  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
+  constexpr int R = SchemeInfo<S>::reach;
+  TileSplit t;
+  t.ntx = (nx + TX - 1) / TX;
+  t.nty = (ny + TY - 1) / TY;
+  auto in_x = [&](int x0) {
+    return x0 - H >= 1 && x0 + TX + H - 1 <= nx - 2 && x0 - 1 >= R && x0 + TX <= nx - 1 - R;
+  };
+  auto in_y = [&](int y0) {
+    return y0 - H >= 1 && y0 + TY + H - 1 <= ny - 2 && y0 - 1 >= R && y0 + TY <= ny - 1 - R;
+  };
+  t.txa = 0; while (t.txa < t.ntx && !in_x(t.txa * TX)) ++t.txa;
+  t.txb = t.txa; while (t.txb + 1 < t.ntx && in_x((t.txb + 1) * TX)) ++t.txb;
+  t.tya = 0; while (t.tya < t.nty && !in_y(t.tya * TY)) ++t.tya;
+  t.tyb = t.tya; while (t.tyb + 1 < t.nty && in_y((t.tyb + 1) * TY)) ++t.tyb;
+  if (t.txa >= t.ntx || t.tya >= t.nty) { t.txa = 1; t.txb = 0; t.tya = 1; t.tyb = 0; }  // no interior tile
+  return t;
+}
+
+// Block b -> tile: the boundary tiles (the slow, general body) get the
+// lowest block indices so that they start first instead of forming the
+// launch's tail, then the interior rectangle row by row.
+DEV void tile_of_block(const TileSplit& t, int b, int& tx, int& ty) {
+  const int wi = t.txb - t.txa + 1, hi = t.tyb - t.tya + 1;
+  const int ni = (wi > 0 && hi > 0) ? wi * hi : 0;
+  const int nb = t.ntx * t.nty - ni;
+  if (b >= nb) {
+    const int k = b - nb;
+    ty = t.tya + k / wi;
+    tx = t.txa + k % wi;
+    return;
+  }
+  // rows below the rectangle, rows beside it (the columns outside), rows above
+  const int full_lo = ni ? t.tya * t.ntx : nb;
+  if (b < full_lo) { ty = b / t.ntx; tx = b % t.ntx; return; }
+  const int side = t.ntx - wi;
+  const int mid = hi * side;
+  if (b < full_lo + mid) {
+    const int k = b - full_lo;
+    ty = t.tya + k / side;
+    const int c = k % side;
+    tx = c < t.txa ? c : c + wi;
+    return;
+  }
+  const int k = b - full_lo - mid;
+  ty = t.tyb + 1 + k / t.ntx;
+  tx = k % t.ntx;
+}
+
 template <typename T, int S, int TX, int TY>
 __global__ void __launch_bounds__(THREADS)
-stage_kernel(StageArgs A) {
+stage_kernel(StageArgs A, TileSplit ts) {
   extern __shared__ __align__(16) uint8_t sm[];
-  stage_tile<T, S, TX, TY>(A, sm, blockIdx.x * TX, blockIdx.y * TY);
+  int tx, ty;
+  tile_of_block(ts, blockIdx.x, tx, ty);
+  stage_tile<T, S, TX, TY>(A, sm, tx * TX, ty * TY);
 }
 
 template <typename T, int S, int TX, int TY>
