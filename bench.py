@@ -311,6 +311,33 @@ def ensemble_section(members, n_steps, rank=0):
             "launches_per_step": ens.launches_per_step, "autotuned_blocks_per_sm": tuned["blocks_per_sm"]}
 
 
+def per_launch_ms(launch, flush, reps: int = 20, rounds: int = 5) -> float:
+    """Device time of one launch with L2 flushed before it: `reps` (flush,
+    launch) pairs between two events on the launching stream, minus `reps`
+    flushes alone, divided by reps (the median of `rounds`).  The flushes keep
+    the GPU busy while the host queues the next launch, so no host launch
+    gap enters the window."""
+    import torch
+
+    est = []
+    for _ in range(rounds):
+        ts = []
+        for with_launch in (True, False):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            flush.fill_(0.0)
+            e0.record()
+            for k in range(reps):
+                flush.fill_(float(k))
+                if with_launch:
+                    launch()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        est.append((ts[0] - ts[1]) / reps)
+    return statistics.median(est)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -343,7 +370,8 @@ def main():
     tuned = {}
     if not args.profile:
         tuned = {"stage_tile": autotune.tune_qg_stage(model, qa, dt)["tile"],
-                 "fused_split": autotune.tune_qg_split(model, qa, dt)["fused"]}
+                 "fused_split": autotune.tune_qg_split(model, qa, dt)["fused"],
+                 "dst_pair_ctas": autotune.tune_dst_kernel(model, qa, dt)["pair"]}
     qa.copy_(q0)
 
     # warm-up (eager), leaves split(qb) in the DST workspace for the graphs
@@ -446,17 +474,7 @@ def main():
 
     # the fused stage kernel alone (HBM roofline): stage 2's form (reads
     # q_stage, q_n, psi; writes q_next and the split DST operand)
-    st_ms = []
-    for k in range(20):
-        flush.fill_(float(k))
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        model._stage(qa, qb, qb, 0.75, 0.25, 0.25 * dt, True, False)
-        e1.record()
-        e1.synchronize()
-        st_ms.append(e0.elapsed_time(e1))
-    stage_ms = statistics.mean(st_ms)
+    stage_ms = per_launch_ms(lambda: model._stage(qa, qb, qb, 0.75, 0.25, 0.25 * dt, True, False), flush)
     # algorithmic bytes: q_stage, q_n, psi read, q_next written (FP32, one
     # pass each) = 16 B/cell, plus the DST operand written as bf16 hi/lo
     # (4 B/cell)
@@ -475,18 +493,7 @@ def main():
     gemm = fn("fvx_dst_gemm_step")
     for _ in range(5):
         gemm(h, I(0), I(1), stream_ptr())
-    reps = 20
-    gt = []
-    for _ in range(reps):
-        flush.fill_(1.0)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        L.check(gemm(h, I(0), I(1), stream_ptr()), "gemm")
-        e1.record()
-        e1.synchronize()
-        gt.append(e0.elapsed_time(e1))
-    gemm_ms = statistics.mean(gt)
+    gemm_ms = per_launch_ms(lambda: L.check(gemm(h, I(0), I(1), stream_ptr()), "gemm"), flush)
     flops = 2.0 * n * n * n
     peaks = {}
     try:

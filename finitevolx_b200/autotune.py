@@ -8,6 +8,8 @@ fastest:
   128x8 cells; the halo follows the scheme) for one scheme and dtype.
 * ``tune_qg_split``: whether the stage kernel writes the next DST operand
   split itself (fused) or a separate split pass does (unfused).
+* ``tune_dst_kernel``: the even/odd DST product on CTA pairs (cta_group::2,
+  each pair sharing its B blocks) or on single CTAs.
 * ``tune_ensemble``: the persistent work-queue grid (CTAs per SM).
 
 Results are cached in a JSON file keyed by device name and workload
@@ -118,6 +120,37 @@ def tune_qg_split(model, q, dt: float, use_cache: bool = True) -> dict:
     fused = ms["fused"] <= ms["unfused"]
     model.fuse_split = fused
     res = {"fused": fused, "ms": ms}
+    _store(key, res)
+    return res
+
+
+def set_dst_kernel(pair: bool) -> None:
+    check(fn("fvx_dst_kernel_config")(I(1 if pair else 0)), "dst kernel config")
+
+
+def tune_dst_kernel(model, q, dt: float, use_cache: bool = True) -> dict:
+    """CTA-pair against single-CTA even/odd DST products, timed over whole
+    QG steps of ``model`` (a QGModel); returns {"pair": bool, "ms": {...}}."""
+    g = model.grid
+    key = f"{_device_key()}/dst_kernel/{model.dtype}/{g.Ny}x{g.Nx}"
+    if use_cache:
+        hit = _load().get(key)
+        if hit:
+            set_dst_kernel(bool(hit["pair"]))
+            return hit
+    out = torch.empty_like(q)
+
+    def steps():
+        for _ in range(3):
+            model.step(q, dt, out=out)
+
+    ms = {}
+    for name, pair in (("pair", True), ("single", False)):
+        set_dst_kernel(pair)
+        ms[name] = _time(steps)
+    pair = ms["pair"] <= ms["single"]
+    set_dst_kernel(pair)
+    res = {"pair": pair, "ms": ms}
     _store(key, res)
     return res
 

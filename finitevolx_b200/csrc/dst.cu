@@ -124,6 +124,50 @@ DEV void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint
 DEV void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
 }
+// ---- CTA-pair (cta_group::2) forms ----------------------------------------
+DEV uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+// The same shared-memory variable in CTA `rank` of the cluster.
+DEV uint32_t map_to_rank(uint32_t a, uint32_t rank) {
+  uint32_t o;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(o) : "r"(a), "r"(rank));
+  return o;
+}
+// Every thread of both CTAs (the non-.aligned form: callers may arrive from
+// diverged lanes).
+DEV void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire;" ::: "memory");
+}
+// Tile load into this CTA's shared memory whose completion is counted on the
+// pair leader's barrier `bar` (a shared::cluster address).  No multicast.
+DEV void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(bar), "r"(c0), "r"(c1)
+      : "memory");
+}
+// M = 256 product over the pair: A rows 0-127 from the leader's shared
+// memory, 128-255 from the peer's; B's N columns split in halves likewise.
+DEV void umma_bf16_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+// Arrive on barrier `bar` of both CTAs of the pair once the issued MMAs end.
+DEV void umma_commit_pair(uint32_t bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+          bar),
+      "h"((uint16_t)3)
+      : "memory");
+}
 DEV void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 DEV void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 DEV void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
@@ -305,8 +349,137 @@ constexpr int S_STAGE = 2 * S_A_TILE + 2 * S_B_TILE;        // 64 KiB
 constexpr int S_SMEM = SSTAGES * S_STAGE + 1024 + 256;
 constexpr uint32_t kIdesc128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SBN >> 3) << 17) |
                                ((uint32_t)(BM >> 4) << 24);
+// TMA warp, MMA warp and 8 epilogue warps: two per TMEM lane quadrant
+// (warp % 4), each converting half of the tile's columns, so that the
+// epilogue has two warps per scheduler to hide its latencies.
+constexpr int S_THREADS = 320;
 
-__global__ void __launch_bounds__(THREADS, 1)
+// Epilogue of the even/odd product, run by the 8 epilogue warps of a CTA
+// (warps 2-9): P and Q of this CTA's 128 rows from TMEM (columns 0-127 and
+// 128-255) become C[:, k] = P + Q and C[:, K-1-k] = P - Q, scaled, divided
+// by Lambda when the plan asks, and stored (staged in shared memory and
+// written by TMA when ep.tma_out, else by scattered stores).
+DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n0, int K, const Epi& ep,
+                      volatile int* abort_flag, const CUtensorMap* mO0, const CUtensorMap* mO1, int warp,
+                      int lane) {
+  const int KH = K >> 1;
+  const int wq = warp & 3;
+  const int cbeg = ((warp - 2) >> 2) * (SBN / 2);  // this warp's half of the columns
+  const int row = wq * 32 + lane;
+  const int m = m0 + row;
+  const bool mvalid = m < ep.m_total;
+  const int b = mvalid ? m / ep.rows_per_batch : 0;
+  const int r = mvalid ? m - b * ep.rows_per_batch : 0;
+  const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+  if (ok) tc_fence_after();
+  if (ep.tma_out) {
+    // Tile staged in the idle operand ring (all MMAs have completed), then
+    // written by TMA bulk-tensor stores.  The host enables this only when
+    // R is a multiple of 128 and the outputs satisfy TMA's alignment, so
+    // the tile has one batch index b and starts at an even r0.
+    const int R = ep.rows_per_batch;
+    const int bb = m0 / R, r0 = m0 - bb * R;
+    const int be = bb % ep.n_eig;
+    const bool go = ok && !*abort_flag;
+    if (go) {
+      const float alpha = (float)ep.alpha;
+      const bool scaled = ep.alpha != 1.0;
+      const int half = row & 1, rl = row >> 1;
+      const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
+#pragma unroll 1
+      for (int cc = 0; cc < SBN / 2; cc += 32) {
+        const int c0 = cbeg + cc;
+        // 1/Lambda of the chunk's 64 outputs, all loads in flight before use
+        float ivp[32], ivm[32];
+        if (ie) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int k = n0 + c0 + j;
+            ivp[j] = __ldg(ie + (long long)k * R);
+            ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
+          }
+        }
+        uint32_t vp[32], vq[32];
+        const uint32_t lanes = (uint32_t)(wq * 32) << 16;
+        tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
+        tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int kl = c0 + j;
+          const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
+          float xp = P + Q, xm = P - Q;
+          if (scaled) { xp *= alpha; xm *= alpha; }
+          if (ie) {
+            xp *= ivp[j];
+            xm *= ivm[j];
+          }
+          if (ep.mode == EPI_SPLIT) {
+            // boxes [which][half][hi/lo][128 n][64 r] bf16
+            bf16* box = (bf16*)smem;
+            // both values of the pair converted by one packed cvt
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(xp, xm);
+            const __nv_bfloat162 l2 = __floats2bfloat162_rn(xp - __low2float(h2), xm - __high2float(h2));
+            const int op = kl * 64 + rl, om = (127 - kl) * 64 + rl;
+            box[((0 * 2 + half) * 2 + 0) * 8192 + op] = h2.x;
+            box[((0 * 2 + half) * 2 + 1) * 8192 + op] = l2.x;
+            box[((1 * 2 + half) * 2 + 0) * 8192 + om] = h2.y;
+            box[((1 * 2 + half) * 2 + 1) * 8192 + om] = l2.y;
+          } else {
+            // boxes [which][128 n][128 r] fp32
+            float* box = (float*)smem;
+            box[kl * 128 + row] = xp;
+            box[16384 + (127 - kl) * 128 + row] = xm;
+          }
+        }
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("bar.sync 1, 256;" ::: "memory");
+    if (go && warp == 2 && lane == 0) {
+      const uint32_t sb = smem_u32(smem);
+      if (ep.mode == EPI_SPLIT) {
+        for (int which = 0; which < 2; ++which)
+          for (int hf = 0; hf < 2; ++hf)
+            for (int hl = 0; hl < 2; ++hl) {
+              const uint32_t src = sb + (uint32_t)(((which * 2 + hf) * 2 + hl) * 8192 * 2);
+              const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
+              const int y = which ? K - n0 - SBN : n0;
+              tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
+            }
+      } else {
+        tma_store_3d(mO0, sb, r0, n0, bb);
+        tma_store_3d(mO0, sb + 16384 * 4, r0, K - n0 - SBN, bb);
+      }
+      tma_store_commit_wait();
+    }
+  } else if (ok) {
+    if (!*abort_flag) {
+#pragma unroll 1
+      for (int cc = 0; cc < SBN / 2; cc += 32) {
+        const int c0 = cbeg + cc;
+        uint32_t vp[32], vq[32];
+        const uint32_t lanes = (uint32_t)(wq * 32) << 16;
+        tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
+        tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+        tmem_wait_ld();
+        if (mvalid) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int k = n0 + c0 + j;
+            if (k < KH) {
+              const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
+              epi_store(ep, b, r, k, P + Q);
+              epi_store(ep, b, r, K - 1 - k, P - Q);
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+__global__ void __launch_bounds__(S_THREADS, 1)
 gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                      const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
                      const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl,
@@ -382,123 +555,125 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
     }
     umma_commit(accb);
   } else if (warp >= 2) {
-    const int wq = warp & 3;
-    const int row = wq * 32 + lane;
-    const int m = m0 + row;
-    const bool mvalid = m < ep.m_total;
-    const int b = mvalid ? m / ep.rows_per_batch : 0;
-    const int r = mvalid ? m - b * ep.rows_per_batch : 0;
-    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
-    if (ok) tc_fence_after();
-    if (ep.tma_out) {
-      // Tile staged in the idle operand ring (all MMAs have completed), then
-      // written by TMA bulk-tensor stores.  The host enables this only when
-      // R is a multiple of 128 and the outputs satisfy TMA's alignment, so
-      // the tile has one batch index b and starts at an even r0.
-      const int R = ep.rows_per_batch;
-      const int bb = m0 / R, r0 = m0 - bb * R;
-      const int be = bb % ep.n_eig;
-      const bool go = ok && !*abort_flag;
-      if (go) {
-        const float alpha = (float)ep.alpha;
-        const bool scaled = ep.alpha != 1.0;
-        const int half = row & 1, rl = row >> 1;
-        const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
-#pragma unroll 1
-        for (int c0 = 0; c0 < SBN; c0 += 32) {
-          // 1/Lambda of the chunk's 64 outputs, all loads in flight before use
-          float ivp[32], ivm[32];
-          if (ie) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int k = n0 + c0 + j;
-              ivp[j] = __ldg(ie + (long long)k * R);
-              ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
-            }
-          }
-          uint32_t vp[32], vq[32];
-          const uint32_t lanes = (uint32_t)(wq * 32) << 16;
-          tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
-          tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
-          tmem_wait_ld();
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int kl = c0 + j;
-            const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
-            float xp = P + Q, xm = P - Q;
-            if (scaled) { xp *= alpha; xm *= alpha; }
-            if (ie) {
-              xp *= ivp[j];
-              xm *= ivm[j];
-            }
-            if (ep.mode == EPI_SPLIT) {
-              // boxes [which][half][hi/lo][128 n][64 r] bf16
-              bf16* box = (bf16*)smem;
-              // both values of the pair converted by one packed cvt
-              const __nv_bfloat162 h2 = __floats2bfloat162_rn(xp, xm);
-              const __nv_bfloat162 l2 = __floats2bfloat162_rn(xp - __low2float(h2), xm - __high2float(h2));
-              const int op = kl * 64 + rl, om = (127 - kl) * 64 + rl;
-              box[((0 * 2 + half) * 2 + 0) * 8192 + op] = h2.x;
-              box[((0 * 2 + half) * 2 + 1) * 8192 + op] = l2.x;
-              box[((1 * 2 + half) * 2 + 0) * 8192 + om] = h2.y;
-              box[((1 * 2 + half) * 2 + 1) * 8192 + om] = l2.y;
-            } else {
-              // boxes [which][128 n][128 r] fp32
-              float* box = (float*)smem;
-              box[kl * 128 + row] = xp;
-              box[16384 + (127 - kl) * 128 + row] = xm;
-            }
-          }
-        }
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("bar.sync 1, 128;" ::: "memory");
-      if (go && warp == 2 && lane == 0) {
-        const uint32_t sb = smem_u32(smem);
-        if (ep.mode == EPI_SPLIT) {
-          for (int which = 0; which < 2; ++which)
-            for (int hf = 0; hf < 2; ++hf)
-              for (int hl = 0; hl < 2; ++hl) {
-                const uint32_t src = sb + (uint32_t)(((which * 2 + hf) * 2 + hl) * 8192 * 2);
-                const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
-                const int y = which ? K - n0 - SBN : n0;
-                tma_store_3d(hl ? &mO1 : &mO0, src, x, y, bb);
-              }
-        } else {
-          tma_store_3d(&mO0, sb, r0, n0, bb);
-          tma_store_3d(&mO0, sb + 16384 * 4, r0, K - n0 - SBN, bb);
-        }
-        tma_store_commit_wait();
-      }
-    } else if (ok) {
-      if (!*abort_flag) {
-#pragma unroll 1
-        for (int c0 = 0; c0 < SBN; c0 += 32) {
-          uint32_t vp[32], vq[32];
-          const uint32_t lanes = (uint32_t)(wq * 32) << 16;
-          tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
-          tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
-          tmem_wait_ld();
-          if (mvalid) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-              const int k = n0 + c0 + j;
-              if (k < KH) {
-                const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
-                epi_store(ep, b, r, k, P + Q);
-                epi_store(ep, b, r, K - 1 - k, P - Q);
-              }
-            }
-          }
-        }
-      }
-    }
+    sym_epilogue(smem, tmem, accb, m0, n0, K, ep, abort_flag, &mO0, &mO1, warp, lane);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * SBN));
+  }
+}
+
+// The even/odd product on CTA pairs (cta_group::2): the two CTAs of a
+// cluster own rows m0..m0+127 and m0+128..m0+255 of one 256-row tile and
+// share its B blocks, each CTA loading 64 of the 128 table rows.  Per stage
+// a CTA moves 48 KiB (its A hi/lo, half of B hi/lo) instead of 64 KiB, and
+// its tensor core reads 6 KiB of shared memory per 128x128x16 product
+// instead of 8 KiB: shared-memory bandwidth bounds the single-CTA main
+// loop.  The leader (rank 0) issues the M = 256 MMAs; both CTAs' TMA loads
+// complete on the leader's full barriers; each MMA commit arrives on both
+// CTAs' empty barriers.  The epilogue is per CTA (its own TMEM lanes).
+constexpr int P_STAGES = 4;
+constexpr int P_A_TILE = BM * BK * 2;                       // 16 KiB
+constexpr int P_B_TILE = (SBN / 2) * BK * 2;                // 8 KiB
+constexpr int P_STAGE = 2 * P_A_TILE + 2 * P_B_TILE;        // 48 KiB
+constexpr int P_SMEM = P_STAGES * P_STAGE + 1024 + 256;
+constexpr uint32_t kIdescPair = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SBN >> 3) << 17) |
+                                ((uint32_t)((2 * BM) >> 4) << 24);
+static_assert(P_STAGES * P_STAGE >= 2 * 2 * 2 * 8192 * 2, "epilogue staging fits in the operand ring");
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(S_THREADS, 1)
+gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                     const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
+                     const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl,
+                     const __grid_constant__ CUtensorMap mO0, const __grid_constant__ CUtensorMap mO1, int K,
+                     Epi ep) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  uint64_t* bars = (uint64_t*)(smem + P_STAGES * P_STAGE);  // full[S], empty[S], acc
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * P_STAGES + 1);
+  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t rank = cluster_rank();
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * SBN;
+  const int KH = K >> 1;
+  const int KT = 2 * ((KH + BK - 1) / BK);  // P and Q blocks alternate
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[P_STAGES + s]); };
+  const uint32_t accb = smem_u32(&bars[2 * P_STAGES]);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P_STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
+    mbar_init(accb, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {  // the same warp in both CTAs, as the paired allocation requires
+    __syncwarp();
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * SBN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+  }
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs' barriers initialised before any cross-CTA arrive
+  tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  // staggered start, the same for both CTAs of the pair (an even shift
+  // keeps the P / Q alternation)
+  const int kshift = 2 * (int)(((blockIdx.x >> 1) * 5u + blockIdx.y * 3u) % (unsigned)(KT / 2));
+  if (warp == 0 && lane == 0) {
+    for (int kt0 = 0; kt0 < KT; ++kt0) {
+      const int s = kt0 % P_STAGES;
+      if (kt0 >= P_STAGES && !mbar_wait(empty(s), ((kt0 / P_STAGES) - 1) & 1, abort_flag, ep.err)) break;
+      if (rank == 0) mbar_expect_tx(full(s), 2 * P_STAGE);
+      const uint32_t fb = map_to_rank(full(s), 0);
+      const uint32_t base = smem_u32(smem + s * P_STAGE);
+      const int kt = (kt0 + kshift) % KT;
+      const int kb = kt >> 1;
+      const bool odd = kt & 1;
+      const int ac = (odd ? KH : 0) + kb * BK;
+      const int brow = n0 + (int)rank * (SBN / 2);
+      tma_load_2d_pair(base, &mAh, fb, ac, m0);
+      tma_load_2d_pair(base + P_A_TILE, &mAl, fb, ac, m0);
+      tma_load_2d_pair(base + 2 * P_A_TILE, odd ? &mQh : &mPh, fb, kb * BK, brow);
+      tma_load_2d_pair(base + 2 * P_A_TILE + P_B_TILE, odd ? &mQl : &mPl, fb, kb * BK, brow);
+    }
+  } else if (warp == 1 && lane == 0) {
+    if (rank == 0) {
+      bool ok = true;
+      for (int kt0 = 0; kt0 < KT && ok; ++kt0) {
+        const int s = kt0 % P_STAGES;
+        ok = mbar_wait(full(s), (kt0 / P_STAGES) & 1, abort_flag, ep.err);
+        if (!ok) break;
+        tc_fence_after();
+        const uint32_t base = smem_u32(smem + s * P_STAGE);
+        const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + P_A_TILE);
+        const uint64_t bh = sdesc_sw128(base + 2 * P_A_TILE), bl = sdesc_sw128(base + 2 * P_A_TILE + P_B_TILE);
+        const int kt = (kt0 + kshift) % KT;
+        const uint32_t d = tmem + ((kt & 1) ? (uint32_t)SBN : 0u);
+        const bool first = kt0 < 2;  // the first P block and the first Q block overwrite
+#pragma unroll
+        for (int kk = 0; kk < BK / 16; ++kk) {
+          const uint64_t o = (uint64_t)(kk * 32 >> 4);
+          umma_bf16_pair(d, ah + o, bh + o, kIdescPair, !(first && kk == 0));
+          umma_bf16_pair(d, ah + o, bl + o, kIdescPair, 1u);
+          umma_bf16_pair(d, al + o, bh + o, kIdescPair, 1u);
+        }
+        umma_commit_pair(empty(s));
+      }
+      umma_commit_pair(accb);
+    }
+  } else if (warp >= 2) {
+    sym_epilogue(smem, tmem, accb, m0, n0, K, ep, abort_flag, &mO0, &mO1, warp, lane);
+  }
+  tc_fence_before();
+  cluster_sync_all();  // no CTA frees TMEM or exits while its peer may still signal it
+  if (warp == 1) {
+    __syncwarp();
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * SBN));
   }
 }
 
@@ -713,6 +888,11 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Which even/odd kernel runs for row counts that are multiples of 256:
+// 1 = CTA pairs (default), 0 = single CTAs (fvx_dst_kernel_config).
+static int g_sym_pair = 1;
+static bool sym_pair_enabled() { return g_sym_pair == 1; }
+
 // C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns
 // de-interleaved; P/Q: the [K/2][K/2] hi/lo tables.  Needs K % 256 == 0.
 static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph, const bf16* Pl, const bf16* Qh,
@@ -746,9 +926,27 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
                    : make_out_map(&o0, ep.out0, true, R, K, B, ep.ld, ep.batch_stride, 128);
     ep.tma_out = okm ? 1 : 0;
   }
+  if (M % (2 * BM) == 0 && sym_pair_enabled()) {
+    // CTA pairs: B blocks of 64 table rows per CTA
+    static bool pattr = false;
+    if (!pattr) {
+      if (cudaFuncSetAttribute(gemm_sym_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM) !=
+          cudaSuccess)
+        return FVX_ERR_CUDA;
+      pattr = true;
+    }
+    CUtensorMap p2h, p2l, q2h, q2l;
+    if (!make_map(&p2h, Ph, KH, KH, SBN / 2) || !make_map(&p2l, Pl, KH, KH, SBN / 2) ||
+        !make_map(&q2h, Qh, KH, KH, SBN / 2) || !make_map(&q2l, Ql, KH, KH, SBN / 2))
+      return FVX_ERR_ARG;
+    dim3 grid(M / BM, KH / SBN);
+    if (grid.y > 65535) return FVX_ERR_SHAPE;
+    gemm_sym_pair_kernel<<<grid, S_THREADS, P_SMEM, st>>>(a_h, a_l, p2h, p2l, q2h, q2l, o0, o1, K, ep);
+    return fvx_cuda_status();
+  }
   dim3 grid(KH / SBN, (M + BM - 1) / BM);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  gemm_sym_bf16_kernel<<<grid, THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
+  gemm_sym_bf16_kernel<<<grid, S_THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
   return fvx_cuda_status();
 }
 
@@ -1082,6 +1280,13 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
 // One product of the split chain on the plan's workspaces, for timing the
 // tensor-core GEMM in isolation: which 0 = (W1 S_x)^T -> W2, 1 = (W2 S_y) ./
 // Lambda -> W1.  Operands are whatever the workspaces currently hold.
+extern "C" int fvx_dst_kernel_config(int pair) {
+  if (pair < 0) return g_sym_pair;
+  if (pair > 1) return FVX_ERR_ARG;
+  g_sym_pair = pair;
+  return FVX_OK;
+}
+
 extern "C" int fvx_dst_gemm_step(fvx_dst_plan* p, int which, int batch, void* stream) {
   if (!p || !p->split_ok) return FVX_ERR_ARG;
   if (batch < 1 || batch > p->batch_max) return FVX_ERR_SHAPE;

@@ -47,6 +47,33 @@ def test_dst_split_bf16_chain(cuda_ok, shape, lam):
     assert e < 1e-4, e
 
 
+@pytest.mark.parametrize("shape", [(256, 512), (512, 256), (768, 512)])
+def test_dst_pair_and_single_cta_products_agree(cuda_ok, shape):
+    # the even/odd products on CTA pairs (cta_group::2, B blocks shared by the
+    # pair) and on single CTAs: the same 3xBF16 sums in another k order.  Both
+    # within the chain's 1e-4 of the oracle; against each other within 5e-5:
+    # an intermediate that differs by one FP32 ulp can round to another bf16
+    # hi/lo pair, which moves it by up to 2^-16 relative (~1e-5 after the chain)
+    from finitevolx_b200.autotune import set_dst_kernel
+    from finitevolx_b200._lib import fn
+    ny, nx = shape
+    f = O.kminus3_field(ny, nx, 4)
+    ref = O.solve_helmholtz_dst(f, 0.05, 0.07, 1.0)
+    outs = []
+    try:
+        for pair in (True, False):
+            set_dst_kernel(pair)
+            assert fn("fvx_dst_kernel_config")(-1) == int(pair)
+            plan = DSTHelmholtzPlan(ny, nx, 0.05, 0.07, (1.0,))
+            outs.append(host(plan.solve(dev(f, torch.float32))))
+            plan.check_device()
+    finally:
+        set_dst_kernel(True)
+    for o in outs:
+        assert rel_err(o, ref) < 1e-4
+    assert rel_err(outs[0], outs[1]) < 5e-5
+
+
 @pytest.mark.parametrize("shape", [(40, 56), (37, 29), (128, 128)])
 def test_dst_fp64_chain(cuda_ok, shape):
     ny, nx = shape
@@ -167,7 +194,10 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     r2 = autotune.tune_qg_split(m, qd, dt)
     assert set(r2["ms"]) == {"fused", "unfused"}
     assert autotune.tune_qg_stage(m, qd, dt) == r1  # from the cache
+    r3 = autotune.tune_dst_kernel(m, qd, dt)
+    assert set(r3["ms"]) == {"pair", "single"}
     autotune.set_stage_tile("weno5", torch.float32, 0)
+    autotune.set_dst_kernel(True)
 
 
 @pytest.mark.parametrize("method", ("wenoz5", "weno5"))
