@@ -82,6 +82,29 @@ DEV void cp_async_elem(T* dst, const T* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
 }
 DEV void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+DEV void cp_async_8(void* dst, const void* src) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
+
+// ---- tile geometry ----------------------------------------------------------
+// The q tile covers rows y0-H .. y0+TY+H-1 and columns x0-H .. x0+TX+H-1;
+// element (ly, lx) sits at [ly * QW + SH + lx].  The SH leading elements
+// make each stored row start at column x0-H-SH, an even column (x0 is even),
+// so that FP32 rows can be copied in 8-byte pieces; the pitch QW is even and,
+// for FP32, 2 mod 4 (a row per lane then spreads over the banks).
+template <typename T, int S, int TX, int TY>
+struct Geom {
+  static constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
+  static constexpr int QWD = TX + 2 * H;  // q columns the body reads
+  static constexpr int SH = sizeof(T) == 4 ? (H & 1) : 0;
+  static constexpr int QWL = sizeof(T) == 4 ? ((QWD + SH + 1) & ~1) : QWD;  // columns per 8-byte row copy
+  static constexpr int QW = sizeof(T) == 4 ? (QWL % 4 == 0 ? QWL + 2 : QWL) : QWD;
+  static constexpr int QH = TY + 2 * H;
+  static constexpr int NQ = QH * QW;
+  static constexpr int NP = (TY + 2) * (TX + 2);  // psi, origin (y0-1, x0-1)
+  static constexpr int NWORK = (TY + 1) * (TX + 1) + TY * (TX + 1) + 2 * (TY + 1) * TX;  // X, fe, fn, v
+};
 
 // ---- packed FP32 pairs (Blackwell f32x2 arithmetic) -----------------------
 // Two independent values per instruction; each lane is an IEEE round-to-
@@ -159,11 +182,12 @@ DEV float2 weno5_x2(float2 qmm, float2 qm, float2 q0, float2 qp, float2 qpp) {
 // no bounds tests, wrap-around loads, ghost writes or boundary ladder.
 template <typename T, int S, bool IN, int TX, int TY>
 DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0) {
-  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
-  constexpr int QW = TX + 2 * H, QH = TY + 2 * H;
-  T* qt = (T*)sm;                          // [QH][QW]
-  T* pt = qt + QH * QW;                    // psi [TY+2][TX+2], origin (y0-1, x0-1)
-  T* xt = pt + (TY + 2) * (TX + 2);        // X [TY+1][TX+1], origin (y0-1, x0-1)
+  using G = Geom<T, S, TX, TY>;
+  constexpr int H = G::H, QW = G::QW, QWD = G::QWD, QH = G::QH;
+  T* base = (T*)sm;
+  T* qt = base + G::SH;                    // q (ly, lx) at qt[ly * QW + lx]
+  T* pt = base + G::NQ;                    // psi [TY+2][TX+2], origin (y0-1, x0-1)
+  T* xt = pt + G::NP;                      // X [TY+1][TX+1], origin (y0-1, x0-1)
   T* fe = xt + (TY + 1) * (TX + 1);        // [TY][TX+1]
   T* fn = fe + TY * (TX + 1);              // [TY+1][TX]
   T* vs = fn + (TY + 1) * TX;              // v on north faces [TY+1][TX], origin (y0-1, x0)
@@ -174,20 +198,46 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   const int nxi = nx - 2;
   // ---- loads: q with BC applied on the fly, psi with zero outside --------
   if constexpr (IN) {
-    for (int k = tid; k < QH * QW; k += THREADS) {
-      const int ly = k / QW, lx = k - ly * QW;
-      cp_async_elem(qt + k, qs + (size_t)(y0 - H + ly) * nx + (x0 - H + lx));
+    {
+      const bool v8 = sizeof(T) == 8 || (((uintptr_t)qs | (uintptr_t)psi) & 7) == 0 && (nx & 1) == 0;
+      if (v8) {
+        // 8-byte pieces; each thread keeps one column of pieces and walks
+        // the rows with pointer increments
+        constexpr int E = 8 / (int)sizeof(T);
+        constexpr int CQ = G::QWL / E, RQ = THREADS / CQ;
+        constexpr int CP = (TX + 2) / E, RP = THREADS / CP;
+        static_assert(RQ >= 1 && RP >= 1, "tile rows wider than the block");
+        int r = tid / CQ;
+        if (r < RQ) {
+          const int c = tid - r * CQ;
+          const T* src = qs + (size_t)(y0 - H + r) * nx + (x0 - H - G::SH + c * E);
+          T* dst = base + r * QW + c * E;
+          for (; r < QH; r += RQ, src += (size_t)RQ * nx, dst += RQ * QW) cp_async_8(dst, src);
+        }
+        r = tid / CP;
+        if (r < RP) {
+          const int c = tid - r * CP;
+          const T* src = psi + (size_t)(y0 - 2 + r) * nxi + (x0 - 2 + c * E);
+          T* dst = pt + r * (TX + 2) + c * E;
+          for (; r < TY + 2; r += RP, src += (size_t)RP * nxi, dst += RP * (TX + 2)) cp_async_8(dst, src);
+        }
+      } else {
+        for (int k = tid; k < QH * QWD; k += THREADS) {
+          const int ly = k / QWD, lx = k - ly * QWD;
+          cp_async_elem(qt + ly * QW + lx, qs + (size_t)(y0 - H + ly) * nx + (x0 - H + lx));
+        }
+        for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
+          const int ly = k / (TX + 2), lx = k - ly * (TX + 2);
+          cp_async_elem(pt + k, psi + (size_t)(y0 - 2 + ly) * nxi + (x0 - 2 + lx));
+        }
+      }
+      cp_async_wait_all();
     }
-    for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
-      const int ly = k / (TX + 2), lx = k - ly * (TX + 2);
-      cp_async_elem(pt + k, psi + (size_t)(y0 - 2 + ly) * nxi + (x0 - 2 + lx));
-    }
-    cp_async_wait_all();
   } else {
   // general tiles: wrap-around / zero-ring sources resolved per element, the
   // copies themselves asynchronous (one wait for the whole tile)
-  for (int k = tid; k < QH * QW; k += THREADS) {
-    int ly = k / QW, lx = k - ly * QW;
+  for (int k = tid; k < QH * QWD; k += THREADS) {
+    int ly = k / QWD, lx = k - ly * QWD;
     int gy = y0 - H + ly, gx = x0 - H + lx;
     const T* src = nullptr;
     if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) {
@@ -199,8 +249,8 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
         src = qs + (size_t)sy * nx + sx;
       }
     }
-    if (src) cp_async_elem(qt + k, src);
-    else qt[k] = T(0);
+    if (src) cp_async_elem(qt + ly * QW + lx, src);
+    else qt[ly * QW + lx] = T(0);
   }
   for (int k = tid; k < (TY + 2) * (TX + 2); k += THREADS) {
     int ly = k / (TX + 2), lx = k - ly * (TX + 2);
@@ -212,6 +262,25 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   }
   __syncthreads();
   // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
+  if constexpr (IN && THREADS % TX == 0 && THREADS / TX <= TY + 1) {
+    // a column of X per thread group, walking down the rows (two new psi
+    // loads per row); the last column by the first TY + 1 threads
+    constexpr int RG = THREADS / TX, RPG = (TY + 1 + RG - 1) / RG;
+    const int lx = tid % TX, g = tid / TX;
+    const int r0 = g * RPG, r1 = r0 + RPG < TY + 1 ? r0 + RPG : TY + 1;
+    const T* p = pt + r0 * (TX + 2) + lx;
+    T a0 = p[0] + p[1];
+    for (int ly = r0; ly < r1; ++ly) {
+      p += TX + 2;
+      const T a1 = p[0] + p[1];
+      xt[ly * (TX + 1) + lx] = T(0.25) * (a0 + a1);
+      a0 = a1;
+    }
+    if (tid < TY + 1) {
+      const T* q = pt + tid * (TX + 2) + TX;
+      xt[tid * (TX + 1) + TX] = T(0.25) * (q[0] + q[1] + q[TX + 2] + q[TX + 3]);
+    }
+  } else
   for (int k = tid; k < (TY + 1) * (TX + 1); k += THREADS) {
     int ly = k / (TX + 1), lx = k - ly * (TX + 1);
     int gy = y0 - 1 + ly, gx = x0 - 1 + lx;
@@ -237,9 +306,73 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     return divr(p[0] - p[-1], dx, rdx);
   };
   // ---- face fluxes --------------------------------------------------------
+  // FP32 WENO5 / WENO-Z5 interior tiles: each thread reconstructs a run of
+  // SEG east faces along a row and a run of SEG north faces along a column
+  // from a register window of SEG + 5 cells (one shared-memory load per
+  // face instead of six), the upwind stencil picked from the window and two
+  // neighbouring faces evaluated as one packed f32x2 pair.
+  constexpr int SEG = TX * TY / THREADS;
+  constexpr bool WIN = IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && SEG >= 2 && SEG % 2 == 0 &&
+                       SEG * THREADS == TX * TY && TX % SEG == 0 && TY % SEG == 0;
   constexpr bool PACK =
-      IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
-  if constexpr (PACK) {
+      !WIN && IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
+  if constexpr (WIN) {
+    constexpr bool Z = SchemeInfo<S>::zfam;
+    const float* q32 = (const float*)qt;
+    {  // east faces of cells x0 + xs .. x0 + xs + SEG - 1 on row ly
+      const int ly = tid % TY, xs = (tid / TY) * SEG;
+      const float* p = q32 + (ly + H) * QW + (xs + H);  // q at (y0 + ly, x0 + xs)
+      float w[SEG + 5];
+#pragma unroll
+      for (int k = 0; k < SEG + 5; ++k) w[k] = p[k - 2];
+#pragma unroll
+      for (int f = 0; f < SEG; f += 2) {  // faces f and f + 1 as one packed pair
+        const float u0 = (float)uvel(y0 + ly, x0 + xs + f), u1 = (float)uvel(y0 + ly, x0 + xs + f + 1);
+        const bool p0 = u0 >= 0.f, p1 = u1 >= 0.f;
+        float2 e[5];
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+          e[j] = make_float2(p0 ? w[f + j] : w[f + 5 - j], p1 ? w[f + 1 + j] : w[f + 6 - j]);
+        const float2 r = weno5_x2<Z>(e[0], e[1], e[2], e[3], e[4]);
+        fe[ly * (TX + 1) + xs + f + 1] = (T)(r.x * u0);
+        fe[ly * (TX + 1) + xs + f + 2] = (T)(r.y * u1);
+      }
+    }
+    {  // north faces of cells y0 + ys .. y0 + ys + SEG - 1 in column lx
+      const int lx = tid % TX, ys = (tid / TX) * SEG;
+      const float* p = q32 + (ys + H) * QW + (lx + H);  // q at (y0 + ys, x0 + lx)
+      float w[SEG + 5];
+#pragma unroll
+      for (int k = 0; k < SEG + 5; ++k) w[k] = p[(k - 2) * QW];
+#pragma unroll
+      for (int f = 0; f < SEG; f += 2) {
+        const float v0 = (float)vvel(y0 + ys + f, x0 + lx), v1 = (float)vvel(y0 + ys + f + 1, x0 + lx);
+        const bool p0 = v0 >= 0.f, p1 = v1 >= 0.f;
+        float2 e[5];
+#pragma unroll
+        for (int j = 0; j < 5; ++j)
+          e[j] = make_float2(p0 ? w[f + j] : w[f + 5 - j], p1 ? w[f + 1 + j] : w[f + 6 - j]);
+        const float2 r = weno5_x2<Z>(e[0], e[1], e[2], e[3], e[4]);
+        fn[(ys + f + 1) * TX + lx] = (T)(r.x * v0);
+        fn[(ys + f + 2) * TX + lx] = (T)(r.y * v1);
+        vs[(ys + f + 1) * TX + lx] = (T)v0;
+        vs[(ys + f + 2) * TX + lx] = (T)v1;
+      }
+    }
+    // the tile's west-most east faces and south-most north faces
+    for (int k = tid; k < TY + TX; k += THREADS) {
+      if (k < TY) {
+        const int ly = k, gj = y0 + ly, gi = x0 - 1;
+        const T uu = uvel(gj, gi);
+        fe[ly * (TX + 1)] = face_value_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
+      } else {
+        const int lx = k - TY, gj = y0 - 1, gi = x0 + lx;
+        const T vv = vvel(gj, gi);
+        fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+        vs[lx] = vv;
+      }
+    }
+  } else if constexpr (PACK) {
     // each cell's east and north faces as one packed pair of reconstructions
     for (int k = tid; k < TY * TX; k += THREADS) {
       const int ly = k / TX, lx = k % TX;
@@ -307,6 +440,46 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   T* out = (T*)A.out;
   const T beta = T(A.beta), drag = T(A.drag), visc = T(A.visc);
   const T ca = T(A.a), cb = T(A.b), cc = T(A.c);
+  constexpr int SEGT = TX * TY / THREADS;
+  if constexpr (IN && SEGT >= 1 && SEGT * THREADS == TX * TY && TY % SEGT == 0) {
+    if (!F && A.drag == 0.0 && A.visc == 0.0) {
+      // interior tile without forcing, drag or viscosity: a run of SEGT
+      // cells down one column per thread (coalesced rows across a warp),
+      // each north face / v reused as the next cell's south one
+      const int lx = tid % TX, ly0 = (tid / TX) * SEGT;
+      const int gi = x0 + lx;
+      size_t g = (size_t)(y0 + ly0) * nx + gi;
+      const T* fep = fe + ly0 * (TX + 1) + lx;
+      const T* fnp = fn + ly0 * TX + lx;
+      const T* vsp = vs + ly0 * TX + lx;
+      const T* qp = qt + (ly0 + H) * QW + (lx + H);
+      const int xi = gi - 1;
+      const int scol = A.split_layout ? ((xi & 1) ? (nxi >> 1) + (xi >> 1) : (xi >> 1)) : xi;
+      size_t sidx = (size_t)(y0 + ly0 - 1) * nxi + scol;
+      T fs = fnp[0], vsv = vsp[0];
+#pragma unroll
+      for (int f = 0; f < SEGT; ++f) {
+        const T fnn = fnp[(f + 1) * TX], vn = vsp[(f + 1) * TX];
+        T rhs = -(divr(fep[f * (TX + 1) + 1] - fep[f * (TX + 1)], dx, rdx) + divr(fnn - fs, dy, rdy));
+        rhs = rhs + (-beta * (T(0.5) * (vn + vsv)));
+        T r = cb * qp[f * QW];
+        if (qn) r = ca * qn[g] + r;
+        r = r + cc * rhs;
+        out[g] = r;
+        if (A.split_hi) {
+          const float fv = (float)r;
+          const __nv_bfloat16 h = __float2bfloat16_rn(fv);
+          A.split_hi[sidx] = h;
+          A.split_lo[sidx] = __float2bfloat16_rn(fv - __bfloat162float(h));
+        }
+        g += nx;
+        sidx += nxi;
+        fs = fnn;
+        vsv = vn;
+      }
+      return;
+    }
+  }
   for (int k = tid; k < TY * TX; k += THREADS) {
     int ly = k / TX, lx = k - ly * TX;
     int gj = y0 + ly, gi = x0 + lx;
@@ -446,10 +619,8 @@ stage_kernel(StageArgs A, TileSplit ts) {
 
 template <typename T, int S, int TX, int TY>
 static size_t smem_bytes() {
-  constexpr int H = SchemeInfo<S>::halo_hi > 3 ? SchemeInfo<S>::halo_hi : 3;
-  size_t n = (size_t)(TY + 2 * H) * (TX + 2 * H) + (TY + 2) * (TX + 2) + (TY + 1) * (TX + 1) + TY * (TX + 1) +
-             2 * (TY + 1) * TX;
-  return n * sizeof(T);
+  using G = Geom<T, S, TX, TY>;
+  return (size_t)(G::NQ + G::NP + G::NWORK) * sizeof(T);
 }
 
 }  // namespace qg
