@@ -31,17 +31,29 @@ from finitevolx_b200.diffusion import BiharmonicDiffusion2D, Diffusion2D, diffus
 from finitevolx_b200.boundary import enforce_periodic, enforce_periodic_, pad_interior
 from finitevolx_b200.timestepping import euler_step, heun_step, rk3_ssp_step
 from finitevolx_b200.solvers import (
+    CapacitanceSolver,
     CGInfo,
     DSTHelmholtzPlan,
     MaskedHelmholtzPCG,
     MultigridSolver,
+    SpectralHelmholtzPlan,
+    build_capacitance_solver,
     build_multigrid_solver,
+    dct2_eigenvalues,
+    dst1_eigenvalues,
+    fft_eigenvalues,
     make_multigrid_preconditioner,
+    make_spectral_preconditioner,
     masked_laplacian,
+    pressure_from_divergence,
     pv_inversion,
     solve_cg,
+    solve_helmholtz_dct,
     solve_helmholtz_dst,
+    solve_helmholtz_fft,
+    solve_poisson_dct,
     solve_poisson_dst,
+    solve_poisson_fft,
     streamfunction_from_vorticity,
 )
 from finitevolx_b200.vertical import (
@@ -63,6 +75,9 @@ __all__ = [
     "enforce_periodic_", "pad_interior", "euler_step", "heun_step", "rk3_ssp_step", "CGInfo",
     "DSTHelmholtzPlan", "MaskedHelmholtzPCG", "MultigridSolver", "build_multigrid_solver",
     "make_multigrid_preconditioner", "masked_laplacian", "pv_inversion", "solve_cg", "solve_helmholtz_dst",
+    "CapacitanceSolver", "SpectralHelmholtzPlan", "build_capacitance_solver", "dct2_eigenvalues",
+    "dst1_eigenvalues", "fft_eigenvalues", "make_spectral_preconditioner", "pressure_from_divergence",
+    "solve_helmholtz_dct", "solve_helmholtz_fft", "solve_poisson_dct", "solve_poisson_fft",
     "solve_poisson_dst", "streamfunction_from_vorticity", "build_coupling_matrix",
     "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel", "QGEnsemble",
     "Coriolis2D", "MomentumAdvection2D", "Vorticity2D", "diagnostics",

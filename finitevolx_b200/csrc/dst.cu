@@ -970,7 +970,9 @@ using namespace fvx::dst;
 
 struct fvx_dst_plan {
   int ny, nx, batch_max, n_lam;
+  int kind = FVX_SPECTRAL_DST;  // transform pair (fvx_spectral_plan_create)
   double dx, dy;
+  double cfin = 1.0;            // scale of the last product
   bool split_ok;
   std::vector<double> lam_host;
   double* lam_dev = nullptr;
@@ -979,6 +981,9 @@ struct fvx_dst_plan {
   bf16 *xPh = nullptr, *xPl = nullptr, *xQh = nullptr, *xQl = nullptr;  // [nx/2][nx/2]
   bf16 *yPh = nullptr, *yPl = nullptr, *yQh = nullptr, *yQl = nullptr;  // [ny/2][ny/2]
   double *Sx64 = nullptr, *Sy64 = nullptr;
+  // inverse-transform operands (DCT-II, periodic); the DST-I plan reuses S
+  bf16 *Ixh = nullptr, *Ixl = nullptr, *Iyh = nullptr, *Iyl = nullptr;
+  double *Ix64 = nullptr, *Iy64 = nullptr;
   float* inv32 = nullptr;   // [n_lam][ny][nx]
   double* inv64 = nullptr;  // [n_lam][ny][nx]
   bf16 *W1h = nullptr, *W1l = nullptr, *W2h = nullptr, *W2l = nullptr;
@@ -990,27 +995,93 @@ struct fvx_dst_plan {
 static void dst_free(fvx_dst_plan* p) {
   void* ptrs[] = {p->lam_dev, p->Sxh, p->Sxl, p->Syh, p->Syl, p->Sx64, p->Sy64, p->inv32, p->inv64,
                   p->W1h,     p->W1l, p->W2h, p->W2l, p->V1,  p->V2,  p->norms, p->err,
-                  p->xPh,     p->xPl, p->xQh, p->xQl, p->yPh, p->yPl, p->yQh,   p->yQl};
+                  p->xPh,     p->xPl, p->xQh, p->xQl, p->yPh, p->yPl, p->yQh,   p->yQl,
+                  p->Ixh,     p->Ixl, p->Iyh, p->Iyl, p->Ix64, p->Iy64};
   for (void* q : ptrs)
     if (q) cudaFree(q);
 }
 
+// Transform pairs of one axis of length n: forward T[k][j] (coefficient k
+// of sample j) and inverse Tinv[j][k] (sample j from coefficient k), FP64,
+// row-major, with the 1-D eigenvalues of the 3-point second difference they
+// diagonalise.
+//   DST-I  (Dirichlet, n interior points): T = sin(pi (j+1)(k+1)/(n+1)),
+//          Tinv = T (the 2/(n+1) factors go to the last product's scale),
+//          e_k = -4/h^2 sin^2(pi (k+1) / (2(n+1)))
+//   DCT-II (Neumann, cell-centred): T = cos(pi k (2j+1) / (2n)),
+//          Tinv[j][k] = w_k T[k][j], w_0 = 1/n, w_k = 2/n,
+//          e_k = -4/h^2 sin^2(pi k / (2n))
+//   periodic: the real Hartley basis T = cos(2 pi k j / n) + sin(2 pi k j / n)
+//          (symmetric, T T = n I, and it diagonalises the periodic second
+//          difference because e_k = e_{n-k}), Tinv = T / n,
+//          e_k = -4/h^2 sin^2(pi k / n)
+// Arguments are reduced exactly in integers before the FP64 sin / cos.
+static void transform_pair(int kind, int n, double h, std::vector<double>& T, std::vector<double>& Ti,
+                           std::vector<double>& e) {
+  T.assign((size_t)n * n, 0.0);
+  Ti.assign((size_t)n * n, 0.0);
+  e.assign(n, 0.0);
+  for (int k = 0; k < n; ++k) {
+    double sarg;
+    if (kind == FVX_SPECTRAL_DST) sarg = M_PI * (k + 1) / (2.0 * (n + 1));
+    else if (kind == FVX_SPECTRAL_DCT) sarg = M_PI * k / (2.0 * n);
+    else sarg = M_PI * k / (double)n;
+    const double sv = std::sin(sarg);
+    e[k] = -4.0 / (h * h) * sv * sv;
+    for (int j = 0; j < n; ++j) {
+      double t;
+      if (kind == FVX_SPECTRAL_DST) {
+        const long long q = ((long long)(j + 1) * (k + 1)) % (2LL * (n + 1));
+        t = std::sin(M_PI * (double)q / (double)(n + 1));
+      } else if (kind == FVX_SPECTRAL_DCT) {
+        const long long q = ((long long)k * (2 * j + 1)) % (4LL * n);
+        t = std::cos(M_PI * (double)q / (2.0 * n));
+      } else {
+        const long long q = ((long long)k * j) % (long long)n;
+        const double a = 2.0 * M_PI * (double)q / (double)n;
+        t = std::cos(a) + std::sin(a);
+      }
+      T[(size_t)k * n + j] = t;
+      double w = 1.0;
+      if (kind == FVX_SPECTRAL_DCT) w = (k == 0 ? 1.0 : 2.0) / n;
+      else if (kind == FVX_SPECTRAL_PERIODIC) w = 1.0 / n;
+      Ti[(size_t)j * n + k] = w * t;
+    }
+  }
+}
+
+extern "C" int fvx_spectral_plan_create(int kind, int ny, int nx, double dx, double dy, int batch_max,
+                                        const double* lambdas, int n_lambda, int want_fp64, fvx_dst_plan** out);
+
 extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int batch_max, const double* lambdas,
                                    int n_lambda, int want_fp64, fvx_dst_plan** out) {
+  return fvx_spectral_plan_create(FVX_SPECTRAL_DST, ny, nx, dx, dy, batch_max, lambdas, n_lambda, want_fp64, out);
+}
+
+extern "C" int fvx_spectral_plan_create(int kind, int ny, int nx, double dx, double dy, int batch_max,
+                                        const double* lambdas, int n_lambda, int want_fp64, fvx_dst_plan** out) {
   if (!out || !lambdas) return FVX_ERR_ARG;
   *out = nullptr;
+  if (kind != FVX_SPECTRAL_DST && kind != FVX_SPECTRAL_DCT && kind != FVX_SPECTRAL_PERIODIC) return FVX_ERR_METHOD;
   if (ny < 1 || nx < 1 || batch_max < 1 || n_lambda < 1) return FVX_ERR_SHAPE;
   fvx_dst_plan* p = new fvx_dst_plan();
+  p->kind = kind;
   p->ny = ny; p->nx = nx; p->dx = dx; p->dy = dy; p->batch_max = batch_max; p->n_lam = n_lambda;
   p->lam_host.assign(lambdas, lambdas + n_lambda);
   p->split_ok = (nx % 8 == 0) && (ny % 8 == 0);
-  p->sym = p->split_ok && nx % (2 * SBN) == 0 && ny % (2 * SBN) == 0;
+  p->sym = kind == FVX_SPECTRAL_DST && p->split_ok && nx % (2 * SBN) == 0 && ny % (2 * SBN) == 0;
+  p->cfin = kind == FVX_SPECTRAL_DST ? 4.0 / ((double)(ny + 1) * (double)(nx + 1)) : 1.0;
+  const bool dst = kind == FVX_SPECTRAL_DST;
   const size_t plane = (size_t)ny * nx, work = plane * batch_max;
   bool ok = true;
   auto A = [&](void** q, size_t bytes) { if (ok && cudaMalloc(q, bytes) != cudaSuccess) ok = false; };
   A((void**)&p->lam_dev, sizeof(double) * n_lambda);
   A((void**)&p->Sx64, sizeof(double) * nx * nx);
   A((void**)&p->Sy64, sizeof(double) * ny * ny);
+  if (!dst) {
+    A((void**)&p->Ix64, sizeof(double) * nx * nx);
+    A((void**)&p->Iy64, sizeof(double) * ny * ny);
+  }
   A((void**)&p->inv32, sizeof(float) * plane * n_lambda);
   A((void**)&p->inv64, sizeof(double) * plane * n_lambda);
   A((void**)&p->norms, sizeof(double) * 4);
@@ -1018,6 +1089,10 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
   if (p->split_ok) {
     A((void**)&p->Sxh, sizeof(bf16) * nx * nx); A((void**)&p->Sxl, sizeof(bf16) * nx * nx);
     A((void**)&p->Syh, sizeof(bf16) * ny * ny); A((void**)&p->Syl, sizeof(bf16) * ny * ny);
+    if (!dst) {
+      A((void**)&p->Ixh, sizeof(bf16) * nx * nx); A((void**)&p->Ixl, sizeof(bf16) * nx * nx);
+      A((void**)&p->Iyh, sizeof(bf16) * ny * ny); A((void**)&p->Iyl, sizeof(bf16) * ny * ny);
+    }
     A((void**)&p->W1h, sizeof(bf16) * work); A((void**)&p->W1l, sizeof(bf16) * work);
     A((void**)&p->W2h, sizeof(bf16) * work); A((void**)&p->W2l, sizeof(bf16) * work);
   }
@@ -1033,34 +1108,41 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
     A((void**)&p->V2, sizeof(double) * work);
   }
   if (!ok) { dst_free(p); delete p; return FVX_ERR_CUDA; }
-  // host-side tables in FP64
-  auto fill_S = [](int n, std::vector<double>& S) {
-    S.resize((size_t)n * n);
-    for (int j = 0; j < n; ++j)
-      for (int k = 0; k < n; ++k) {
-        // sin(pi (j+1)(k+1)/(n+1)) with the argument reduced mod 2(n+1) to keep it exact
-        long long q = ((long long)(j + 1) * (k + 1)) % (2LL * (n + 1));
-        S[(size_t)j * n + k] = std::sin(M_PI * (double)q / (double)(n + 1));
-      }
+  // host-side tables in FP64.  Operands: the tensor-core products read B
+  // as [out][in] (T itself for the forward, Tinv for the inverse); the FP64
+  // products read [in][out] (the transposes).
+  std::vector<double> Tx, Tix, ex, Ty, Tiy, ey;
+  transform_pair(kind, nx, dx, Tx, Tix, ex);
+  transform_pair(kind, ny, dy, Ty, Tiy, ey);
+  auto transpose = [](const std::vector<double>& M, int n) {
+    std::vector<double> R(M.size());
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) R[(size_t)b * n + a] = M[(size_t)a * n + b];
+    return R;
   };
-  std::vector<double> Sx, Sy;
-  fill_S(nx, Sx);
-  fill_S(ny, Sy);
-  std::vector<double> ex(nx), ey(ny);
-  for (int i = 0; i < nx; ++i) { double s = std::sin(M_PI * (i + 1) / (2.0 * (nx + 1))); ex[i] = -4.0 / (dx * dx) * s * s; }
-  for (int j = 0; j < ny; ++j) { double s = std::sin(M_PI * (j + 1) / (2.0 * (ny + 1))); ey[j] = -4.0 / (dy * dy) * s * s; }
+  const std::vector<double> Sx = Tx, Sy = Ty;  // split operands [out][in]
   std::vector<double> inv64(plane * n_lambda);
   std::vector<float> inv32(plane * n_lambda);
   for (int l = 0; l < n_lambda; ++l)
     for (int j = 0; j < ny; ++j)
       for (int i = 0; i < nx; ++i) {
-        double v = 1.0 / ((ey[j] + ex[i]) - lambdas[l]);
+        // the null mode (Neumann / periodic Poisson) gets 0: the zero-mean solution
+        const double d = (ey[j] + ex[i]) - lambdas[l];
+        const double v = d == 0.0 ? 0.0 : 1.0 / d;
         inv64[(size_t)l * plane + (size_t)j * nx + i] = v;
         inv32[(size_t)l * plane + (size_t)j * nx + i] = (float)v;
       }
   cudaMemcpy(p->lam_dev, lambdas, sizeof(double) * n_lambda, cudaMemcpyHostToDevice);
-  cudaMemcpy(p->Sx64, Sx.data(), sizeof(double) * Sx.size(), cudaMemcpyHostToDevice);
-  cudaMemcpy(p->Sy64, Sy.data(), sizeof(double) * Sy.size(), cudaMemcpyHostToDevice);
+  {
+    const std::vector<double> fx = transpose(Tx, nx), fy = transpose(Ty, ny);
+    cudaMemcpy(p->Sx64, fx.data(), sizeof(double) * fx.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(p->Sy64, fy.data(), sizeof(double) * fy.size(), cudaMemcpyHostToDevice);
+    if (!dst) {
+      const std::vector<double> ix = transpose(Tix, nx), iy = transpose(Tiy, ny);
+      cudaMemcpy(p->Ix64, ix.data(), sizeof(double) * ix.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(p->Iy64, iy.data(), sizeof(double) * iy.size(), cudaMemcpyHostToDevice);
+    }
+  }
   cudaMemcpy(p->inv64, inv64.data(), sizeof(double) * inv64.size(), cudaMemcpyHostToDevice);
   cudaMemcpy(p->inv32, inv32.data(), sizeof(float) * inv32.size(), cudaMemcpyHostToDevice);
   if (p->split_ok) {
@@ -1079,6 +1161,14 @@ extern "C" int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int bat
     split(Sy, h, l);
     cudaMemcpy(p->Syh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
     cudaMemcpy(p->Syl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+    if (!dst) {
+      split(Tix, h, l);
+      cudaMemcpy(p->Ixh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(p->Ixl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+      split(Tiy, h, l);
+      cudaMemcpy(p->Iyh, h.data(), sizeof(bf16) * h.size(), cudaMemcpyHostToDevice);
+      cudaMemcpy(p->Iyl, l.data(), sizeof(bf16) * l.size(), cudaMemcpyHostToDevice);
+    }
     if (p->sym) {
       // B_P[k][j'] = S[2j'][k], B_Q[k][j'] = S[2j'+1][k] for k, j' < n/2
       auto halves = [&](const std::vector<double>& S, int n, bf16* Ph, bf16* Pl, bf16* Qh, bf16* Ql) {
@@ -1142,7 +1232,10 @@ static Epi make_epi(fvx_dst_plan* p, int mode, int R, int M, int N, void* o0, vo
 static int chain_split(fvx_dst_plan* p, int B, int out_mode, void* out, long long ob, long long old,
                        cudaStream_t st) {
   const int ny = p->ny, nx = p->nx;
-  const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
+  const double c = p->cfin;
+  const bool dst = p->kind == FVX_SPECTRAL_DST;
+  const bf16 *Ixh = dst ? p->Sxh : p->Ixh, *Ixl = dst ? p->Sxl : p->Ixl;
+  const bf16 *Iyh = dst ? p->Syh : p->Iyh, *Iyl = dst ? p->Syl : p->Iyl;
   int rc;
   if (p->sym) {
     // even/odd products; every intermediate is stored de-interleaved along
@@ -1164,24 +1257,27 @@ static int chain_split(fvx_dst_plan* p, int B, int out_mode, void* out, long lon
   Epi e2 = make_epi(p, EPI_SPLIT, nx, B * nx, ny, p->W1h, p->W1l, (long long)ny * nx, nx, 0, 0, 1.0, true);
   // inv_eig is indexed [n][r] = [y'][x'] = the [ny][nx] grid
   if ((rc = gemm_split(p->W2h, p->W2l, B * nx, ny, p->Syh, p->Syl, ny, e2, st))) return rc;
-  // 3: (G S_x)^T -> W2
-  if ((rc = gemm_split(p->W1h, p->W1l, B * ny, nx, p->Sxh, p->Sxl, nx, e1, st))) return rc;
-  // 4: c S_y G S_x -> out [B][ny][nx]
+  // 3: inverse along x -> W2
+  if ((rc = gemm_split(p->W1h, p->W1l, B * ny, nx, Ixh, Ixl, nx, e1, st))) return rc;
+  // 4: inverse along y, scaled -> out [B][ny][nx]
   Epi e4 = make_epi(p, out_mode, nx, B * nx, ny, out, nullptr, ob, old, 0, 0, c, false);
-  return gemm_split(p->W2h, p->W2l, B * nx, ny, p->Syh, p->Syl, ny, e4, st);
+  return gemm_split(p->W2h, p->W2l, B * nx, ny, Iyh, Iyl, ny, e4, st);
 }
 
 static int chain_f64(fvx_dst_plan* p, int B, int out_mode, void* out, long long ob, long long old, cudaStream_t st) {
   const int ny = p->ny, nx = p->nx;
-  const double c = 4.0 / ((double)(ny + 1) * (double)(nx + 1));
+  const double c = p->cfin;
+  const bool dst = p->kind == FVX_SPECTRAL_DST;
+  const double* Ix = dst ? p->Sx64 : p->Ix64;
+  const double* Iy = dst ? p->Sy64 : p->Iy64;
   int rc;
   Epi e1 = make_epi(p, EPI_F64, ny, B * ny, nx, p->V2, nullptr, (long long)nx * ny, ny, 0, 0, 1.0, false);
   if ((rc = gemm_f64(p->V1, nx, B * ny, nx, p->Sx64, nx, e1, st))) return rc;
   Epi e2 = make_epi(p, EPI_F64, nx, B * nx, ny, p->V1, nullptr, (long long)ny * nx, nx, 0, 0, 1.0, true);
   if ((rc = gemm_f64(p->V2, ny, B * nx, ny, p->Sy64, ny, e2, st))) return rc;
-  if ((rc = gemm_f64(p->V1, nx, B * ny, nx, p->Sx64, nx, e1, st))) return rc;
+  if ((rc = gemm_f64(p->V1, nx, B * ny, nx, Ix, nx, e1, st))) return rc;
   Epi e4 = make_epi(p, out_mode, nx, B * nx, ny, out, nullptr, ob, old, 0, 0, c, false);
-  return gemm_f64(p->V2, ny, B * nx, ny, p->Sy64, ny, e4, st);
+  return gemm_f64(p->V2, ny, B * nx, ny, Iy, ny, e4, st);
 }
 
 // FP32 solve through the split-BF16 tensor-core chain.  rhs / psi are
@@ -1249,6 +1345,7 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
     if (info) { info[0] = 1; info[1] = -1; info[2] = -1; }
     return rc;
   }
+  if (p->kind != FVX_SPECTRAL_DST) return FVX_ERR_METHOD;  // refinement: Dirichlet residual only
   double lam_max = 0;
   for (double l : p->lam_host) lam_max = fmax(lam_max, fabs(l));
   const double anorm = 4.0 / (p->dx * p->dx) + 4.0 / (p->dy * p->dy) + lam_max;

@@ -42,6 +42,14 @@ enum fvx_scheme {
   FVX_NUM_SCHEMES = 14,
 };
 
+// Rectangular spectral Helmholtz solvers (solvers/spectral.py:105-128 bc
+// names "dst", "dct", "fft").
+enum fvx_spectral_kind {
+  FVX_SPECTRAL_DST = 0,       // Dirichlet, DST-I
+  FVX_SPECTRAL_DCT = 1,       // Neumann, DCT-II
+  FVX_SPECTRAL_PERIODIC = 2,  // periodic (FFT), as the real Hartley pair
+};
+
 static inline int fvx_cuda_status() {
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? FVX_OK : FVX_ERR_CUDA;

@@ -1,9 +1,16 @@
-"""Dirichlet Helmholtz solves by DST-I matrix products on the tensor cores.
+"""Rectangular spectral Helmholtz solves by transform-matrix products on
+the tensor cores.
 
 ``solve_helmholtz_dst(rhs, dx, dy, lambda_)`` is the drop-in for
 spectraldiffx's ``solve_helmholtz_dst`` that finitevolX re-exports
 (solvers/spectral.py:14-98): it solves (nabla^2 - lambda) psi = rhs on the
 interior-only array ``rhs`` [..., Ny, Nx] with psi = 0 outside.
+``solve_helmholtz_dct`` (Neumann, DCT-II) and ``solve_helmholtz_fft``
+(periodic) are the other two solvers that finitevolX's ``_spectral_solve``
+dispatches on (spectral.py:105-128); they take the whole [..., Ny, Nx]
+array and return the zero-mean solution when the problem has a null mode
+(lambda = 0).  The periodic solve uses the real Hartley transform pair, the
+same linear map as the FFT solve on real data.
 
 * float32 input: 3xBF16-split tcgen05 GEMM chain, FP32 accumulation
   (relative error ~1e-5 of the FP64 answer);
@@ -28,25 +35,34 @@ from finitevolx_b200._lib import D, I, P, check, fn, stream_ptr
 I64 = ctypes.c_longlong
 
 
+KINDS = {"dst": 0, "dct": 1, "fft": 2}
+
+
 class DSTHelmholtzPlan:
-    """Pre-built DST-I matrices, eigenvalue grids and workspaces for one size.
+    """Pre-built transform matrices, eigenvalue grids and workspaces for one
+    size and boundary condition (``bc``: "dst" Dirichlet, "dct" Neumann,
+    "fft" periodic).
 
     Creating a plan allocates device memory once; ``solve`` allocates
     nothing on the device besides its output (pass ``out=`` to avoid that).
     """
 
     def __init__(self, ny: int, nx: int, dx: float, dy: float, lambdas=(0.0,), batch_max: int = 1,
-                 fp64: bool = True):
+                 fp64: bool = True, bc: str = "dst"):
         L.require_cuda()
+        if bc not in KINDS:
+            raise ValueError(f"bc must be 'fft', 'dst', or 'dct'; got {bc!r}")
         lam = np.atleast_1d(np.asarray(lambdas, dtype=np.float64))
         self.ny, self.nx, self.dx, self.dy = int(ny), int(nx), float(dx), float(dy)
+        self.bc = bc
         self.lambdas = lam
         self.batch_max = int(batch_max)
         self._h = ctypes.c_void_p()
         lam_c = (ctypes.c_double * len(lam))(*lam.tolist())
-        check(fn("fvx_dst_plan_create")(I(self.ny), I(self.nx), D(self.dx), D(self.dy), I(self.batch_max),
-                                        lam_c, I(len(lam)), I(int(fp64)), ctypes.byref(self._h)),
-              "DSTHelmholtzPlan")
+        check(fn("fvx_spectral_plan_create")(I(KINDS[bc]), I(self.ny), I(self.nx), D(self.dx), D(self.dy),
+                                             I(self.batch_max), lam_c, I(len(lam)), I(int(fp64)),
+                                             ctypes.byref(self._h)),
+              "SpectralHelmholtzPlan")
         self.split_ok = (self.nx % 8 == 0) and (self.ny % 8 == 0)
 
     def __del__(self):
@@ -89,11 +105,13 @@ class DSTHelmholtzPlan:
         return out
 
     def solve_refined(self, rhs, tol: float = 1e-12, max_iter: int = 8, out=None):
-        """Split-BF16 solve + FP64 iterative refinement.
+        """Split-BF16 solve + FP64 iterative refinement (Dirichlet plans).
 
         Returns (psi, info) with info = {passes, backward_error, rel_residual};
         backward_error = ||r|| / (||A|| ||psi|| + ||rhs||).
         """
+        if self.bc != "dst":
+            raise ValueError("iterative refinement is provided for the Dirichlet (DST) plan only")
         rhs = L.as_field(rhs, dtype=torch.float64)
         b = self._views(rhs)
         out = torch.empty_like(rhs) if out is None else out
@@ -114,14 +132,75 @@ class DSTHelmholtzPlan:
 _CACHE: dict = {}
 
 
-def get_plan(ny, nx, dx, dy, lambdas, batch, fp64=True) -> DSTHelmholtzPlan:
+SpectralHelmholtzPlan = DSTHelmholtzPlan
+
+
+def get_plan(ny, nx, dx, dy, lambdas, batch, fp64=True, bc: str = "dst") -> DSTHelmholtzPlan:
     lam = tuple(np.atleast_1d(np.asarray(lambdas, dtype=np.float64)).tolist())
-    key = (ny, nx, float(dx), float(dy), lam, torch.cuda.current_device())
+    key = (bc, ny, nx, float(dx), float(dy), lam, torch.cuda.current_device())
     p = _CACHE.get(key)
     if p is None or p.batch_max < batch:
-        p = DSTHelmholtzPlan(ny, nx, dx, dy, lam, batch_max=max(batch, 1), fp64=fp64)
+        p = DSTHelmholtzPlan(ny, nx, dx, dy, lam, batch_max=max(batch, 1), fp64=fp64, bc=bc)
         _CACHE[key] = p
     return p
+
+
+def _solve(rhs, dx, dy, lambda_, method, bc):
+    rhs = L.as_field(rhs)
+    if rhs.ndim < 2:
+        raise ValueError("rhs must be at least 2-D")
+    lam = np.atleast_1d(np.asarray(lambda_.cpu() if isinstance(lambda_, torch.Tensor) else lambda_,
+                                   dtype=np.float64))
+    if lam.size > 1 and (rhs.ndim < 3 or rhs.shape[-3] != lam.size):
+        raise ValueError(f"rhs.shape[-3] must match the {lam.size} lambda values")
+    ny, nx = rhs.shape[-2:]
+    b = int(np.prod(rhs.shape[:-2])) if rhs.ndim > 2 else 1
+    return get_plan(ny, nx, dx, dy, lam, b, bc=bc).solve(rhs, method=method)
+
+
+def solve_helmholtz_dct(rhs, dx: float, dy: float, lambda_=0.0) -> torch.Tensor:
+    """(nabla^2 - lambda) psi = rhs with homogeneous Neumann walls (cell-centred,
+    DCT-II); zero-mean psi when lambda = 0."""
+    return _solve(rhs, dx, dy, lambda_, "fp64", "dct")
+
+
+def solve_helmholtz_fft(rhs, dx: float, dy: float, lambda_=0.0) -> torch.Tensor:
+    """(nabla^2 - lambda) psi = rhs on a doubly periodic grid; zero-mean psi
+    when lambda = 0."""
+    return _solve(rhs, dx, dy, lambda_, "fp64", "fft")
+
+
+def solve_poisson_dct(rhs, dx: float, dy: float) -> torch.Tensor:
+    return solve_helmholtz_dct(rhs, dx, dy, 0.0)
+
+
+def solve_poisson_fft(rhs, dx: float, dy: float) -> torch.Tensor:
+    return solve_helmholtz_fft(rhs, dx, dy, 0.0)
+
+
+def spectral_solve(rhs, dx: float, dy: float, lambda_, bc: str) -> torch.Tensor:
+    """The rectangular solver for ``bc`` (spectral.py:105-128 ``_spectral_solve``)."""
+    if bc not in KINDS:
+        raise ValueError(f"base_bc must be 'fft', 'dst', or 'dct'; got {bc!r}")
+    return _solve(rhs, dx, dy, lambda_, "fp64", bc)
+
+
+def make_spectral_preconditioner(dx: float, dy: float, lambda_: float = 0.0, bc: str = "fft"):
+    """M_inv(r) = the rectangular spectral solve of (nabla^2 - lambda)
+    (preconditioners.py:44-84); default periodic."""
+    if bc not in KINDS:
+        raise ValueError(f"bc must be 'fft', 'dst', or 'dct'; got {bc!r}")
+    return lambda r: spectral_solve(r, dx, dy, lambda_, bc)
+
+
+def dct2_eigenvalues(n: int, d: float) -> np.ndarray:
+    k = np.arange(n)
+    return -4.0 / d ** 2 * np.sin(np.pi * k / (2 * n)) ** 2
+
+
+def fft_eigenvalues(n: int, d: float) -> np.ndarray:
+    k = np.arange(n)
+    return -4.0 / d ** 2 * np.sin(np.pi * k / n) ** 2
 
 
 def solve_helmholtz_dst(rhs, dx: float, dy: float, lambda_=0.0, method: str = "fp64") -> torch.Tensor:

@@ -162,6 +162,28 @@ typedef struct fvx_dst_plan fvx_dst_plan;
 int fvx_dst_plan_create(int ny, int nx, double dx, double dy, int batch_max, const double* lambdas, int n_lambda,
                         int want_fp64, fvx_dst_plan** plan);
 int fvx_dst_plan_destroy(fvx_dst_plan* plan);
+/* The same plan for the other rectangular spectral solvers that
+ * solvers/spectral.py:14-98 re-exports and _spectral_solve (:105-128)
+ * dispatches: kind 0 = DST-I (Dirichlet, = fvx_dst_plan_create), 1 =
+ * DCT-II (Neumann, solve_helmholtz_dct), 2 = periodic (solve_helmholtz_fft,
+ * computed with the real Hartley transform pair, which diagonalises the
+ * same periodic 5-point operator).  Input and output are the full [ny, nx]
+ * array (no ghost ring); the null mode of a Neumann / periodic Poisson
+ * problem is set to zero (the zero-mean solution).  DCT-II and periodic
+ * plans take the dense product path; fvx_dst_solve_f64 supports method 0
+ * only for them. */
+int fvx_spectral_plan_create(int kind, int ny, int nx, double dx, double dy, int batch_max, const double* lambdas,
+                             int n_lambda, int want_fp64, fvx_dst_plan** plan);
+/* Capacitance-matrix step between the two rectangular solves of a masked
+ * solve (the online part of the CapacitanceSolver that
+ * solvers/elliptic.py:146-183 builds): out = f, then out[idx[k]] -=
+ * sum_l cinv[k][l] u[idx[l]] (FP64 sums), k < nb; f, u, out hold n
+ * elements (out may be f); idx are distinct flat indices, cinv is the
+ * inverse capacitance matrix (nb x nb, row-major FP64). */
+int fvx_capacitance_rhs_f32(const float* f, const float* u, const double* cinv, const long long* idx, int nb,
+                            long long n, float* out, void* stream);
+int fvx_capacitance_rhs_f64(const double* f, const double* u, const double* cinv, const long long* idx, int nb,
+                            long long n, double* out, void* stream);
 /* Reads the plan's device error flag (7 if a bounded wait gave up); syncs. */
 int fvx_dst_plan_check(fvx_dst_plan* plan, void* stream);
 /* FP32: 3xBF16 split tcgen05 chain (ny, nx multiples of 8; otherwise the

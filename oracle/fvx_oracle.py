@@ -20,7 +20,13 @@ Pinning (which results are checked against the reference's own data):
     identity (5-point Dirichlet operator minus lambda applied to the
     solution reproduces the right-hand side), not by a golden vector;
   * CG: third-party (lineax 0.1.0); iterate-level parity unpinned, pinned by
-    the outcome tests (converged flag, residual bound).
+    the outcome tests (converged flag, residual bound);
+  * solve_helmholtz_dct / solve_helmholtz_fft / capacitance_solve:
+    third-party (spectraldiffx v0.0.10, as above); pinned by the discrete
+    identities (the Neumann / periodic 5-point operator minus lambda applied
+    to the solution reproduces the right-hand side, less its mean when
+    lambda = 0) and by the reference's own capacitance tests (the solution
+    vanishes on the inner-boundary points; no boundary point is an error).
 """
 
 from __future__ import annotations
@@ -872,6 +878,108 @@ def dirichlet_helmholtz_apply(psi, dx, dy, lambda_=0.0):
         p[..., 2:, 1:-1] - 2 * c + p[..., :-2, 1:-1]) / dy ** 2
     lam = np.asarray(lambda_, dtype=float)
     return lap - (lam[..., None, None] if lam.ndim else lam) * c
+
+
+def dct2_eigenvalues(n, d):
+    """-4/d^2 sin^2(pi k / (2n)): the Neumann (cell-centred) 3-point second
+    difference's eigenvalues (docs/elliptic_solvers.md eigenvalue table)."""
+    k = np.arange(n)
+    return -4.0 / d ** 2 * np.sin(np.pi * k / (2 * n)) ** 2
+
+
+def fft_eigenvalues(n, d):
+    """-4/d^2 sin^2(pi k / n): the periodic 3-point second difference."""
+    k = np.arange(n)
+    return -4.0 / d ** 2 * np.sin(np.pi * k / n) ** 2
+
+
+def _spectral_den(ny, nx, dx, dy, lambda_, ey, ex):
+    den = ey(ny, dy)[:, None] + ex(nx, dx)[None, :]
+    lam = np.asarray(lambda_, dtype=float)
+    return den - (lam[..., None, None] if lam.ndim else lam)
+
+
+def _safe_div(a, den):
+    # the null mode (den == 0: Neumann / periodic Poisson) -> 0, the zero-mean gauge
+    return np.where(den == 0.0, 0.0, a / np.where(den == 0.0, 1.0, den))
+
+
+def solve_helmholtz_dct(rhs, dx, dy, lambda_=0.0):
+    """(nabla^2 - lambda) psi = rhs with homogeneous Neumann walls by DCT-II
+    (spectraldiffx solve_helmholtz_dct, re-exported at solvers/spectral.py:14-98;
+    published algorithm: forward DCT-II, divide by the eigenvalue grid,
+    inverse; null mode set to zero)."""
+    from scipy.fft import dctn, idctn
+    rhs = np.asarray(rhs, dtype=float)
+    ny, nx = rhs.shape[-2:]
+    den = _spectral_den(ny, nx, dx, dy, lambda_, dct2_eigenvalues, dct2_eigenvalues)
+    return idctn(_safe_div(dctn(rhs, type=2, axes=(-2, -1)), den), type=2, axes=(-2, -1))
+
+
+def solve_helmholtz_fft(rhs, dx, dy, lambda_=0.0):
+    """(nabla^2 - lambda) psi = rhs, doubly periodic, by FFT (spectraldiffx
+    solve_helmholtz_fft; null mode set to zero)."""
+    rhs = np.asarray(rhs, dtype=float)
+    ny, nx = rhs.shape[-2:]
+    den = _spectral_den(ny, nx, dx, dy, lambda_, fft_eigenvalues, fft_eigenvalues)
+    return np.real(np.fft.ifft2(_safe_div(np.fft.fft2(rhs, axes=(-2, -1)), den), axes=(-2, -1)))
+
+
+def neumann_helmholtz_apply(psi, dx, dy, lambda_=0.0):
+    """5-point (nabla^2 - lambda) with mirror ghosts (zero normal gradient)."""
+    p = np.pad(psi, ((0, 0),) * (psi.ndim - 2) + ((1, 1), (1, 1)), mode="edge")
+    c = p[..., 1:-1, 1:-1]
+    lap = (p[..., 1:-1, 2:] - 2 * c + p[..., 1:-1, :-2]) / dx ** 2 + (
+        p[..., 2:, 1:-1] - 2 * c + p[..., :-2, 1:-1]) / dy ** 2
+    return lap - float(lambda_) * c
+
+
+def periodic_helmholtz_apply(psi, dx, dy, lambda_=0.0):
+    """5-point (nabla^2 - lambda) with periodic wrap."""
+    lap = (np.roll(psi, -1, -1) - 2 * psi + np.roll(psi, 1, -1)) / dx ** 2 + (
+        np.roll(psi, -1, -2) - 2 * psi + np.roll(psi, 1, -2)) / dy ** 2
+    return lap - float(lambda_) * psi
+
+
+def spectral_solve(rhs, dx, dy, lambda_, bc):
+    """_spectral_solve (solvers/spectral.py:105-128)."""
+    f = {"fft": solve_helmholtz_fft, "dst": solve_helmholtz_dst, "dct": solve_helmholtz_dct}.get(bc)
+    if f is None:
+        raise ValueError(f"base_bc must be 'fft', 'dst', or 'dct'; got {bc!r}")
+    return f(rhs, dx, dy, lambda_)
+
+
+def inner_boundary_indices(mask):
+    """Interior (True) cells 4-connected to an exterior (False) cell; cells
+    beyond the array edge count as interior (the reference test helper's
+    binary_dilation of ~mask with the cross structure, tests/test_elliptic.py:492-503)."""
+    m = np.asarray(mask, dtype=bool)
+    land = ~m
+    d = land.copy()
+    d[1:, :] |= land[:-1, :]
+    d[:-1, :] |= land[1:, :]
+    d[:, 1:] |= land[:, :-1]
+    d[:, :-1] |= land[:, 1:]
+    return np.where(m & d)
+
+
+def capacitance_solve(rhs, mask, dx, dy, lambda_=0.0, base_bc="fft"):
+    """Capacitance-matrix masked solve (elliptic.py:146-183 builds it;
+    Buzbee-Golub-Nielson as docs/elliptic_solvers.md states): Green's
+    functions g_l = L^-1 e_{b_l} of the rectangular solver, C = G[B, :],
+    alpha = C^-1 u[B] with u = L^-1 rhs, psi = u - G alpha (zero on B)."""
+    jb, ib = inner_boundary_indices(mask)
+    nb = len(jb)
+    if nb == 0:
+        raise ValueError("No inner-boundary points found in mask")
+    ny, nx = np.asarray(mask).shape
+    E = np.zeros((nb, ny, nx))
+    E[np.arange(nb), jb, ib] = 1.0
+    G = spectral_solve(E, dx, dy, lambda_, base_bc)
+    C = G[:, jb, ib].T                       # C[k, l] = g_l(b_k)
+    u = spectral_solve(np.asarray(rhs, float), dx, dy, lambda_, base_bc)
+    alpha = np.linalg.solve(C, u[jb, ib])
+    return u - np.tensordot(alpha, G, axes=(0, 0))
 
 
 def dst1_matrix(n):
