@@ -889,8 +889,8 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
 }
 
 // Which even/odd kernel runs for row counts that are multiples of 256:
-// 1 = CTA pairs (default), 0 = single CTAs (fvx_dst_kernel_config).
-static int g_sym_pair = 1;
+// 0 = single CTAs (default), 1 = CTA pairs (fvx_dst_kernel_config).
+static int g_sym_pair = 0;
 static bool sym_pair_enabled() { return g_sym_pair == 1; }
 
 // C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns

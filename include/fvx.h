@@ -207,8 +207,8 @@ int fvx_dst_operand_layout(fvx_dst_plan* plan);
 /* One product of the chain on the current workspaces (timing only). */
 int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
 /* Even/odd product kernel for row counts that are multiples of 256 (process-
- * wide, for the autotuner): 1 = CTA pairs sharing each B block (cta_group::2,
- * default), 0 = one CTA per 128-row tile; pair < 0 returns the current
+ * wide, for the autotuner): 1 = CTA pairs sharing each B block (cta_group::2),
+ * 0 = one CTA per 128-row tile (default); pair < 0 returns the current
  * choice.  No counterpart in finitevolX (launch configuration). */
 int fvx_dst_kernel_config(int pair);
 

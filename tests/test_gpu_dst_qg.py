@@ -68,7 +68,7 @@ def test_dst_pair_and_single_cta_products_agree(cuda_ok, shape):
             outs.append(host(plan.solve(dev(f, torch.float32))))
             plan.check_device()
     finally:
-        set_dst_kernel(True)
+        set_dst_kernel(False)
     for o in outs:
         assert rel_err(o, ref) < 1e-4
     assert rel_err(outs[0], outs[1]) < 5e-5
@@ -197,7 +197,7 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     r3 = autotune.tune_dst_kernel(m, qd, dt)
     assert set(r3["ms"]) == {"pair", "single"}
     autotune.set_stage_tile("weno5", torch.float32, 0)
-    autotune.set_dst_kernel(True)
+    autotune.set_dst_kernel(False)
 
 
 @pytest.mark.parametrize("method", ("wenoz5", "weno5"))
