@@ -371,7 +371,7 @@ def main():
     if not args.profile:
         tuned = {"stage_tile": autotune.tune_qg_stage(model, qa, dt)["tile"],
                  "fused_split": autotune.tune_qg_split(model, qa, dt)["fused"],
-                 "dst_pair_ctas": autotune.tune_dst_kernel(model, qa, dt)["pair"]}
+                 "dst_kernel": autotune.tune_dst_kernel(model, qa, dt)["kernel"]}
     qa.copy_(q0)
 
     # warm-up (eager), leaves split(qb) in the DST workspace for the graphs

@@ -5,11 +5,13 @@ of several launches) through the library's own entry points and applies the
 fastest:
 
 * ``tune_qg_stage``: the fused QG stage kernel's tile shape (64x16, 32x16,
-  128x8 cells; the halo follows the scheme) for one scheme and dtype.
+  128x8, 64x32, 128x16 cells; the halo follows the scheme) for one scheme
+  and dtype.
 * ``tune_qg_split``: whether the stage kernel writes the next DST operand
   split itself (fused) or a separate split pass does (unfused).
-* ``tune_dst_kernel``: the even/odd DST product on CTA pairs (cta_group::2,
-  each pair sharing its B blocks) or on single CTAs.
+* ``tune_dst_kernel``: the even/odd DST product on single CTAs with 64- or
+  32-element K blocks (3 or 6 ring stages) or on CTA pairs (cta_group::2,
+  each pair sharing its B blocks).
 * ``tune_ensemble``: the persistent work-queue grid (CTAs per SM).
 
 Results are cached in a JSON file keyed by device name and workload
@@ -28,7 +30,7 @@ import torch
 
 from finitevolx_b200._lib import I, SCHEMES, check, fn
 
-_TILES = ("64x16", "32x16", "128x8")
+_TILES = ("64x16", "32x16", "128x8", "64x32", "128x16")
 
 
 def _cache_path() -> pathlib.Path:
@@ -124,19 +126,24 @@ def tune_qg_split(model, q, dt: float, use_cache: bool = True) -> dict:
     return res
 
 
-def set_dst_kernel(pair: bool) -> None:
-    check(fn("fvx_dst_kernel_config")(I(1 if pair else 0)), "dst kernel config")
+DST_KERNELS = ("single64", "pair", "single32")
+
+
+def set_dst_kernel(kind) -> None:
+    """``kind``: one of DST_KERNELS (or its index)."""
+    k = DST_KERNELS.index(kind) if isinstance(kind, str) else int(kind)
+    check(fn("fvx_dst_kernel_config")(I(k)), "dst kernel config")
 
 
 def tune_dst_kernel(model, q, dt: float, use_cache: bool = True) -> dict:
-    """CTA-pair against single-CTA even/odd DST products, timed over whole
-    QG steps of ``model`` (a QGModel); returns {"pair": bool, "ms": {...}}."""
+    """The even/odd DST product forms timed over whole QG steps of ``model``
+    (a QGModel); returns {"kernel": name, "ms": {name: median ms}}."""
     g = model.grid
     key = f"{_device_key()}/dst_kernel/{model.dtype}/{g.Ny}x{g.Nx}"
     if use_cache:
         hit = _load().get(key)
-        if hit:
-            set_dst_kernel(bool(hit["pair"]))
+        if hit and hit.get("kernel") in DST_KERNELS:
+            set_dst_kernel(hit["kernel"])
             return hit
     out = torch.empty_like(q)
 
@@ -145,12 +152,12 @@ def tune_dst_kernel(model, q, dt: float, use_cache: bool = True) -> dict:
             model.step(q, dt, out=out)
 
     ms = {}
-    for name, pair in (("pair", True), ("single", False)):
-        set_dst_kernel(pair)
+    for name in DST_KERNELS:
+        set_dst_kernel(name)
         ms[name] = _time(steps)
-    pair = ms["pair"] <= ms["single"]
-    set_dst_kernel(pair)
-    res = {"pair": pair, "ms": ms}
+    best = min(ms, key=ms.get)
+    set_dst_kernel(best)
+    res = {"kernel": best, "ms": ms}
     _store(key, res)
     return res
 

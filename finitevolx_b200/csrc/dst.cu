@@ -189,6 +189,16 @@ DEV uint64_t sdesc_sw128(uint32_t saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
+// The same for 64-byte rows (32 bf16 of K): 64-byte swizzle, 8-row groups
+// 512 B apart.
+DEV uint64_t sdesc_sw64(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+template <int BKT> DEV uint64_t sdesc_k(uint32_t saddr) {
+  if constexpr (BKT == 64) return sdesc_sw128(saddr);
+  else return sdesc_sw64(saddr);
+}
 // Instruction descriptor: kind::f16 with BF16 A/B, FP32 accumulator,
 // both operands K-major, M = 128, N = 256.
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
@@ -342,11 +352,17 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
 // N/2 x N/2 K-major tables.  Each CTA owns a 128-row x 128-k tile of P and
 // of Q (TMEM columns 0-127 and 128-255); the k loop alternates P and Q
 // blocks through a 3-stage TMA ring of 64 KiB stages.
-constexpr int SBN = 128, SSTAGES = 3;
-constexpr int S_A_TILE = BM * BK * 2;                       // 16 KiB
-constexpr int S_B_TILE = SBN * BK * 2;                      // 16 KiB
-constexpr int S_STAGE = 2 * S_A_TILE + 2 * S_B_TILE;        // 64 KiB
-constexpr int S_SMEM = SSTAGES * S_STAGE + 1024 + 256;
+constexpr int SBN = 128;
+// Ring geometry for a K block of BKT elements: 192 KiB of stages (3 of 64
+// KiB for BKT = 64, 6 of 32 KiB for BKT = 32; the smaller stages keep more
+// loads in flight).
+template <int BKT> struct SymCfg {
+  static constexpr int A_T = BM * BKT * 2, B_T = SBN * BKT * 2;
+  static constexpr int STAGE = 2 * A_T + 2 * B_T;
+  static constexpr int STAGES = (3 * 64) / BKT;
+  static constexpr int SMEM = STAGES * STAGE + 1024 + 256;
+  static_assert(STAGES * STAGE >= 2 * 2 * 2 * 8192 * 2, "epilogue staging fits in the operand ring");
+};
 constexpr uint32_t kIdesc128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SBN >> 3) << 17) |
                                ((uint32_t)(BM >> 4) << 24);
 // TMA warp, MMA warp and 8 epilogue warps: two per TMEM lane quadrant
@@ -479,27 +495,29 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
   }
 }
 
+template <int BKT>
 __global__ void __launch_bounds__(S_THREADS, 1)
 gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
                      const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
                      const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl,
                      const __grid_constant__ CUtensorMap mO0, const __grid_constant__ CUtensorMap mO1, int K,
                      Epi ep) {
+  using C = SymCfg<BKT>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint64_t* bars = (uint64_t*)(smem + SSTAGES * S_STAGE);  // full[S], empty[S], acc
-  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * SSTAGES + 1);
+  uint64_t* bars = (uint64_t*)(smem + C::STAGES * C::STAGE);  // full[S], empty[S], acc
+  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * C::STAGES + 1);
   volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.y * BM, n0 = blockIdx.x * SBN;
   const int KH = K >> 1;
-  const int KT = 2 * ((KH + BK - 1) / BK);  // P and Q blocks alternate
+  const int KT = 2 * ((KH + BKT - 1) / BKT);  // P and Q blocks alternate
   auto full = [&](int s) { return smem_u32(&bars[s]); };
-  auto empty = [&](int s) { return smem_u32(&bars[SSTAGES + s]); };
-  const uint32_t accb = smem_u32(&bars[2 * SSTAGES]);
+  auto empty = [&](int s) { return smem_u32(&bars[C::STAGES + s]); };
+  const uint32_t accb = smem_u32(&bars[2 * C::STAGES]);
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < SSTAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
+    for (int s = 0; s < C::STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
     mbar_init(accb, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -518,34 +536,34 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   const int kshift = 2 * (int)((blockIdx.x * 5u + blockIdx.y * 3u) % (unsigned)(KT / 2));
   if (warp == 0 && lane == 0) {
     for (int kt0 = 0; kt0 < KT; ++kt0) {
-      const int s = kt0 % SSTAGES;
-      if (kt0 >= SSTAGES && !mbar_wait(empty(s), ((kt0 / SSTAGES) - 1) & 1, abort_flag, ep.err)) break;
-      mbar_expect_tx(full(s), S_STAGE);
-      const uint32_t base = smem_u32(smem + s * S_STAGE);
+      const int s = kt0 % C::STAGES;
+      if (kt0 >= C::STAGES && !mbar_wait(empty(s), ((kt0 / C::STAGES) - 1) & 1, abort_flag, ep.err)) break;
+      mbar_expect_tx(full(s), C::STAGE);
+      const uint32_t base = smem_u32(smem + s * C::STAGE);
       const int kt = (kt0 + kshift) % KT;
       const int kb = kt >> 1;
       const bool odd = kt & 1;
-      const int ac = (odd ? KH : 0) + kb * BK;
+      const int ac = (odd ? KH : 0) + kb * BKT;
       tma_load_2d(base, &mAh, full(s), ac, m0);
-      tma_load_2d(base + S_A_TILE, &mAl, full(s), ac, m0);
-      tma_load_2d(base + 2 * S_A_TILE, odd ? &mQh : &mPh, full(s), kb * BK, n0);
-      tma_load_2d(base + 2 * S_A_TILE + S_B_TILE, odd ? &mQl : &mPl, full(s), kb * BK, n0);
+      tma_load_2d(base + C::A_T, &mAl, full(s), ac, m0);
+      tma_load_2d(base + 2 * C::A_T, odd ? &mQh : &mPh, full(s), kb * BKT, n0);
+      tma_load_2d(base + 2 * C::A_T + C::B_T, odd ? &mQl : &mPl, full(s), kb * BKT, n0);
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
     for (int kt0 = 0; kt0 < KT && ok; ++kt0) {
-      const int s = kt0 % SSTAGES;
-      ok = mbar_wait(full(s), (kt0 / SSTAGES) & 1, abort_flag, ep.err);
+      const int s = kt0 % C::STAGES;
+      ok = mbar_wait(full(s), (kt0 / C::STAGES) & 1, abort_flag, ep.err);
       if (!ok) break;
       tc_fence_after();
-      const uint32_t base = smem_u32(smem + s * S_STAGE);
-      const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + S_A_TILE);
-      const uint64_t bh = sdesc_sw128(base + 2 * S_A_TILE), bl = sdesc_sw128(base + 2 * S_A_TILE + S_B_TILE);
+      const uint32_t base = smem_u32(smem + s * C::STAGE);
+      const uint64_t ah = sdesc_k<BKT>(base), al = sdesc_k<BKT>(base + C::A_T);
+      const uint64_t bh = sdesc_k<BKT>(base + 2 * C::A_T), bl = sdesc_k<BKT>(base + 2 * C::A_T + C::B_T);
       const int kt = (kt0 + kshift) % KT;
       const uint32_t d = tmem + ((kt & 1) ? (uint32_t)SBN : 0u);
       const bool first = kt0 < 2;  // the first P block and the first Q block overwrite
 #pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
+      for (int kk = 0; kk < BKT / 16; ++kk) {
         const uint64_t o = (uint64_t)(kk * 32 >> 4);
         umma_bf16(d, ah + o, bh + o, kIdesc128, !(first && kk == 0));
         umma_bf16(d, ah + o, bl + o, kIdesc128, 1u);
@@ -836,17 +854,20 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 // 2-D bf16 tensor map over [outer][inner] (inner contiguous), box
 // {BK, box_outer}, 128-byte swizzle, zero fill out of bounds.
-static bool make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint32_t box_outer) {
+static bool make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_t outer, uint32_t box_outer,
+                     uint32_t box_inner = BK) {
   auto enc = encode_fn();
   if (!enc) return false;
   if (((uintptr_t)base & 15) != 0 || (inner * 2) % 16 != 0) return false;
+  if (box_inner != 64 && box_inner != 32) return false;
   cuuint64_t dims[2] = {inner, outer};
   cuuint64_t strides[1] = {inner * 2};
-  cuuint32_t box[2] = {(cuuint32_t)BK, box_outer};
+  cuuint32_t box[2] = {box_inner, box_outer};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   box_inner == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS;
 }
 
@@ -888,10 +909,10 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Which even/odd kernel runs for row counts that are multiples of 256:
-// 0 = single CTAs (default), 1 = CTA pairs (fvx_dst_kernel_config).
-static int g_sym_pair = 0;
-static bool sym_pair_enabled() { return g_sym_pair == 1; }
+// Which even/odd kernel runs (fvx_dst_kernel_config): 0 = single CTAs with
+// 64-element K blocks (default), 1 = CTA pairs (row counts that are
+// multiples of 256), 2 = single CTAs with 32-element K blocks.
+static int g_sym_kernel = 0;
 
 // C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns
 // de-interleaved; P/Q: the [K/2][K/2] hi/lo tables.  Needs K % 256 == 0.
@@ -900,16 +921,20 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
   Epi ep = ep_in;
   static bool attr_set = false;
   if (!attr_set) {
-    if (cudaFuncSetAttribute(gemm_sym_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, S_SMEM) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(gemm_sym_bf16_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SymCfg<64>::SMEM) != cudaSuccess ||
+        cudaFuncSetAttribute(gemm_sym_bf16_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             SymCfg<32>::SMEM) != cudaSuccess)
       return FVX_ERR_CUDA;
     attr_set = true;
   }
   if (K % (2 * SBN) != 0) return FVX_ERR_SHAPE;
   const int KH = K / 2;
+  const uint32_t bki = g_sym_kernel == 2 ? 32 : 64;  // K block of the single-CTA forms
   CUtensorMap a_h, a_l, p_h, p_l, q_h, q_l;
-  if (!make_map(&a_h, Xh, K, M, BM) || !make_map(&a_l, Xl, K, M, BM) || !make_map(&p_h, Ph, KH, KH, SBN) ||
-      !make_map(&p_l, Pl, KH, KH, SBN) || !make_map(&q_h, Qh, KH, KH, SBN) || !make_map(&q_l, Ql, KH, KH, SBN))
+  if (!make_map(&a_h, Xh, K, M, BM, bki) || !make_map(&a_l, Xl, K, M, BM, bki) ||
+      !make_map(&p_h, Ph, KH, KH, SBN, bki) || !make_map(&p_l, Pl, KH, KH, SBN, bki) ||
+      !make_map(&q_h, Qh, KH, KH, SBN, bki) || !make_map(&q_l, Ql, KH, KH, SBN, bki))
     return FVX_ERR_ARG;
   // staged TMA stores for the split and FP32 outputs when their layout allows
   CUtensorMap o0, o1;
@@ -926,7 +951,7 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
                    : make_out_map(&o0, ep.out0, true, R, K, B, ep.ld, ep.batch_stride, 128);
     ep.tma_out = okm ? 1 : 0;
   }
-  if (M % (2 * BM) == 0 && sym_pair_enabled()) {
+  if (M % (2 * BM) == 0 && g_sym_kernel == 1) {
     // CTA pairs: B blocks of 64 table rows per CTA
     static bool pattr = false;
     if (!pattr) {
@@ -946,7 +971,10 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
   }
   dim3 grid(KH / SBN, (M + BM - 1) / BM);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  gemm_sym_bf16_kernel<<<grid, S_THREADS, S_SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
+  if (bki == 32)
+    gemm_sym_bf16_kernel<32><<<grid, S_THREADS, SymCfg<32>::SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
+  else
+    gemm_sym_bf16_kernel<64><<<grid, S_THREADS, SymCfg<64>::SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
   return fvx_cuda_status();
 }
 
@@ -1377,10 +1405,10 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
 // One product of the split chain on the plan's workspaces, for timing the
 // tensor-core GEMM in isolation: which 0 = (W1 S_x)^T -> W2, 1 = (W2 S_y) ./
 // Lambda -> W1.  Operands are whatever the workspaces currently hold.
-extern "C" int fvx_dst_kernel_config(int pair) {
-  if (pair < 0) return g_sym_pair;
-  if (pair > 1) return FVX_ERR_ARG;
-  g_sym_pair = pair;
+extern "C" int fvx_dst_kernel_config(int kind) {
+  if (kind < 0) return g_sym_kernel;
+  if (kind > 2) return FVX_ERR_ARG;
+  g_sym_kernel = kind;
   return FVX_OK;
 }
 

@@ -41,6 +41,8 @@ static int launch(const StageArgs& a, cudaStream_t st) {
   switch (g_tile_cfg[S][sizeof(T) == 8]) {
     case 1: return launch_t<T, S, kTileTX[1], kTileTY[1]>(a, st);
     case 2: return launch_t<T, S, kTileTX[2], kTileTY[2]>(a, st);
+    case 3: return launch_t<T, S, kTileTX[3], kTileTY[3]>(a, st);
+    case 4: return launch_t<T, S, kTileTX[4], kTileTY[4]>(a, st);
     default: return launch_t<T, S, kTileTX[0], kTileTY[0]>(a, st);
   }
 }

@@ -10,9 +10,9 @@ namespace qg {
 
 constexpr int THREADS = 256;
 // Tile shapes the autotuner chooses from (fvx_qg_tile_config): TX x TY cells.
-constexpr int kTileTX[3] = {64, 32, 128};
-constexpr int kTileTY[3] = {16, 16, 8};
-constexpr int kTileConfigs = 3;
+constexpr int kTileTX[5] = {64, 32, 128, 64, 128};
+constexpr int kTileTY[5] = {16, 16, 8, 32, 16};
+constexpr int kTileConfigs = 5;
 
 // a / d: exact division in FP64; multiplication by the rounded reciprocal in
 // FP32 (<= 1 ulp from the quotient).

@@ -206,11 +206,13 @@ int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
 int fvx_dst_operand_layout(fvx_dst_plan* plan);
 /* One product of the chain on the current workspaces (timing only). */
 int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
-/* Even/odd product kernel for row counts that are multiples of 256 (process-
- * wide, for the autotuner): 1 = CTA pairs sharing each B block (cta_group::2),
- * 0 = one CTA per 128-row tile (default); pair < 0 returns the current
- * choice.  No counterpart in finitevolX (launch configuration). */
-int fvx_dst_kernel_config(int pair);
+/* Even/odd product kernel (process-wide, for the autotuner): 0 = one CTA
+ * per 128-row tile with 64-element K blocks (3 ring stages, default), 1 =
+ * CTA pairs sharing each B block (cta_group::2; row counts that are
+ * multiples of 256), 2 = one CTA per tile with 32-element K blocks (6 ring
+ * stages); kind < 0 returns the current choice.  No counterpart in
+ * finitevolX (launch configuration). */
+int fvx_dst_kernel_config(int kind);
 
 /* Allocation-free FP32 DST Helmholtz solve.  No counterpart in the
  * reference: it serves callers that cannot call cudaMalloc while they run
@@ -364,7 +366,7 @@ int fvx_nn_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, i
 int fvx_nn_to_bf16(const float* src, void* dst, int n, void* stream);
 
 /* ---- QG fused-stage tile shape (autotuner) -------------------------------- */
-/* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8 cells for (method, dtype 0 FP32 / 1
+/* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8, 3 = 64x32, 4 = 128x16 cells for (method, dtype 0 FP32 / 1
  * FP64); cfg < 0 returns the number of configurations.  No counterpart in
  * finitevolX (launch configuration). */
 int fvx_qg_tile_config(int method, int dtype, int cfg);

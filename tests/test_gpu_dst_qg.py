@@ -48,30 +48,32 @@ def test_dst_split_bf16_chain(cuda_ok, shape, lam):
 
 
 @pytest.mark.parametrize("shape", [(256, 512), (512, 256), (768, 512)])
-def test_dst_pair_and_single_cta_products_agree(cuda_ok, shape):
-    # the even/odd products on CTA pairs (cta_group::2, B blocks shared by the
-    # pair) and on single CTAs: the same 3xBF16 sums in another k order.  Both
-    # within the chain's 1e-4 of the oracle; against each other within 5e-5:
-    # an intermediate that differs by one FP32 ulp can round to another bf16
-    # hi/lo pair, which moves it by up to 2^-16 relative (~1e-5 after the chain)
-    from finitevolx_b200.autotune import set_dst_kernel
+def test_dst_product_forms_agree(cuda_ok, shape):
+    # the even/odd products on single CTAs (64- and 32-element K blocks) and
+    # on CTA pairs (cta_group::2, B blocks shared by the pair): the same
+    # 3xBF16 sums in another k order.  All within the chain's 1e-4 of the
+    # oracle; against each other within 5e-5: an intermediate that differs
+    # by one FP32 ulp can round to another bf16 hi/lo pair, which moves it by
+    # up to 2^-16 relative (~1e-5 after the chain)
+    from finitevolx_b200.autotune import DST_KERNELS, set_dst_kernel
     from finitevolx_b200._lib import fn
     ny, nx = shape
     f = O.kminus3_field(ny, nx, 4)
     ref = O.solve_helmholtz_dst(f, 0.05, 0.07, 1.0)
     outs = []
     try:
-        for pair in (True, False):
-            set_dst_kernel(pair)
-            assert fn("fvx_dst_kernel_config")(-1) == int(pair)
+        for k, name in enumerate(DST_KERNELS):
+            set_dst_kernel(name)
+            assert fn("fvx_dst_kernel_config")(-1) == k
             plan = DSTHelmholtzPlan(ny, nx, 0.05, 0.07, (1.0,))
             outs.append(host(plan.solve(dev(f, torch.float32))))
             plan.check_device()
     finally:
-        set_dst_kernel(False)
+        set_dst_kernel("single64")
     for o in outs:
         assert rel_err(o, ref) < 1e-4
-    assert rel_err(outs[0], outs[1]) < 5e-5
+    for o in outs[1:]:
+        assert rel_err(o, outs[0]) < 5e-5
 
 
 @pytest.mark.parametrize("shape", [(40, 56), (37, 29), (128, 128)])
@@ -181,7 +183,7 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     m = QGModel(grid, beta, lam, method="weno5", dtype=torch.float32)
     qd = dev(q, torch.float32)
     outs = []
-    for cfg in range(3):
+    for cfg in range(5):
         autotune.set_stage_tile("weno5", torch.float32, cfg)
         outs.append(host(m.step(qd, dt)))
     m.fuse_split = False
@@ -190,14 +192,14 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     for o in outs[1:]:
         assert rel_err(o, outs[0]) < 1e-6
     r1 = autotune.tune_qg_stage(m, qd, dt)
-    assert r1["tile"] in ("64x16", "32x16", "128x8") and len(r1["ms"]) == 3
+    assert r1["tile"] in ("64x16", "32x16", "128x8", "64x32", "128x16") and len(r1["ms"]) == 5
     r2 = autotune.tune_qg_split(m, qd, dt)
     assert set(r2["ms"]) == {"fused", "unfused"}
     assert autotune.tune_qg_stage(m, qd, dt) == r1  # from the cache
     r3 = autotune.tune_dst_kernel(m, qd, dt)
-    assert set(r3["ms"]) == {"pair", "single"}
+    assert set(r3["ms"]) == set(autotune.DST_KERNELS) and r3["kernel"] in autotune.DST_KERNELS
     autotune.set_stage_tile("weno5", torch.float32, 0)
-    autotune.set_dst_kernel(False)
+    autotune.set_dst_kernel("single64")
 
 
 @pytest.mark.parametrize("method", ("wenoz5", "weno5"))
