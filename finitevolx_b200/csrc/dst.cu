@@ -110,6 +110,10 @@ DEV void tma_store_3d(const CUtensorMap* map, uint32_t src, int c0, int c1, int 
                "r"(src), "r"(c0), "r"(c1), "r"(c2)
                : "memory");
 }
+DEV void tma_store_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+DEV void prefetch_map(const CUtensorMap* map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)map) : "memory");
+}
 DEV void tma_store_commit_wait() {
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
@@ -397,7 +401,7 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
     const int bb = m0 / R, r0 = m0 - bb * R;
     const int be = bb % ep.n_eig;
     const bool go = ok && !*abort_flag;
-    if (go) {
+    {  // every epilogue thread runs the chunk loop (its named barriers), work only when go
       const float alpha = (float)ep.alpha;
       const bool scaled = ep.alpha != 1.0;
       const int half = row & 1, rl = row >> 1;
@@ -405,8 +409,10 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
 #pragma unroll 1
       for (int cc = 0; cc < SBN / 2; cc += 32) {
         const int c0 = cbeg + cc;
+        const int grp = (warp - 2) >> 2;
         // 1/Lambda of the chunk's 64 outputs, all loads in flight before use
         float ivp[32], ivm[32];
+        if (go) {
         if (ie) {
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
@@ -448,27 +454,34 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
             box[16384 + (127 - kl) * 128 + row] = xm;
           }
         }
+        }  // go
+        // the chunk's rows of every box are complete once the group's four
+        // warps (one per 32-row quadrant) pass: its first thread writes them
+        // (32-row sub-boxes) while the group converts the next chunk
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
+        if (go && lane == 0 && (warp & 3) == 2) {
+          const uint32_t sb = smem_u32(smem);
+          if (ep.mode == EPI_SPLIT) {
+            for (int which = 0; which < 2; ++which)
+              for (int hf = 0; hf < 2; ++hf)
+                for (int hl = 0; hl < 2; ++hl) {
+                  const int brow = which ? 96 - c0 : c0;  // first box row of the chunk
+                  const uint32_t src =
+                      sb + (uint32_t)((((which * 2 + hf) * 2 + hl) * 8192 + brow * 64) * 2);
+                  const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
+                  const int y = (which ? K - n0 - SBN : n0) + brow;
+                  tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
+                }
+          } else {
+            tma_store_3d(mO0, sb + (uint32_t)(c0 * 128 * 4), r0, n0 + c0, bb);
+            tma_store_3d(mO0, sb + (uint32_t)((16384 + (96 - c0) * 128) * 4), r0, K - n0 - SBN + 96 - c0, bb);
+          }
+          tma_store_commit();
+        }
       }
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("bar.sync 1, 256;" ::: "memory");
-    if (go && warp == 2 && lane == 0) {
-      const uint32_t sb = smem_u32(smem);
-      if (ep.mode == EPI_SPLIT) {
-        for (int which = 0; which < 2; ++which)
-          for (int hf = 0; hf < 2; ++hf)
-            for (int hl = 0; hl < 2; ++hl) {
-              const uint32_t src = sb + (uint32_t)(((which * 2 + hf) * 2 + hl) * 8192 * 2);
-              const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
-              const int y = which ? K - n0 - SBN : n0;
-              tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
-            }
-      } else {
-        tma_store_3d(mO0, sb, r0, n0, bb);
-        tma_store_3d(mO0, sb + 16384 * 4, r0, K - n0 - SBN, bb);
-      }
-      tma_store_commit_wait();
-    }
+    if (go && lane == 0 && (warp & 3) == 2) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   } else if (ok) {
     if (!*abort_flag) {
 #pragma unroll 1
@@ -517,6 +530,10 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   const uint32_t accb = smem_u32(&bars[2 * C::STAGES]);
 
   if (threadIdx.x == 0) {
+    // descriptor fetches overlap the barrier and TMEM set-up
+    prefetch_map(&mAh); prefetch_map(&mAl); prefetch_map(&mPh);
+    prefetch_map(&mPl); prefetch_map(&mQh); prefetch_map(&mQl);
+    if (ep.tma_out) { prefetch_map(&mO0); prefetch_map(&mO1); }
     for (int s = 0; s < C::STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
     mbar_init(accb, 1);
     *abort_flag = 0;
@@ -622,6 +639,10 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   const uint32_t accb = smem_u32(&bars[2 * P_STAGES]);
 
   if (threadIdx.x == 0) {
+    // descriptor fetches overlap the barrier and TMEM set-up
+    prefetch_map(&mAh); prefetch_map(&mAl); prefetch_map(&mPh);
+    prefetch_map(&mPl); prefetch_map(&mQh); prefetch_map(&mQl);
+    if (ep.tma_out) { prefetch_map(&mO0); prefetch_map(&mO1); }
     for (int s = 0; s < P_STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
     mbar_init(accb, 1);
     *abort_flag = 0;
@@ -902,7 +923,7 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
     return false;
   cuuint64_t dims[3] = {R, N, B};
   cuuint64_t strides[2] = {(cuuint64_t)ld * es, (cuuint64_t)(B > 1 ? bs : ld * (long long)N) * es};
-  cuuint32_t box[3] = {box_r, (cuuint32_t)SBN, 1};
+  cuuint32_t box[3] = {box_r, 32, 1};  // one 32-column chunk of the epilogue tile
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides,
              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
