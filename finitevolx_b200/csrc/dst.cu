@@ -392,6 +392,7 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
   const int r = mvalid ? m - b * ep.rows_per_batch : 0;
   const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
   if (ok) tc_fence_after();
+  grid_dep_launch();  // the next kernel may start its set-up while this tile drains
   if (ep.tma_out) {
     // Tile staged in the idle operand ring (all MMAs have completed), then
     // written by TMA bulk-tensor stores.  The host enables this only when
@@ -552,19 +553,31 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   // staggered start (an even shift keeps the P / Q alternation)
   const int kshift = 2 * (int)((blockIdx.x * 5u + blockIdx.y * 3u) % (unsigned)(KT / 2));
   if (warp == 0 && lane == 0) {
-    for (int kt0 = 0; kt0 < KT; ++kt0) {
+    // B blocks (the DST tables) of the first ring fill before waiting for
+    // the previous kernel; A (its output) only after
+    auto load_b = [&](int kt0) {
       const int s = kt0 % C::STAGES;
-      if (kt0 >= C::STAGES && !mbar_wait(empty(s), ((kt0 / C::STAGES) - 1) & 1, abort_flag, ep.err)) break;
       mbar_expect_tx(full(s), C::STAGE);
       const uint32_t base = smem_u32(smem + s * C::STAGE);
       const int kt = (kt0 + kshift) % KT;
       const int kb = kt >> 1;
       const bool odd = kt & 1;
-      const int ac = (odd ? KH : 0) + kb * BKT;
-      tma_load_2d(base, &mAh, full(s), ac, m0);
-      tma_load_2d(base + C::A_T, &mAl, full(s), ac, m0);
       tma_load_2d(base + 2 * C::A_T, odd ? &mQh : &mPh, full(s), kb * BKT, n0);
       tma_load_2d(base + 2 * C::A_T + C::B_T, odd ? &mQl : &mPl, full(s), kb * BKT, n0);
+    };
+    for (int kt0 = 0; kt0 < KT && kt0 < C::STAGES; ++kt0) load_b(kt0);
+    grid_dep_wait();
+    for (int kt0 = 0; kt0 < KT; ++kt0) {
+      const int s = kt0 % C::STAGES;
+      if (kt0 >= C::STAGES) {
+        if (!mbar_wait(empty(s), ((kt0 / C::STAGES) - 1) & 1, abort_flag, ep.err)) break;
+        load_b(kt0);
+      }
+      const uint32_t base = smem_u32(smem + s * C::STAGE);
+      const int kt = (kt0 + kshift) % KT;
+      const int ac = ((kt & 1) ? KH : 0) + (kt >> 1) * BKT;
+      tma_load_2d(base, &mAh, full(s), ac, m0);
+      tma_load_2d(base + C::A_T, &mAl, full(s), ac, m0);
     }
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
@@ -663,21 +676,34 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   // keeps the P / Q alternation)
   const int kshift = 2 * (int)(((blockIdx.x >> 1) * 5u + blockIdx.y * 3u) % (unsigned)(KT / 2));
   if (warp == 0 && lane == 0) {
-    for (int kt0 = 0; kt0 < KT; ++kt0) {
+    // B blocks of the first ring fill before waiting for the previous
+    // kernel; A (its output) only after
+    const int brow = n0 + (int)rank * (SBN / 2);
+    auto load_b = [&](int kt0) {
       const int s = kt0 % P_STAGES;
-      if (kt0 >= P_STAGES && !mbar_wait(empty(s), ((kt0 / P_STAGES) - 1) & 1, abort_flag, ep.err)) break;
       if (rank == 0) mbar_expect_tx(full(s), 2 * P_STAGE);
       const uint32_t fb = map_to_rank(full(s), 0);
       const uint32_t base = smem_u32(smem + s * P_STAGE);
       const int kt = (kt0 + kshift) % KT;
       const int kb = kt >> 1;
       const bool odd = kt & 1;
-      const int ac = (odd ? KH : 0) + kb * BK;
-      const int brow = n0 + (int)rank * (SBN / 2);
-      tma_load_2d_pair(base, &mAh, fb, ac, m0);
-      tma_load_2d_pair(base + P_A_TILE, &mAl, fb, ac, m0);
       tma_load_2d_pair(base + 2 * P_A_TILE, odd ? &mQh : &mPh, fb, kb * BK, brow);
       tma_load_2d_pair(base + 2 * P_A_TILE + P_B_TILE, odd ? &mQl : &mPl, fb, kb * BK, brow);
+    };
+    for (int kt0 = 0; kt0 < KT && kt0 < P_STAGES; ++kt0) load_b(kt0);
+    grid_dep_wait();
+    for (int kt0 = 0; kt0 < KT; ++kt0) {
+      const int s = kt0 % P_STAGES;
+      if (kt0 >= P_STAGES) {
+        if (!mbar_wait(empty(s), ((kt0 / P_STAGES) - 1) & 1, abort_flag, ep.err)) break;
+        load_b(kt0);
+      }
+      const uint32_t fb = map_to_rank(full(s), 0);
+      const uint32_t base = smem_u32(smem + s * P_STAGE);
+      const int kt = (kt0 + kshift) % KT;
+      const int ac = ((kt & 1) ? KH : 0) + (kt >> 1) * BK;
+      tma_load_2d_pair(base, &mAh, fb, ac, m0);
+      tma_load_2d_pair(base + P_A_TILE, &mAl, fb, ac, m0);
     }
   } else if (warp == 1 && lane == 0) {
     if (rank == 0) {
@@ -987,15 +1013,21 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
       return FVX_ERR_ARG;
     dim3 grid(M / BM, KH / SBN);
     if (grid.y > 65535) return FVX_ERR_SHAPE;
-    gemm_sym_pair_kernel<<<grid, S_THREADS, P_SMEM, st>>>(a_h, a_l, p2h, p2l, q2h, q2l, o0, o1, K, ep);
+    if (fvx_launch_pdl(gemm_sym_pair_kernel, grid, dim3(S_THREADS), P_SMEM, st, a_h, a_l, p2h, p2l, q2h, q2l, o0,
+                       o1, K, ep) != cudaSuccess)
+      return FVX_ERR_CUDA;
     return fvx_cuda_status();
   }
   dim3 grid(KH / SBN, (M + BM - 1) / BM);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  if (bki == 32)
-    gemm_sym_bf16_kernel<32><<<grid, S_THREADS, SymCfg<32>::SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
-  else
-    gemm_sym_bf16_kernel<64><<<grid, S_THREADS, SymCfg<64>::SMEM, st>>>(a_h, a_l, p_h, p_l, q_h, q_l, o0, o1, K, ep);
+  // programmatic launch: the kernel's set-up and its first table loads
+  // overlap the previous kernel's tail (the producer waits before reading X)
+  const cudaError_t le =
+      bki == 32 ? fvx_launch_pdl(gemm_sym_bf16_kernel<32>, grid, dim3(S_THREADS), SymCfg<32>::SMEM, st, a_h, a_l, p_h,
+                                 p_l, q_h, q_l, o0, o1, K, ep)
+                : fvx_launch_pdl(gemm_sym_bf16_kernel<64>, grid, dim3(S_THREADS), SymCfg<64>::SMEM, st, a_h, a_l, p_h,
+                                 p_l, q_h, q_l, o0, o1, K, ep);
+  if (le != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 

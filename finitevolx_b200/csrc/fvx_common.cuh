@@ -57,6 +57,35 @@ static inline int fvx_cuda_status() {
 
 static inline cudaStream_t fvx_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// ---- programmatic dependent launch ------------------------------------------
+// A kernel launched with fvx_launch_pdl may start while the kernel before it
+// on the stream is still running (once every CTA of that kernel has executed
+// grid_dep_launch or exited).  Such a kernel must execute grid_dep_wait --
+// which returns when the previous kernel has completed and its writes are
+// visible -- before it reads anything the previous kernel wrote or writes
+// anything it may still read.  Without the launch attribute both
+// instructions return at once.
+#ifdef __CUDACC__
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+static inline cudaError_t fvx_launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                                         cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+#endif
+
 // Preconditioner / coarse-solver callback: z = M rho on the given stream;
 // returns a status.
 typedef int (*fvx_precond_fn)(void* ctx, const void* rho, void* z, void* stream);

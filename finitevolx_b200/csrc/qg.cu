@@ -29,7 +29,9 @@ static int launch_t(const StageArgs& a, cudaStream_t st) {
     set = true;
   }
   const TileSplit ts = tile_split<S, TX, TY>(a.ny, a.nx);
-  stage_kernel<T, S, TX, TY><<<ts.ntx * ts.nty, THREADS, sm, st>>>(a, ts);
+  if (fvx_launch_pdl(stage_kernel<T, S, TX, TY>, dim3(ts.ntx * ts.nty), dim3(THREADS), sm, st, a, ts) !=
+      cudaSuccess)
+    return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 

@@ -612,6 +612,9 @@ template <typename T, int S, int TX, int TY>
 __global__ void __launch_bounds__(THREADS)
 stage_kernel(StageArgs A, TileSplit ts) {
   extern __shared__ __align__(16) uint8_t sm[];
+  // launched programmatically: psi comes from the kernel before this one
+  grid_dep_wait();
+  grid_dep_launch();
   int tx, ty;
   tile_of_block(ts, blockIdx.x, tx, ty);
   stage_tile<T, S, TX, TY>(A, sm, tx * TX, ty * TY);
