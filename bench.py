@@ -12,12 +12,14 @@ field (std 1e-5 s^-1), synthetic.
 * value: device time (CUDA events on the launching stream) of K steps, each
   replayed from a CUDA graph; L2 flushed (256 MiB write) before every step,
   outside the timed events; max over ranks.
-* e2e: the same step through the public API (``QGModel.step``) from pinned
-  host memory: host->device copy of q, the step, device->host copy of
-  q_{n+1}, all inside the timed region.
+* e2e: the same step through the public API (``QGPipeline``, a stream of
+  host-resident states): every step uploads its state from pinned host
+  memory, steps it and downloads q_{n+1}, all inside the timed region; the
+  upload of state k+1 and the download of state k-1 overlap the step of
+  state k on separate streams.
 * roofline: the dominant kernel is the tcgen05 DST GEMM (one of the four
   products per solve); achieved = algorithmic 2*M*N*K flops per launch /
-  its mean CUDA-event duration, vs the measured bf16 peak.
+  its device time per launch (per_launch_ms), vs the measured bf16 peak.
 * cpu_baseline: the FP64 NumPy oracle's QG step on this host.
 * --impl reference: the reference's CPU implementation of the path
   (finitevolX's JAX stack is not installable here; the oracle port restates
@@ -430,23 +432,34 @@ def main():
             dist.destroy_process_group()
         return
 
-    # e2e through the public API with pinned host buffers
-    host_in = torch.empty(q0.shape, dtype=torch.float32, pin_memory=True)
-    host_in.copy_(q0.cpu())
+    # e2e through the public API (QGPipeline): every step uploads its input
+    # state from pinned host memory and downloads its result; the pipeline
+    # overlaps the upload of state k+1 and the download of state k-1 with
+    # the step of state k.  L2 flushed before every step on the step stream.
+    from finitevolx_b200.qg import QGPipeline
+    pipe = QGPipeline(model, dt)
+    n_host = 4
+    host_in = torch.empty((n_host,) + tuple(q0.shape), dtype=torch.float32, pin_memory=True)
+    for h in range(n_host):
+        host_in[h].copy_(q0.cpu())
     host_out = torch.empty_like(host_in, pin_memory=True)
-    e2e_ms = 0.0
-    for k in range(args.warmup + args.steps):
-        flush.fill_(float(k))
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        qd = host_in.to("cuda", non_blocking=True)
-        out = model.step(qd, dt)
-        host_out.copy_(out, non_blocking=True)
-        e1.record()
-        e1.synchronize()
-        if k >= args.warmup:
-            e2e_ms += e0.elapsed_time(e1)
+    flush_fn = lambda: flush.fill_(1.0)  # noqa: E731
+    pipe.run(host_in, host_out, n=max(args.warmup, 3), between_steps=flush_fn)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    pipe.run(host_in, host_out, n=args.steps, between_steps=flush_fn)
+    e1.record()
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    # the pipeline steps the same state as the graphs above: check its result
+    if rank == 0:
+        ref_out = model.step(host_in[0].to("cuda"), dt).cpu()
+        diff = (host_out[(args.steps - 1) % n_host] - ref_out).abs().max() / ref_out.abs().max()
+        if not float(diff) <= 1e-6:
+            raise RuntimeError(f"e2e pipeline result differs from QGModel.step ({float(diff):.3e})")
+    host_in = host_in[0]
     if world > 1:
         tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -513,7 +526,9 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(config(n, args.method), autotuned=tuned),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
-                    "ms_per_step": e2e_ms / args.steps},
+                    "ms_per_step": e2e_ms / args.steps,
+                    "form": "QGPipeline: upload of state k+1, step k (CUDA graph), download of k-1 on three "
+                            "streams; L2 flushed before every step"},
             "gpu_launches": per_step_launches * args.steps,
             "roofline": {"bound": "tensor",
                          "kernel": ("gemm_sym_bf16_kernel (even/odd DST-I product, 3xBF16)" if sym

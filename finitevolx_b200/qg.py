@@ -168,6 +168,74 @@ class QGModel:
         return bc(lincomb(1.0 / 3.0, q, 2.0 / 3.0, y2, (2.0 / 3.0) * dt, k3))
 
 
+class QGPipeline:
+    """Steps a stream of host-resident states through one QGModel with the
+    transfers hidden behind the arithmetic.
+
+    Each state is uploaded from pinned host memory, advanced by one fused
+    RK3 step (a CUDA graph replay) and downloaded.  Three CUDA streams run
+    the upload of state k+1, the step of state k and the download of state
+    k-1 at once (device buffers double-buffered, ordered by events), so a
+    run of K states takes about K steps when the step is longer than either
+    copy.  This is the serving / ensemble-of-requests form of the step; a
+    single trajectory keeps its state on the device instead.
+    """
+
+    def __init__(self, model: QGModel, dt: float):
+        self.model, self.dt = model, float(dt)
+        g = model.grid
+        self.din = [torch.zeros((g.Ny, g.Nx), dtype=model.dtype, device="cuda") for _ in range(2)]
+        self.dout = [torch.empty_like(self.din[0]) for _ in range(2)]
+        self.s_up, self.s_step, self.s_down = (torch.cuda.Stream() for _ in range(3))
+        for i in range(2):  # resolves kernel attributes outside capture
+            model.step(self.din[i], self.dt, out=self.dout[i])
+        torch.cuda.synchronize()
+        self.graphs = []
+        self.s_step.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(self.s_step):
+            for i in range(2):
+                gph = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(gph, stream=self.s_step):
+                    model.step(self.din[i], self.dt, out=self.dout[i])
+                self.graphs.append(gph)
+        torch.cuda.current_stream().wait_stream(self.s_step)
+        self._ev = {k: [torch.cuda.Event() for _ in range(2)] for k in ("up", "step", "down")}
+
+    def run(self, host_in, host_out, n=None, between_steps=None) -> None:
+        """Step state ``host_in[k % len(host_in)]`` into ``host_out[k % len(host_out)]``
+        for k < n (default len(host_in)).  Host tensors must be pinned and
+        [.., Ny, Nx] of the model's dtype.  ``between_steps``: optional
+        callable enqueued on the step stream before every step.  Returns
+        when everything is enqueued; the current stream waits for the last
+        download."""
+        n = len(host_in) if n is None else int(n)
+        cur = torch.cuda.current_stream()
+        for s in (self.s_up, self.s_step, self.s_down):
+            s.wait_stream(cur)
+        ev = self._ev
+        for k in range(n):
+            i = k % 2
+            with torch.cuda.stream(self.s_up):
+                if k >= 2:
+                    self.s_up.wait_event(ev["step"][i])  # step k-2 has read din[i]
+                self.din[i].copy_(host_in[k % len(host_in)], non_blocking=True)
+                ev["up"][i].record(self.s_up)
+            with torch.cuda.stream(self.s_step):
+                self.s_step.wait_event(ev["up"][i])
+                if k >= 2:
+                    self.s_step.wait_event(ev["down"][i])  # download k-2 has read dout[i]
+                if between_steps is not None:
+                    between_steps()
+                self.graphs[i].replay()
+                ev["step"][i].record(self.s_step)
+            with torch.cuda.stream(self.s_down):
+                self.s_down.wait_event(ev["step"][i])
+                host_out[k % len(host_out)].copy_(self.dout[i], non_blocking=True)
+                ev["down"][i].record(self.s_down)
+        for s in (self.s_up, self.s_step, self.s_down):
+            cur.wait_stream(s)
+
+
 def geostrophic_velocity(psi, grid: ArakawaCGrid2D):
     """(u, v) from a T-point streamfunction (qg_1p5_layer.py:115-145)."""
     from finitevolx_b200 import operators as O
