@@ -5,6 +5,8 @@
 
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 namespace fvx {
 namespace qg {
 
@@ -261,8 +263,15 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   cp_async_wait_all();
   }
   __syncthreads();
+  constexpr int SEG = TX * TY / THREADS;
+  constexpr bool WIN = IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && SEG >= 2 && SEG % 2 == 0 &&
+                       SEG * THREADS == TX * TY && TX % SEG == 0 && TY % SEG == 0;
+  constexpr bool PACK =
+      !WIN && IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
   // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
-  if constexpr (IN && THREADS % TX == 0 && THREADS / TX <= TY + 1) {
+  // (not built by the WIN body, which takes u and v from psi directly)
+  if constexpr (WIN) {
+  } else if constexpr (IN && THREADS % TX == 0 && THREADS / TX <= TY + 1) {
     // a column of X per thread group, walking down the rows (two new psi
     // loads per row); the last column by the first TY + 1 threads
     constexpr int RG = THREADS / TX, RPG = (TY + 1 + RG - 1) / RG;
@@ -291,7 +300,7 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     }
     xt[k] = val;
   }
-  __syncthreads();
+  if constexpr (!WIN) __syncthreads();
   const T dx = T(A.dx), dy = T(A.dy);
   const T rdx = T(1.0 / A.dx), rdy = T(1.0 / A.dy);
   // u at U-point (j, i) = -(X[j,i] - X[j-1,i]) / dy on [1, N-2]^2
@@ -306,17 +315,18 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     return divr(p[0] - p[-1], dx, rdx);
   };
   // ---- face fluxes --------------------------------------------------------
-  // FP32 WENO5 / WENO-Z5 interior tiles: each thread reconstructs a run of
-  // SEG east faces along a row and a run of SEG north faces along a column
-  // from a register window of SEG + 5 cells (one shared-memory load per
-  // face instead of six), the upwind stencil picked from the window and two
-  // neighbouring faces evaluated as one packed f32x2 pair.
-  constexpr int SEG = TX * TY / THREADS;
-  constexpr bool WIN = IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && SEG >= 2 && SEG % 2 == 0 &&
-                       SEG * THREADS == TX * TY && TX % SEG == 0 && TY % SEG == 0;
-  constexpr bool PACK =
-      !WIN && IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
+  // FP32 WENO5 / WENO-Z5 interior tiles (WIN): each thread reconstructs a
+  // run of SEG east faces along a row and a run of SEG north faces along a
+  // column from a register window of SEG + 5 cells (one shared-memory load
+  // per face instead of six), the upwind stencil picked from the window and
+  // two neighbouring faces evaluated as one packed f32x2 pair.  Velocities
+  // come straight from psi: u = -(X[j] - X[j-1]) / dy with
+  // X = T_to_X(psi) is -(psi[j+1][i] + psi[j+1][i+1] - psi[j-1][i] -
+  // psi[j-1][i+1]) / (4 dy) (the psi[j] terms cancel), v likewise, summed as
+  // sliding differences along the walk, so no X array is built.
   if constexpr (WIN) {
+    const float cu = -0.25f * (float)rdy, cv = 0.25f * (float)rdx;
+    const float* ps = (const float*)pt;  // psi (gy, gx) at ps[(gy - y0 + 1) * (TX + 2) + gx - x0 + 1]
     constexpr bool Z = SchemeInfo<S>::zfam;
     const float* q32 = (const float*)qt;
     {  // east faces of cells x0 + xs .. x0 + xs + SEG - 1 on row ly
@@ -325,9 +335,15 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
       float w[SEG + 5];
 #pragma unroll
       for (int k = 0; k < SEG + 5; ++k) w[k] = p[k - 2];
+      // d[m] = psi(j+1, i) - psi(j-1, i) at i = x0 + xs + m, j = y0 + ly
+      float d[SEG + 1];
+      const float* pn = ps + (ly + 2) * (TX + 2) + (xs + 1);
+      const float* pm = ps + ly * (TX + 2) + (xs + 1);
+#pragma unroll
+      for (int m = 0; m <= SEG; ++m) d[m] = pn[m] - pm[m];
 #pragma unroll
       for (int f = 0; f < SEG; f += 2) {  // faces f and f + 1 as one packed pair
-        const float u0 = (float)uvel(y0 + ly, x0 + xs + f), u1 = (float)uvel(y0 + ly, x0 + xs + f + 1);
+        const float u0 = cu * (d[f] + d[f + 1]), u1 = cu * (d[f + 1] + d[f + 2]);
         const bool p0 = u0 >= 0.f, p1 = u1 >= 0.f;
         float2 e[5];
 #pragma unroll
@@ -344,9 +360,14 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
       float w[SEG + 5];
 #pragma unroll
       for (int k = 0; k < SEG + 5; ++k) w[k] = p[(k - 2) * QW];
+      // e[m] = psi(j, i+1) - psi(j, i-1) at j = y0 + ys + m, i = x0 + lx
+      float e2[SEG + 1];
+      const float* pc = ps + (ys + 1) * (TX + 2) + lx;
+#pragma unroll
+      for (int m = 0; m <= SEG; ++m) e2[m] = pc[m * (TX + 2) + 2] - pc[m * (TX + 2)];
 #pragma unroll
       for (int f = 0; f < SEG; f += 2) {
-        const float v0 = (float)vvel(y0 + ys + f, x0 + lx), v1 = (float)vvel(y0 + ys + f + 1, x0 + lx);
+        const float v0 = cv * (e2[f] + e2[f + 1]), v1 = cv * (e2[f + 1] + e2[f + 2]);
         const bool p0 = v0 >= 0.f, p1 = v1 >= 0.f;
         float2 e[5];
 #pragma unroll
@@ -362,12 +383,14 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     // the tile's west-most east faces and south-most north faces
     for (int k = tid; k < TY + TX; k += THREADS) {
       if (k < TY) {
-        const int ly = k, gj = y0 + ly, gi = x0 - 1;
-        const T uu = uvel(gj, gi);
+        const int ly = k, gi = x0 - 1;
+        const float* a = ps + ly * (TX + 2);  // psi rows j-1 and j+1 at columns x0-1, x0
+        const T uu = (T)(cu * ((a[2 * (TX + 2)] - a[0]) + (a[2 * (TX + 2) + 1] - a[1])));
         fe[ly * (TX + 1)] = face_value_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
       } else {
-        const int lx = k - TY, gj = y0 - 1, gi = x0 + lx;
-        const T vv = vvel(gj, gi);
+        const int lx = k - TY, gj = y0 - 1;
+        const float* a = ps + lx;  // psi rows y0-1, y0 at columns i-1, i+1
+        const T vv = (T)(cv * ((a[2] - a[0]) + (a[(TX + 2) + 2] - a[TX + 2])));
         fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
         vs[lx] = vv;
       }
@@ -456,26 +479,40 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
       const int xi = gi - 1;
       const int scol = A.split_layout ? ((xi & 1) ? (nxi >> 1) + (xi >> 1) : (xi >> 1)) : xi;
       size_t sidx = (size_t)(y0 + ly0 - 1) * nxi + scol;
-      T fs = fnp[0], vsv = vsp[0];
+      // one loop per (q_n present, split wanted) pair: no per-cell branches
+      auto run = [&](auto has_qn, auto do_split) {
+        T fs = fnp[0], vsv = vsp[0];
+        const T* qnp = decltype(has_qn)::value ? qn + g : nullptr;
+        T* op = out + g;
+        __nv_bfloat16* hp = decltype(do_split)::value ? A.split_hi + sidx : nullptr;
+        __nv_bfloat16* lp = decltype(do_split)::value ? A.split_lo + sidx : nullptr;
 #pragma unroll
-      for (int f = 0; f < SEGT; ++f) {
-        const T fnn = fnp[(f + 1) * TX], vn = vsp[(f + 1) * TX];
-        T rhs = -(divr(fep[f * (TX + 1) + 1] - fep[f * (TX + 1)], dx, rdx) + divr(fnn - fs, dy, rdy));
-        rhs = rhs + (-beta * (T(0.5) * (vn + vsv)));
-        T r = cb * qp[f * QW];
-        if (qn) r = ca * qn[g] + r;
-        r = r + cc * rhs;
-        out[g] = r;
-        if (A.split_hi) {
-          const float fv = (float)r;
-          const __nv_bfloat16 h = __float2bfloat16_rn(fv);
-          A.split_hi[sidx] = h;
-          A.split_lo[sidx] = __float2bfloat16_rn(fv - __bfloat162float(h));
+        for (int f = 0; f < SEGT; ++f) {
+          const T fnn = fnp[(f + 1) * TX], vn = vsp[(f + 1) * TX];
+          T rhs = -(divr(fep[f * (TX + 1) + 1] - fep[f * (TX + 1)], dx, rdx) + divr(fnn - fs, dy, rdy));
+          rhs = rhs + (-beta * (T(0.5) * (vn + vsv)));
+          T r = cb * qp[f * QW];
+          if constexpr (decltype(has_qn)::value) r = ca * qnp[(size_t)f * nx] + r;
+          r = r + cc * rhs;
+          op[(size_t)f * nx] = r;
+          if constexpr (decltype(do_split)::value) {
+            const float fv = (float)r;
+            const __nv_bfloat16 h = __float2bfloat16_rn(fv);
+            hp[(size_t)f * nxi] = h;
+            lp[(size_t)f * nxi] = __float2bfloat16_rn(fv - __bfloat162float(h));
+          }
+          fs = fnn;
+          vsv = vn;
         }
-        g += nx;
-        sidx += nxi;
-        fs = fnn;
-        vsv = vn;
+      };
+      using yes = std::true_type;
+      using no = std::false_type;
+      if (qn) {
+        if (A.split_hi) run(yes{}, yes{});
+        else run(yes{}, no{});
+      } else {
+        if (A.split_hi) run(no{}, yes{});
+        else run(no{}, no{});
       }
       return;
     }
