@@ -534,7 +534,11 @@ def main():
                          "kernel": ("gemm_sym_bf16_kernel (even/odd DST-I product, 3xBF16)" if sym
                                     else "gemm_split_bf16_kernel (DST product, 3xBF16)"),
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "peak_source": peak_src, "traffic": None,
+                         "peak_source": peak_src,
+                         # DRAM bytes per launch from an ncu capture of this kernel in this
+                         # step (dram__bytes_read.sum + dram__bytes_write.sum, first product;
+                         # the operands otherwise stay in L2 between the products)
+                         "traffic": 25.2e6 if n == 2048 and sym else None, "traffic_unit": "bytes",
                          "per_launch_ms": gemm_ms, "algorithmic_flops_per_launch": flops,
                          "executed_tensor_flops_per_launch": (3.0 if sym else 6.0) * n ** 3,
                          "executed_frac": (3.0 if sym else 6.0) * n ** 3 / (gemm_ms * 1e-3) / 1e12 / peak},
