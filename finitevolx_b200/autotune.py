@@ -60,7 +60,10 @@ def _device_key() -> str:
     return torch.cuda.get_device_name(torch.cuda.current_device()).replace(" ", "_")
 
 
-def _time(fn_call, reps: int = 7, warm: int = 2) -> float:
+def _time(fn_call, reps: int = 7, warm: int = 2, batch: int = 5) -> float:
+    """Median over ``reps`` of the device time of ``batch`` back-to-back
+    calls between two events, per call: the calls queue behind each other,
+    so the host's launch latency does not enter the window."""
     for _ in range(warm):
         fn_call()
     ts = []
@@ -68,10 +71,11 @@ def _time(fn_call, reps: int = 7, warm: int = 2) -> float:
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record()
-        fn_call()
+        for _ in range(batch):
+            fn_call()
         e1.record()
         e1.synchronize()
-        ts.append(e0.elapsed_time(e1))
+        ts.append(e0.elapsed_time(e1) / batch)
     return statistics.median(ts)
 
 
@@ -174,7 +178,7 @@ def tune_ensemble(ens, candidates=(0, 1, 2, 4), steps: int = 3, use_cache: bool 
     ms = {}
     for c in candidates:
         ens.set_blocks_per_sm(c)
-        ms[str(c)] = _time(lambda: ens.step(steps), reps=3, warm=1)
+        ms[str(c)] = _time(lambda: ens.step(steps), reps=3, warm=1, batch=1)
     best = min(ms, key=ms.get)
     ens.set_blocks_per_sm(int(best))
     res = {"blocks_per_sm": int(best), "ms": ms}
