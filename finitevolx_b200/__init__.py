@@ -66,6 +66,7 @@ from finitevolx_b200.qg import QGModel, QGPipeline
 from finitevolx_b200.ensemble import QGEnsemble
 from finitevolx_b200.swm import Coriolis2D, MomentumAdvection2D, Vorticity2D
 from finitevolx_b200 import diagnostics
+from finitevolx_b200.snapshots import QGSnapshotRecorder, read_zarr_v3
 
 __all__ = [
     "ArakawaCGrid2D", "CartesianGrid2D", "Mask2D", "StencilCapability2D", "count_contiguous",
@@ -79,6 +80,6 @@ __all__ = [
     "dst1_eigenvalues", "fft_eigenvalues", "make_spectral_preconditioner", "pressure_from_divergence",
     "solve_helmholtz_dct", "solve_helmholtz_fft", "solve_poisson_dct", "solve_poisson_fft",
     "solve_poisson_dst", "streamfunction_from_vorticity", "build_coupling_matrix",
-    "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel", "QGPipeline", "QGEnsemble",
+    "decompose_vertical_modes", "layer_to_mode", "mode_to_layer", "QGModel", "QGPipeline", "QGEnsemble", "QGSnapshotRecorder", "read_zarr_v3",
     "Coriolis2D", "MomentumAdvection2D", "Vorticity2D", "diagnostics",
 ]

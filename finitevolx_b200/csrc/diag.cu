@@ -136,6 +136,32 @@ __global__ void interior_sum_kernel(const T* __restrict__ a, const T* __restrict
   }
 }
 
+// The seven interior planes of a QG snapshot (scripts/qg_1p5_layer.py:514-545,
+// record_snapshot): q, psi, eta = eta_scale psi, U_to_T(u), V_to_T(v),
+// speed = sqrt(u_T^2 + v_T^2), X_to_T(zeta) -- the interpolation formulas of
+// operators/interpolation.py (0.5 (c + w), 0.5 (c + s), 0.25 (c + s + w + sw))
+// on the full [ny][nx] arrays, written to out[7][ny-2][nx-2] in one pass.
+template <typename T>
+__global__ void snapshot_pack_kernel(const T* __restrict__ q, const T* __restrict__ psi, const T* __restrict__ u,
+                                     const T* __restrict__ v, const T* __restrict__ z, int ny, int nx, T eta_scale,
+                                     T* __restrict__ out) {
+  const int nyi = ny - 2, nxi = nx - 2;
+  const size_t plane = (size_t)nyi * nxi;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < plane; k += (size_t)gridDim.x * blockDim.x) {
+    const int jj = (int)(k / nxi), ii = (int)(k - (size_t)jj * nxi);
+    const size_t g = (size_t)(jj + 1) * nx + (ii + 1);
+    const T uT = T(0.5) * (u[g] + u[g - 1]);
+    const T vT = T(0.5) * (v[g] + v[g - nx]);
+    out[k] = q[g];
+    out[plane + k] = psi[g];
+    out[2 * plane + k] = eta_scale * psi[g];
+    out[3 * plane + k] = uT;
+    out[4 * plane + k] = vT;
+    out[5 * plane + k] = sqrt(uT * uT + vT * vT);
+    out[6 * plane + k] = T(0.25) * (z[g] + z[g - nx] + z[g - 1] + z[g - nx - 1]);
+  }
+}
+
 static int grid_for(size_t n) {
   size_t b = (n + 255) / 256;
   return (int)(b > 148 * 16 ? 148 * 16 : (b < 1 ? 1 : b));
@@ -170,6 +196,19 @@ using namespace fvx::diag;
                                                                        out_dev);                                 \
     return fvx_cuda_status();                                                                                    \
   }
+
+#define FVX_DEF_SNAP(SFX, T)                                                                                  \
+  extern "C" int fvx_qg_snapshot_pack_##SFX(const T* q, const T* psi, const T* u, const T* v, const T* z, int ny, \
+                                            int nx, double eta_scale, T* out, void* stream) {                   \
+    if (!q || !psi || !u || !v || !z || !out) return FVX_ERR_ARG;                                              \
+    if (ny < 3 || nx < 3) return FVX_ERR_SHAPE;                                                                \
+    snapshot_pack_kernel<T><<<grid_for((size_t)(ny - 2) * (nx - 2)), 256, 0, fvx_stream(stream)>>>(            \
+        q, psi, u, v, z, ny, nx, (T)eta_scale, out);                                                           \
+    return fvx_cuda_status();                                                                                  \
+  }
+
+FVX_DEF_SNAP(f32, float)
+FVX_DEF_SNAP(f64, double)
 
 FVX_DEF_DIAG(f32, float)
 FVX_DEF_DIAG(f64, double)

@@ -365,6 +365,16 @@ int fvx_nn_adam(float* w, void* w_bf16, const float* grad, float* m, float* v, i
                 double beta2, double eps, int step, void* stream);
 int fvx_nn_to_bf16(const float* src, void* dst, int n, void* stream);
 
+/* ---- QG snapshot planes ------------------------------------------------- */
+/* record_snapshot of scripts/qg_1p5_layer.py:514-545 on the device: from
+ * the full [ny, nx] q, psi (zero ghost ring), u (U points), v (V points) and
+ * relative vorticity z (X points), writes out[7][ny-2][nx-2] = q, psi,
+ * eta_scale * psi, U_to_T(u), V_to_T(v), speed, X_to_T(z) (interiors). */
+int fvx_qg_snapshot_pack_f32(const float* q, const float* psi, const float* u, const float* v, const float* z,
+                             int ny, int nx, double eta_scale, float* out, void* stream);
+int fvx_qg_snapshot_pack_f64(const double* q, const double* psi, const double* u, const double* v,
+                             const double* z, int ny, int nx, double eta_scale, double* out, void* stream);
+
 /* ---- QG fused-stage tile shape (autotuner) -------------------------------- */
 /* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8, 3 = 64x32, 4 = 128x16 cells for (method, dtype 0 FP32 / 1
  * FP64); cfg < 0 returns the number of configurations.  No counterpart in

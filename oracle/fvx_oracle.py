@@ -1284,6 +1284,22 @@ def qg_velocity(psi, dx, dy):
     return -diff2d("diff_y_X_to_U", px, dx, dy), diff2d("diff_x_X_to_V", px, dx, dy)
 
 
+def qg_snapshot(q, dx, dy, lam, eta_scale):
+    """record_snapshot (qg_1p5_layer.py:514-545) on a full [Ny, Nx] state:
+    psi by the DST with a zero ghost ring, geostrophic u, v, relative
+    vorticity (Vorticity2D.relative_vorticity, the curl at X points), then the
+    seven interior planes q, psi, eta, U_to_T(u), V_to_T(v), speed,
+    X_to_T(zeta) and 0.5 mean(q^2)."""
+    psi = np.zeros_like(q)
+    psi[1:-1, 1:-1] = solve_helmholtz_dst(q[1:-1, 1:-1], dx, dy, lam)
+    u, v = qg_velocity(psi, dx, dy)
+    zeta = diff2d("curl", u, dx, dy, None, v)
+    uc, vc, zc = interp2d("U_to_T", u), interp2d("V_to_T", v), interp2d("X_to_T", zeta)
+    i = (slice(1, -1), slice(1, -1))
+    planes = np.stack([q[i], psi[i], eta_scale * psi[i], uc[i], vc[i], np.sqrt(uc[i] ** 2 + vc[i] ** 2), zc[i]])
+    return planes, float(0.5 * np.mean(q[i] ** 2))
+
+
 def qg_tendency(q, dx, dy, beta, lam, method="weno5", bc="periodic", forcing=None,
                 drag=0.0, viscosity=0.0):
     """PV tendency (qg_1p5_layer.py:454-487), psi by DST with zero ghosts."""
