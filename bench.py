@@ -414,14 +414,12 @@ def main():
             e1.synchronize()
             total_ms += e0.elapsed_time(e1)
     torch.cuda.synchronize()
-    t_max = total_ms
+    from finitevolx_b200.replicas import max_over_ranks, whole_job_rate
+    t_max = max_over_ranks(total_ms, device="cuda")
     if world > 1:
-        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
         dist.barrier()
     cells = n * n
-    value = world * cells * args.steps / (t_max * 1e-3) / 1e6
+    value = whole_job_rate(cells, args.steps, t_max, world)
     if args.profile:
         if rank == 0:
             print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "steps": args.steps,
@@ -460,11 +458,8 @@ def main():
         if not float(diff) <= 1e-6:
             raise RuntimeError(f"e2e pipeline result differs from QGModel.step ({float(diff):.3e})")
     host_in = host_in[0]
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e = world * cells * args.steps / (e2e_ms * 1e-3) / 1e6
+    e2e_ms = max_over_ranks(e2e_ms, device="cuda")
+    e2e = whole_job_rate(cells, args.steps, e2e_ms, world)
     nbytes = host_in.numel() * host_in.element_size()
 
     # fused vs unfused: the same step as the reference's operator sequence,
