@@ -800,17 +800,26 @@ template <typename T>
 __global__ void split_input_kernel(const T* __restrict__ in, long long bstride, long long ld, int ny, int nx,
                                    int batch, bf16* __restrict__ hi, bf16* __restrict__ lo, double scale,
                                    int perm = 0) {
-  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)batch * ny * nx;
-  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
-    long long b = k / ((long long)ny * nx);
-    long long rem = k - b * ny * nx;
-    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
-    float v = (float)((double)in[b * bstride + (long long)y * ld + x] * scale);
-    bf16 h = __float2bfloat16_rn(v);
-    const long long o = perm ? k - x + deinterleave(x, nx) : k;
-    hi[o] = h;
-    lo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+  // rows of the [batch][ny][nx] input over the grid, (even, odd) pairs of a
+  // row over the threads: no 64-bit divisions, and with perm the two halves
+  // of the de-interleaved row are written by consecutive threads
+  const int rows = batch * ny, half = (nx + 1) >> 1;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int b = r / ny, y = r - b * ny;
+    const T* src = in + (long long)b * bstride + (long long)y * ld;
+    const long long o = (long long)r * nx;
+    for (int p = threadIdx.x; p < half; p += blockDim.x) {
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int x = 2 * p + e;
+        if (x >= nx) break;
+        const float v = (float)((double)src[x] * scale);
+        const bf16 h = __float2bfloat16_rn(v);
+        const long long d = o + (perm ? (e ? (nx >> 1) + p : p) : x);
+        hi[d] = h;
+        lo[d] = __float2bfloat16_rn(v - __bfloat162float(h));
+      }
+    }
   }
 }
 
