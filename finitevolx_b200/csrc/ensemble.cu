@@ -145,6 +145,11 @@ struct fvx_ens {
     int perm = 0;
   };
   std::vector<Group> groups;
+  // one stream per size group after the first: the groups' DST chains are
+  // independent, and the small groups alone would leave most SMs idle
+  std::vector<cudaStream_t> gst;
+  std::vector<cudaEvent_t> gdone;
+  cudaEvent_t fork = nullptr;
   FieldDesc* fd = nullptr;
   unsigned* counter = nullptr;
   std::vector<void*> allocs;
@@ -153,6 +158,14 @@ struct fvx_ens {
 static void ens_free(fvx_ens* e) {
   for (auto& g : e->groups)
     if (g.plan) fvx_dst_plan_destroy(g.plan);
+  for (cudaStream_t s : e->gst)
+    if (s) cudaStreamDestroy(s);
+  for (cudaEvent_t ev : e->gdone)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  e->gst.clear();
+  e->gdone.clear();
+  e->fork = nullptr;
   for (void* p : e->allocs) cudaFree(p);
   e->allocs.clear();
 }
@@ -400,16 +413,37 @@ extern "C" int fvx_ens_launches_per_step(fvx_ens* e) {
 extern "C" int fvx_ens_step(fvx_ens* e, int n_steps, void* stream) {
   if (!e || n_steps < 0) return FVX_ERR_ARG;
   cudaStream_t st = fvx_stream(stream);
+  const int ng = (int)e->groups.size();
+  if (e->gst.size() + 1 < (size_t)ng) {  // created on first use, on the caller's device
+    for (int k = (int)e->gst.size(); k < ng - 1; ++k) {
+      cudaStream_t s2 = nullptr;
+      cudaEvent_t ev = nullptr;
+      if (cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess)
+        return FVX_ERR_CUDA;
+      e->gst.push_back(s2);
+      e->gdone.push_back(ev);
+    }
+    if (!e->fork && cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) != cudaSuccess) return FVX_ERR_CUDA;
+  }
   for (int it = 0; it < n_steps; ++it)
     for (int s = 0; s < 3; ++s) {
-      for (auto& g : e->groups) {
+      // fork: group 0 on the caller's stream, the others on their own
+      if (ng > 1 && cudaEventRecord(e->fork, st) != cudaSuccess) return FVX_ERR_CUDA;
+      for (int k = 0; k < ng; ++k) {
+        auto& g = e->groups[k];
+        cudaStream_t gs = k == 0 ? st : e->gst[k - 1];
+        if (k > 0 && cudaStreamWaitEvent(gs, e->fork, 0) != cudaSuccess) return FVX_ERR_CUDA;
         const size_t tot = (size_t)g.B * g.n * g.n;
-        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, st>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm);
-        int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, (long long)g.n * g.n, g.n, g.B, st);
+        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, gs>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm);
+        int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, (long long)g.n * g.n, g.n, g.B, gs);
         if (rc) return rc;
         const size_t tl = (size_t)g.nlay * g.n * g.n;
-        ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, st>>>(g.ld, g.nlay, g.n, g.psim);
+        ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, gs>>>(g.ld, g.nlay, g.n, g.psim);
+        if (k > 0 && cudaEventRecord(e->gdone[k - 1], gs) != cudaSuccess) return FVX_ERR_CUDA;
       }
+      for (int k = 1; k < ng; ++k)  // join before the stage kernel reads every psi
+        if (cudaStreamWaitEvent(st, e->gdone[k - 1], 0) != cudaSuccess) return FVX_ERR_CUDA;
       int rc = ens_stage_dispatch(e, s, st);
       if (rc) return rc;
     }
