@@ -266,8 +266,6 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
   constexpr int SEG = TX * TY / THREADS;
   constexpr bool WIN = IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && SEG >= 2 && SEG % 2 == 0 &&
                        SEG * THREADS == TX * TY && TX % SEG == 0 && TY % SEG == 0;
-  constexpr bool PACK =
-      !WIN && IN && sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5) && (TX & (TX - 1)) == 0;
   // ---- X = interior(T_to_X(psi)) on rows y0-1.., cols x0-1.. -------------
   // (not built by the WIN body, which takes u and v from psi directly)
   if constexpr (WIN) {
@@ -391,40 +389,6 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
         const int lx = k - TY, gj = y0 - 1;
         const float* a = ps + lx;  // psi rows y0-1, y0 at columns i-1, i+1
         const T vv = (T)(cv * ((a[2] - a[0]) + (a[(TX + 2) + 2] - a[TX + 2])));
-        fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
-        vs[lx] = vv;
-      }
-    }
-  } else if constexpr (PACK) {
-    // each cell's east and north faces as one packed pair of reconstructions
-    for (int k = tid; k < TY * TX; k += THREADS) {
-      const int ly = k / TX, lx = k % TX;
-      const int gj = y0 + ly, gi = x0 + lx;
-      const float uu = (float)uvel(gj, gi), vv = (float)vvel(gj, gi);
-      const float* p = (const float*)qt + (ly + H) * QW + (lx + H);
-      const bool px = uu >= 0.f, py = vv >= 0.f;
-      // oriented stencils (face_value_full): pos e(k) = p[k], neg e(k) = p[1-k]
-      float2 e[5];
-#pragma unroll
-      for (int j = 0; j < 5; ++j) {
-        const float xa = p[j - 2], xb = p[3 - j];
-        const float ya = p[(j - 2) * QW], yb = p[(3 - j) * QW];
-        e[j] = make_float2(px ? xa : xb, py ? ya : yb);
-      }
-      const float2 f = weno5_x2<SchemeInfo<S>::zfam>(e[0], e[1], e[2], e[3], e[4]);
-      fe[ly * (TX + 1) + lx + 1] = (T)(f.x * uu);
-      fn[(ly + 1) * TX + lx] = (T)(f.y * vv);
-      vs[(ly + 1) * TX + lx] = (T)vv;
-    }
-    // the tile's west-most east faces and south-most north faces
-    for (int k = tid; k < TY + TX; k += THREADS) {
-      if (k < TY) {
-        const int ly = k, gj = y0 + ly, gi = x0 - 1;
-        const T uu = uvel(gj, gi);
-        fe[ly * (TX + 1)] = face_value_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
-      } else {
-        const int lx = k - TY, gj = y0 - 1, gi = x0 + lx;
-        const T vv = vvel(gj, gi);
         fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
         vs[lx] = vv;
       }
