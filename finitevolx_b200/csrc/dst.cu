@@ -118,12 +118,23 @@ DEV void tma_store_commit_wait() {
   asm volatile("cp.async.bulk.commit_group;" ::: "memory");
   asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
 }
+// A-operand collector buffer (tcgen05.mma .collector::a::*): an MMA with
+// COLL_FILL keeps the A tile it reads from shared memory in the tensor
+// core's collector; the next MMA, with COLL_LASTUSE and the same A
+// descriptor, takes A from there instead of shared memory and frees it.
+// The split products reuse A_hi this way (A_hi B_hi, then A_hi B_lo).
+enum { COLL_NONE = 0, COLL_FILL = 1, COLL_LASTUSE = 2 };
+#define FVX_UMMA(GROUP, QUAL)                                                      \
+  asm volatile(                                                                    \
+      "{\n\t.reg .pred p;\n\t"                                                     \
+      "setp.ne.b32 p, %4, 0;\n\t"                                                  \
+      "tcgen05.mma.cta_group::" GROUP ".kind::f16" QUAL " [%0], %1, %2, %3, p;\n\t}" \
+      ::"r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(accumulate))
+template <int COLL = COLL_NONE>
 DEV void umma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+  if constexpr (COLL == COLL_FILL) FVX_UMMA("1", ".collector::a::fill");
+  else if constexpr (COLL == COLL_LASTUSE) FVX_UMMA("1", ".collector::a::lastuse");
+  else FVX_UMMA("1", "");
 }
 DEV void umma_commit(uint32_t bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -157,13 +168,13 @@ DEV void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, uint32_t bar, in
 }
 // M = 256 product over the pair: A rows 0-127 from the leader's shared
 // memory, 128-255 from the peer's; B's N columns split in halves likewise.
+template <int COLL = COLL_NONE>
 DEV void umma_bf16_pair(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+  if constexpr (COLL == COLL_FILL) FVX_UMMA("2", ".collector::a::fill");
+  else if constexpr (COLL == COLL_LASTUSE) FVX_UMMA("2", ".collector::a::lastuse");
+  else FVX_UMMA("2", "");
 }
+#undef FVX_UMMA
 // Arrive on barrier `bar` of both CTAs of the pair once the issued MMAs end.
 DEV void umma_commit_pair(uint32_t bar) {
   asm volatile(
@@ -304,8 +315,8 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
 #pragma unroll
       for (int kk = 0; kk < BK / 16; ++kk) {
         const uint64_t o = (uint64_t)(kk * 32 >> 4);
-        umma_bf16(tmem, ah + o, bh + o, kIdesc, (kt | kk) != 0);
-        umma_bf16(tmem, ah + o, bl + o, kIdesc, 1u);
+        umma_bf16<COLL_FILL>(tmem, ah + o, bh + o, kIdesc, (kt | kk) != 0);
+        umma_bf16<COLL_LASTUSE>(tmem, ah + o, bl + o, kIdesc, 1u);
         umma_bf16(tmem, al + o, bh + o, kIdesc, 1u);
       }
       umma_commit(empty(s));
@@ -369,13 +380,27 @@ template <int BKT> struct SymCfg {
 };
 constexpr uint32_t kIdesc128 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(SBN >> 3) << 17) |
                                ((uint32_t)(BM >> 4) << 24);
-// TMA warp, MMA warp and 8 epilogue warps: two per TMEM lane quadrant
-// (warp % 4), each converting half of the tile's columns, so that the
-// epilogue has two warps per scheduler to hide its latencies.
-constexpr int S_THREADS = 320;
+// TMA warp, MMA warp and 16 epilogue warps in four groups of four (one warp
+// per TMEM lane quadrant, warp % 4); group g converts columns 32g..32g+31 of
+// P and Q.  Four warps per scheduler hide the epilogue's TMEM, conversion
+// and store latencies (the epilogue does not overlap the main loop: one
+// tile per CTA).
+constexpr int EPI_GROUPS = 4;
+constexpr int EPI_COLS = SBN / EPI_GROUPS;  // 32 columns per group
+constexpr int S_THREADS = 64 + 128 * EPI_GROUPS;
 
-// Epilogue of the even/odd product, run by the 8 epilogue warps of a CTA
-// (warps 2-9): P and Q of this CTA's 128 rows from TMEM (columns 0-127 and
+DEV void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+DEV void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// Epilogue of the even/odd product, run by the 16 epilogue warps of a CTA
+// (warps 2-17): P and Q of this CTA's 128 rows from TMEM (columns 0-127 and
 // 128-255) become C[:, k] = P + Q and C[:, K-1-k] = P - Q, scaled, divided
 // by Lambda when the plan asks, and stored (staged in shared memory and
 // written by TMA when ep.tma_out, else by scattered stores).
@@ -384,15 +409,14 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
                       int lane) {
   const int KH = K >> 1;
   const int wq = warp & 3;
-  const int cbeg = ((warp - 2) >> 2) * (SBN / 2);  // this warp's half of the columns
+  const int grp = (warp - 2) >> 2;
+  const int cbeg = grp * EPI_COLS;  // this group's columns
   const int row = wq * 32 + lane;
   const int m = m0 + row;
   const bool mvalid = m < ep.m_total;
   const int b = mvalid ? m / ep.rows_per_batch : 0;
   const int r = mvalid ? m - b * ep.rows_per_batch : 0;
-  const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
-  if (ok) tc_fence_after();
-  grid_dep_launch();  // the next kernel may start its set-up while this tile drains
+  const uint32_t lanes = (uint32_t)(wq * 32) << 16;
   if (ep.tma_out) {
     // Tile staged in the idle operand ring (all MMAs have completed), then
     // written by TMA bulk-tensor stores.  The host enables this only when
@@ -401,34 +425,46 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
     const int R = ep.rows_per_batch;
     const int bb = m0 / R, r0 = m0 - bb * R;
     const int be = bb % ep.n_eig;
-    const bool go = ok && !*abort_flag;
-    {  // every epilogue thread runs the chunk loop (its named barriers), work only when go
-      const float alpha = (float)ep.alpha;
-      const bool scaled = ep.alpha != 1.0;
-      const int half = row & 1, rl = row >> 1;
-      const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
-#pragma unroll 1
-      for (int cc = 0; cc < SBN / 2; cc += 32) {
-        const int c0 = cbeg + cc;
-        const int grp = (warp - 2) >> 2;
-        // 1/Lambda of the chunk's 64 outputs, all loads in flight before use
-        float ivp[32], ivm[32];
-        if (go) {
-        if (ie) {
+    const float alpha = (float)ep.alpha;
+    const bool scaled = ep.alpha != 1.0;
+    const int half = row & 1, rl = row >> 1;
+    const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
+    // 1/Lambda while the main loop runs: the first 16 columns' values into
+    // registers, the next 16 columns' lines into L2
+    float ivp[16], ivm[16];
+    if (ie) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
+      for (int j = 0; j < 16; ++j) {
+        const int k = n0 + cbeg + j;
+        ivp[j] = __ldg(ie + (long long)k * R);
+        ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
+      }
+      const float* base = ie - row + wq * 32;  // the warp's first row
+      const int k = n0 + cbeg + 16 + (lane & 15);
+      prefetch_l2(base + (long long)((lane < 16) ? k : K - 1 - k) * R);
+    }
+    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+    if (ok) tc_fence_after();
+    grid_dep_launch();  // the next kernel may start its set-up while this tile drains
+    const bool go = ok && !*abort_flag;
+    if (go) {
+#pragma unroll 1
+      for (int sc = 0; sc < EPI_COLS; sc += 16) {
+        const int c0 = cbeg + sc;
+        if (ie && sc) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
             const int k = n0 + c0 + j;
             ivp[j] = __ldg(ie + (long long)k * R);
             ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
           }
         }
-        uint32_t vp[32], vq[32];
-        const uint32_t lanes = (uint32_t)(wq * 32) << 16;
-        tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
-        tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+        uint32_t vp[16], vq[16];
+        tmem_ld16(tmem + lanes + (uint32_t)c0, vp);
+        tmem_ld16(tmem + lanes + (uint32_t)(SBN + c0), vq);
         tmem_wait_ld();
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
+        for (int j = 0; j < 16; ++j) {
           const int kl = c0 + j;
           const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
           float xp = P + Q, xm = P - Q;
@@ -455,47 +491,49 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
             box[16384 + (127 - kl) * 128 + row] = xm;
           }
         }
-        }  // go
-        // the chunk's rows of every box are complete once the group's four
-        // warps (one per 32-row quadrant) pass: its first thread writes them
-        // (32-row sub-boxes) while the group converts the next chunk
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
-        if (go && lane == 0 && (warp & 3) == 2) {
-          const uint32_t sb = smem_u32(smem);
-          if (ep.mode == EPI_SPLIT) {
-            for (int which = 0; which < 2; ++which)
-              for (int hf = 0; hf < 2; ++hf)
-                for (int hl = 0; hl < 2; ++hl) {
-                  const int brow = which ? 96 - c0 : c0;  // first box row of the chunk
-                  const uint32_t src =
-                      sb + (uint32_t)((((which * 2 + hf) * 2 + hl) * 8192 + brow * 64) * 2);
-                  const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
-                  const int y = (which ? K - n0 - SBN : n0) + brow;
-                  tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
-                }
-          } else {
-            tma_store_3d(mO0, sb + (uint32_t)(c0 * 128 * 4), r0, n0 + c0, bb);
-            tma_store_3d(mO0, sb + (uint32_t)((16384 + (96 - c0) * 128) * 4), r0, K - n0 - SBN + 96 - c0, bb);
-          }
-          tma_store_commit();
-        }
       }
     }
-    if (go && lane == 0 && (warp & 3) == 2) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-  } else if (ok) {
-    if (!*abort_flag) {
+    // the group's 32 columns of every box are complete once its four warps
+    // (one per 32-row quadrant) pass: its first thread writes them
+    // (32-row sub-boxes) with TMA
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
+    if (go && lane == 0 && (warp & 3) == 2) {
+      const uint32_t sb = smem_u32(smem);
+      const int c0 = cbeg;
+      if (ep.mode == EPI_SPLIT) {
+        for (int which = 0; which < 2; ++which)
+          for (int hf = 0; hf < 2; ++hf)
+            for (int hl = 0; hl < 2; ++hl) {
+              const int brow = which ? 96 - c0 : c0;  // first box row of the group's columns
+              const uint32_t src = sb + (uint32_t)((((which * 2 + hf) * 2 + hl) * 8192 + brow * 64) * 2);
+              const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
+              const int y = (which ? K - n0 - SBN : n0) + brow;
+              tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
+            }
+      } else {
+        tma_store_3d(mO0, sb + (uint32_t)(c0 * 128 * 4), r0, n0 + c0, bb);
+        tma_store_3d(mO0, sb + (uint32_t)((16384 + (96 - c0) * 128) * 4), r0, K - n0 - SBN + 96 - c0, bb);
+      }
+      tma_store_commit();
+      // shared memory stays allocated until the stores have read it
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
+  } else {
+    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+    if (ok) tc_fence_after();
+    grid_dep_launch();
+    if (ok && !*abort_flag) {
 #pragma unroll 1
-      for (int cc = 0; cc < SBN / 2; cc += 32) {
-        const int c0 = cbeg + cc;
-        uint32_t vp[32], vq[32];
-        const uint32_t lanes = (uint32_t)(wq * 32) << 16;
-        tmem_ld32(tmem + lanes + (uint32_t)c0, vp);
-        tmem_ld32(tmem + lanes + (uint32_t)(SBN + c0), vq);
+      for (int sc = 0; sc < EPI_COLS; sc += 16) {
+        const int c0 = cbeg + sc;
+        uint32_t vp[16], vq[16];
+        tmem_ld16(tmem + lanes + (uint32_t)c0, vp);
+        tmem_ld16(tmem + lanes + (uint32_t)(SBN + c0), vq);
         tmem_wait_ld();
         if (mvalid) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
+          for (int j = 0; j < 16; ++j) {
             const int k = n0 + c0 + j;
             if (k < KH) {
               const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
@@ -595,8 +633,8 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
 #pragma unroll
       for (int kk = 0; kk < BKT / 16; ++kk) {
         const uint64_t o = (uint64_t)(kk * 32 >> 4);
-        umma_bf16(d, ah + o, bh + o, kIdesc128, !(first && kk == 0));
-        umma_bf16(d, ah + o, bl + o, kIdesc128, 1u);
+        umma_bf16<COLL_FILL>(d, ah + o, bh + o, kIdesc128, !(first && kk == 0));
+        umma_bf16<COLL_LASTUSE>(d, ah + o, bl + o, kIdesc128, 1u);
         umma_bf16(d, al + o, bh + o, kIdesc128, 1u);
       }
       umma_commit(empty(s));
@@ -722,8 +760,8 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
 #pragma unroll
         for (int kk = 0; kk < BK / 16; ++kk) {
           const uint64_t o = (uint64_t)(kk * 32 >> 4);
-          umma_bf16_pair(d, ah + o, bh + o, kIdescPair, !(first && kk == 0));
-          umma_bf16_pair(d, ah + o, bl + o, kIdescPair, 1u);
+          umma_bf16_pair<COLL_FILL>(d, ah + o, bh + o, kIdescPair, !(first && kk == 0));
+          umma_bf16_pair<COLL_LASTUSE>(d, ah + o, bl + o, kIdescPair, 1u);
           umma_bf16_pair(d, al + o, bh + o, kIdescPair, 1u);
         }
         umma_commit_pair(empty(s));

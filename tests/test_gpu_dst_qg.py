@@ -203,12 +203,56 @@ def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
 
 
 @pytest.mark.parametrize("method", ("wenoz5", "weno5"))
-def test_qg_step_fp32_packed_interior(cuda_ok, method):
-    # 320^2: interior tiles take the packed (f32x2) two-face WENO path, edge
-    # tiles the scalar one; both must sit within the FP32 bar of the oracle
+def test_qg_step_fp32_register_window_interior(cuda_ok, method):
+    # 320^2: interior tiles take the register-window WENO path (packed f32x2
+    # face pairs, u and v from psi differences), edge tiles the shared-memory
+    # one; both must sit within the FP32 bar of the oracle
     n = 320
     grid, q = qg_setup(n, torch.float32, 6)
     lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
     m = QGModel(grid, beta, lam, method=method, dtype=torch.float32)
     ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method)
     assert rel_err(host(m.step(dev(q, torch.float32), dt)), ref) < 1e-5
+
+
+def qg_setup_rect(ny, nx, seed, bc="periodic"):
+    L = 5.12e6
+    grid = fvx.ArakawaCGrid2D.from_interior(nx, ny, L * nx / 256, L * ny / 256)
+    q = np.zeros((ny + 2, nx + 2))
+    q[1:-1, 1:-1] = O.kminus3_field(ny, nx, seed, std=1e-5)
+    q = O.enforce_periodic(q) if bc == "periodic" else O.pad_interior_constant(q)
+    return grid, q
+
+
+# FP32 stage-kernel fallbacks, each against the FP64 oracle at the FP32-step
+# bar (1e-5 relative on q_{n+1}):
+#  - odd total width (Nx = 203): rows are not 8-byte aligned, so the tile
+#    loads fall back to 4-byte copies (and the DST to the FP64 chain);
+#  - wall boundaries (zero ghosts, no periodic refill);
+#  - forcing, bottom drag and viscosity: interior tiles leave the fast
+#    column-walk tendency for the general per-cell loop.
+@pytest.mark.parametrize("ny,nx,bc,method", [(256, 201, "periodic", "weno5"), (192, 201, "wall", "wenoz5"),
+                                             (256, 256, "wall", "weno5"), (320, 256, "wall", "weno7")])
+def test_qg_step_fp32_fallback_paths(cuda_ok, ny, nx, bc, method):
+    grid, q = qg_setup_rect(ny, nx, 8, bc)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * grid.dx
+    m = QGModel(grid, beta, lam, method=method, bc=bc, dtype=torch.float32)
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method, bc)
+    assert rel_err(host(m.step(dev(q, torch.float32), dt)), ref) < 1e-5
+    assert rel_err(host(m.step_unfused(dev(q, torch.float32), dt)), ref) < 1e-5
+
+
+@pytest.mark.parametrize("n,method", [(256, "weno5"), (320, "wenoz5"), (256, "upwind3")])
+def test_qg_step_fp32_forcing_drag_viscosity(cuda_ok, n, method):
+    grid, q = qg_setup(n, torch.float32, 9)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    forcing = np.zeros_like(q)
+    forcing[1:-1, 1:-1] = 1e-12 * O.kminus3_field(n, n, 10)
+    kw = dict(forcing=forcing, drag=1e-7, viscosity=50.0)
+    m = QGModel(grid, beta, lam, method=method, dtype=torch.float32, **kw)
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method, **kw)
+    got = host(m.step(dev(q, torch.float32), dt))
+    assert rel_err(got, ref) < 1e-5
+    # the extra terms change the step by far more than the bar
+    plain = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method)
+    assert rel_err(plain, ref) > 1e-4
