@@ -447,10 +447,12 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
     if (ok) tc_fence_after();
     grid_dep_launch();  // the next kernel may start its set-up while this tile drains
     const bool go = ok && !*abort_flag;
-    if (go) {
+    // 16 columns per step; each step's stores run while the group converts
+    // the next step's columns
 #pragma unroll 1
-      for (int sc = 0; sc < EPI_COLS; sc += 16) {
-        const int c0 = cbeg + sc;
+    for (int sc = 0; sc < EPI_COLS; sc += 16) {
+      const int c0 = cbeg + sc;
+      if (go) {
         if (ie && sc) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
@@ -492,33 +494,32 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
           }
         }
       }
-    }
-    // the group's 32 columns of every box are complete once its four warps
-    // (one per 32-row quadrant) pass: its first thread writes them
-    // (32-row sub-boxes) with TMA
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
-    if (go && lane == 0 && (warp & 3) == 2) {
-      const uint32_t sb = smem_u32(smem);
-      const int c0 = cbeg;
-      if (ep.mode == EPI_SPLIT) {
-        for (int which = 0; which < 2; ++which)
-          for (int hf = 0; hf < 2; ++hf)
-            for (int hl = 0; hl < 2; ++hl) {
-              const int brow = which ? 96 - c0 : c0;  // first box row of the group's columns
-              const uint32_t src = sb + (uint32_t)((((which * 2 + hf) * 2 + hl) * 8192 + brow * 64) * 2);
-              const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
-              const int y = (which ? K - n0 - SBN : n0) + brow;
-              tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
-            }
-      } else {
-        tma_store_3d(mO0, sb + (uint32_t)(c0 * 128 * 4), r0, n0 + c0, bb);
-        tma_store_3d(mO0, sb + (uint32_t)((16384 + (96 - c0) * 128) * 4), r0, K - n0 - SBN + 96 - c0, bb);
+      // the step's 16 columns of every box are complete once the group's
+      // four warps (one per 32-row quadrant) pass: its first thread writes
+      // them (16-row sub-boxes) with TMA
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
+      if (go && lane == 0 && (warp & 3) == 2) {
+        const uint32_t sb = smem_u32(smem);
+        if (ep.mode == EPI_SPLIT) {
+          for (int which = 0; which < 2; ++which)
+            for (int hf = 0; hf < 2; ++hf)
+              for (int hl = 0; hl < 2; ++hl) {
+                const int brow = which ? 112 - c0 : c0;  // first box row of the step's columns
+                const uint32_t src = sb + (uint32_t)((((which * 2 + hf) * 2 + hl) * 8192 + brow * 64) * 2);
+                const int x = (hf ? (R >> 1) : 0) + (r0 >> 1);
+                const int y = (which ? K - n0 - SBN : n0) + brow;
+                tma_store_3d(hl ? mO1 : mO0, src, x, y, bb);
+              }
+        } else {
+          tma_store_3d(mO0, sb + (uint32_t)(c0 * 128 * 4), r0, n0 + c0, bb);
+          tma_store_3d(mO0, sb + (uint32_t)((16384 + (112 - c0) * 128) * 4), r0, K - n0 - SBN + 112 - c0, bb);
+        }
+        tma_store_commit();
       }
-      tma_store_commit();
-      // shared memory stays allocated until the stores have read it
-      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
     }
+    // shared memory stays allocated until the stores have read it
+    if (go && lane == 0 && (warp & 3) == 2) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
   } else {
     const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
     if (ok) tc_fence_after();
@@ -996,7 +997,7 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
     return false;
   cuuint64_t dims[3] = {R, N, B};
   cuuint64_t strides[2] = {(cuuint64_t)ld * es, (cuuint64_t)(B > 1 ? bs : ld * (long long)N) * es};
-  cuuint32_t box[3] = {box_r, 32, 1};  // one 32-column chunk of the epilogue tile
+  cuuint32_t box[3] = {box_r, 16, 1};  // one 16-column step of an epilogue group
   cuuint32_t estr[3] = {1, 1, 1};
   return enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, base, dims, strides,
              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,

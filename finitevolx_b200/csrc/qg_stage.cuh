@@ -138,8 +138,21 @@ DEV float2 f2mul(float2 a, float2 b) {
 }
 DEV float2 f2s(float c) { return make_float2(c, c); }
 
-// WENO5 / WENO-Z5 (weno5<float, Z> in recon.cuh, same formulas and order)
-// on two stencils at once; divisions stay scalar (__fdividef per lane).
+// WENO5 / WENO-Z5 (weno5<float, Z> in recon.cuh, the same formulas) on two
+// stencils at once.  WENO5 normalises with one reciprocal per lane (the
+// common-denominator weights of weno5_core), WENO-Z5 with four; stencils
+// whose WENO5 products overflow go through the scalar four-division form.
+__noinline__ DEV float2 weno5_js_x2_fallback(float2 qi1, float2 qi2, float2 qi3, float2 b1, float2 b2, float2 b3) {
+  const float e = 1e-8f;
+  float r[2];
+  for (int l = 0; l < 2; ++l) {
+    const float w1 = fdiv(0.1f, sq((l ? b1.y : b1.x) + e)), w2 = fdiv(0.6f, sq((l ? b2.y : b2.x) + e)),
+                w3 = fdiv(0.3f, sq((l ? b3.y : b3.x) + e));
+    r[l] = fdiv(w1 * (l ? qi1.y : qi1.x) + w2 * (l ? qi2.y : qi2.x) + w3 * (l ? qi3.y : qi3.x), w1 + w2 + w3);
+  }
+  return make_float2(r[0], r[1]);
+}
+DEV float2 f2rcp(float2 a) { return make_float2(rcp_approx(a.x), rcp_approx(a.y)); }
 template <bool Z>
 DEV float2 weno5_x2(float2 qmm, float2 qm, float2 q0, float2 qp, float2 qpp) {
   const float2 qi1 = f2fma(f2s(11.f / 6.f), q0, f2fma(f2s(-7.f / 6.f), qm, f2mul(f2s(1.f / 3.f), qmm)));
@@ -155,28 +168,29 @@ DEV float2 weno5_x2(float2 qmm, float2 qm, float2 q0, float2 qp, float2 qpp) {
   const float2 a3 = f2add(f2fma(f2s(-2.f), qp, q0), qpp);
   const float2 c3 = f2add(f2fma(f2s(-4.f), qp, f2mul(f2s(3.f), q0)), qpp);
   const float2 b3 = f2fma(k2, f2mul(c3, c3), f2mul(k1, f2mul(a3, a3)));
-  float2 w1, w2, w3;
   if (Z) {
     const float2 eps = f2s(1e-16f);
     const float2 tau = make_float2(fabsf(b1.x - b3.x), fabsf(b1.y - b3.y));
-    const float2 d1 = f2add(b1, eps), d2 = f2add(b2, eps), d3 = f2add(b3, eps);
-    const float2 r1 = make_float2(__fdividef(tau.x, d1.x), __fdividef(tau.y, d1.y));
-    const float2 r2 = make_float2(__fdividef(tau.x, d2.x), __fdividef(tau.y, d2.y));
-    const float2 r3 = make_float2(__fdividef(tau.x, d3.x), __fdividef(tau.y, d3.y));
-    w1 = f2mul(f2s(0.1f), f2add(f2s(1.f), r1));
-    w2 = f2mul(f2s(0.6f), f2add(f2s(1.f), r2));
-    w3 = f2mul(f2s(0.3f), f2add(f2s(1.f), r3));
+    const float2 r1 = f2mul(tau, f2rcp(f2add(b1, eps)));
+    const float2 r2 = f2mul(tau, f2rcp(f2add(b2, eps)));
+    const float2 r3 = f2mul(tau, f2rcp(f2add(b3, eps)));
+    const float2 w1 = f2mul(f2s(0.1f), f2add(f2s(1.f), r1));
+    const float2 w2 = f2mul(f2s(0.6f), f2add(f2s(1.f), r2));
+    const float2 w3 = f2mul(f2s(0.3f), f2add(f2s(1.f), r3));
+    const float2 num = f2fma(w3, qi3, f2fma(w2, qi2, f2mul(w1, qi1)));
+    return f2mul(num, f2rcp(f2add(f2add(w1, w2), w3)));
   } else {
     const float2 eps = f2s(1e-8f);
     const float2 d1 = f2add(b1, eps), d2 = f2add(b2, eps), d3 = f2add(b3, eps);
     const float2 s1 = f2mul(d1, d1), s2 = f2mul(d2, d2), s3 = f2mul(d3, d3);
-    w1 = make_float2(__fdividef(0.1f, s1.x), __fdividef(0.1f, s1.y));
-    w2 = make_float2(__fdividef(0.6f, s2.x), __fdividef(0.6f, s2.y));
-    w3 = make_float2(__fdividef(0.3f, s3.x), __fdividef(0.3f, s3.y));
+    const float2 W1 = f2mul(f2s(0.1f), f2mul(s2, s3)), W2 = f2mul(f2s(0.6f), f2mul(s1, s3));
+    const float2 W3 = f2mul(f2s(0.3f), f2mul(s1, s2));
+    const float2 num = f2fma(W3, qi3, f2fma(W2, qi2, f2mul(W1, qi1)));
+    const float2 den = f2add(f2add(W1, W2), W3);
+    const float2 r = f2mul(num, f2rcp(den));
+    if (den.x < 3e38f && den.y < 3e38f && fabsf(r.x) < 3.4e38f && fabsf(r.y) < 3.4e38f) return r;
+    return weno5_js_x2_fallback(qi1, qi2, qi3, b1, b2, b3);
   }
-  const float2 num = f2fma(w3, qi3, f2fma(w2, qi2, f2mul(w1, qi1)));
-  const float2 den = f2add(f2add(w1, w2), w3);
-  return make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
 }
 
 // IN: the tile and its halo lie inside the interior and every face is at

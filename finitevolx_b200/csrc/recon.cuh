@@ -18,13 +18,21 @@
 namespace fvx {
 
 template <typename T> DEV T sq(T x) { return x * x; }
+// FP32 reciprocal by the hardware approximation (rcp.approx.ftz.f32, at
+// most 1 ulp): +inf for 0, 0 for |b| > 2^126 (the result would be
+// subnormal and is flushed).
+DEV float rcp_approx(float b) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(b));
+  return r;
+}
 // Division in the reconstruction formulas: exact IEEE division in FP64 (the
-// correctness path tracks the reference's operation order), the fast
-// reciprocal form in FP32 (<= 2 ulp; its 2^126 < |b| < 2^128 corner maps to
-// the weights an FP32 reference overflows on anyway).
+// correctness path tracks the reference's operation order), a times the
+// approximate reciprocal of b in FP32 (<= 2 ulp; its 2^126 < |b| < 2^128
+// corner maps to the weights an FP32 reference overflows on anyway).
 template <typename T> DEV T fdiv(T a, T b) {
   if constexpr (sizeof(T) == 8) return a / b;
-  else return __fdividef(a, b);
+  else return a * rcp_approx(b);
 }
 template <typename T> DEV T tabs(T x) { return x < T(0) ? -x : x; }
 template <typename T> DEV T tmax(T a, T b) { return a > b ? a : b; }
@@ -63,6 +71,18 @@ DEV T weno5_core(T qi1, T qi2, T qi3, T b1, T b2, T b3) {
     return fdiv(w1 * qi1 + w2 * qi2 + w3 * qi3, w1 + w2 + w3);
   } else {
     const T eps = T(1e-8);
+    if constexpr (sizeof(T) == 4) {
+      // FP32: the weights d_k / s_k (s_k = (b_k + eps)^2) times s1 s2 s3,
+      // d_k prod_{j != k} s_j, give the same normalised combination with one
+      // reciprocal instead of four.  s_k >= 1e-16, so no product underflows;
+      // the few stencils whose products overflow (|q| jumps above ~1e4) take
+      // the four-division form.
+      const float s1 = sq(b1 + eps), s2 = sq(b2 + eps), s3 = sq(b3 + eps);
+      const float W1 = 0.1f * (s2 * s3), W2 = 0.6f * (s1 * s3), W3 = 0.3f * (s1 * s2);
+      const float den = W1 + W2 + W3;
+      const float r = (W1 * qi1 + W2 * qi2 + W3 * qi3) * rcp_approx(den);
+      if (den < 3e38f && fabsf(r) < 3.4e38f) return r;
+    }
     T w1 = fdiv(T(0.1), sq(b1 + eps));
     T w2 = fdiv(T(0.6), sq(b2 + eps));
     T w3 = fdiv(T(0.3), sq(b3 + eps));
