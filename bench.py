@@ -66,6 +66,7 @@ def parse():
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed QG steps (for ncu launch lists); no extra sections")
     ap.add_argument("--ens-steps", type=int, default=100)
+    ap.add_argument("--stage-tile", default=None, help="fix the stage tile (e.g. 64x32) instead of autotuning")
     return ap.parse_args()
 
 
@@ -370,8 +371,11 @@ def main():
     # autotuned launch choices (stage tile shape; fused or separate DST split)
     from finitevolx_b200 import autotune
     tuned = {}
+    if args.stage_tile:
+        autotune.set_stage_tile(args.method, torch.float32, autotune._TILES.index(args.stage_tile))
+        tuned["stage_tile"] = args.stage_tile
     if not args.profile:
-        tuned = {"stage_tile": autotune.tune_qg_stage(model, qa, dt)["tile"],
+        tuned = {"stage_tile": tuned.get("stage_tile") or autotune.tune_qg_stage(model, qa, dt)["tile"],
                  "fused_split": autotune.tune_qg_split(model, qa, dt)["fused"],
                  "dst_kernel": autotune.tune_dst_kernel(model, qa, dt)["kernel"]}
     qa.copy_(q0)
