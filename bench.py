@@ -251,7 +251,9 @@ def helmholtz_section(n, pairs, reps=5):
                        "FP64 iterate/dots/residual, rtol 1e-8", "levels": mg.n_levels}
     out["mg_pcg"] = timed(dict(precond="mg", graph=True))
     t0 = time.time()
-    pc = LearnedPreconditioner(mg, n_pre=4, n_post=4, batch_max=64, seed=0)
+    # the MG baseline's smoothing (6 pre, 6 post) on the fine levels: the
+    # fastest of 2, 3, 4 and 6 at this workload (2: 18 it, 3: 14, 4: 11, 6: 9)
+    pc = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=64, seed=0)
     F, E = generate_pairs(mg, pc.lvl, pairs, pc.n_pre, seed=1)
     torch.cuda.synchronize()
     t_gen = time.time() - t0
@@ -262,7 +264,7 @@ def helmholtz_section(n, pairs, reps=5):
                        "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "level": pc.lvl}
     del F, E
     out["learned_pcg"] = timed(dict(precond=pc, flexible=True, graph=True, max_iter=500))
-    pc0 = LearnedPreconditioner(mg, n_pre=4, n_post=4, batch_max=1, coarse=False, scale=False)
+    pc0 = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=1, coarse=False, scale=False)
     out["same_cycle_without_network"] = timed(dict(precond=pc0, flexible=True, graph=True, max_iter=500))
     out["speedup_learned_vs_mg"] = out["mg_pcg"]["ms"] / out["learned_pcg"]["ms"]
     return out

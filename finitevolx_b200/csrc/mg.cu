@@ -21,7 +21,7 @@
 namespace fvx {
 namespace mg {
 
-constexpr int kCoarseCells = 128 * 128;
+constexpr int kCoarseCells = 32 * 32;
 constexpr int kCoarseThreads = 1024;
 
 template <typename T>
@@ -84,16 +84,14 @@ DEV T apply_at(const Lev<T>& L, const T* u, int j, int i) {
 }
 
 template <typename T>
-DEV void jacobi_at(const Lev<T>& L, const T* u, const T* f, T* out, T omega, size_t c) {
-  const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+DEV void jacobi_at(const Lev<T>& L, const T* u, const T* f, T* out, T omega, int j, int i, size_t c) {
   const T r = f[c] - apply_at(L, u, j, i);
   out[c] = (u[c] + omega * L.inv[c] * r) * L.mask[c];
 }
 
 // coarse cell (J, I): r = (f - A u) * m on the 4 fine cells, mask-weighted mean
 template <typename T>
-DEV void restrict_at(const Lev<T>& F, const T* u, const T* f, const Lev<T>& C, T* fc, size_t cc) {
-  const int J = (int)(cc / C.nx), I = (int)(cc - (size_t)J * C.nx);
+DEV void restrict_at(const Lev<T>& F, const T* u, const T* f, const Lev<T>& C, T* fc, int J, int I, size_t cc) {
   T s[4], m[4];
   const int dj[4] = {0, 1, 0, 1}, di[4] = {0, 0, 1, 1};
 #pragma unroll
@@ -112,8 +110,7 @@ DEV void restrict_at(const Lev<T>& F, const T* u, const T* f, const Lev<T>& C, T
 
 // fine cell: u = (u + P e_c) * m_f, P the mask-normalised 9/3/3/1 bilinear form
 template <typename T>
-DEV void prolong_at(const Lev<T>& F, T* u, const Lev<T>& C, const T* ec, size_t c) {
-  const int j = (int)(c / F.nx), i = (int)(c - (size_t)j * F.nx);
+DEV void prolong_at(const Lev<T>& F, T* u, const Lev<T>& C, const T* ec, int j, int i, size_t c) {
   const int J = j >> 1, I = i >> 1, dj = j & 1, di = i & 1;
   const int sj = 2 * dj - 1, si = 2 * di - 1;
   auto V = [&](int jj, int ii) -> T {
@@ -134,20 +131,26 @@ DEV void prolong_at(const Lev<T>& F, T* u, const Lev<T>& C, const T* ec, size_t 
 template <typename T>
 __global__ void jacobi_kernel(Lev<T> L, const T* u, const T* f, T* out, T omega) {
   const size_t n = (size_t)L.ny * L.nx;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-    jacobi_at(L, u, f, out, omega, c);
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+    jacobi_at(L, u, f, out, omega, j, i, c);
+  }
 }
 template <typename T>
 __global__ void restrict_kernel(Lev<T> F, const T* u, const T* f, Lev<T> C, T* fc) {
   const size_t n = (size_t)C.ny * C.nx;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-    restrict_at(F, u, f, C, fc, c);
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int J = (int)(c / C.nx), I = (int)(c - (size_t)J * C.nx);
+    restrict_at(F, u, f, C, fc, J, I, c);
+  }
 }
 template <typename T>
 __global__ void prolong_kernel(Lev<T> F, T* u, Lev<T> C, const T* ec) {
   const size_t n = (size_t)F.ny * F.nx;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x)
-    prolong_at(F, u, C, ec, c);
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+    const int j = (int)(c / F.nx), i = (int)(c - (size_t)j * F.nx);
+    prolong_at(F, u, C, ec, j, i, c);
+  }
 }
 template <typename T>
 __global__ void apply_kernel(Lev<T> L, const T* u, T* out) {
@@ -173,18 +176,34 @@ struct LevArray {
   Lev<T> L[kMaxLevels];
 };
 
+// fnc(j, i, c) on this thread's cells c = tid, tid + kCoarseThreads, ... of
+// an ny x nx level (row j, column i), the indices advanced without divisions.
+template <typename F>
+DEV void coarse_cells(int ny, int nx, F&& fnc) {
+  const int cells = ny * nx;
+  const int dq = kCoarseThreads / nx, dr = kCoarseThreads - dq * nx;
+  int j = (int)threadIdx.x / nx, i = (int)threadIdx.x - j * nx;
+  for (int c = threadIdx.x; c < cells; c += kCoarseThreads) {
+    fnc(j, i, (size_t)c);
+    i += dr;
+    j += dq;
+    if (i >= nx) { i -= nx; ++j; }
+  }
+}
+
 // Whole coarse part of a V-cycle in one CTA: levels lc .. nl-1, entered with
 // f[lc] set and u[lc] = 0 (the recursion's zero initial guess).  S is the
-// level table in shared memory.
+// level table in shared memory; each level's entry is copied to registers
+// before its loops (its fields are read at every cell).
 template <typename T>
 DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
   const int tid = threadIdx.x;
-  auto sweeps = [&](const Lev<T>& L, int n) {
+  auto sweeps = [&](const Lev<T> L, int n) {
     const size_t cells = (size_t)L.ny * L.nx;
     T* a = L.u;
     T* b = L.tmp;
     for (int s = 0; s < n; ++s) {
-      for (size_t c = tid; c < cells; c += kCoarseThreads) jacobi_at(L, a, L.f, b, omega, c);
+      coarse_cells(L.ny, L.nx, [&](int j, int i, size_t c) { jacobi_at(L, a, L.f, b, omega, j, i, c); });
       __syncthreads();
       T* t = a; a = b; b = t;
     }
@@ -194,22 +213,22 @@ DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, in
     }
   };
   for (int l = lc; l < nl; ++l) {
-    const Lev<T>& L = S[l];
+    const Lev<T> L = S[l];
     const size_t cells = (size_t)L.ny * L.nx;
     for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = T(0);
     __syncthreads();
     if (l == nl - 1) { sweeps(L, n_coarse); break; }
     sweeps(L, n_pre);
-    const Lev<T>& C = S[l + 1];
+    const Lev<T> C = S[l + 1];
     const size_t cc = (size_t)C.ny * C.nx;
-    for (size_t c = tid; c < cc; c += kCoarseThreads) restrict_at(L, L.u, L.f, C, C.f, c);
+    coarse_cells(C.ny, C.nx, [&](int J, int I, size_t c) { restrict_at(L, L.u, L.f, C, C.f, J, I, c); });
     __syncthreads();
   }
   for (int l = nl - 2; l >= lc; --l) {
-    const Lev<T>& L = S[l];
-    const Lev<T>& C = S[l + 1];
+    const Lev<T> L = S[l];
+    const Lev<T> C = S[l + 1];
     const size_t cells = (size_t)L.ny * L.nx;
-    for (size_t c = tid; c < cells; c += kCoarseThreads) prolong_at(L, L.u, C, C.u, c);
+    coarse_cells(L.ny, L.nx, [&](int j, int i, size_t c) { prolong_at(L, L.u, C, C.u, j, i, c); });
     __syncthreads();
     sweeps(L, n_post);
   }
@@ -253,10 +272,7 @@ coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post
   for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) ub[c] = T(0);
   __syncthreads();
   for (int k = 0; k < n_cycles; ++k) {
-    for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) {
-      const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
-      L.f[c] = (fb[c] - apply_at(L, ub, j, i)) * L.mask[c];
-    }
+    coarse_cells(L.ny, L.nx, [&](int j, int i, size_t c) { L.f[c] = (fb[c] - apply_at(L, ub, j, i)) * L.mask[c]; });
     __syncthreads();
     coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
     for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) ub[c] += L.u[c];
@@ -352,6 +368,21 @@ DEV T res_s(const T* u, const T* f, const T* m, const T* cx, const T* cy, int k,
   return (f[k] - (lap - lam * um) * mc) * mc;
 }
 
+// fnc(ly, lx) on the cells of the w x h region with corner (s, s) that this
+// thread owns (region index tid, tid + blockDim.x, ...), the indices
+// advanced without divisions.
+template <typename F>
+DEV void leg_region(int s, int w, int h, F&& fnc) {
+  const int n = w * h, dq = (int)blockDim.x / w, dr = (int)blockDim.x - dq * w;
+  int j = (int)threadIdx.x / w, i = (int)threadIdx.x - j * w;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) {
+    fnc(s + j, s + i);
+    i += dr;
+    j += dq;
+    if (i >= w) { i -= w; ++j; }
+  }
+}
+
 template <typename T>
 static size_t leg_smem(int k) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
@@ -359,6 +390,54 @@ static size_t leg_smem(int k) {
   const size_t RN = (size_t)(TX + 2 * H) * (TY + 2 * H);
   const size_t CN = (size_t)((TX + 2 * H) / 2 + 3) * ((TY + 2 * H) / 2 + 3);
   return (7 * RN + 2 * CN) * sizeof(T);
+}
+
+// Shared-memory tile (origin (y0, x0), RW wide, RN cells) of the level's
+// mask, cx, cy and inv_diag, zero outside the level.
+template <typename T>
+DEV void leg_load_tile(const Lev<T>& L, int x0, int y0, int RW, int RN, T* sm, T* scx, T* scy, T* sinv) {
+  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
+    T v[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      const int ly = q / RW, lx = q - ly * RW;
+      const int gy = y0 + ly, gx = x0 + lx;
+      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+      v[u][0] = in ? L.mask[c] : T(0);
+      v[u][1] = in ? L.cx[c] : T(0);
+      v[u][2] = in ? L.cy[c] : T(0);
+      v[u][3] = in ? L.inv[c] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      if (q < RN) { sm[q] = v[u][0]; scx[q] = v[u][1]; scy[q] = v[u][2]; sinv[q] = v[u][3]; }
+    }
+  }
+}
+// The same tile of two level arrays a and b (b may be null: zeros).
+template <typename T>
+DEV void leg_load_pair(const Lev<T>& L, int x0, int y0, int RW, int RN, const T* a, T* sa_, const T* b, T* sb_) {
+  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
+    T v[4][2];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      const int ly = q / RW, lx = q - ly * RW;
+      const int gy = y0 + ly, gx = x0 + lx;
+      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
+      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
+      v[u][0] = in ? a[c] : T(0);
+      v[u][1] = (in && b) ? b[c] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int q = q0 + u * blockDim.x;
+      if (q < RN) { sa_[q] = v[u][0]; sb_[q] = v[u][1]; }
+    }
+  }
 }
 
 // L.u (tile) <- k sweeps; C.f <- restricted residual.  Halo k + 1.
@@ -377,41 +456,21 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
   T* sa = sinv + RN;
   T* sb = sa + RN;
   const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
-  // batches of 4 cells per thread: all 24 loads in flight before any store
-  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
-    T v[4][6];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      const int ly = q / RW, lx = q - ly * RW;
-      const int gy = y0 + ly, gx = x0 + lx;
-      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-      v[u][0] = in ? f[c] : T(0);
-      v[u][1] = in ? L.mask[c] : T(0);
-      v[u][2] = in ? L.cx[c] : T(0);
-      v[u][3] = in ? L.cy[c] : T(0);
-      v[u][4] = in ? L.inv[c] : T(0);
-      v[u][5] = (in && u_init) ? u_init[c] : T(0);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      if (q < RN) {
-        sf[q] = v[u][0]; sm[q] = v[u][1]; scx[q] = v[u][2]; scy[q] = v[u][3]; sinv[q] = v[u][4]; sa[q] = v[u][5];
-      }
-    }
-  }
+  // the level's constant arrays, then (after the previous kernel, which
+  // wrote f and u_init) f and u_init; batches of 4 cells per thread, all
+  // loads of a batch in flight before any store
+  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv);
+  grid_dep_wait();
+  leg_load_pair(L, x0, y0, RW, RN, f, sf, u_init, sa);
   __syncthreads();
+  grid_dep_launch();  // the next kernel may start loading its constants
   T* a = sa;
   T* b = sb;
   for (int s = 1; s <= k; ++s) {
-    const int w = RW - 2 * s, h = RH - 2 * s;
-    for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
-      const int ly = s + q / w, lx = s + q % w;
+    leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
       const int kk = ly * RW + lx;
       b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
-    }
+    });
     __syncthreads();
     T* t = a; a = b; b = t;
   }
@@ -466,6 +525,10 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
   const int CX0 = (x0 >> 1) - 1, CY0 = (y0 >> 1) - 1;
   const int CW = ((x0 + RW - 1) >> 1) + 1 - CX0 + 1, CH = ((y0 + RH - 1) >> 1) + 1 - CY0 + 1;
   T* scm = sv + CW * CH;  // coarse mask
+  // constants first; the coarse correction ec, f and u_pre come from the
+  // kernels before this one
+  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv);
+  grid_dep_wait();
   for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
     const int J = CY0 + q / CW, I = CX0 + q % CW;
     const bool in = J >= 0 && J < C.ny && I >= 0 && I < C.nx;
@@ -474,32 +537,11 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
     sv[q] = in ? ec[c] * cm : T(0);
     scm[q] = cm;
   }
+  leg_load_pair(L, x0, y0, RW, RN, f, sf, u_pre, sa);
   __syncthreads();
-  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
-    T v[4][6];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int q = q0 + t * blockDim.x;
-      const int ly = q / RW, lx = q - ly * RW;
-      const int gy = y0 + ly, gx = x0 + lx;
-      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-      v[t][0] = in ? f[c] : T(0);
-      v[t][1] = in ? L.mask[c] : T(0);
-      v[t][2] = in ? L.cx[c] : T(0);
-      v[t][3] = in ? L.cy[c] : T(0);
-      v[t][4] = in ? L.inv[c] : T(0);
-      v[t][5] = in ? u_pre[c] : T(0);
-    }
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int q = q0 + t * blockDim.x;
-      if (q < RN) { sf[q] = v[t][0]; sm[q] = v[t][1]; scx[q] = v[t][2]; scy[q] = v[t][3]; sinv[q] = v[t][4]; sa[q] = v[t][5]; }
-    }
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < RN; q += blockDim.x) {
-    const int ly = q / RW, lx = q - ly * RW;
+  grid_dep_launch();
+  leg_region(0, RW, RH, [&](int ly, int lx) {
+    const int q = ly * RW + lx;
     const int gy = y0 + ly, gx = x0 + lx;
     const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
     const T mf = sm[q];
@@ -514,17 +556,15 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
       u = (sa[q] + e) * mf;
     }
     sb[q] = u;
-  }
+  });
   __syncthreads();
   T* a = sb;  // u_pre + P e
   T* b = sa;
   for (int s = 1; s <= k; ++s) {
-    const int w = RW - 2 * s, h = RH - 2 * s;
-    for (int q = threadIdx.x; q < w * h; q += blockDim.x) {
-      const int ly = s + q / w, lx = s + q % w;
+    leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
       const int kk = ly * RW + lx;
       b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
-    }
+    });
     __syncthreads();
     T* t = a; a = b; b = t;
   }
@@ -748,6 +788,14 @@ static int leg_attr() {
   return FVX_OK;
 }
 
+// The single-CTA coarse V-cycle from level l.
+template <typename T>
+static int coarse_vcycle(fvx_mg* g, int l, cudaStream_t st) {
+  coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(levs<T>(g), l, g->nl, g->n_pre, g->n_post, g->n_coarse,
+                                                        (T)g->omega);
+  return fvx_cuda_status();
+}
+
 // Downward leg at host-driven level l: L.u <- k sweeps on f from u_init
 // (NULL = 0), level l+1's f <- the restricted residual.
 template <typename T>
@@ -759,7 +807,11 @@ static int leg_down(fvx_mg* g, int l, const T* f, const T* u_init, int k, cudaSt
   Lev<T>& L = A.L[l];
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  down_leg_kernel<T><<<gr, 256, leg_smem<T>(k), st>>>(L, f, u_init, k, (T)g->omega, A.L[l + 1]);
+  // programmatic launch: the constant tiles load while the kernel before
+  // finishes (the kernel waits before reading f and u_init)
+  if (fvx_launch_pdl(down_leg_kernel<T>, gr, dim3(256), leg_smem<T>(k), st, L, f, u_init, k, (T)g->omega,
+                     A.L[l + 1]) != cudaSuccess)
+    return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 
@@ -773,7 +825,9 @@ static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cuda
   Lev<T>& L = A.L[l];
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  up_leg_kernel<T><<<gr, 256, leg_smem<T>(k), st>>>(L, f, L.u, A.L[l + 1], ec, k, (T)g->omega, out);
+  if (fvx_launch_pdl(up_leg_kernel<T>, gr, dim3(256), leg_smem<T>(k), st, L, f, (const T*)L.u, A.L[l + 1],
+                     (const T*)ec, k, (T)g->omega, out) != cudaSuccess)
+    return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 
@@ -785,9 +839,8 @@ static int vcycle_levels(fvx_mg* g, int l, T** result, cudaStream_t st) {
   LevArray<T>& A = levs<T>(g);
   const T om = (T)g->omega;
   if (l >= g->lc) {
-    coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, l, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
     *result = A.L[l].u;
-    return fvx_cuda_status();
+    return coarse_vcycle<T>(g, l, st);
   }
   Lev<T>& L = A.L[l];
   int rc = leg_down<T>(g, l, L.f, nullptr, g->n_pre, st);
@@ -819,7 +872,8 @@ static int vcycle0(fvx_mg* g, const T* u_in, const T* f, T* u_out, cudaStream_t 
   }
   if (g->lc == 0 && !u_in) {  // whole cycle fits the single-CTA kernel
     copy_kernel<T><<<gr, 256, 0, st>>>(L.f, f, n);
-    coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(A, 0, g->nl, g->n_pre, g->n_post, g->n_coarse, om);
+    int rc = coarse_vcycle<T>(g, 0, st);
+    if (rc) return rc;
     copy_kernel<T><<<gr, 256, 0, st>>>(u_out, L.u, n);
     return fvx_cuda_status();
   }

@@ -45,6 +45,8 @@ __host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
 // input channel staged in shared memory by one cooperative load (one
 // barrier), each thread accumulating CPT output channels of one pixel.
 // Small tiles give enough blocks for single-field inference on coarse grids.
+// Launched as a programmatic dependent of the previous layer (inference), a
+// block stages the weights before waiting for that layer's output.
 template <int COUT, int CPT, int T>
 __global__ void __launch_bounds__(T * T * (COUT / CPT))
 conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
@@ -72,6 +74,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
     for (int u = 0; u < 8; ++u)
       if (k0 + u * NT < nw) ws[k0 + u * NT] = v[u];
   }
+  grid_dep_wait();  // the input (and skip) come from the previous kernel
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
   const int nt = cin * TW * TW;
@@ -89,6 +92,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
       if (k0 + u * NT < nt) tile[k0 + u * NT] = v[u];
   }
   __syncthreads();
+  grid_dep_launch();
   const int p = tid % (T * T), co0 = (tid / (T * T)) * CPT;
   const int ty = p / T, tx = p % T;
   float acc[CPT];
@@ -121,7 +125,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
 template <int COUT, int CPT, int T>
 static int launch_conv_tile(const float* in, int mode, int batch, int cin, const __nv_bfloat16* wb,
                             const float* bias, const float* skip, float* out, int h, int w, int relu,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool pdl) {
   constexpr int NT = T * T * (COUT / CPT);
   const size_t smem = ((size_t)cin * 9 * COUT + (size_t)cin * (T + 2) * (T + 2)) * sizeof(float);
   static bool attr_set = false;  // per instantiation; the largest use needs > 48 KB
@@ -133,7 +137,13 @@ static int launch_conv_tile(const float* in, int mode, int batch, int cin, const
     attr_set = true;
   }
   dim3 g((w + T - 1) / T, (h + T - 1) / T, batch);
-  conv_tile_kernel<COUT, CPT, T><<<g, NT, smem, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu);
+  if (pdl) {
+    if (fvx_launch_pdl(conv_tile_kernel<COUT, CPT, T>, g, dim3(NT), smem, st, in, mode, cin, wb, bias, skip, out, h,
+                       w, relu) != cudaSuccess)
+      return FVX_ERR_CUDA;
+  } else {
+    conv_tile_kernel<COUT, CPT, T><<<g, NT, smem, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu);
+  }
   return fvx_cuda_status();
 }
 
@@ -313,12 +323,14 @@ static int blocks_for(size_t n) {
 using namespace fvx;
 using namespace fvx::nn;
 
-extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
-                               const float* skip, float* out, int cout, int h, int w, int relu, void* stream) {
+// One conv layer; pdl: launched as a programmatic dependent of the kernel
+// before it, which must not have written the weights or biases (the kernel
+// reads them before waiting for it).
+static int conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
+                    const float* skip, float* out, int cout, int h, int w, int relu, cudaStream_t st, bool pdl) {
   if (!in || !w_bf16 || !bias || !out) return FVX_ERR_ARG;
   if (cin < 1 || cin > CMAX || batch < 1 || h < 1 || w < 1 || mode < 0 || mode > 2) return FVX_ERR_SHAPE;
   if ((mode == IN_UP) && ((h % 2) || (w % 2))) return FVX_ERR_SHAPE;
-  cudaStream_t st = fvx_stream(stream);
   const __nv_bfloat16* wb = (const __nv_bfloat16*)w_bf16;
   // 8 x 8 tiles with 4 or 8 output channels per thread while that gives at
   // least one block per SM; else 4 x 4 tiles with 1 or 2 channels per
@@ -326,16 +338,21 @@ extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, co
   const bool big = (size_t)((h + 7) / 8) * ((w + 7) / 8) * batch >= 148;
   switch (cout) {
     case 1:
-      return big ? launch_conv_tile<1, 1, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
-                 : launch_conv_tile<1, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
+      return big ? launch_conv_tile<1, 1, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
+                 : launch_conv_tile<1, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
     case 16:
-      return big ? launch_conv_tile<16, 4, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
-                 : launch_conv_tile<16, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
+      return big ? launch_conv_tile<16, 4, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
+                 : launch_conv_tile<16, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
     case 32:
-      return big ? launch_conv_tile<32, 8, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
-                 : launch_conv_tile<32, 2, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
+      return big ? launch_conv_tile<32, 8, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
+                 : launch_conv_tile<32, 2, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
     default: return FVX_ERR_SHAPE;
   }
+}
+
+extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
+                               const float* skip, float* out, int cout, int h, int w, int relu, void* stream) {
+  return conv_fwd(in, mode, batch, cin, w_bf16, bias, skip, out, cout, h, w, relu, fvx_stream(stream), false);
 }
 
 // Backward of one conv layer (wb: the BF16 weights of the forward pass).
@@ -620,14 +637,16 @@ extern "C" int fvx_unet_sync_params(fvx_unet* n, void* stream) {
   return fvx_nn_to_bf16(n->wf, n->wb, (int)n->n_params, stream);
 }
 
-static int unet_forward(fvx_unet* n, int batch, cudaStream_t st) {
+// pdl: each layer launched as a programmatic dependent of the kernel before
+// it (inference only: no kernel between the layers writes the weights).
+static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = false) {
   size_t off = 0;
   for (const LayerDef& L : kNet) {
     const int hh = n->h >> L.div, ww = n->w >> L.div;
     const __nv_bfloat16* W = n->wb + off;
     const float* wf_b = n->wf + off + (size_t)L.cout * L.cin * 9;  // biases stay FP32
-    int rc = fvx_nn_conv_fwd(n->act[L.in], L.mode, batch, L.cin, W, wf_b, L.skip >= 0 ? n->act[L.skip] : nullptr,
-                             n->act[L.out], L.cout, hh, ww, L.relu, st);
+    int rc = conv_fwd(n->act[L.in], L.mode, batch, L.cin, W, wf_b, L.skip >= 0 ? n->act[L.skip] : nullptr,
+                      n->act[L.out], L.cout, hh, ww, L.relu, st, pdl);
     if (rc) return rc;
     off += layer_params(L);
   }
@@ -714,7 +733,7 @@ extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) 
   const size_t plane = (size_t)n->h * n->w;
   rms_kernel<<<kRmsBlocks, 256, 0, st>>>((const float*)f, n->mask, plane, n->rms_part, n->rms_ticket, n->scale);
   prep_kernel<<<blocks_for(plane), 256, 0, st>>>((const float*)f, n->scale, n->act[0], plane);
-  int rc = unet_forward(n, 1, st);
+  int rc = unet_forward(n, 1, st, true);
   if (rc) return rc;
   finish_kernel<<<blocks_for(plane), 256, 0, st>>>(n->act[8], n->scale, n->mask, n->sigma, (float*)u, plane);
   return fvx_cuda_status();

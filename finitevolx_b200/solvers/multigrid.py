@@ -4,8 +4,8 @@ Mirrors finitevolX solvers/multigrid.py (build_multigrid_solver :905-1062,
 MultigridSolver :601-897) and make_multigrid_preconditioner
 (solvers/preconditioners.py:207-244).  The level hierarchy is built once in
 FP64 inside libfvx.so (the reference builds it offline in NumPy); V-cycles
-run on the device: one launch per sweep on the fine levels, one single-CTA
-launch for every level at or below 128 x 128.
+run on the device: one launch per leg (all of its sweeps plus the transfer)
+on the fine levels, one single-CTA launch for every level at or below 32 x 32.
 """
 
 from __future__ import annotations
