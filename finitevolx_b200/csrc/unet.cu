@@ -60,35 +60,35 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const int b = blockIdx.z;
   const int x0 = blockIdx.x * T, y0 = blockIdx.y * T;
   const int tid = threadIdx.x;
-  // staging in batches of 8 per thread so the loads overlap
+  // staging in batches of 16 per thread so the loads overlap
   const int nw = cin * 9 * COUT;
-  for (int k0 = tid; k0 < nw; k0 += 8 * NT) {
-    float v[8];
+  for (int k0 = tid; k0 < nw; k0 += 16 * NT) {
+    float v[16];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int k = k0 + u * NT;
       const int co = k % COUT, rest = k / COUT;
       v[u] = k < nw ? __bfloat162float(wb[(size_t)co * cin * 9 + rest]) : 0.f;
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
+    for (int u = 0; u < 16; ++u)
       if (k0 + u * NT < nw) ws[k0 + u * NT] = v[u];
   }
   grid_dep_wait();  // the input (and skip) come from the previous kernel
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
   const int nt = cin * TW * TW;
-  for (int k0 = tid; k0 < nt; k0 += 4 * NT) {
-    float v[4];
+  for (int k0 = tid; k0 < nt; k0 += 16 * NT) {
+    float v[16];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int k = k0 + u * NT;
       const int ci = k / (TW * TW), r = k - ci * (TW * TW);
       const int ly = r / TW, lx = r - ly * TW;
       v[u] = k < nt ? in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int u = 0; u < 16; ++u)
       if (k0 + u * NT < nt) tile[k0 + u * NT] = v[u];
   }
   __syncthreads();
@@ -464,17 +464,16 @@ static size_t total_params() {
   return n;
 }
 
+constexpr int kRmsThreads = 1024;
 // s = sqrt(sum(f^2 m) / max(sum m, 1)), stored as [s, 1/s] (1/s = 0 when
-// s = 0).  Each block writes its partial sums; the last block to finish
-// (counted with an atomic ticket after a fence) adds them in block order
-// and resets the ticket, so the result is deterministic.
-constexpr int kRmsBlocks = 64;
-__global__ void rms_kernel(const float* f, const float* mask, size_t n, double* part, unsigned* ticket,
-                           float* scale) {
-  __shared__ double sh[2][32];
-  __shared__ bool last;
+// s = 0), by one block (the coarse level has tens of thousands of cells):
+// FP64 partial sums per thread, then a fixed-order tree, so the result is
+// deterministic.
+__global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const float* mask, size_t n,
+                                                          float* scale) {
+  __shared__ double sh[2][kRmsThreads / 32];
   double a = 0.0, c = 0.0;
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+  for (size_t k = threadIdx.x; k < n; k += kRmsThreads) {
     const double m = mask[k];
     a += (double)f[k] * f[k] * m;
     c += m;
@@ -485,26 +484,18 @@ __global__ void rms_kernel(const float* f, const float* mask, size_t n, double* 
   }
   if ((threadIdx.x & 31) == 0) { sh[0][threadIdx.x >> 5] = a; sh[1][threadIdx.x >> 5] = c; }
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double A = 0.0, C = 0.0;
-    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { A += sh[0][k]; C += sh[1][k]; }
-    part[2 * blockIdx.x] = A;
-    part[2 * blockIdx.x + 1] = C;
-    __threadfence();
-    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last && threadIdx.x == 0) {
-    __threadfence();
-    double A = 0.0, C = 0.0;
-    for (int k = 0; k < (int)gridDim.x; ++k) {
-      A += ((volatile double*)part)[2 * k];
-      C += ((volatile double*)part)[2 * k + 1];
+  if (threadIdx.x < 32) {
+    a = sh[0][threadIdx.x];
+    c = sh[1][threadIdx.x];
+    for (int o = 16; o; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
     }
-    const double s = sqrt(A / (C > 1.0 ? C : 1.0));
-    scale[0] = (float)s;
-    scale[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
-    *ticket = 0u;
+    if (threadIdx.x == 0) {
+      const double s = sqrt(a / (c > 1.0 ? c : 1.0));
+      scale[0] = (float)s;
+      scale[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
+    }
   }
 }
 
@@ -538,8 +529,6 @@ struct fvx_unet {
   // inference on one field: level mask, scale [s, 1/s], output scale sigma
   float* mask = nullptr;
   float* scale = nullptr;
-  double* rms_part = nullptr;
-  unsigned* rms_ticket = nullptr;
   float sigma = 1.f;
   std::vector<void*> allocs;
 };
@@ -596,8 +585,6 @@ extern "C" int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out) {
   n->loss = (double*)alloc(8);
   n->mask = (float*)alloc((size_t)h * w * 4);
   n->scale = (float*)alloc(16);
-  n->rms_part = (double*)alloc(2 * kRmsBlocks * sizeof(double));
-  n->rms_ticket = (unsigned*)alloc(sizeof(unsigned));
   if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
     unet_free(n);
     delete n;
@@ -731,7 +718,7 @@ extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) 
   if (!n || !f || !u) return FVX_ERR_ARG;
   cudaStream_t st = fvx_stream(stream);
   const size_t plane = (size_t)n->h * n->w;
-  rms_kernel<<<kRmsBlocks, 256, 0, st>>>((const float*)f, n->mask, plane, n->rms_part, n->rms_ticket, n->scale);
+  rms_kernel<<<1, kRmsThreads, 0, st>>>((const float*)f, n->mask, plane, n->scale);
   prep_kernel<<<blocks_for(plane), 256, 0, st>>>((const float*)f, n->scale, n->act[0], plane);
   int rc = unet_forward(n, 1, st, true);
   if (rc) return rc;
