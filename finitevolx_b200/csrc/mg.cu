@@ -334,6 +334,7 @@ constexpr int kOmegaBlocks = 64;
 // every cell is jacobi_at / restrict_at / prolong_at's, in the same order.
 // ---------------------------------------------------------------------------
 constexpr int kLegMaxSweeps = 16;
+constexpr int kLegFewTiles = 148;  // legs with fewer tiles run 1024-thread CTAs
 
 template <typename T> struct LegTile;
 template <> struct LegTile<float> { static constexpr int TX = 64, TY = 32; };
@@ -441,8 +442,10 @@ DEV void leg_load_pair(const Lev<T>& L, int x0, int y0, int RW, int RN, const T*
 }
 
 // L.u (tile) <- k sweeps; C.f <- restricted residual.  Halo k + 1.
-template <typename T>
-__global__ void __launch_bounds__(256)
+// NT threads: 256 on the fine levels (two CTAs per SM), 1024 on levels with
+// fewer tiles than SMs, where one CTA's sweeps are the whole leg's latency.
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT)
 down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init, int k, T omega, Lev<T> C) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   const int H = k + 1;
@@ -503,8 +506,8 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
 }
 
 // out (tile) <- k sweeps from u_pre + P ec.  Halo k.
-template <typename T>
-__global__ void __launch_bounds__(256)
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT)
 up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Lev<T> C, const T* __restrict__ ec,
               int k, T omega, T* __restrict__ out) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
@@ -779,9 +782,14 @@ static int leg_attr() {
   static bool done = false;
   if (!done) {
     const int bytes = (int)leg_smem<T>(kLegMaxSweeps);
-    if (cudaFuncSetAttribute(down_leg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+    if (cudaFuncSetAttribute(down_leg_kernel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
             cudaSuccess ||
-        cudaFuncSetAttribute(up_leg_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+        cudaFuncSetAttribute(up_leg_kernel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(down_leg_kernel<T, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(up_leg_kernel<T, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
+            cudaSuccess)
       return FVX_ERR_CUDA;
     done = true;
   }
@@ -809,9 +817,13 @@ static int leg_down(fvx_mg* g, int l, const T* f, const T* u_init, int k, cudaSt
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
   // programmatic launch: the constant tiles load while the kernel before
   // finishes (the kernel waits before reading f and u_init)
-  if (fvx_launch_pdl(down_leg_kernel<T>, gr, dim3(256), leg_smem<T>(k), st, L, f, u_init, k, (T)g->omega,
-                     A.L[l + 1]) != cudaSuccess)
-    return FVX_ERR_CUDA;
+  const bool few = (size_t)gr.x * gr.y < (size_t)kLegFewTiles;
+  const cudaError_t e =
+      few ? fvx_launch_pdl(down_leg_kernel<T, 1024>, gr, dim3(1024), leg_smem<T>(k), st, L, f, u_init, k,
+                           (T)g->omega, A.L[l + 1])
+          : fvx_launch_pdl(down_leg_kernel<T, 256>, gr, dim3(256), leg_smem<T>(k), st, L, f, u_init, k,
+                           (T)g->omega, A.L[l + 1]);
+  if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 
@@ -825,9 +837,13 @@ static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cuda
   Lev<T>& L = A.L[l];
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  if (fvx_launch_pdl(up_leg_kernel<T>, gr, dim3(256), leg_smem<T>(k), st, L, f, (const T*)L.u, A.L[l + 1],
-                     (const T*)ec, k, (T)g->omega, out) != cudaSuccess)
-    return FVX_ERR_CUDA;
+  const bool few = (size_t)gr.x * gr.y < (size_t)kLegFewTiles;
+  const cudaError_t e =
+      few ? fvx_launch_pdl(up_leg_kernel<T, 1024>, gr, dim3(1024), leg_smem<T>(k), st, L, f, (const T*)L.u,
+                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out)
+          : fvx_launch_pdl(up_leg_kernel<T, 256>, gr, dim3(256), leg_smem<T>(k), st, L, f, (const T*)L.u,
+                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out);
+  if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 
