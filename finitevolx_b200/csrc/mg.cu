@@ -12,7 +12,7 @@
 // Device layout per level: mask, cx, cy, inv_diag, u, f, tmp (T = float or
 // double, row-major [ny, nx]).  Levels at or below kCoarseCells cells run
 // inside one CTA (one launch for the whole coarse part of the V-cycle);
-// finer levels use one launch per sweep / transfer.
+// finer levels use one launch per leg (all of its sweeps and the transfer).
 #include "fvx_common.cuh"
 
 #include <cmath>
