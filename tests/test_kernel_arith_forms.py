@@ -1,0 +1,95 @@
+"""CPU checks of arithmetic reformulations the CUDA kernels rely on (NumPy
+emulation of the kernels' FP32 formulas and index walks; the GPU parity
+tests check the kernels themselves against the oracle).
+
+* FP32 WENO5 (Jiang-Shu) weights normalised with one reciprocal: the
+  weights d_k / s_k times s_1 s_2 s_3 give the same reconstruction as the
+  four-division form (csrc/recon.cuh weno5_core, csrc/qg_stage.cuh
+  weno5_x2), and stencils whose products overflow are the ones the kernels
+  send to the four-division fallback.
+* Division-free (row, column) walks of the multigrid kernels (csrc/mg.cu
+  coarse_cells, leg_region): the same cells as c -> (c / w, c % w).
+"""
+
+import numpy as np
+import pytest
+
+F = np.float32
+
+
+def _smoothness(qmm, qm, q0, qp, qpp):
+    k1, k2 = F(13.0 / 12.0), F(0.25)
+    b1 = k1 * (qmm - F(2) * qm + q0) ** 2 + k2 * (qmm - F(4) * qm + F(3) * q0) ** 2
+    b2 = k1 * (qm - F(2) * q0 + qp) ** 2 + k2 * (qm - qp) ** 2
+    b3 = k1 * (q0 - F(2) * qp + qpp) ** 2 + k2 * (F(3) * q0 - F(4) * qp + qpp) ** 2
+    qi1 = F(1.0 / 3.0) * qmm - F(7.0 / 6.0) * qm + F(11.0 / 6.0) * q0
+    qi2 = F(-1.0 / 6.0) * qm + F(5.0 / 6.0) * q0 + F(1.0 / 3.0) * qp
+    qi3 = F(1.0 / 3.0) * q0 + F(5.0 / 6.0) * qp - F(1.0 / 6.0) * qpp
+    return (b1, b2, b3), (qi1, qi2, qi3)
+
+
+def weno5_four_divisions(b, qi):
+    eps = F(1e-8)
+    w = [F(d) / (bk + eps) ** 2 for d, bk in zip((0.1, 0.6, 0.3), b)]
+    return (w[0] * qi[0] + w[1] * qi[1] + w[2] * qi[2]) / (w[0] + w[1] + w[2])
+
+
+def weno5_one_reciprocal(b, qi):
+    """The kernels' form; returns (value, takes_fallback)."""
+    eps = F(1e-8)
+    s1, s2, s3 = ((bk + eps) ** 2 for bk in b)
+    with np.errstate(over="ignore", invalid="ignore"):
+        W1, W2, W3 = F(0.1) * (s2 * s3), F(0.6) * (s1 * s3), F(0.3) * (s1 * s2)
+        den = W1 + W2 + W3
+        r = (W1 * qi[0] + W2 * qi[1] + W3 * qi[2]) * (F(1) / den)
+        ok = (den < F(3e38)) & (np.abs(r) < F(3.4e38))
+    return r, ~ok
+
+
+@pytest.mark.parametrize("scale", [1e-5, 1.0, 1e3])
+def test_weno5_one_reciprocal_matches_four_divisions(scale):
+    rng = np.random.default_rng(7)
+    q = (rng.standard_normal((5, 200000)) * scale).astype(F)
+    b, qi = _smoothness(*q)
+    ref = weno5_four_divisions(b, qi)
+    got, fb = weno5_one_reciprocal(b, qi)
+    assert not fb.any()
+    # the reconstruction is a convex combination of qi: bound the difference
+    # by a few FP32 ulps of the largest candidate
+    mag = np.maximum.reduce([np.abs(x) for x in qi]) + np.float32(1e-30)
+    assert np.max(np.abs(got - ref) / mag) < 8 * np.finfo(F).eps
+
+
+def test_weno5_overflowing_products_take_the_fallback():
+    # jumps of 1e5 make s ~ 1e20 and the products overflow: the kernels'
+    # test routes exactly these stencils to the four-division form, which
+    # stays finite
+    q = np.array([[0.0], [0.0], [1e5], [0.0], [0.0]], dtype=F)
+    b, qi = _smoothness(*q)
+    _, fb = weno5_one_reciprocal(b, qi)
+    assert fb.all()
+    assert np.isfinite(weno5_four_divisions(b, qi)).all()
+
+
+def _walk(n_cells, w, nthreads, tid):
+    """(j, i) sequence of csrc/mg.cu's division-free walk for one thread."""
+    dq, dr = nthreads // w, nthreads % w
+    j, i = tid // w, tid % w
+    out = []
+    for _ in range(tid, n_cells, nthreads):
+        out.append((j, i))
+        i += dr
+        j += dq
+        if i >= w:
+            i -= w
+            j += 1
+    return out
+
+
+@pytest.mark.parametrize("h,w,nthreads", [(32, 32, 1024), (16, 16, 1024), (8, 8, 1024), (46, 78, 256),
+                                          (44, 76, 1024), (3, 2000, 256), (5, 1, 1024), (30, 37, 256)])
+def test_division_free_walk_visits_the_same_cells(h, w, nthreads):
+    n = h * w
+    for tid in range(nthreads):
+        ref = [divmod(c, w) for c in range(tid, n, nthreads)]
+        assert _walk(n, w, nthreads, tid) == ref
