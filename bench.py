@@ -17,16 +17,24 @@ field (std 1e-5 s^-1), synthetic.
   memory, steps it and downloads q_{n+1}, all inside the timed region; the
   upload of state k+1 and the download of state k-1 overlap the step of
   state k on separate streams.
+* parity: the GPU step from the bench's initial state against the FP64
+  oracle's step (relative max-norm error on q_{n+1}; the FP32 bar is 1e-5).
 * roofline: the dominant kernel is the tcgen05 DST GEMM (one of the four
   products per solve); achieved = algorithmic 2*M*N*K flops per launch /
   its device time per launch (per_launch_ms), vs the measured bf16 peak.
-* cpu_baseline: the FP64 NumPy oracle's QG step on this host.
-* --impl reference: the reference's CPU implementation of the path
-  (finitevolX's JAX stack is not installable here; the oracle port restates
-  it) on the same config, one bounded sample per step.
+* cpu_baseline and --impl reference: the FP64 oracle (NumPy/SciPy
+  restatement of the reference's path; finitevolX's JAX stack cannot be
+  installed offline) on all host threads (oracle/threaded.py, bit-identical
+  to the single-threaded oracle), at the same 2048^2 size.
+* extra sections (N = 1): the metric's own configuration (256^2, FP64),
+  the stencil throughput sweep, the batched split-precision DST with FP64
+  refinement, the masked Helmholtz learned-PCG vs MG-PCG comparison and the
+  ensemble of uneven members.
 
 Multi-GPU (--gpus N under torchrun): the single-field step does not shard;
 each rank runs an independent replica ("replicas only"), value sums ranks.
+The ensemble shards by members (each rank its own members, no collective
+in the step) and reports the whole-job rate.
 """
 
 from __future__ import annotations
@@ -53,16 +61,20 @@ UNIT = "Mcell-steps/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
-    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--method", default="weno5")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-helmholtz", action="store_true")
-    ap.add_argument("--helm-n", type=int, default=1024)
     ap.add_argument("--helm-pairs", type=int, default=20000)
+    ap.add_argument("--helm-reps", type=int, default=20)
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-dst", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--dst-rhs", type=int, default=64)
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed QG steps (for ncu launch lists); no extra sections")
     ap.add_argument("--ens-steps", type=int, default=100)
@@ -71,10 +83,11 @@ def parse():
 
 
 def config(n, method):
-    return {"workload": f"qg1.5_rk3ssp_{method}_dst_{n}x{n}_fp32", "interior": [n, n], "scheme": method,
-            "helmholtz": "DST-I dense GEMMs, 3xBF16 split, FP32 accumulate", "bc": "periodic q, Dirichlet psi",
-            "lambda": 1.0 / LD ** 2, "beta": BETA, "dt": 0.5 * LX / n, "l2": "flushed (256 MiB write) before every step",
-            "parallelism": "replicas"}
+    """The workload (identical for both arms); how each arm computes it is
+    in the line's dtype and notes."""
+    return {"workload": f"qg1.5_rk3ssp_{method}_dst_{n}x{n}", "interior": [n, n], "scheme": method,
+            "bc": "periodic q, Dirichlet psi", "lambda": 1.0 / LD ** 2, "beta": BETA, "dt": 0.5 * LX / n,
+            "l2": "flushed (256 MiB write) before every step", "parallelism": "replicas"}
 
 
 def initial_q(n, seed=0):
@@ -143,177 +156,65 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline(n, method):
-    """One FP64 oracle QG step at the full size on this host (single core)."""
-    import numpy as np
-    import oracle.fvx_oracle as O
-    q = initial_q(n)
+def _oracle_steps(n, method, steps, q=None):
+    """`steps` FP64 oracle steps at n^2 on all host threads; (q_after_first, seconds per step list, cores)."""
+    from oracle.threaded import host_threads, qg_step_threaded
+    q = initial_q(n) if q is None else q
     dx = LX / n
-    t = time.perf_counter()
-    O.qg_step(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, method)
-    t = time.perf_counter() - t
-    return {"value": n * n / t / 1e6, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"1 rk3_ssp_step at {n}x{n}, FP64 NumPy/SciPy oracle (restatement of the reference "
-                      f"math; finitevolX's JAX stack is not installable offline), {t:.1f} s"}
+    cores = host_threads()
+    first, times = None, []
+    for _ in range(steps):
+        t = time.perf_counter()
+        q = qg_step_threaded(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, method, workers=cores)
+        times.append(time.perf_counter() - t)
+        if first is None:
+            first = q
+    return first, times, cores
+
+
+def cpu_baseline(n, method, steps=3):
+    """A bounded sample of the same workload on the host: `steps` FP64 oracle
+    steps at the full size on all host threads.  Also returns the oracle's
+    first step for the parity check."""
+    first, times, cores = _oracle_steps(n, method, steps)
+    t = sum(times)
+    return {"value": n * n * steps / t / 1e6, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} rk3_ssp_steps at {n}x{n} from the bench's initial state, FP64 NumPy/SciPy oracle "
+                      f"(restatement of the reference math; finitevolX's JAX stack is not installable offline), "
+                      f"{cores} host threads (row bands + SciPy FFT workers), {t:.1f} s"}, first
 
 
 def run_reference(args, rank):
-    """Reference arm: the oracle port of the reference's CPU path, all host threads."""
+    """Reference arm: the oracle port of the reference's CPU path at the
+    labelled size, all host threads; every warm-up and timed step is a full
+    step.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return
-    import numpy as np
-    import scipy.fft
-    import oracle.fvx_oracle as O
-    # bounded per-step sample (same physics, smaller interior) so K + W steps stay within minutes
-    ns = min(args.n, 512 if args.steps + args.warmup <= 200 else 256)
-    q = initial_q(ns)
-    dx = LX / ns
-    cores = os.cpu_count() or 1
+    from oracle.threaded import host_threads, qg_step_threaded
+    n = args.n
+    q = initial_q(n)
+    dx = LX / n
+    cores = host_threads()
     times = []
-    with scipy.fft.set_workers(cores):
-        for k in range(args.warmup + args.steps):
-            t = time.perf_counter()
-            q = O.qg_step(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, args.method)
-            t = time.perf_counter() - t
-            if k >= args.warmup:
-                times.append(t)
+    for k in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        q = qg_step_threaded(q, dx, dx, BETA, 1.0 / LD ** 2, 0.5 * dx, args.method, workers=cores)
+        t = time.perf_counter() - t
+        if k >= args.warmup:
+            times.append(t)
     tot = sum(times)
-    val = ns * ns * len(times) / tot / 1e6
+    val = n * n * len(times) / tot / 1e6
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config(args.n, args.method),
+        "config": config(n, args.method),
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"per step: 1 rk3_ssp_step at {ns}x{ns} (FP64 NumPy oracle port of the "
-                                   "reference path; SciPy FFT on all host threads)"},
+                         "sample": f"per step: 1 rk3_ssp_step at {n}x{n} (FP64 NumPy/SciPy oracle port of the "
+                                   f"reference path, oracle/threaded.py: row bands on {cores} threads, SciPy FFT "
+                                   f"workers = {cores})"},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
-
-
-def masked_basin(n, seed=0):
-    """Masked-Helmholtz workload: Gaussian-filtered (sigma = 20 cells) seeded
-    field thresholded at 30% land, largest connected ocean kept, closed
-    boundary ring; c = exp(0.5 g) with g a second smooth field (unit std);
-    white-noise right-hand side on the ocean."""
-    import numpy as np
-    from scipy import ndimage
-    rng = np.random.default_rng(seed)
-    g = ndimage.gaussian_filter(rng.standard_normal((n, n)), sigma=20, mode="wrap")
-    m = g > np.quantile(g, 0.3)
-    lab, k = ndimage.label(m)
-    if k > 1:
-        sizes = ndimage.sum(m, lab, range(1, k + 1))
-        m = lab == (1 + int(np.argmax(sizes)))
-    m[0, :] = m[-1, :] = m[:, 0] = m[:, -1] = False
-    g2 = ndimage.gaussian_filter(rng.standard_normal((n, n)), sigma=20, mode="wrap")
-    c = np.exp(0.5 * g2 / g2.std())
-    f = rng.standard_normal((n, n)) * m
-    return m.astype(np.float64), c, f
-
-
-def helmholtz_section(n, pairs, reps=5):
-    """Masked variable-coefficient Helmholtz, time to 1e-8 relative residual
-    (FP64-checked): MG-PCG (one V-cycle per iteration, the reference's
-    6/6/50 sweeps) against flexible PCG with the learned coarse solver
-    (U-Net at the 128^2 level, 4+4 fine sweeps, energy-scaled correction)
-    and the same cycle without the network.  Each solve is timed with CUDA
-    events around the whole call (set-up, iterations, final FP64 check);
-    median of ``reps``; the network is trained once beforehand (not timed)."""
-    import numpy as np
-    import torch
-
-    import finitevolx_b200 as fvx
-    from finitevolx_b200.learned import LearnedPreconditioner, generate_pairs
-
-    m, c, f = masked_basin(n, 1)
-    dx = LX / n
-    mg = fvx.build_multigrid_solver(m, dx, dx, lambda_=1.0 / LD ** 2, coeff=c, dtype=torch.float32)
-    pcg = fvx.MaskedHelmholtzPCG(mg)
-    b = torch.from_numpy(f).float().cuda()
-
-    def timed(kw):
-        pcg.solve(b, rtol=1e-8, **kw)
-        ts, info = [], None
-        for _ in range(reps):
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            x, info = pcg.solve(b, rtol=1e-8, **kw)
-            e1.record()
-            e1.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        return {"ms": statistics.median(ts), "iterations": info["iterations"],
-                "rel_residual_fp64": info["rel_residual"], "converged": info["converged"]}
-
-    out = {"workload": f"masked Helmholtz {n}^2, Ld {LD / 1e3:.0f} km, variable c, FP32 work vectors, "
-                       "FP64 iterate/dots/residual, rtol 1e-8", "levels": mg.n_levels}
-    out["mg_pcg"] = timed(dict(precond="mg", graph=True))
-    t0 = time.time()
-    # the MG baseline's smoothing (6 pre, 6 post) on the fine levels: the
-    # fastest of 2, 3, 4 and 6 at this workload (2: 18 it, 3: 14, 4: 11, 6: 9)
-    pc = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=64, seed=0)
-    F, E = generate_pairs(mg, pc.lvl, pairs, pc.n_pre, seed=1)
-    torch.cuda.synchronize()
-    t_gen = time.time() - t0
-    t0 = time.time()
-    hist = pc.train(F, E, epochs=6, batch=64, lr=2e-3, seed=1)
-    torch.cuda.synchronize()
-    out["training"] = {"pairs": pairs, "epochs": 6, "batch": 64, "gen_s": t_gen, "train_s": time.time() - t0,
-                       "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "level": pc.lvl}
-    del F, E
-    out["learned_pcg"] = timed(dict(precond=pc, flexible=True, graph=True, max_iter=500))
-    pc0 = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=1, coarse=False, scale=False)
-    out["same_cycle_without_network"] = timed(dict(precond=pc0, flexible=True, graph=True, max_iter=500))
-    out["speedup_learned_vs_mg"] = out["mg_pcg"]["ms"] / out["learned_pcg"]["ms"]
-    return out
-
-
-def ensemble_members(count=64, seed=0):
-    """Config-2 ensemble: sizes drawn (seeded) from {128, 256, 512, 1024}^2,
-    1-3 layers (H = 400/1100/2600 m)."""
-    import numpy as np
-    rng = np.random.default_rng(seed)
-    sizes = rng.choice([128, 256, 512, 1024], size=count)
-    nls = rng.integers(1, 4, size=count)
-    return list(zip(sizes.tolist(), nls.tolist()))
-
-
-def ensemble_section(members, n_steps, rank=0):
-    """All members advanced n_steps RK3-SSP steps by one CUDA graph (per RK
-    stage: one batched DST chain per grid size, one persistent work-queue
-    launch of the fused stage over every tile of every layer).  Metric:
-    interior layer-cells x steps / s."""
-    import torch
-
-    import finitevolx_b200 as fvx
-
-    ens = fvx.QGEnsemble(members)
-    for m, (n, nl) in enumerate(members):
-        g = torch.Generator(device="cuda").manual_seed(1000 * rank + m)
-        for k in range(nl):
-            q = torch.zeros((n + 2, n + 2), device="cuda")
-            q[1:-1, 1:-1] = torch.randn((n, n), device="cuda", generator=g) * 1e-5
-            ens.set_layer(m, k, q)
-    from finitevolx_b200 import autotune
-    tuned = autotune.tune_ensemble(ens)
-    g = ens.capture(n_steps)
-    g.replay()  # warm-up run of the graph
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    g.replay()
-    e1.record()
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
-    cells = ens.cells_per_step()
-    return {"workload": f"{len(members)} multi-layer QG members, sizes {{128,256,512,1024}}^2, 1-3 layers, "
-                        f"WENO5, FP32, {n_steps} RK3 steps in one CUDA graph",
-            "members": len(members), "layer_cells_per_step": cells, "steps": n_steps, "ms": ms,
-            "ms_per_step": ms / n_steps, "value": cells * n_steps / (ms * 1e-3) / 1e6, "unit": "Mcell-steps/s",
-            "launches_per_step": ens.launches_per_step, "autotuned_blocks_per_sm": tuned["blocks_per_sm"]}
 
 
 def per_launch_ms(launch, flush, reps: int = 20, rounds: int = 5) -> float:
@@ -343,6 +244,387 @@ def per_launch_ms(launch, flush, reps: int = 20, rounds: int = 5) -> float:
     return statistics.median(est)
 
 
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def _graph_steps(model, qa, qb, dt, steps, warmup, flush):
+    """Device ms of `steps` graph-replayed steps (L2 flushed before each),
+    launches per step."""
+    import torch
+    for _ in range(max(warmup, 3)):
+        model.step(qa, dt, out=qb)
+        qa.copy_(qb)
+    model.step(qa, dt, out=qb)
+    torch.cuda.synchronize()
+    graphs = []
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        for src, dst in ((qb, qa), (qa, qb)):
+            g = torch.cuda.CUDAGraph()
+            l0 = model.kernel_launches
+            with torch.cuda.graph(g, stream=s):
+                model.step(src, dt, out=dst, presplit=model.dtype == torch.float32)
+            per_step = model.kernel_launches - l0
+            graphs.append(g)
+    torch.cuda.current_stream().wait_stream(s)
+    for g in graphs:
+        g.replay()
+    torch.cuda.synchronize()
+    return graphs, per_step
+
+
+def _time_graphs(graphs, steps, flush):
+    import torch
+    total = 0.0
+    for k in range(steps):
+        flush.fill_(float(k))
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        graphs[k % 2].replay()
+        e1.record()
+        e1.synchronize()
+        total += e0.elapsed_time(e1)
+    return total
+
+
+def fp64_metric_section(method, steps, flush, n=256):
+    """The metric's own configuration: 256^2 interior, FP64 state, DST by the
+    FP64 chain; K graph-replayed steps (L2 flushed before each), parity vs
+    the FP64 oracle after one step (bar 1e-12), and the oracle on the host
+    at the same size."""
+    import numpy as np
+    import torch
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200.qg import QGModel
+    grid = fvx.ArakawaCGrid2D.from_interior(n, n, LX, LX)
+    dt = 0.5 * grid.dx
+    model = QGModel(grid, BETA, 1.0 / LD ** 2, method=method, dtype=torch.float64)
+    q0 = initial_q(n, seed=7)
+    qd = torch.as_tensor(q0, device="cuda")
+    got = model.step(qd, dt).cpu().numpy()
+    ref, times, cores = _oracle_steps(n, method, 3, q=q0)
+    err = float(np.abs(got - ref).max() / np.abs(ref).max())
+    qa, qb = qd.clone(), torch.empty_like(qd)
+    graphs, per_step = _graph_steps(model, qa, qb, dt, steps, 3, flush)
+    ms = _time_graphs(graphs, steps, flush)
+    return {"workload": f"qg1.5_rk3ssp_{method}_dst_{n}x{n}", "dtype": "f64", "steps": steps,
+            "ms_per_step": ms / steps, "value": n * n * steps / (ms * 1e-3) / 1e6, "unit": UNIT,
+            "launches_per_step": per_step, "dst": "FP64 SIMT transform-matrix chain",
+            "parity": {"rel_err_vs_fp64_oracle": err, "bar": 1e-12},
+            "cpu_oracle": {"value": n * n * len(times) / sum(times) / 1e6, "unit": UNIT, "cores": cores}}
+
+
+def _kminus3_torch(ny, nx, gen, count=1, dtype=None):
+    """Seeded k^-3 Gaussian fields on the device (unit std), [count, ny, nx]."""
+    import torch
+    w = torch.randn((count, ny, nx), generator=gen, device="cuda", dtype=torch.float64)
+    ky = torch.fft.fftfreq(ny, device="cuda", dtype=torch.float64)[:, None]
+    kx = torch.fft.rfftfreq(nx, device="cuda", dtype=torch.float64)[None, :]
+    k = torch.sqrt(kx ** 2 + ky ** 2)
+    k[0, 0] = float("inf")
+    f = torch.fft.irfft2(torch.fft.rfft2(w) * k ** -1.5, s=(ny, nx))
+    f = f - f.mean(dim=(-2, -1), keepdim=True)
+    f = f / f.std(dim=(-2, -1), keepdim=True)
+    return f if dtype is None else f.to(dtype)
+
+
+def stencil_sweep_section(flush, sizes=(512, 2048, 4096)):
+    """Config 1: single-field stencil throughput, FP32 and FP64, periodic
+    ghost ring, seeded k^-3 tracer and divergence-free C-grid (u, v) from a
+    random streamfunction.  Per operator: the library's fused kernel and the
+    unfused form (the reference's sequence of array passes: face fluxes then
+    their divergence; two Laplacian passes then the scale), device time per
+    launch with L2 flushed, algorithmic bytes (each array once at full size)
+    per second against the measured HBM copy bandwidth."""
+    import torch
+
+    from finitevolx_b200 import boundary as B
+    from finitevolx_b200._lib import D, I, P, SCHEMES, check, fn, sfx, stream_ptr
+    from finitevolx_b200 import operators as O
+    from finitevolx_b200.timestepping import lincomb
+
+    hbm = _peaks().get("hbm_gbs")
+    out = {"workload": "config 1: 2-D stencils, periodic, seeded k^-3 tracer, u/v from a random streamfunction",
+           "bytes_per_cell": {"advection": "h,u,v read + out written (16 B FP32, 32 B FP64)",
+                              "jacobian": "f,g read + J written (12 / 24 B)",
+                              "biharmonic": "h read + out written (8 / 16 B)"},
+           "peak_gbs": hbm, "peak_source": "measured HBM copy (MEASURED_PEAKS.json)", "rows": []}
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    for n in sizes:
+        for dt in (torch.float32, torch.float64):
+            es = 4 if dt == torch.float32 else 8
+            N = n + 2
+            dx = LX / n
+            h = torch.zeros((N, N), dtype=dt, device="cuda")
+            h[1:-1, 1:-1] = _kminus3_torch(n, n, gen, dtype=dt)[0]
+            h = B.enforce_periodic(h)
+            psi = torch.zeros_like(h)
+            psi[1:-1, 1:-1] = _kminus3_torch(n, n, gen, dtype=dt)[0] * (dx / 10.0)
+            px = O.cgrid_op("T_to_X", psi)
+            u = lincomb(-1.0, O.cgrid_op("diff_y_X_to_U", px, dx=dx, dy=dx))
+            v = O.cgrid_op("diff_x_X_to_V", px, dx=dx, dy=dx)
+            o = torch.empty_like(h)
+            fe, fnn, lap = torch.empty_like(h), torch.empty_like(h), torch.empty_like(h)
+            jo = torch.empty((N - 2, N - 2), dtype=dt, device="cuda")
+            s = sfx(h)
+            st = stream_ptr()
+            adv = fn(f"fvx_advect2d_{s}")
+            ff = fn(f"fvx_face_flux2d_{s}")
+            fd = fn(f"fvx_flux_divergence2d_{s}")
+            cg = fn(f"fvx_cgrid_op2d_{s}")
+            cells = N * N
+            for op in ("weno5", "weno7", "van_leer", "jacobian", "biharmonic"):
+                if op in ("weno5", "weno7", "van_leer"):
+                    m = I(SCHEMES[op])
+                    fused = lambda m=m: check(adv(P(h), P(u), P(v), P(o), I(N), I(N), D(dx), D(dx), m, None, None,  # noqa: E731
+                                                  st), "advect")
+
+                    def unfused(m=m):
+                        check(ff(P(h), P(u), P(v), P(fe), P(fnn), I(N), I(N), m, None, st), "face flux")
+                        check(fd(P(fe), P(fnn), P(o), I(N), I(N), D(dx), D(dx), None, st), "divergence")
+                    nbytes = 4 * es * cells
+                    form = "face fluxes (fe, fn to HBM) + flux divergence"
+                elif op == "jacobian":
+                    jac = fn(f"fvx_arakawa_jacobian_{s}")
+                    fused = lambda: check(jac(P(h), P(psi), P(jo), I(1), I(N), I(N), D(dx), D(dx), st), "J")  # noqa: E731
+                    unfused = None
+                    nbytes = 3 * es * cells
+                    form = None
+                else:
+                    bh = fn(f"fvx_biharmonic2d_{s}")
+                    fused = lambda: check(bh(P(h), D(1e9), P(o), I(N), I(N), D(dx), D(dx), None, st), "biharm")  # noqa: E731
+
+                    def unfused():
+                        check(cg(I(8), P(h), None, P(lap), None, I(N), I(N), D(dx), D(dx), None, None, st), "lap")
+                        check(cg(I(8), P(lap), None, P(o), None, I(N), I(N), D(dx), D(dx), None, None, st), "lap")
+                        o.mul_(-1e9)
+                    nbytes = 2 * es * cells
+                    form = "laplacian -> HBM, laplacian, scale"
+                for _ in range(3):
+                    fused()
+                    if unfused:
+                        unfused()
+                t_f = per_launch_ms(fused, flush, reps=10, rounds=3)
+                row = {"n": n, "dtype": "f32" if es == 4 else "f64", "op": op, "fused_ms": t_f,
+                       "gbs": nbytes / (t_f * 1e-3) / 1e9}
+                row["frac"] = row["gbs"] / hbm if hbm else None
+                if unfused:
+                    t_u = per_launch_ms(unfused, flush, reps=10, rounds=3)
+                    row.update(unfused_ms=t_u, fused_speedup=t_u / t_f, unfused_form=form)
+                out["rows"].append(row)
+            del h, psi, px, u, v, o, fe, fnn, lap, jo
+            torch.cuda.empty_cache()
+    return out
+
+
+def dst_batch_section(n_rhs, sizes=(1024, 2048)):
+    """Config 3: Dirichlet box (Lx = 5.12e6 m), lambda in {0, 1/(4e4)^2,
+    1/(1e4)^2}, n_rhs seeded k^-3 right-hand sides per size.  FP32: the
+    3xBF16 tensor-core chain; FP64: the same chain plus FP64 iterative
+    refinement on the 5-point residual to a 1e-12 normwise backward error.
+    Times per right-hand side (CUDA events, whole batch), the refinement's
+    passes and backward error, and every result's max-norm error against
+    the FP64 DST oracle (SciPy, all host threads)."""
+    import numpy as np
+    import scipy.fft
+    import torch
+
+    from finitevolx_b200.solvers import DSTHelmholtzPlan
+    from oracle.threaded import host_threads
+
+    peak = _peaks().get("bf16_tflops") or 1590.0
+    cores = host_threads()
+    out = {"workload": f"config 3: DST Helmholtz, Dirichlet box, {n_rhs} seeded k^-3 RHS per size", "cases": []}
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    for n in sizes:
+        dx = LX / n
+        f64 = _kminus3_torch(n, n, gen, count=n_rhs) * 1e-5
+        f32 = f64.float()
+        fh = f64.cpu().numpy()
+        with scipy.fft.set_workers(cores):
+            fhat = scipy.fft.dstn(fh, type=1, axes=(-2, -1))
+        k = np.arange(n)
+        ev = -4.0 / dx ** 2 * np.sin(np.pi * (k + 1) / (2 * (n + 1))) ** 2
+        for lam in (0.0, 1.0 / 4e4 ** 2, 1.0 / 1e4 ** 2):
+            plan = DSTHelmholtzPlan(n, n, dx, dx, (lam,), batch_max=n_rhs)
+            with scipy.fft.set_workers(cores):
+                ref = scipy.fft.idstn(fhat / (ev[:, None] + ev[None, :] - lam), type=1, axes=(-2, -1))
+            refmax = np.abs(ref).reshape(n_rhs, -1).max(axis=1)
+            o32 = torch.empty_like(f32)
+            o64 = torch.empty_like(f64)
+            plan.solve(f32, out=o32)
+            plan.solve_refined(f64, tol=1e-12, out=o64)
+            torch.cuda.synchronize()
+            res = {}
+            for name, call in (("fp32_split", lambda: plan.solve(f32, out=o32)),
+                               ("fp64_refined", lambda: plan.solve_refined(f64, tol=1e-12, out=o64)[1])):
+                ts, info = [], None
+                for _ in range(3):
+                    torch.cuda.synchronize()
+                    e0 = torch.cuda.Event(enable_timing=True)
+                    e1 = torch.cuda.Event(enable_timing=True)
+                    e0.record()
+                    info = call()
+                    e1.record()
+                    e1.synchronize()
+                    ts.append(e0.elapsed_time(e1))
+                ms = statistics.median(ts)
+                res[name] = {"ms_batch": ms, "us_per_rhs": 1e3 * ms / n_rhs}
+                if isinstance(info, dict):
+                    res[name].update(passes=info["passes"], backward_error=info["backward_error"],
+                                     converged=info["converged"])
+            plan.check_device()
+            for name, o in (("fp32_split", o32), ("fp64_refined", o64)):
+                got = o.double().cpu().numpy()
+                e = np.abs(got - ref).reshape(n_rhs, -1).max(axis=1) / refmax
+                res[name].update(err_max=float(e.max()), err_median=float(np.median(e)),
+                                 errors=[float(f"{x:.3g}") for x in e])
+            flops = 4 * 2.0 * n ** 3 * n_rhs  # 4 dense products of 2 N^3 per RHS
+            res["fp32_split"]["tflops_algorithmic"] = flops / (res["fp32_split"]["ms_batch"] * 1e-3) / 1e12
+            res["fp32_split"]["frac_of_bf16_peak"] = res["fp32_split"]["tflops_algorithmic"] / peak
+            out["cases"].append({"n": n, "lambda": lam, **res})
+            del plan, o32, o64, ref
+            torch.cuda.empty_cache()
+        del f64, f32, fh, fhat
+    out["error"] = "max|psi - psi_oracle| / max|psi_oracle| per right-hand side; oracle = SciPy FP64 DST-I"
+    return out
+
+
+def masked_basin(n, seed=0):
+    """Masked-Helmholtz workload: Gaussian-filtered (sigma = 20 cells) seeded
+    field thresholded at 30% land, largest connected ocean kept, closed
+    boundary ring; c = exp(0.5 g) with g a second smooth field (unit std);
+    white-noise right-hand side on the ocean."""
+    import numpy as np
+    from scipy import ndimage
+    rng = np.random.default_rng(seed)
+    g = ndimage.gaussian_filter(rng.standard_normal((n, n)), sigma=20, mode="wrap")
+    m = g > np.quantile(g, 0.3)
+    lab, k = ndimage.label(m)
+    if k > 1:
+        sizes = ndimage.sum(m, lab, range(1, k + 1))
+        m = lab == (1 + int(np.argmax(sizes)))
+    m[0, :] = m[-1, :] = m[:, 0] = m[:, -1] = False
+    g2 = ndimage.gaussian_filter(rng.standard_normal((n, n)), sigma=20, mode="wrap")
+    c = np.exp(0.5 * g2 / g2.std())
+    f = rng.standard_normal((n, n)) * m
+    return m.astype(np.float64), c, f
+
+
+def helmholtz_case(n, ld, pairs, reps):
+    """Masked variable-coefficient Helmholtz, time to 1e-8 relative residual
+    (FP64-checked): MG-PCG (one V-cycle per iteration, the reference's
+    6/6/50 sweeps) against flexible PCG with the learned coarse solver
+    (U-Net at the first level at or below 128^2, the same fine sweeps,
+    energy-scaled correction) and the same cycle without the network.  Each
+    solve is timed with CUDA events around the whole call (set-up,
+    iterations, final FP64 check); median, min, max over ``reps``; the
+    network is trained once beforehand (not timed)."""
+    import torch
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200.learned import LearnedPreconditioner, generate_pairs
+
+    m, c, f = masked_basin(n, 1)
+    dx = LX / n
+    mg = fvx.build_multigrid_solver(m, dx, dx, lambda_=1.0 / ld ** 2, coeff=c, dtype=torch.float32)
+    pcg = fvx.MaskedHelmholtzPCG(mg)
+    b = torch.from_numpy(f).float().cuda()
+
+    def timed(kw):
+        pcg.solve(b, rtol=1e-8, **kw)
+        ts, info = [], None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            x, info = pcg.solve(b, rtol=1e-8, **kw)
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return {"ms": statistics.median(ts), "ms_min": min(ts), "ms_max": max(ts), "reps": reps,
+                "iterations": info["iterations"], "rel_residual_fp64": info["rel_residual"],
+                "converged": info["converged"]}
+
+    out = {"workload": f"masked Helmholtz {n}^2, Ld {ld / 1e3:.0f} km, variable c, FP32 work vectors, "
+                       "FP64 iterate/dots/residual, rtol 1e-8", "levels": mg.n_levels}
+    out["mg_pcg"] = timed(dict(precond="mg", graph=True))
+    t0 = time.time()
+    pc = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=64, seed=0)
+    F, E = generate_pairs(mg, pc.lvl, pairs, pc.n_pre, seed=1)
+    torch.cuda.synchronize()
+    t_gen = time.time() - t0
+    t0 = time.time()
+    hist = pc.train(F, E, epochs=6, batch=64, lr=2e-3, seed=1)
+    torch.cuda.synchronize()
+    out["training"] = {"pairs": pairs, "epochs": 6, "batch": 64, "gen_s": t_gen, "train_s": time.time() - t0,
+                       "loss_first_epoch": hist[0], "loss_last_epoch": hist[-1], "level": pc.lvl}
+    del F, E
+    out["learned_pcg"] = timed(dict(precond=pc, flexible=True, graph=True, max_iter=500))
+    pc0 = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=1, coarse=False, scale=False)
+    out["same_cycle_without_network"] = timed(dict(precond=pc0, flexible=True, graph=True, max_iter=500))
+    out["speedup_learned_vs_mg"] = out["mg_pcg"]["ms"] / out["learned_pcg"]["ms"]
+    return out
+
+
+def helmholtz_section(pairs, reps):
+    return {"cases": [helmholtz_case(n, ld, pairs, reps) for n, ld in ((1024, LD), (512, LD), (1024, 4.0e5))]}
+
+
+def ensemble_members(count=64, seed=0):
+    """Config-2 ensemble: sizes drawn (seeded) from {128, 256, 512, 1024}^2,
+    1-3 layers (H = 400/1100/2600 m)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    sizes = rng.choice([128, 256, 512, 1024], size=count)
+    nls = rng.integers(1, 4, size=count)
+    return list(zip(sizes.tolist(), nls.tolist()))
+
+
+def ensemble_section(members, n_steps):
+    """All members advanced n_steps RK3-SSP steps by one CUDA graph per rank
+    (per RK stage: one batched DST chain per grid size, one persistent
+    work-queue launch of the fused stage over every tile of every layer).
+    With N ranks each rank runs the members ``shard_members`` gives it.
+    Metric: interior layer-cells x steps / s over all ranks."""
+    import torch
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200 import autotune
+    from finitevolx_b200.replicas import sharded_ensemble_run
+
+    tuned = {}
+
+    def factory(sub, idx):
+        ens = fvx.QGEnsemble(sub)
+        for m, ((n, nl), gi) in enumerate(zip(sub, idx)):
+            g = torch.Generator(device="cuda").manual_seed(1000 + gi)
+            for k in range(nl):
+                q = torch.zeros((n + 2, n + 2), device="cuda")
+                q[1:-1, 1:-1] = torch.randn((n, n), device="cuda", generator=g) * 1e-5
+                ens.set_layer(m, k, q)
+        tuned.update(autotune.tune_ensemble(ens))
+        return ens
+
+    r = sharded_ensemble_run(members, n_steps, factory)
+    ms = r["t_max_ms"]
+    return {"workload": f"{len(members)} multi-layer QG members, sizes {{128,256,512,1024}}^2, 1-3 layers, "
+                        f"WENO5, FP32, {n_steps} RK3 steps in one CUDA graph per rank",
+            "members": len(members), "layer_cells_per_step": r["cells_per_step"], "steps": n_steps, "ms": ms,
+            "ms_per_step": ms / n_steps, "value": r["value"], "unit": "Mcell-steps/s",
+            "ranks": r["world"], "members_per_rank": r["members_per_rank"],
+            "launches_per_step": r["launches_per_step"], "autotuned_blocks_per_sm": tuned.get("blocks_per_sm")}
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -358,6 +640,7 @@ def main():
     import finitevolx_b200 as fvx
     from finitevolx_b200 import _lib as L
     from finitevolx_b200.qg import QGModel
+    from finitevolx_b200.replicas import max_over_ranks, whole_job_rate
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -366,9 +649,13 @@ def main():
     grid = fvx.ArakawaCGrid2D.from_interior(n, n, LX, LX)
     dt = 0.5 * grid.dx / 1.0
     model = QGModel(grid, BETA, 1.0 / LD ** 2, method=args.method, dtype=torch.float32)
-    q0 = torch.as_tensor(initial_q(n, seed=rank), dtype=torch.float32, device="cuda")
+    q0_host = initial_q(n, seed=rank)
+    q0 = torch.as_tensor(q0_host, dtype=torch.float32, device="cuda")
     qa, qb = q0.clone(), torch.empty_like(q0)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # the GPU step from the bench's initial state, for the parity check
+    q1_gpu = model.step(q0, dt).double().cpu().numpy()
 
     # autotuned launch choices (stage tile shape; fused or separate DST split)
     from finitevolx_b200 import autotune
@@ -382,45 +669,13 @@ def main():
                  "dst_kernel": autotune.tune_dst_kernel(model, qa, dt)["kernel"]}
     qa.copy_(q0)
 
-    # warm-up (eager), leaves split(qb) in the DST workspace for the graphs
-    for _ in range(max(args.warmup, 3)):
-        model.step(qa, dt, out=qb)
-        qa.copy_(qb)
-    model.step(qa, dt, out=qb)
-    torch.cuda.synchronize()
-    # CUDA graphs of one step each way (qa -> qb, qb -> qa), chained presplit
-    graphs = []
-    s = torch.cuda.Stream()
-    s.wait_stream(torch.cuda.current_stream())
-    with torch.cuda.stream(s):
-        for src, dst in ((qb, qa), (qa, qb)):
-            g = torch.cuda.CUDAGraph()
-            launches0 = model.kernel_launches
-            with torch.cuda.graph(g, stream=s):
-                model.step(src, dt, out=dst, presplit=True)
-            per_step_launches = model.kernel_launches - launches0
-            graphs.append(g)
-    torch.cuda.current_stream().wait_stream(s)
-    for g in graphs:  # graph warm-up
-        g.replay()
-    torch.cuda.synchronize()
-
+    graphs, per_step_launches = _graph_steps(model, qa, qb, dt, args.steps, args.warmup, flush)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    total_ms = 0.0
     with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            flush.fill_(float(k))
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            graphs[k % 2].replay()
-            e1.record()
-            e1.synchronize()
-            total_ms += e0.elapsed_time(e1)
+        total_ms = _time_graphs(graphs, args.steps, flush)
     torch.cuda.synchronize()
-    from finitevolx_b200.replicas import max_over_ranks, whole_job_rate
     t_max = max_over_ranks(total_ms, device="cuda")
     if world > 1:
         dist.barrier()
@@ -457,16 +712,14 @@ def main():
     e1.record()
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
-    # the pipeline steps the same state as the graphs above: check its result
-    if rank == 0:
-        ref_out = model.step(host_in[0].to("cuda"), dt).cpu()
-        diff = (host_out[(args.steps - 1) % n_host] - ref_out).abs().max() / ref_out.abs().max()
-        if not float(diff) <= 1e-6:
-            raise RuntimeError(f"e2e pipeline result differs from QGModel.step ({float(diff):.3e})")
-    host_in = host_in[0]
+    # the pipeline's output is the step of q0: the same q_{n+1} as above
+    e2e_diff = float(np.abs(host_out[(args.steps - 1) % n_host].double().numpy() - q1_gpu).max()
+                     / np.abs(q1_gpu).max())
+    if not e2e_diff <= 1e-6:
+        raise RuntimeError(f"e2e pipeline result differs from QGModel.step ({e2e_diff:.3e})")
     e2e_ms = max_over_ranks(e2e_ms, device="cuda")
     e2e = whole_job_rate(cells, args.steps, e2e_ms, world)
-    nbytes = host_in.numel() * host_in.element_size()
+    nbytes = host_in[0].numel() * host_in.element_size()
 
     # fused vs unfused: the same step as the reference's operator sequence,
     # one kernel (or torch copy) per operator, through the same library
@@ -493,12 +746,8 @@ def main():
     # pass each) = 16 B/cell, plus the DST operand written as bf16 hi/lo
     # (4 B/cell)
     stage_bytes = 20.0 * n * n
-    hbm_peak = None
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            hbm_peak = json.load(f).get("hbm_gbs")
-    except Exception:
-        pass
+    peaks = _peaks()
+    hbm_peak = peaks.get("hbm_gbs")
 
     # dominant kernel: one tcgen05 DST GEMM (2048 x 2048 x 2048, 3xBF16)
     from finitevolx_b200._lib import I, fn, stream_ptr
@@ -509,23 +758,30 @@ def main():
         gemm(h, I(0), I(1), stream_ptr())
     gemm_ms = per_launch_ms(lambda: L.check(gemm(h, I(0), I(1), stream_ptr()), "gemm"), flush)
     flops = 2.0 * n * n * n
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except Exception:
-        pass
     peak = peaks.get("bf16_tflops")
     peak_src = "measured burst bf16 (MEASURED_PEAKS.json)" if peak else "fallback 1590"
     peak = peak or 1590.0
     achieved = flops / (gemm_ms * 1e-3) / 1e12
+    # DRAM traffic of this kernel per launch, from the ncu capture of the
+    # 2048^2 step committed under profiles/ (dram__bytes_read.sum +
+    # dram__bytes_write.sum of the first product of a solve)
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "dst_product_traffic.json")) as f:
+            tr = json.load(f)
+        if tr.get("n") == n and tr.get("kernel") == ("gemm_sym_bf16_kernel" if sym else "gemm_split_bf16_kernel"):
+            traffic = tr.get("dram_bytes_per_launch")
+    except Exception:
+        pass
 
+    res = {}
     if rank == 0:
         res = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": dict(config(n, args.method), autotuned=tuned),
+            "config": dict(config(n, args.method), autotuned=tuned,
+                           helmholtz="DST-I as tensor-core transform-matrix products, 3xBF16 split, FP32 accumulate"),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
                     "ms_per_step": e2e_ms / args.steps,
                     "form": "QGPipeline: upload of state k+1, step k (CUDA graph), download of k-1 on three "
@@ -536,14 +792,13 @@ def main():
                                     else "gemm_split_bf16_kernel (DST product, 3xBF16)"),
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": peak_src,
-                         # DRAM bytes per launch from an ncu capture of this kernel in this
-                         # step (dram__bytes_read.sum + dram__bytes_write.sum, first product;
-                         # the operands otherwise stay in L2 between the products)
-                         "traffic": 25.2e6 if n == 2048 and sym else None, "traffic_unit": "bytes",
+                         "traffic": traffic, "traffic_unit": "bytes",
+                         "traffic_source": "profiles/dst_product_traffic.json (ncu capture of this kernel)"
+                                           if traffic else None,
                          "per_launch_ms": gemm_ms, "algorithmic_flops_per_launch": flops,
                          "executed_tensor_flops_per_launch": (3.0 if sym else 6.0) * n ** 3,
                          "executed_frac": (3.0 if sym else 6.0) * n ** 3 / (gemm_ms * 1e-3) / 1e12 / peak},
-            "stage_kernel": {"bound": "hbm", "kernel": "qg stage_kernel<float, WENO5>",
+            "stage_kernel": {"bound": "hbm", "kernel": f"qg stage_kernel<float, {args.method.upper()}>",
                              "per_launch_ms": stage_ms, "algorithmic_bytes_per_launch": stage_bytes,
                              "achieved": stage_bytes / (stage_ms * 1e-3) / 1e9, "unit": "GB/s",
                              "peak": hbm_peak,
@@ -555,11 +810,26 @@ def main():
             "clocks": clk.summary(),
         }
         if world == 1 and not args.no_cpu_baseline:
-            res["cpu_baseline"] = cpu_baseline(n, args.method)
+            cb, q1_ref = cpu_baseline(n, args.method)
+            res["cpu_baseline"] = cb
+            if rank == 0 and np.array_equal(q0_host, initial_q(n)):
+                err = float(np.abs(q1_gpu - q1_ref).max() / np.abs(q1_ref).max())
+                res["parity"] = {"rel_err_vs_fp64_oracle": err, "bar": 1e-5, "passed": err < 1e-5,
+                                 "what": "max|q1_gpu - q1_oracle| / max|q1_oracle| after one step from the bench's "
+                                         "initial state (FP64 oracle)"}
+        if world == 1 and not args.no_fp64:
+            res["fp64_metric_config"] = fp64_metric_section(args.method, args.steps, flush)
+        if world == 1 and not args.no_sweep:
+            res["stencil_sweep"] = stencil_sweep_section(flush)
+        if world == 1 and not args.no_dst:
+            res["dst_batched"] = dst_batch_section(args.dst_rhs)
         if world == 1 and not args.no_helmholtz:
-            res["helmholtz"] = helmholtz_section(args.helm_n, args.helm_pairs)
-        if world == 1 and not args.no_ensemble:
-            res["ensemble"] = ensemble_section(ensemble_members(), args.ens_steps)
+            res["helmholtz"] = helmholtz_section(args.helm_pairs, args.helm_reps)
+    if not args.no_ensemble:
+        ens = ensemble_section(ensemble_members(), args.ens_steps)  # every rank: its own members
+        if rank == 0:
+            res["ensemble"] = ens
+    if rank == 0:
         print(json.dumps(res))
     if world > 1:
         dist.barrier()

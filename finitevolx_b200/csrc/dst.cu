@@ -40,9 +40,9 @@ constexpr int B_TILE = BN * BK * 2;                        // 32 KiB
 constexpr int STAGE_BYTES = 2 * A_TILE + 2 * B_TILE;       // 96 KiB
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
 constexpr int THREADS = 192;                               // TMA warp, MMA warp, 4 epilogue warps
-constexpr long long kWaitCycles = 4000000000LL;            // ~2 s bound on every spin-wait
+constexpr long long kWaitCycles = 4000000000LL;            // default bound on every spin-wait (~2 s)
 
-enum EpiMode { EPI_SPLIT = 0, EPI_F32 = 1, EPI_F64 = 2, EPI_F64_ACC = 3 };
+enum EpiMode { EPI_SPLIT = 0, EPI_F32 = 1, EPI_F64 = 2, EPI_F64_ACC = 3, EPI_F32_ACC = 4 };
 
 struct Epi {
   int mode;
@@ -61,6 +61,9 @@ struct Epi {
   int* err;
   int perm_r = 0;          // store r at its even/odd de-interleaved position (the next product's layout)
   int tma_out = 0;         // even/odd kernel: stage the tile in shared memory, TMA bulk-tensor stores
+  long long wait_cycles = kWaitCycles;  // bound on every barrier wait of the main loop and epilogue
+  int stall = 0;           // fault injection for tests: the producer issues no loads, so the
+                           // MMA warp's first wait runs out (nothing is ever in flight)
 };
 
 // ---- PTX helpers ----------------------------------------------------------
@@ -83,19 +86,33 @@ DEV bool mbar_try(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after ~2 s, raises the CTA abort flag and the
-// global error flag instead of spinning forever.
-DEV bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag, int* err) {
+// Bounded wait: gives up after ``limit`` SM cycles (default ~2 s), raises the
+// CTA abort flag and the global error flag instead of spinning forever.
+DEV bool mbar_wait(uint32_t a, uint32_t parity, volatile int* abort_flag, int* err, long long limit = kWaitCycles) {
   long long t0 = clock64();
   while (!mbar_try(a, parity)) {
     if (*abort_flag) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       *abort_flag = 1;
       if (err) atomicExch(err, 1);
       return false;
     }
   }
   return true;
+}
+// Wait for phase ``parity`` of barrier ``a`` regardless of the abort flag,
+// bounded by the default limit: used after an abort so that no copy or MMA
+// issued earlier is still in flight when the CTA frees TMEM and exits.
+DEV void mbar_drain(uint32_t a, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(a, parity))
+    if (clock64() - t0 > kWaitCycles) return;
+}
+// The loads issued for ring slots issued-stages .. issued-1 (the last one
+// into each stage) have landed.
+DEV void drain_ring(uint32_t full0, int stages, int issued) {
+  for (int k = issued > stages ? issued - stages : 0; k < issued; ++k)
+    mbar_drain(full0 + 8u * (uint32_t)(k % stages), (uint32_t)((k / stages) & 1));
 }
 DEV void tma_load_2d(uint32_t dst, const CUtensorMap* map, uint32_t bar, int c0, int c1) {
   asm volatile(
@@ -246,6 +263,9 @@ DEV void epi_store(const Epi& ep, int b, int r, int n, float acc) {
     case EPI_F64:
       ((double*)ep.out0)[idx] = (double)acc * ep.alpha;
       break;
+    case EPI_F32_ACC:
+      ((float*)ep.out0)[idx] += acc * (float)ep.alpha;
+      break;
     default:
       ((double*)ep.out0)[idx] += (double)acc * ep.alpha;
       break;
@@ -289,10 +309,11 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
   // A or B tile do not all read the same L2 lines at the same time
   const int kshift = (int)((blockIdx.x * 5u + blockIdx.y * 3u) % (unsigned)KT);
   if (warp == 0 && lane == 0) {
-    // TMA producer
-    for (int kt = 0; kt < KT; ++kt) {
+    // TMA producer (with ep.stall: no loads, for the timeout test)
+    int issued = 0;
+    for (int kt = 0; kt < KT && !ep.stall; ++kt) {
       const int s = kt % STAGES;
-      if (kt >= STAGES && !mbar_wait(empty(s), ((kt / STAGES) - 1) & 1, abort_flag, ep.err)) break;
+      if (kt >= STAGES && !mbar_wait(empty(s), ((kt / STAGES) - 1) & 1, abort_flag, ep.err, ep.wait_cycles)) break;
       mbar_expect_tx(full(s), STAGE_BYTES);
       const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
       const int kc = ((kt + kshift) % KT) * BK;
@@ -300,13 +321,15 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
       tma_load_2d(base + A_TILE, &mAl, full(s), kc, m0);
       tma_load_2d(base + 2 * A_TILE, &mBh, full(s), kc, n0);
       tma_load_2d(base + 2 * A_TILE + B_TILE, &mBl, full(s), kc, n0);
+      issued = kt + 1;
     }
+    drain_ring(full(0), STAGES, issued);
   } else if (warp == 1 && lane == 0) {
     // MMA issuer: three split products per 16-wide K step
     bool ok = true;
     for (int kt = 0; kt < KT && ok; ++kt) {
       const int s = kt % STAGES;
-      ok = mbar_wait(full(s), (kt / STAGES) & 1, abort_flag, ep.err);
+      ok = mbar_wait(full(s), (kt / STAGES) & 1, abort_flag, ep.err, ep.wait_cycles);
       if (!ok) break;
       tc_fence_after();
       const uint32_t base = smem_u32(smem + s * STAGE_BYTES);
@@ -330,7 +353,7 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
     const bool mvalid = m < ep.m_total;
     const int b = mvalid ? m / ep.rows_per_batch : 0;
     const int r = mvalid ? m - b * ep.rows_per_batch : 0;
-    if (mbar_wait(accb, 0, abort_flag, ep.err)) {
+    if (mbar_wait(accb, 0, abort_flag, ep.err, ep.wait_cycles)) {
       tc_fence_after();
       if (!*abort_flag) {
 #pragma unroll 1
@@ -352,6 +375,8 @@ gemm_split_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_con
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
+    if (lane == 0) mbar_drain(accb, 0);  // the MMAs issued before an abort have completed
+    __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN));
   }
@@ -443,7 +468,7 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
       const int k = n0 + cbeg + 16 + (lane & 15);
       prefetch_l2(base + (long long)((lane < 16) ? k : K - 1 - k) * R);
     }
-    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err, ep.wait_cycles);
     if (ok) tc_fence_after();
     grid_dep_launch();  // the next kernel may start its set-up while this tile drains
     const bool go = ok && !*abort_flag;
@@ -521,7 +546,7 @@ DEV void sym_epilogue(uint8_t* smem, uint32_t tmem, uint32_t accb, int m0, int n
     // shared memory stays allocated until the stores have read it
     if (go && lane == 0 && (warp & 3) == 2) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
   } else {
-    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err);
+    const bool ok = mbar_wait(accb, 0, abort_flag, ep.err, ep.wait_cycles);
     if (ok) tc_fence_after();
     grid_dep_launch();
     if (ok && !*abort_flag) {
@@ -604,12 +629,14 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
       tma_load_2d(base + 2 * C::A_T, odd ? &mQh : &mPh, full(s), kb * BKT, n0);
       tma_load_2d(base + 2 * C::A_T + C::B_T, odd ? &mQl : &mPl, full(s), kb * BKT, n0);
     };
-    for (int kt0 = 0; kt0 < KT && kt0 < C::STAGES; ++kt0) load_b(kt0);
+    const int KTL = ep.stall ? 0 : KT;  // ep.stall: no loads (the timeout test)
+    for (int kt0 = 0; kt0 < KTL && kt0 < C::STAGES; ++kt0) load_b(kt0);
     grid_dep_wait();
-    for (int kt0 = 0; kt0 < KT; ++kt0) {
+    int issued = 0;
+    for (int kt0 = 0; kt0 < KTL; ++kt0) {
       const int s = kt0 % C::STAGES;
       if (kt0 >= C::STAGES) {
-        if (!mbar_wait(empty(s), ((kt0 / C::STAGES) - 1) & 1, abort_flag, ep.err)) break;
+        if (!mbar_wait(empty(s), ((kt0 / C::STAGES) - 1) & 1, abort_flag, ep.err, ep.wait_cycles)) break;
         load_b(kt0);
       }
       const uint32_t base = smem_u32(smem + s * C::STAGE);
@@ -617,12 +644,14 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
       const int ac = ((kt & 1) ? KH : 0) + (kt >> 1) * BKT;
       tma_load_2d(base, &mAh, full(s), ac, m0);
       tma_load_2d(base + C::A_T, &mAl, full(s), ac, m0);
+      issued = kt0 + 1;
     }
+    drain_ring(full(0), C::STAGES, issued);
   } else if (warp == 1 && lane == 0) {
     bool ok = true;
     for (int kt0 = 0; kt0 < KT && ok; ++kt0) {
       const int s = kt0 % C::STAGES;
-      ok = mbar_wait(full(s), (kt0 / C::STAGES) & 1, abort_flag, ep.err);
+      ok = mbar_wait(full(s), (kt0 / C::STAGES) & 1, abort_flag, ep.err, ep.wait_cycles);
       if (!ok) break;
       tc_fence_after();
       const uint32_t base = smem_u32(smem + s * C::STAGE);
@@ -647,6 +676,8 @@ gemm_sym_bf16_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   tc_fence_before();
   __syncthreads();
   if (warp == 1) {
+    if (lane == 0) mbar_drain(accb, 0);  // the MMAs issued before an abort have completed
+    __syncwarp();
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * SBN));
   }
@@ -734,7 +765,7 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
     for (int kt0 = 0; kt0 < KT; ++kt0) {
       const int s = kt0 % P_STAGES;
       if (kt0 >= P_STAGES) {
-        if (!mbar_wait(empty(s), ((kt0 / P_STAGES) - 1) & 1, abort_flag, ep.err)) break;
+        if (!mbar_wait(empty(s), ((kt0 / P_STAGES) - 1) & 1, abort_flag, ep.err, ep.wait_cycles)) break;
         load_b(kt0);
       }
       const uint32_t fb = map_to_rank(full(s), 0);
@@ -749,7 +780,7 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
       bool ok = true;
       for (int kt0 = 0; kt0 < KT && ok; ++kt0) {
         const int s = kt0 % P_STAGES;
-        ok = mbar_wait(full(s), (kt0 / P_STAGES) & 1, abort_flag, ep.err);
+        ok = mbar_wait(full(s), (kt0 / P_STAGES) & 1, abort_flag, ep.err, ep.wait_cycles);
         if (!ok) break;
         tc_fence_after();
         const uint32_t base = smem_u32(smem + s * P_STAGE);
@@ -895,8 +926,8 @@ DEV double warp_sum(double v) {
 // into bf16 hi/lo (the next correction's GEMM operand, scaled by 1/rscale)
 // and accumulates sum r^2, sum f^2, sum psi^2, sum |A|^2-weighted norm parts
 // into norms[0..3] with warp-shuffle reductions.
-template <typename T>
-__global__ void residual_kernel(const T* __restrict__ f, long long fb, long long fld, const double* __restrict__ psi,
+template <typename T, typename PT>
+__global__ void residual_kernel(const T* __restrict__ f, long long fb, long long fld, const PT* __restrict__ psi,
                                 long long pb, long long pld, int ny, int nx, int batch, double dx, double dy,
                                 const double* __restrict__ lam, int nlam, bf16* __restrict__ hi,
                                 bf16* __restrict__ lo, double* norms, int perm) {
@@ -908,10 +939,10 @@ __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long
     long long b = k / ((long long)ny * nx);
     long long rem = k - b * ny * nx;
     int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
-    const double* P = psi + b * pb + (long long)y * pld + x;
-    double c = P[0];
-    double e = x + 1 < nx ? P[1] : 0.0, w = x > 0 ? P[-1] : 0.0;
-    double nn = y + 1 < ny ? P[pld] : 0.0, s = y > 0 ? P[-pld] : 0.0;
+    const PT* P = psi + b * pb + (long long)y * pld + x;
+    double c = (double)P[0];
+    double e = x + 1 < nx ? (double)P[1] : 0.0, w = x > 0 ? (double)P[-1] : 0.0;
+    double nn = y + 1 < ny ? (double)P[pld] : 0.0, s = y > 0 ? (double)P[-pld] : 0.0;
     double lap = ((e - 2.0 * c) + w) * idx2 + ((nn - 2.0 * c) + s) * idy2;
     double fv = (double)f[b * fb + (long long)y * fld + x];
     double r = fv - (lap - lam[b % nlam] * c);
@@ -924,6 +955,7 @@ __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long
     s_f += fv * fv;
     s_p += c * c;
   }
+  if (!norms) return;
   s_r = warp_sum(s_r);
   s_f = warp_sum(s_f);
   s_p = warp_sum(s_p);
@@ -969,13 +1001,9 @@ static bool make_map(CUtensorMap* map, const void* base, uint64_t inner, uint64_
 // C[M, N] = X[M, K] S[K, N] (S symmetric, given as hi/lo rows of length K).
 static int gemm_split(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Sh, const bf16* Sl, int N,
                       const Epi& ep, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(gemm_split_bf16_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES) !=
-        cudaSuccess)
-      return FVX_ERR_CUDA;
-    attr_set = true;
-  }
+  static fvx_once_per_device attr;
+  if (fvx_once_on_device(attr, [] { return fvx_set_max_smem(gemm_split_bf16_kernel, SMEM_BYTES); }))
+    return FVX_ERR_CUDA;
   CUtensorMap a_h, a_l, b_h, b_l;
   if (!make_map(&a_h, Xh, K, M, BM) || !make_map(&a_l, Xl, K, M, BM) || !make_map(&b_h, Sh, K, N, BN) ||
       !make_map(&b_l, Sl, K, N, BN))
@@ -1014,15 +1042,12 @@ static int g_sym_kernel = 0;
 static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph, const bf16* Pl, const bf16* Qh,
                     const bf16* Ql, const Epi& ep_in, cudaStream_t st) {
   Epi ep = ep_in;
-  static bool attr_set = false;
-  if (!attr_set) {
-    if (cudaFuncSetAttribute(gemm_sym_bf16_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SymCfg<64>::SMEM) != cudaSuccess ||
-        cudaFuncSetAttribute(gemm_sym_bf16_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             SymCfg<32>::SMEM) != cudaSuccess)
-      return FVX_ERR_CUDA;
-    attr_set = true;
-  }
+  static fvx_once_per_device attr;
+  if (fvx_once_on_device(attr, [] {
+        return fvx_set_max_smem(gemm_sym_bf16_kernel<64>, SymCfg<64>::SMEM) &&
+               fvx_set_max_smem(gemm_sym_bf16_kernel<32>, SymCfg<32>::SMEM);
+      }))
+    return FVX_ERR_CUDA;
   if (K % (2 * SBN) != 0) return FVX_ERR_SHAPE;
   const int KH = K / 2;
   const uint32_t bki = g_sym_kernel == 2 ? 32 : 64;  // K block of the single-CTA forms
@@ -1048,13 +1073,9 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
   }
   if (M % (2 * BM) == 0 && g_sym_kernel == 1) {
     // CTA pairs: B blocks of 64 table rows per CTA
-    static bool pattr = false;
-    if (!pattr) {
-      if (cudaFuncSetAttribute(gemm_sym_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, P_SMEM) !=
-          cudaSuccess)
-        return FVX_ERR_CUDA;
-      pattr = true;
-    }
+    static fvx_once_per_device pattr;
+    if (fvx_once_on_device(pattr, [] { return fvx_set_max_smem(gemm_sym_pair_kernel, P_SMEM); }))
+      return FVX_ERR_CUDA;
     CUtensorMap p2h, p2l, q2h, q2l;
     if (!make_map(&p2h, Ph, KH, KH, SBN / 2) || !make_map(&p2l, Pl, KH, KH, SBN / 2) ||
         !make_map(&q2h, Qh, KH, KH, SBN / 2) || !make_map(&q2l, Ql, KH, KH, SBN / 2))
@@ -1119,6 +1140,8 @@ struct fvx_dst_plan {
   double *V1 = nullptr, *V2 = nullptr;  // FP64 chain work
   double* norms = nullptr;              // [4]
   int* err = nullptr;
+  long long wait_cycles = kWaitCycles;  // fvx_dst_plan_set_wait_limit
+  int stall = 0;                        // fvx_dst_plan_inject_stall (tests only)
 };
 
 static void dst_free(fvx_dst_plan* p) {
@@ -1339,10 +1362,31 @@ extern "C" int fvx_dst_plan_destroy(fvx_dst_plan* p) {
 extern "C" int fvx_dst_plan_check(fvx_dst_plan* p, void* stream) {
   if (!p) return FVX_ERR_ARG;
   int e = 0;
-  if (cudaMemcpyAsync(&e, p->err, sizeof(int), cudaMemcpyDeviceToHost, fvx_stream(stream)) != cudaSuccess ||
-      cudaStreamSynchronize(fvx_stream(stream)) != cudaSuccess)
+  cudaStream_t st = fvx_stream(stream);
+  if (cudaMemcpyAsync(&e, p->err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
     return FVX_ERR_CUDA;
+  if (e && (cudaMemsetAsync(p->err, 0, sizeof(int), st) != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess))
+    return FVX_ERR_CUDA;  // reported once, then cleared for the plan's next solves
   return e ? FVX_ERR_TIMEOUT : FVX_OK;
+}
+
+// Bound on every barrier wait of the plan's tensor-core products, in SM
+// clock cycles (default 4e9, about 2 s at 1.97 GHz); a wait that runs out
+// ends its CTA without trapping and sets the flag fvx_dst_plan_check reads.
+extern "C" int fvx_dst_plan_set_wait_limit(fvx_dst_plan* p, long long cycles) {
+  if (!p || cycles < 1000) return FVX_ERR_ARG;
+  p->wait_cycles = cycles;
+  return FVX_OK;
+}
+
+// Fault injection for tests: while on, the products' producer warps issue
+// no loads, so their MMA warps wait on barriers that nothing will complete,
+// run out after the wait limit and abort (no copy or MMA is in flight).
+extern "C" int fvx_dst_plan_inject_stall(fvx_dst_plan* p, int on) {
+  if (!p) return FVX_ERR_ARG;
+  p->stall = on ? 1 : 0;
+  return FVX_OK;
 }
 
 static Epi make_epi(fvx_dst_plan* p, int mode, int R, int M, int N, void* o0, void* o1, long long bstride,
@@ -1352,6 +1396,8 @@ static Epi make_epi(fvx_dst_plan* p, int mode, int R, int M, int N, void* o0, vo
   e.batch_stride = bstride; e.ld = ld; e.off_n = off_n; e.off_r = off_r; e.alpha = alpha;
   e.inv_eig = eig ? p->inv32 : nullptr; e.inv_eig64 = eig ? p->inv64 : nullptr; e.n_eig = p->n_lam;
   e.err = p->err;
+  e.wait_cycles = p->wait_cycles;
+  e.stall = p->stall;
   return e;
 }
 
@@ -1439,6 +1485,31 @@ extern "C" int fvx_dst_solve_presplit_f32(fvx_dst_plan* p, float* psi, long long
   return chain_split(p, batch, EPI_F32, psi, psi_bstride, psi_ld, fvx_stream(stream));
 }
 
+// FP64-residual iterative refinement of an FP32 result: ``passes`` times,
+// r = rhs - (lap - lambda) psi evaluated in FP64 from the FP32 rhs and psi,
+// split into the chain's operand, and psi += the chain's solve of r.  One
+// pass takes the split chain's ~1e-5 relative error (16-bit hi + lo
+// intermediates) to the FP32 rounding of psi.  Stream-ordered, no host
+// synchronisation (capturable).  Dirichlet plans with split-capable sizes.
+extern "C" int fvx_dst_refine_f32(fvx_dst_plan* p, const float* rhs, long long rhs_bstride, long long rhs_ld,
+                                  float* psi, long long psi_bstride, long long psi_ld, int batch, int passes,
+                                  void* stream) {
+  if (!p || !rhs || !psi || passes < 0) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max || !p->split_ok) return FVX_ERR_SHAPE;
+  if (p->kind != FVX_SPECTRAL_DST) return FVX_ERR_METHOD;
+  cudaStream_t st = fvx_stream(stream);
+  const long long n = (long long)batch * p->ny * p->nx;
+  for (int it = 0; it < passes; ++it) {
+    residual_kernel<float, float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld,
+                                                              p->ny, p->nx, batch, p->dx, p->dy, p->lam_dev,
+                                                              p->n_lam, p->W1h, p->W1l, nullptr, p->sym ? 1 : 0);
+    int rc = fvx_cuda_status();
+    if (rc) return rc;
+    if ((rc = chain_split(p, batch, EPI_F32_ACC, psi, psi_bstride, psi_ld, st))) return rc;
+  }
+  return FVX_OK;
+}
+
 // Layout of the chain's first operand (the fvx_dst_workspace buffers): 0
 // natural [b][y][x]; 1 x de-interleaved, x stored at x / 2 (even x) or
 // nx / 2 + x / 2 (odd x) -- the even/odd products of plans whose ny and nx
@@ -1487,7 +1558,7 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
   for (it = 1; it <= max_iter; ++it) {
     if ((rc = chain_split(p, batch, EPI_F64_ACC, psi, psi_bstride, psi_ld, st))) return rc;
     cudaMemsetAsync(p->norms, 0, sizeof(double) * 4, st);
-    residual_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
+    residual_kernel<double, double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
                                                         batch, p->dx, p->dy, p->lam_dev, p->n_lam, p->W1h, p->W1l,
                                                         p->norms, p->sym ? 1 : 0);
     double h[4];
@@ -1596,7 +1667,8 @@ __global__ void noalloc_tables_kernel(int ny, int nx, double dx, double dy, doub
       const double sy = sinpi((double)(j + 1) / (2.0 * (ny + 1)));
       const double sx = sinpi((double)(i + 1) / (2.0 * (nx + 1)));
       const double ey = -4.0 / (dy * dy) * sy * sy, ex = -4.0 / (dx * dx) * sx * sx;
-      inv[kk] = (float)(1.0 / ((ey + ex) - lam));
+      const double d = (ey + ex) - lam;
+      inv[kk] = d == 0.0 ? 0.f : (float)(1.0 / d);  // the plan's rule: a zero eigenvalue divides out as 0
     }
   }
 }
@@ -1609,39 +1681,51 @@ __global__ void noalloc_tables_kernel(int ny, int nx, double dx, double dy, doub
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_addr[128] = {nullptr};
 
+// The device address of the scratch array on the current device (looked up
+// on first use when ``setup``), or null.
+static unsigned char* noalloc_base(bool setup) {
+  using namespace fvx::dst;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev] && setup) {
+    // Load this file's module on the current device first (with lazy module
+    // loading nothing may have loaded it yet), then look up the array.
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, noalloc_tables_kernel) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    void* ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, g_dst_noalloc_scratch) != cudaSuccess || !ptr) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    g_noalloc_addr[dev] = ptr;
+  }
+  return (unsigned char*)g_noalloc_addr[dev];
+}
+
+// The error flag inside the scratch array (after the eight bf16 planes and
+// the 1/Lambda grid).
+static int* noalloc_err(unsigned char* base) {
+  using namespace fvx::dst;
+  return (int*)((float*)((bf16*)base + 8 * kNaPlane) + kNaPlane);
+}
+
 extern "C" int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, float* psi, long long psi_ld, int ny,
                                          int nx, double dx, double dy, double lambda, void* stream) {
   using namespace fvx::dst;
   if (!rhs || !psi) return FVX_ERR_ARG;
   if (ny < 8 || nx < 8 || ny > kNoAllocMaxN || nx > kNoAllocMaxN || ny % 8 || nx % 8) return FVX_ERR_SHAPE;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return FVX_ERR_CUDA;
-  unsigned char* base;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      // Load this file's module on the current device first (with lazy module
-      // loading nothing may have loaded it yet), then look up the array.
-      cudaFuncAttributes fa;
-      if (cudaFuncGetAttributes(&fa, noalloc_tables_kernel) != cudaSuccess) {
-        cudaGetLastError();
-        return FVX_ERR_CUDA;
-      }
-      void* ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_dst_noalloc_scratch) != cudaSuccess || !ptr) {
-        cudaGetLastError();
-        return FVX_ERR_CUDA;
-      }
-      g_noalloc_addr[dev] = ptr;
-    }
-    base = (unsigned char*)g_noalloc_addr[dev];
-  }
+  unsigned char* base = noalloc_base(true);
+  if (!base) return FVX_ERR_CUDA;
   cudaStream_t st = fvx_stream(stream);
   bf16* pl = (bf16*)base;
   bf16 *sxh = pl, *sxl = pl + kNaPlane, *syh = pl + 2 * kNaPlane, *syl = pl + 3 * kNaPlane;
   bf16 *w1h = pl + 4 * kNaPlane, *w1l = pl + 5 * kNaPlane, *w2h = pl + 6 * kNaPlane, *w2l = pl + 7 * kNaPlane;
   float* inv = (float*)(pl + 8 * kNaPlane);
-  int* err = (int*)(inv + kNaPlane);
+  int* err = noalloc_err(base);
   if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) return FVX_ERR_CUDA;
   const int total = nx * nx + ny * ny + ny * nx;
   noalloc_tables_kernel<<<(total + 255) / 256, 256, 0, st>>>(ny, nx, dx, dy, lambda, sxh, sxl, syh, syl, inv);
@@ -1664,4 +1748,20 @@ extern "C" int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, flo
   if ((rc = gemm_split(w1h, w1l, ny, nx, sxh, sxl, nx, epi(EPI_SPLIT, ny, ny, nx, w2h, w2l, (long long)nx * ny, ny, 1.0, false), st)))
     return rc;
   return gemm_split(w2h, w2l, nx, ny, syh, syl, ny, epi(EPI_F32, nx, nx, ny, psi, nullptr, 0, psi_ld, c, false), st);
+}
+
+// Reports whether a bounded wait inside the tensor-core products of the last
+// allocation-free solve on this device gave up (the solve then returned
+// FVX_OK but psi is incomplete): copies the scratch array's error flag to
+// the host on ``stream`` and waits for it.  FVX_ERR_TIMEOUT if it is set,
+// FVX_OK if it is clear or no allocation-free solve ran on this device.
+extern "C" int fvx_dst_noalloc_check(void* stream) {
+  unsigned char* base = noalloc_base(false);
+  if (!base) return FVX_OK;
+  int e = 0;
+  cudaStream_t st = fvx_stream(stream);
+  if (cudaMemcpyAsync(&e, noalloc_err(base), sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return FVX_ERR_CUDA;
+  return e ? FVX_ERR_TIMEOUT : FVX_OK;
 }

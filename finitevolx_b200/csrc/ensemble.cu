@@ -33,6 +33,9 @@ extern "C" int fvx_dst_solve_presplit_f32(fvx_dst_plan* p, float* psi, long long
                                           int batch, void* stream);
 extern "C" int fvx_dst_workspace(fvx_dst_plan* p, void** w1_hi, void** w1_lo);
 extern "C" int fvx_dst_operand_layout(fvx_dst_plan* p);
+extern "C" int fvx_dst_refine_f32(fvx_dst_plan* p, const float* rhs, long long rhs_bstride, long long rhs_ld,
+                                  float* psi, long long psi_bstride, long long psi_ld, int batch, int passes,
+                                  void* stream);
 
 namespace fvx {
 namespace ens {
@@ -84,9 +87,11 @@ ens_stage_kernel(const FieldDesc* __restrict__ fields, int nfields, int stage, i
   }
 }
 
-// Layers -> modes, written split into bf16 hi/lo (x de-interleaved when perm).
+// Layers -> modes, written split into bf16 hi/lo (x de-interleaved when
+// perm) and, when fm is not null, as FP32 in natural order (the right-hand
+// side of the refinement residual).
 __global__ void ens_mode_split_kernel(const ModeDesc* __restrict__ md, int B, int n, __nv_bfloat16* hi,
-                                      __nv_bfloat16* lo, int perm) {
+                                      __nv_bfloat16* lo, int perm, float* __restrict__ fm) {
   const size_t plane = (size_t)n * n, total = plane * B;
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
     const int b = (int)(k / plane);
@@ -101,6 +106,7 @@ __global__ void ens_mode_split_kernel(const ModeDesc* __restrict__ md, int B, in
     const size_t o = (size_t)b * plane + (size_t)y * n + xs;
     hi[o] = h;
     lo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
+    if (fm) fm[k] = v;
   }
 }
 
@@ -130,6 +136,7 @@ using namespace fvx::ens;
 
 struct fvx_ens {
   int method = 5;
+  int refine = 1;  // FP64-residual refinement passes per DST solve
   int nm = 0, nfields = 0, total_tiles = 0, blocks = 0, grid = 0;
   size_t smem = 0;
   std::vector<int> n, nl;
@@ -139,6 +146,7 @@ struct fvx_ens {
     int n = 0, B = 0, nlay = 0;
     fvx_dst_plan* plan = nullptr;
     float* psim = nullptr;
+    float* fm = nullptr;  // FP32 modes (refinement right-hand side)
     ModeDesc* md[3] = {nullptr, nullptr, nullptr};
     LayerDesc* ld = nullptr;
     __nv_bfloat16 *hi = nullptr, *lo = nullptr;
@@ -173,13 +181,10 @@ static void ens_free(fvx_ens* e) {
 template <int S>
 static int ens_stage_smem_and_blocks(int blocks_per_sm, int* blocks, size_t* smem) {
   *smem = qg::smem_bytes<float, S, TXE, TYE>();
-  static bool set = false;
-  if (!set) {
-    if (cudaFuncSetAttribute(ens_stage_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem) !=
-        cudaSuccess)
-      return FVX_ERR_CUDA;
-    set = true;
-  }
+  static fvx_once_per_device attr;
+  const int bytes = (int)*smem;
+  if (fvx_once_on_device(attr, [bytes] { return fvx_set_max_smem(ens_stage_kernel<S>, bytes); }))
+    return FVX_ERR_CUDA;
   int occ = 0, dev = 0, sms = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ens_stage_kernel<S>, qg::THREADS, *smem) != cudaSuccess ||
       cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
@@ -317,6 +322,7 @@ extern "C" int fvx_ens_create(int n_members, const int* n, const int* nl, const 
     g.lo = (__nv_bfloat16*)lo;
     g.perm = fvx_dst_operand_layout(g.plan);
     g.psim = (float*)A((size_t)g.B * sz * sz * 4);
+    g.fm = (float*)A((size_t)g.B * sz * sz * 4);
     for (int s = 0; s < 3; ++s) {
       g.md[s] = (ModeDesc*)A(md[s].size() * sizeof(ModeDesc));
       if (ok) cudaMemcpy(g.md[s], md[s].data(), md[s].size() * sizeof(ModeDesc), cudaMemcpyHostToDevice);
@@ -405,8 +411,17 @@ extern "C" int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm) {
 // Launches of one step (for the caller's launch count).
 extern "C" int fvx_ens_launches_per_step(fvx_ens* e) {
   if (!e) return -1;
-  // per stage: per group (mode split + 4 DST products + layer mix) + counter reset + stage kernel
-  return 3 * ((int)e->groups.size() * 6 + 2);
+  // per stage: per group (mode split + 4 DST products + refine passes x
+  // (residual + 4 products) + layer mix) + counter reset + stage kernel
+  return 3 * ((int)e->groups.size() * (6 + 5 * e->refine) + 2);
+}
+
+// FP64-residual refinement passes per DST solve (default 1; 0 leaves the
+// split chain's ~1e-5 relative error in psi).
+extern "C" int fvx_ens_set_refine(fvx_ens* e, int passes) {
+  if (!e || passes < 0 || passes > 4) return FVX_ERR_ARG;
+  e->refine = passes;
+  return FVX_OK;
 }
 
 // n_steps RK3-SSP steps of every member.
@@ -435,9 +450,13 @@ extern "C" int fvx_ens_step(fvx_ens* e, int n_steps, void* stream) {
         cudaStream_t gs = k == 0 ? st : e->gst[k - 1];
         if (k > 0 && cudaStreamWaitEvent(gs, e->fork, 0) != cudaSuccess) return FVX_ERR_CUDA;
         const size_t tot = (size_t)g.B * g.n * g.n;
-        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, gs>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm);
-        int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, (long long)g.n * g.n, g.n, g.B, gs);
+        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, gs>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm,
+                                                                  e->refine ? g.fm : nullptr);
+        const long long plane = (long long)g.n * g.n;
+        int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, plane, g.n, g.B, gs);
         if (rc) return rc;
+        if (e->refine && (rc = fvx_dst_refine_f32(g.plan, g.fm, plane, g.n, g.psim, plane, g.n, g.B, e->refine, gs)))
+          return rc;
         const size_t tl = (size_t)g.nlay * g.n * g.n;
         ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, gs>>>(g.ld, g.nlay, g.n, g.psim);
         if (k > 0 && cudaEventRecord(e->gdone[k - 1], gs) != cudaSuccess) return FVX_ERR_CUDA;

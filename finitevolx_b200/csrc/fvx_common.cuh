@@ -10,6 +10,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #define DEV __device__ __forceinline__
 
 enum fvx_status {
@@ -56,6 +58,33 @@ static inline int fvx_cuda_status() {
 }
 
 static inline cudaStream_t fvx_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Function attributes (cudaFuncSetAttribute) apply to the current device
+// only, and one process may drive several GPUs from several host threads:
+// a set-up step that must run once per device keeps one of these per site.
+struct fvx_once_per_device {
+  std::mutex mu;
+  bool done[128] = {};
+};
+
+// Runs set() (returns true on success) the first time it is reached with a
+// given device current; FVX_ERR_CUDA if set() fails (it runs again next time).
+template <typename Fn>
+static inline int fvx_once_on_device(fvx_once_per_device& once, Fn&& set) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return FVX_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(once.mu);
+  if (once.done[dev]) return FVX_OK;
+  if (!set()) return FVX_ERR_CUDA;
+  once.done[dev] = true;
+  return FVX_OK;
+}
+
+// cudaFuncAttributeMaxDynamicSharedMemorySize = bytes, once per device.
+template <typename K>
+static inline bool fvx_set_max_smem(K kernel, int bytes) {
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+}
 
 // ---- programmatic dependent launch ------------------------------------------
 // A kernel launched with fvx_launch_pdl may start while the kernel before it

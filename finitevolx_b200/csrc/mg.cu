@@ -747,6 +747,18 @@ extern "C" int fvx_mg_create(const double* mask, const double* coeff, int ny, in
         rc = FVX_ERR_CUDA;
     }
   }
+  if (!rc) {
+    // partial sums, omega and ticket of the hybrid cycle's energy-scaled
+    // coarse correction, allocated here so that no solve-time call allocates
+    const size_t bytes = (2 * kOmegaBlocks + 2) * sizeof(double);
+    if (cudaMalloc((void**)&g->omega_scratch, bytes) != cudaSuccess) {
+      g->omega_scratch = nullptr;
+      rc = FVX_ERR_CUDA;
+    } else {
+      g->allocs.push_back(g->omega_scratch);
+      if (cudaMemset(g->omega_scratch, 0, bytes) != cudaSuccess) rc = FVX_ERR_CUDA;
+    }
+  }
   if (rc) { mg_free(g); delete g; return rc; }
   if (cudaDeviceSynchronize() != cudaSuccess) { mg_free(g); delete g; return FVX_ERR_CUDA; }
   *out = g;
@@ -779,21 +791,12 @@ extern "C" int fvx_mg_num_levels(fvx_mg* g) { return g ? g->nl : -1; }
 
 template <typename T>
 static int leg_attr() {
-  static bool done = false;
-  if (!done) {
+  static fvx_once_per_device attr;
+  return fvx_once_on_device(attr, [] {
     const int bytes = (int)leg_smem<T>(kLegMaxSweeps);
-    if (cudaFuncSetAttribute(down_leg_kernel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(up_leg_kernel<T, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(down_leg_kernel<T, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(up_leg_kernel<T, 1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) !=
-            cudaSuccess)
-      return FVX_ERR_CUDA;
-    done = true;
-  }
-  return FVX_OK;
+    return fvx_set_max_smem(down_leg_kernel<T, 256>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 256>, bytes) &&
+           fvx_set_max_smem(down_leg_kernel<T, 1024>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 1024>, bytes);
+  });
 }
 
 // The single-CTA coarse V-cycle from level l.
@@ -949,12 +952,6 @@ static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int
   if (coarse) {
     if ((rc = coarse(ctx, C.f, C.u, st))) return rc;
     if (scale) {
-      if (!g->omega_scratch) {
-        if (cudaMalloc((void**)&g->omega_scratch, (2 * kOmegaBlocks + 2) * sizeof(double)) != cudaSuccess)
-          return FVX_ERR_CUDA;
-        g->allocs.push_back(g->omega_scratch);
-        cudaMemsetAsync(g->omega_scratch, 0, (2 * kOmegaBlocks + 2) * sizeof(double), st);
-      }
       double* part = g->omega_scratch;
       double* om = part + 2 * kOmegaBlocks;
       unsigned* ticket = (unsigned*)(om + 1);

@@ -21,13 +21,9 @@ namespace qg {
 template <typename T, int S, int TX, int TY>
 static int launch_t(const StageArgs& a, cudaStream_t st) {
   size_t sm = smem_bytes<T, S, TX, TY>();
-  static bool set = false;
-  if (!set) {
-    if (cudaFuncSetAttribute(stage_kernel<T, S, TX, TY>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) !=
-        cudaSuccess)
-      return FVX_ERR_CUDA;
-    set = true;
-  }
+  static fvx_once_per_device attr;
+  if (fvx_once_on_device(attr, [sm] { return fvx_set_max_smem(stage_kernel<T, S, TX, TY>, (int)sm); }))
+    return FVX_ERR_CUDA;
   const TileSplit ts = tile_split<S, TX, TY>(a.ny, a.nx);
   if (fvx_launch_pdl(stage_kernel<T, S, TX, TY>, dim3(ts.ntx * ts.nty), dim3(THREADS), sm, st, a, ts) !=
       cudaSuccess)

@@ -128,14 +128,12 @@ static int launch_conv_tile(const float* in, int mode, int batch, int cin, const
                             cudaStream_t st, bool pdl) {
   constexpr int NT = T * T * (COUT / CPT);
   const size_t smem = ((size_t)cin * 9 * COUT + (size_t)cin * (T + 2) * (T + 2)) * sizeof(float);
-  static bool attr_set = false;  // per instantiation; the largest use needs > 48 KB
-  if (!attr_set) {
-    const int max_smem = (CMAX * 9 * COUT + CMAX * (T + 2) * (T + 2)) * (int)sizeof(float);
-    if (cudaFuncSetAttribute(conv_tile_kernel<COUT, CPT, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             max_smem) != cudaSuccess)
-      return FVX_ERR_CUDA;
-    attr_set = true;
-  }
+  static fvx_once_per_device attr;  // per instantiation; the largest use needs > 48 KB
+  if (fvx_once_on_device(attr, [] {
+        const int max_smem = (CMAX * 9 * COUT + CMAX * (T + 2) * (T + 2)) * (int)sizeof(float);
+        return fvx_set_max_smem(conv_tile_kernel<COUT, CPT, T>, max_smem);
+      }))
+    return FVX_ERR_CUDA;
   dim3 g((w + T - 1) / T, (h + T - 1) / T, batch);
   if (pdl) {
     if (fvx_launch_pdl(conv_tile_kernel<COUT, CPT, T>, g, dim3(NT), smem, st, in, mode, cin, wb, bias, skip, out, h,

@@ -31,7 +31,8 @@ class QGEnsemble:
     dt = cfl * dx / umax per member; beta, f0 shared."""
 
     def __init__(self, members, Lx: float = 5.12e6, beta: float = 1.7e-11, f0: float = 9.375e-5,
-                 H=H_DEFAULT, gprime=GPRIME_DEFAULT, method: str = "weno5", cfl: float = 0.5, umax: float = 1.0):
+                 H=H_DEFAULT, gprime=GPRIME_DEFAULT, method: str = "weno5", cfl: float = 0.5, umax: float = 1.0,
+                 refine_passes: int = 1):
         require_cuda()
         self.members = [(int(n), int(nl)) for n, nl in members]
         self.Lx, self.beta, self.f0, self.method = float(Lx), float(beta), float(f0), method
@@ -59,6 +60,16 @@ class QGEnsemble:
                                    arr(dxs, ctypes.c_double), arr(dxs, ctypes.c_double),
                                    arr(dts, ctypes.c_double), ctypes.c_double(beta), I(SCHEMES[method]),
                                    ctypes.byref(self._h)), "ensemble create")
+        self._graph = None
+        self.set_refine(refine_passes)
+
+    def set_refine(self, passes: int) -> None:
+        """FP64-residual refinement passes after each DST solve: the split
+        tensor-core chain carries its intermediates in 16 bits (about 1e-5
+        relative error in psi, amplified by the velocity differences in
+        weakly screened members); one pass brings psi to FP32 rounding."""
+        check(fn("fvx_ens_set_refine")(self._h, I(int(passes))), "ensemble refine")
+        self.refine_passes = int(passes)
         self._graph = None
 
     def __del__(self):

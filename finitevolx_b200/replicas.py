@@ -52,3 +52,58 @@ def shard_members(members, rank: int, world: int):
         owner[i] = r
         load[r] += cost[i]
     return [i for i in range(len(members)) if owner[i] == rank]
+
+
+def _cuda_ms(run) -> float:
+    """Device milliseconds of run() on the current stream (CUDA events)."""
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    run()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _reduce_device():
+    if dist.is_available() and dist.is_initialized() and dist.get_backend() == "nccl":
+        return "cuda"
+    return None
+
+
+def sharded_ensemble_run(members, n_steps: int, factory, timer=None) -> dict:
+    """Runs an ensemble sharded by members: this rank builds
+    ``factory(sub_members, global_indices)`` (an object with ``capture(n)``
+    returning a replayable graph and ``launches_per_step``) from the members
+    ``shard_members`` assigns it, replays its graph once untimed, then times
+    one replay of ``n_steps`` steps between barriers.  No collective runs
+    inside the step; the only ones are the barrier and the reductions of
+    the time (maximum over ranks) and of the per-rank member counts.
+
+    Returns the slowest rank's time, the whole-job rate (interior
+    layer-cells of all members x steps / s / 1e6), this rank's members and
+    the member count of every rank."""
+    rank, world = world_info()
+    mine = shard_members(members, rank, world)
+    sub = [members[i] for i in mine]
+    ens = factory(sub, mine) if sub else None
+    graph = ens.capture(n_steps) if ens is not None else None
+    run = graph.replay if graph is not None else (lambda: None)
+    run()  # warm-up replay
+    timer = timer or _cuda_ms
+    if world > 1:
+        dist.barrier()
+    ms = timer(run)
+    dev = _reduce_device()
+    t_max = max_over_ranks(ms, device=dev)
+    counts = torch.zeros(world, dtype=torch.float64, device=dev)
+    counts[rank] = len(mine)
+    if world > 1:
+        dist.all_reduce(counts)
+        dist.barrier()
+    cells = sum(int(n) * int(n) * int(nl) for n, nl in members)
+    return {"rank": rank, "world": world, "mine": mine, "t_max_ms": t_max, "rank_ms": ms,
+            "cells_per_step": cells, "value": cells * n_steps / (t_max * 1e-3) / 1e6 if t_max > 0 else 0.0,
+            "members_per_rank": [int(c) for c in counts.tolist()],
+            "launches_per_step": getattr(ens, "launches_per_step", 0) if ens is not None else 0}

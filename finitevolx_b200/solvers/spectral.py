@@ -126,7 +126,13 @@ class DSTHelmholtzPlan:
         return out, res
 
     def check_device(self):
+        """Raises if a bounded device wait of the plan's products gave up
+        since the last check (the flag is cleared once reported)."""
         check(fn("fvx_dst_plan_check")(self._h, stream_ptr()), "DST kernels")
+
+    def set_wait_limit(self, cycles: int) -> None:
+        """Bound, in SM clock cycles, on each barrier wait of the products."""
+        check(fn("fvx_dst_plan_set_wait_limit")(self._h, ctypes.c_longlong(int(cycles))), "wait limit")
 
 
 _CACHE: dict = {}

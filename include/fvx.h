@@ -186,6 +186,16 @@ int fvx_capacitance_rhs_f64(const double* f, const double* u, const double* cinv
                             long long n, double* out, void* stream);
 /* Reads the plan's device error flag (7 if a bounded wait gave up); syncs. */
 int fvx_dst_plan_check(fvx_dst_plan* plan, void* stream);
+/* Bound on every barrier wait inside the plan's tensor-core products, in SM
+ * clock cycles (>= 1000; default 4e9, about 2 s): a wait that runs out ends
+ * its CTA without trapping (after the copies and MMAs it issued have
+ * landed) and sets the flag fvx_dst_plan_check reports (7) and then clears.
+ * No counterpart in finitevolX (its XLA solve has no device waits). */
+int fvx_dst_plan_set_wait_limit(fvx_dst_plan* plan, long long cycles);
+/* Fault injection for tests only (no counterpart in finitevolX): while on,
+ * the single-CTA products' producers issue no loads, so every product's
+ * first wait runs out after the wait limit with nothing in flight. */
+int fvx_dst_plan_inject_stall(fvx_dst_plan* plan, int on);
 /* FP32: 3xBF16 split tcgen05 chain (ny, nx multiples of 8; otherwise the
  * FP64 chain with FP32 output).  Element (b,y,x) at ptr[b*bstride + y*ld + x]. */
 int fvx_dst_solve_f32(fvx_dst_plan* plan, const float* rhs, long long rhs_bstride, long long rhs_ld, float* psi,
@@ -202,6 +212,14 @@ int fvx_dst_solve_f64(fvx_dst_plan* plan, const double* rhs, long long rhs_bstri
  * even/odd products of plans with ny, nx multiples of 256). */
 int fvx_dst_solve_presplit_f32(fvx_dst_plan* plan, float* psi, long long psi_bstride, long long psi_ld, int batch,
                                void* stream);
+/* FP64-residual iterative refinement of an FP32 Dirichlet result (the
+ * accuracy step spectraldiffx's FP64 solve_helmholtz_dst does not need, and
+ * this split-precision chain does): ``passes`` times r = rhs - (lap -
+ * lambda) psi in FP64 from the FP32 arrays, psi += chain(r).  One pass
+ * brings the chain's ~1e-5 relative error down to psi's FP32 rounding.
+ * Overwrites the plan's first workspace; no host synchronisation. */
+int fvx_dst_refine_f32(fvx_dst_plan* plan, const float* rhs, long long rhs_bstride, long long rhs_ld, float* psi,
+                       long long psi_bstride, long long psi_ld, int batch, int passes, void* stream);
 int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
 int fvx_dst_operand_layout(fvx_dst_plan* plan);
 /* One product of the chain on the current workspaces (timing only). */
@@ -227,6 +245,15 @@ int fvx_dst_kernel_config(int kind);
  * share the array: calls that overlap on the GPU race. */
 int fvx_dst_solve_noalloc_f32(const float* rhs, long long rhs_ld, float* psi, long long psi_ld, int ny, int nx,
                               double dx, double dy, double lambda, void* stream);
+/* Companion of fvx_dst_solve_noalloc_f32 (no counterpart in the reference):
+ * the tensor-core products wait on barriers with a time limit, and a wait
+ * that gives up sets an error flag in the scratch array instead of
+ * trapping, while the solve itself has already returned 0.  This copies the
+ * flag to the host on ``stream``, waits for the stream, and returns 7
+ * (timeout: psi is incomplete) if it is set, 0 if not or if no
+ * allocation-free solve ran on the current device.  Each solve clears the
+ * flag, so check after every solve whose result matters. */
+int fvx_dst_noalloc_check(void* stream);
 
 /* ---- fused QG RK stage ---------------------------------------------------- */
 
@@ -396,6 +423,10 @@ int fvx_ens_destroy(fvx_ens* e);
 int fvx_ens_io(fvx_ens* e, int member, int layer, const void* src, void* dst, void* stream);
 int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm);
 int fvx_ens_launches_per_step(fvx_ens* e);
+/* FP64-residual refinement passes after each batched DST solve (0-4,
+ * default 1: the members' psi at FP32 rounding instead of the split
+ * chain's ~1e-5; no counterpart in finitevolX, whose solve is FP64). */
+int fvx_ens_set_refine(fvx_ens* e, int passes);
 int fvx_ens_step(fvx_ens* e, int n_steps, void* stream);
 
 /* ---- diagnostics (operators/diagnostics.py) -------------------------------- */

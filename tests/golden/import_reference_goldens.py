@@ -20,6 +20,9 @@ PREFIXES = (
     "Diffusion2D__",
     "BiharmonicDiffusion2D__",
     "Divergence2D__",
+    "Coriolis2D__",
+    "Vorticity2D__",
+    "MomentumAdvection2D__",
 )
 
 
@@ -37,4 +40,6 @@ def main(ref_root: str) -> int:
 
 
 if __name__ == "__main__":
-    sys.exit(main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/import_reference_goldens.py /path/to/finitevolX")
+    sys.exit(main(sys.argv[1]))

@@ -256,3 +256,50 @@ def test_qg_step_fp32_forcing_drag_viscosity(cuda_ok, n, method):
     # the extra terms change the step by far more than the bar
     plain = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, method)
     assert rel_err(plain, ref) > 1e-4
+
+
+def test_qg_step_fp32_2048_within_1e5(cuda_ok):
+    # the benchmarked configuration: 2048^2 interior, Ld = 40 km, WENO5,
+    # periodic q, DST psi, one rk3_ssp_step at CFL 0.5 for max|u| = 1 m/s;
+    # 1e-5 relative on q_{n+1} against the FP64 oracle (about 10 s of CPU)
+    n = 2048
+    grid, q = qg_setup(n, torch.float32, 11)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method="weno5", dtype=torch.float32)
+    from finitevolx_b200._lib import fn
+    assert fn("fvx_dst_operand_layout")(m.plan.handle) == 1  # the even/odd tensor-core products
+    got = host(m.step(dev(q, torch.float32), dt))
+    m.plan.check_device()
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, "weno5")
+    assert rel_err(got, ref) < 1e-5
+    # and the step's increment itself is resolved (not hidden under q_n)
+    assert rel_err(got - q, ref - q) < 1e-3
+
+
+def test_qg_step_fp64_256_within_1e12(cuda_ok):
+    # the metric's own configuration: 256^2 interior, FP64, Ld = 40 km, WENO5
+    n = 256
+    grid, q = qg_setup(n, torch.float64, 12)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method="weno5", dtype=torch.float64)
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, "weno5")
+    got = host(m.step(dev(q), dt))
+    assert rel_err(got, ref) < 1e-12
+    assert rel_err(got - q, ref - q) < 1e-9
+
+
+@pytest.mark.parametrize("n,ld", [(128, 6.7e5), (512, 4.0e6)])
+def test_qg_step_fp32_refined_weak_screening(cuda_ok, n, ld):
+    # weakly screened fields (lambda dx^2 << 1): the plain split chain misses
+    # the FP32 bar, one FP64-residual refinement pass per solve meets it
+    grid, q = qg_setup(n, torch.float32, 13)
+    lam, beta, dt = 1.0 / ld ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    ref = O.qg_step(q.astype(np.float32).astype(np.float64), grid.dx, grid.dy, beta, lam, dt, "weno5")
+    plain = QGModel(grid, beta, lam, method="weno5", dtype=torch.float32)
+    refined = QGModel(grid, beta, lam, method="weno5", dtype=torch.float32, dst_refine=1)
+    assert rel_err(host(plain.step(dev(q, torch.float32), dt)), ref) > 1e-5
+    assert rel_err(host(refined.step(dev(q, torch.float32), dt)), ref) < 1e-5
+    # the refined unfused path (separate split pass) agrees
+    refined.fuse_split = False
+    assert rel_err(host(refined.step(dev(q, torch.float32), dt)), ref) < 1e-5
+    refined.plan.check_device()

@@ -266,3 +266,45 @@ def test_vertical_modes_roundtrip():
     rr, l2m, m2l = O.decompose_vertical_modes(A, 1e-4)
     np.testing.assert_allclose(l2m @ m2l, np.eye(3), atol=1e-12)
     assert rr.shape == (3,)
+
+
+# ---------------------------------------------------------------------------
+# Shallow-water operators: Coriolis2D (operators/coriolis.py:86-133),
+# Vorticity2D (operators/vorticity.py:60-235), MomentumAdvection2D
+# (diffusion/momentum.py:108-216); goldens from finitevolX
+# tests/fixtures/_gen_golden.py:477-547 (vorticity), :852-864 (momentum),
+# :968-987 (Coriolis), f = 1 + 0.1 y (tests/fixtures/inputs.py:284-287).
+# ---------------------------------------------------------------------------
+
+def _pair(g):
+    return g["out0"], g["out1"]
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_coriolis2d_golden(F, M, variant):
+    mask = M if variant == "masked" else None
+    for got, ref in zip(O.coriolis2d(F["u"], F["v"], F["f"], mask), _pair(golden("Coriolis2D", "__call__", variant))):
+        np.testing.assert_allclose(got, ref, rtol=RTOL, atol=ATOL)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_vorticity2d_golden(F, M, variant):
+    mask = M if variant == "masked" else None
+    g = golden("Vorticity2D", "relative_vorticity", variant)["out"]
+    np.testing.assert_allclose(O.diff2d("curl", F["u"], DX, DY, mask, F["v"]), g, rtol=RTOL, atol=ATOL)
+    g = golden("Vorticity2D", "potential_vorticity", variant)["out"]
+    np.testing.assert_allclose(O.potential_vorticity_x(F["u"], F["v"], F["h"], F["f"], DX, DY, mask), g,
+                               rtol=RTOL, atol=ATOL)
+    for scheme, name in (("energy", "pv_flux_energy_conserving"), ("enstrophy", "pv_flux_enstrophy_conserving"),
+                         ("al", "pv_flux_arakawa_lamb")):
+        got = O.pv_flux(F["q"], F["u"], F["v"], scheme, mask=mask)
+        for a, b in zip(got, _pair(golden("Vorticity2D", name, variant))):
+            np.testing.assert_allclose(a, b, rtol=RTOL, atol=ATOL, err_msg=name)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_momentum_advection2d_golden(F, M, variant):
+    mask = M if variant == "masked" else None
+    got = O.momentum_advection(F["u"], F["v"], DX, DY, "energy", mask)
+    for a, b in zip(got, _pair(golden("MomentumAdvection2D", "__call__", variant))):
+        np.testing.assert_allclose(a, b, rtol=RTOL, atol=ATOL)

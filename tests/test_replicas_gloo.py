@@ -9,7 +9,8 @@ import pytest
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from finitevolx_b200.replicas import max_over_ranks, shard_members, whole_job_rate, world_info
+from finitevolx_b200.replicas import (max_over_ranks, shard_members, sharded_ensemble_run, whole_job_rate,
+                                      world_info)
 
 
 def _free_port() -> int:
@@ -64,3 +65,59 @@ def test_shard_members_balances_and_covers():
 def test_single_process_defaults():
     assert world_info() == (0, 1)
     assert max_over_ranks(3.5) == 3.5
+
+
+class _StubEnsemble:
+    """Stands in for QGEnsemble on CPU: records which global members it
+    holds and how many steps each replay advances them."""
+
+    def __init__(self, idx, log):
+        self.idx, self.log, self.launches_per_step = list(idx), log, 7
+
+    def capture(self, n):
+        stub = self
+
+        class G:
+            def replay(self):
+                for i in stub.idx:
+                    stub.log[i] = stub.log.get(i, 0) + n
+        return G()
+
+
+def _ens_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=__import__("datetime").timedelta(seconds=60))
+    try:
+        members = [(128, 1), (256, 3), (512, 2), (1024, 1), (256, 1), (128, 3), (512, 1)]
+        log = {}
+        times = iter([5.0 + rank])  # one timed replay per rank, rank 1 slower
+        r = sharded_ensemble_run(members, 3, lambda sub, idx: _StubEnsemble(idx, log),
+                                 timer=lambda run: (run(), next(times))[1])
+        out[rank] = (r, dict(log))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_ensemble_run_covers_every_member_once():
+    world = 2
+    port = _free_port()
+    with mp.Manager() as mgr:
+        out = mgr.dict()
+        mp.spawn(_ens_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    members = [(128, 1), (256, 3), (512, 2), (1024, 1), (256, 1), (128, 3), (512, 1)]
+    logs = [res[r][1] for r in range(world)]
+    # every member lives on exactly one rank and was stepped by the warm-up
+    # replay and the timed replay (2 x 3 steps)
+    assert sorted(i for lg in logs for i in lg) == list(range(len(members)))
+    assert all(v == 6 for lg in logs for v in lg.values())
+    for rank in range(world):
+        r = res[rank][0]
+        assert r["t_max_ms"] == 6.0 and r["world"] == world
+        assert sum(r["members_per_rank"]) == len(members)
+        cells = sum(n * n * nl for n, nl in members)
+        assert r["cells_per_step"] == cells
+        assert r["value"] == pytest.approx(cells * 3 / 6e-3 / 1e6)
+        assert sorted(r["mine"]) == sorted(res[rank][1])
