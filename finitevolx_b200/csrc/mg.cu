@@ -243,6 +243,28 @@ coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n
   coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
 }
 
+// The coarse part of an FP32 plan's V-cycle in FP64: level l's right-hand
+// side is widened into the FP64 copy of levels l .. nl-1 (operators built
+// from the same FP64 host hierarchy), the single-CTA cycle (restriction,
+// sweeps, the coarsest-level solve, prolongation) runs in FP64, and the
+// correction is rounded back into the FP32 level.
+__global__ void __launch_bounds__(kCoarseThreads)
+coarse_vcycle_f64_kernel(LevArray<float> A, LevArray<double> D, int lc, int nl, int n_pre, int n_post,
+                         int n_coarse, double omega) {
+  __shared__ Lev<double> S[kMaxLevels];
+  if (threadIdx.x < nl) S[threadIdx.x] = D.L[threadIdx.x];
+  __syncthreads();
+  const size_t cells = (size_t)A.L[lc].ny * A.L[lc].nx;
+  const float* f32 = A.L[lc].f;
+  double* f64 = S[lc].f;
+  for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) f64[c] = (double)f32[c];
+  __syncthreads();
+  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
+  float* u32 = A.L[lc].u;
+  const double* u64 = S[lc].u;
+  for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) u32[c] = (float)u64[c];
+}
+
 // Many independent solves of A_lc u = f at level lc, one CTA per right-hand
 // side: u = sum of n_cycles V-cycle corrections, u += V(f - A u).  Each
 // block's level arrays u, f, tmp come from its own slice of ``work``
@@ -610,7 +632,7 @@ struct fvx_mg {
   double omega = 0.95, lam = 0.0;
   std::vector<void*> allocs;
   LevArray<float> A32;
-  LevArray<double> A64;
+  LevArray<double> A64;  // FP64 plans: every level; FP32 plans: the coarse levels lc .. nl-1
   Lev<double> L0d;  // finest operator in FP64 (residual checks of FP32 solves)
 };
 
@@ -656,9 +678,9 @@ static void host_level_ops(HostLevel& L, double lam) {
 }
 
 template <typename T>
-static int upload_levels(fvx_mg* g, std::vector<HostLevel>& H) {
+static int upload_levels(fvx_mg* g, std::vector<HostLevel>& H, int first = 0) {
   LevArray<T>& A = levs<T>(g);
-  for (int l = 0; l < g->nl; ++l) {
+  for (int l = first; l < g->nl; ++l) {
     HostLevel& h = H[l];
     Lev<T>& L = A.L[l];
     L.ny = h.ny; L.nx = h.nx;
@@ -734,6 +756,10 @@ extern "C" int fvx_mg_create(const double* mask, const double* coeff, int ny, in
   g->lc = n_levels - 1;
   while (g->lc > 0 && (size_t)H[g->lc - 1].ny * H[g->lc - 1].nx <= (size_t)kCoarseCells) --g->lc;
   int rc = dtype == 0 ? upload_levels<float>(g, H) : upload_levels<double>(g, H);
+  // FP32 plans keep an FP64 copy of the single-CTA coarse levels: the
+  // coarse part of every V-cycle, the coarsest-level solve included, runs
+  // in FP64
+  if (!rc && dtype == 0) rc = upload_levels<double>(g, H, g->lc);
   if (!rc) {
     Lev<double>& D = g->L0d;
     D.ny = ny; D.nx = nx; D.dx2 = dx * dx; D.dy2 = dy * dy; D.rdx2 = 1.0 / (dx * dx); D.rdy2 = 1.0 / (dy * dy);
@@ -799,11 +825,15 @@ static int leg_attr() {
   });
 }
 
-// The single-CTA coarse V-cycle from level l.
+// The single-CTA coarse V-cycle from level l (FP32 plans: in FP64).
 template <typename T>
 static int coarse_vcycle(fvx_mg* g, int l, cudaStream_t st) {
-  coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(levs<T>(g), l, g->nl, g->n_pre, g->n_post, g->n_coarse,
-                                                        (T)g->omega);
+  if constexpr (sizeof(T) == 4)
+    coarse_vcycle_f64_kernel<<<1, kCoarseThreads, 0, st>>>(g->A32, g->A64, l, g->nl, g->n_pre, g->n_post,
+                                                           g->n_coarse, g->omega);
+  else
+    coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(levs<T>(g), l, g->nl, g->n_pre, g->n_post, g->n_coarse,
+                                                          (T)g->omega);
   return fvx_cuda_status();
 }
 

@@ -47,10 +47,11 @@ def test_dst_split_bf16_chain(cuda_ok, shape, lam):
     assert e < 1e-4, e
 
 
-@pytest.mark.parametrize("shape", [(256, 512), (512, 256), (768, 512)])
+@pytest.mark.parametrize("shape", [(256, 512), (512, 256), (768, 512), (2048, 2048)])
 def test_dst_product_forms_agree(cuda_ok, shape):
-    # the even/odd products on single CTAs (64- and 32-element K blocks) and
-    # on CTA pairs (cta_group::2, B blocks shared by the pair): the same
+    # the even/odd products on single CTAs (64- and 32-element K blocks), on
+    # CTA pairs (cta_group::2, B blocks shared by the pair) and on the
+    # persistent grid (64-column tiles, two TMEM accumulators): the same
     # 3xBF16 sums in another k order.  All within the chain's 1e-4 of the
     # oracle; against each other within 5e-5: an intermediate that differs
     # by one FP32 ulp can round to another bf16 hi/lo pair, which moves it by
@@ -303,3 +304,24 @@ def test_qg_step_fp32_refined_weak_screening(cuda_ok, n, ld):
     refined.fuse_split = False
     assert rel_err(host(refined.step(dev(q, torch.float32), dt)), ref) < 1e-5
     refined.plan.check_device()
+
+
+@pytest.mark.parametrize("lam", [0.0, 1.0 / 1e4 ** 2])
+def test_dst_refinement_1024_batched(cuda_ok, lam):
+    # config 3's size and batching (a 16-RHS slice of its 64): split chain +
+    # FP64 refinement to a 1e-12 backward error; every result within 1e-10
+    # of the FP64 DST oracle
+    n, b = 1024, 16
+    dx = 5.12e6 / n
+    f = np.stack([O.kminus3_field(n, n, 40 + k, std=1e-5) for k in range(b)])
+    plan = DSTHelmholtzPlan(n, n, dx, dx, (lam,), batch_max=b)
+    psi, info = plan.solve_refined(dev(f), tol=1e-12)
+    assert info["converged"] and info["backward_error"] <= 1e-12, info
+    plan.check_device()
+    ref = O.solve_helmholtz_dst(f, dx, dx, lam)
+    got = host(psi)
+    errs = [rel_err(got[k], ref[k]) for k in range(b)]
+    assert max(errs) < 1e-10, errs
+    # the FP32 chain on the same batch: the split chain's ~1e-5
+    p32 = host(plan.solve(dev(f, torch.float32)))
+    assert max(rel_err(p32[k], ref[k]) for k in range(b)) < 1e-4

@@ -94,6 +94,20 @@ def test_mg_fine_levels_host_driven_path(cuda_ok):
     assert rel(host(mg.v_cycle(None, dev(f))), O.mg_vcycle(ref, np.zeros_like(f), f)) < 1e-10
 
 
+def test_mg_fp32_plan_coarse_part_in_fp64(cuda_ok):
+    # 32^2: the whole V-cycle is the single-CTA coarse part, which FP32
+    # plans run in FP64 (the coarsest-grid solve included): the result is
+    # the FP64 cycle rounded once to FP32 (an FP32 cycle would be ~1e-6 off)
+    n = 32
+    m = basin(n, 17)
+    c = coeff(n, 18)
+    mg = fvx.build_multigrid_solver(m, 1.0 / n, 1.0 / n, lambda_=2.0, coeff=c, dtype=torch.float32)
+    ref = O.mg_build(m, 1.0 / n, 1.0 / n, lambda_=2.0, coeff=c)
+    f = (np.random.default_rng(19).standard_normal((n, n)) * m).astype(np.float32).astype(np.float64)
+    got = host(mg.v_cycle(None, dev(f, torch.float32)))
+    assert rel(got, O.mg_vcycle(ref, np.zeros_like(f), f)) < 2e-7
+
+
 def test_mg_shape_error(cuda_ok):
     with pytest.raises(ValueError):
         fvx.build_multigrid_solver(np.ones((24, 24)), 1.0, 1.0, n_levels=5)
