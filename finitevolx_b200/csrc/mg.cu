@@ -362,19 +362,24 @@ template <typename T> struct LegTile;
 template <> struct LegTile<float> { static constexpr int TX = 64, TY = 32; };
 template <> struct LegTile<double> { static constexpr int TX = 32, TY = 16; };
 
+// One weighted-Jacobi update on a shared-memory tile whose u is already
+// masked (zero on dry cells) and whose winv holds omega * inv_diag (zero on
+// dry cells): jacobi_at's arithmetic with the multiplications by the 0/1
+// mask dropped.  On a wet cell those multiply by 1 (exact); on a dry cell
+// the result is u + 0 * r = 0, as the masked form gives (up to the sign of
+// zero), so the values are the same.
 template <typename T>
-DEV T jac_s(const T* u, const T* f, const T* m, const T* cx, const T* cy, const T* inv, int k, int RW, T dx2,
-            T rdx2, T dy2, T rdy2, T lam, T omega) {
-  const T mc = m[k];
-  const T um = u[k] * mc;
-  const T ue = u[k + 1] * m[k + 1];
-  const T uw = u[k - 1] * m[k - 1];
-  const T un = u[k + RW] * m[k + RW];
-  const T us = u[k - RW] * m[k - RW];
+DEV T jac_s(const T* u, const T* f, const T* cx, const T* cy, const T* winv, int k, int RW, T dx2, T rdx2, T dy2,
+            T rdy2, T lam) {
+  const T um = u[k];
+  const T ue = u[k + 1];
+  const T uw = u[k - 1];
+  const T un = u[k + RW];
+  const T us = u[k - RW];
   const T lap = divd(cx[k] * (ue - um) - cx[k - 1] * (um - uw), dx2, rdx2) +
                 divd(cy[k] * (un - um) - cy[k - RW] * (um - us), dy2, rdy2);
-  const T r = f[k] - (lap - lam * um) * mc;
-  return (u[k] + omega * inv[k] * r) * mc;
+  const T r = f[k] - (lap - lam * um);
+  return um + winv[k] * r;
 }
 
 template <typename T>
@@ -416,9 +421,9 @@ static size_t leg_smem(int k) {
 }
 
 // Shared-memory tile (origin (y0, x0), RW wide, RN cells) of the level's
-// mask, cx, cy and inv_diag, zero outside the level.
+// mask, cx, cy and omega * inv_diag, zero outside the level.
 template <typename T>
-DEV void leg_load_tile(const Lev<T>& L, int x0, int y0, int RW, int RN, T* sm, T* scx, T* scy, T* sinv) {
+DEV void leg_load_tile(const Lev<T>& L, int x0, int y0, int RW, int RN, T* sm, T* scx, T* scy, T* sinv, T omega) {
   for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
     T v[4][4];
 #pragma unroll
@@ -436,7 +441,7 @@ DEV void leg_load_tile(const Lev<T>& L, int x0, int y0, int RW, int RN, T* sm, T
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int q = q0 + u * blockDim.x;
-      if (q < RN) { sm[q] = v[u][0]; scx[q] = v[u][1]; scy[q] = v[u][2]; sinv[q] = v[u][3]; }
+      if (q < RN) { sm[q] = v[u][0]; scx[q] = v[u][1]; scy[q] = v[u][2]; sinv[q] = omega * v[u][3]; }
     }
   }
 }
@@ -484,17 +489,21 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
   // the level's constant arrays, then (after the previous kernel, which
   // wrote f and u_init) f and u_init; batches of 4 cells per thread, all
   // loads of a batch in flight before any store
-  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv);
+  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv, omega);
   grid_dep_wait();
   leg_load_pair(L, x0, y0, RW, RN, f, sf, u_init, sa);
   __syncthreads();
   grid_dep_launch();  // the next kernel may start loading its constants
+  if (u_init) {  // the sweeps take u masked (each thread its own cells)
+    for (int q = threadIdx.x; q < RN; q += blockDim.x) sa[q] *= sm[q];
+    __syncthreads();
+  }
   T* a = sa;
   T* b = sb;
   for (int s = 1; s <= k; ++s) {
     leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
       const int kk = ly * RW + lx;
-      b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
+      b[kk] = jac_s(a, sf, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
     });
     __syncthreads();
     T* t = a; a = b; b = t;
@@ -552,7 +561,7 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
   T* scm = sv + CW * CH;  // coarse mask
   // constants first; the coarse correction ec, f and u_pre come from the
   // kernels before this one
-  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv);
+  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv, omega);
   grid_dep_wait();
   for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
     const int J = CY0 + q / CW, I = CX0 + q % CW;
@@ -583,12 +592,12 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
     sb[q] = u;
   });
   __syncthreads();
-  T* a = sb;  // u_pre + P e
+  T* a = sb;  // u_pre + P e, masked
   T* b = sa;
   for (int s = 1; s <= k; ++s) {
     leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
       const int kk = ly * RW + lx;
-      b[kk] = jac_s(a, sf, sm, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam, omega);
+      b[kk] = jac_s(a, sf, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
     });
     __syncthreads();
     T* t = a; a = b; b = t;

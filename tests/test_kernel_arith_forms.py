@@ -93,3 +93,31 @@ def test_division_free_walk_visits_the_same_cells(h, w, nthreads):
     for tid in range(nthreads):
         ref = [divmod(c, w) for c in range(tid, n, nthreads)]
         assert _walk(n, w, nthreads, tid) == ref
+
+
+def test_mask_free_jacobi_equals_masked_form():
+    # the multigrid legs' sweeps drop the multiplications by the 0/1 mask:
+    # u is kept masked, inv_diag (mask-multiplied by construction) carries
+    # omega; on wet cells the dropped factors are 1, on dry cells both forms
+    # give zero -- the same values as jacobi_at (multigrid.py:408-461)
+    import oracle.fvx_oracle as O
+    rng = np.random.default_rng(3)
+    n = 40
+    mask = (rng.random((n, n)) > 0.3).astype(np.float64)
+    mask[0, :] = mask[-1, :] = mask[:, 0] = mask[:, -1] = 0.0
+    coeff = np.exp(0.5 * rng.standard_normal((n, n)))
+    L = O.mg_build(mask, 0.1, 0.1, lambda_=2.0, coeff=coeff, n_levels=1)["levels"][0]
+    u = rng.standard_normal((n, n)) * mask
+    f = rng.standard_normal((n, n))
+    omega = 0.95
+    ref = O.mg_jacobi(u, f, L, omega, 1)
+    pad = lambda a: np.pad(a, 1)  # noqa: E731
+    up, cxp, cyp = pad(u), pad(L["cx"]), pad(L["cy"])
+    c = (slice(1, -1), slice(1, -1))
+    um, ue, uw = up[c], up[1:-1, 2:], up[1:-1, :-2]
+    un, us = up[2:, 1:-1], up[:-2, 1:-1]
+    lap = (cxp[c] * (ue - um) - cxp[1:-1, :-2] * (um - uw)) / 0.1 ** 2 + \
+          (cyp[c] * (un - um) - cyp[:-2, 1:-1] * (um - us)) / 0.1 ** 2
+    r = f - (lap - 2.0 * um)
+    got = um + (omega * L["inv"]) * r
+    np.testing.assert_array_equal(got, ref)
