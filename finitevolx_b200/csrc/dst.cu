@@ -1179,29 +1179,34 @@ __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long
                                 long long pb, long long pld, int ny, int nx, int batch, double dx, double dy,
                                 const double* __restrict__ lam, int nlam, bf16* __restrict__ hi,
                                 bf16* __restrict__ lo, double* norms, int perm) {
-  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)batch * ny * nx;
+  // a row (b, y) per block iteration, its x over the threads: no 64-bit
+  // index divisions
   double s_r = 0, s_f = 0, s_p = 0;
   const double idx2 = 1.0 / (dx * dx), idy2 = 1.0 / (dy * dy);
-  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
-    long long b = k / ((long long)ny * nx);
-    long long rem = k - b * ny * nx;
-    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
-    const PT* P = psi + b * pb + (long long)y * pld + x;
-    double c = (double)P[0];
-    double e = x + 1 < nx ? (double)P[1] : 0.0, w = x > 0 ? (double)P[-1] : 0.0;
-    double nn = y + 1 < ny ? (double)P[pld] : 0.0, s = y > 0 ? (double)P[-pld] : 0.0;
-    double lap = ((e - 2.0 * c) + w) * idx2 + ((nn - 2.0 * c) + s) * idy2;
-    double fv = (double)f[b * fb + (long long)y * fld + x];
-    double r = fv - (lap - lam[b % nlam] * c);
-    float rv = (float)r;
-    bf16 h = __float2bfloat16_rn(rv);
-    const long long o = perm ? k - x + deinterleave(x, nx) : k;
-    hi[o] = h;
-    lo[o] = __float2bfloat16_rn(rv - __bfloat162float(h));
-    s_r += r * r;
-    s_f += fv * fv;
-    s_p += c * c;
+  const int rows = batch * ny;
+  for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+    const int b = row / ny, y = row - b * ny;
+    const double lb = lam[b % nlam];
+    const PT* P = psi + b * pb + (long long)y * pld;
+    const T* F = f + b * fb + (long long)y * fld;
+    const long long o0 = (long long)row * nx;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) {
+      const PT* Px = P + x;
+      const double c = (double)Px[0];
+      const double e = x + 1 < nx ? (double)Px[1] : 0.0, w = x > 0 ? (double)Px[-1] : 0.0;
+      const double nn = y + 1 < ny ? (double)Px[pld] : 0.0, s = y > 0 ? (double)Px[-pld] : 0.0;
+      const double lap = ((e - 2.0 * c) + w) * idx2 + ((nn - 2.0 * c) + s) * idy2;
+      const double fv = (double)F[x];
+      const double r = fv - (lap - lb * c);
+      const float rv = (float)r;
+      const bf16 h = __float2bfloat16_rn(rv);
+      const long long o = o0 + (perm ? deinterleave(x, nx) : x);
+      hi[o] = h;
+      lo[o] = __float2bfloat16_rn(rv - __bfloat162float(h));
+      s_r += r * r;
+      s_f += fv * fv;
+      s_p += c * c;
+    }
   }
   if (!norms) return;
   s_r = warp_sum(s_r);
@@ -1213,6 +1218,8 @@ __global__ void residual_kernel(const T* __restrict__ f, long long fb, long long
     atomicAdd(&norms[2], s_p);
   }
 }
+
+static int residual_grid(int rows) { return rows < 148 * 16 ? rows : 148 * 16; }
 
 // ---- host side ----------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -1768,9 +1775,8 @@ extern "C" int fvx_dst_refine_f32(fvx_dst_plan* p, const float* rhs, long long r
   if (batch < 1 || batch > p->batch_max || !p->split_ok) return FVX_ERR_SHAPE;
   if (p->kind != FVX_SPECTRAL_DST) return FVX_ERR_METHOD;
   cudaStream_t st = fvx_stream(stream);
-  const long long n = (long long)batch * p->ny * p->nx;
   for (int it = 0; it < passes; ++it) {
-    residual_kernel<float, float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld,
+    residual_kernel<float, float><<<residual_grid(batch * p->ny), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld,
                                                               p->ny, p->nx, batch, p->dx, p->dy, p->lam_dev,
                                                               p->n_lam, p->W1h, p->W1l, nullptr, p->sym ? 1 : 0);
     int rc = fvx_cuda_status();
@@ -1828,7 +1834,7 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
   for (it = 1; it <= max_iter; ++it) {
     if ((rc = chain_split(p, batch, EPI_F64_ACC, psi, psi_bstride, psi_ld, st))) return rc;
     cudaMemsetAsync(p->norms, 0, sizeof(double) * 4, st);
-    residual_kernel<double, double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
+    residual_kernel<double, double><<<residual_grid(batch * ny), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, psi, psi_bstride, psi_ld, ny, nx,
                                                         batch, p->dx, p->dy, p->lam_dev, p->n_lam, p->W1h, p->W1l,
                                                         p->norms, p->sym ? 1 : 0);
     double h[4];

@@ -195,8 +195,12 @@ DEV void coarse_cells(int ny, int nx, F&& fnc) {
 // f[lc] set and u[lc] = 0 (the recursion's zero initial guess).  S is the
 // level table in shared memory; each level's entry is copied to registers
 // before its loops (its fields are read at every cell).
+// D (may be null): the coarsest level in FP64; its n_coarse sweeps -- the
+// coarsest-grid solve -- then run in FP64 on the widened right-hand side and
+// the result is rounded back into S[nl-1].u.
 template <typename T>
-DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
+DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega,
+                      const Lev<double>* D = nullptr) {
   const int tid = threadIdx.x;
   auto sweeps = [&](const Lev<T> L, int n) {
     const size_t cells = (size_t)L.ny * L.nx;
@@ -217,7 +221,25 @@ DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, in
     const size_t cells = (size_t)L.ny * L.nx;
     for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = T(0);
     __syncthreads();
-    if (l == nl - 1) { sweeps(L, n_coarse); break; }
+    if (l == nl - 1) {
+      if (D) {
+        const Lev<double> E = *D;
+        for (size_t c = tid; c < cells; c += kCoarseThreads) { E.f[c] = (double)L.f[c]; E.u[c] = 0.0; }
+        __syncthreads();
+        double* a = E.u;
+        double* b = E.tmp;
+        for (int s = 0; s < n_coarse; ++s) {
+          coarse_cells(E.ny, E.nx, [&](int j, int i, size_t c) { jacobi_at(E, a, E.f, b, (double)omega, j, i, c); });
+          __syncthreads();
+          double* t = a; a = b; b = t;
+        }
+        for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = (T)a[c];
+        __syncthreads();
+      } else {
+        sweeps(L, n_coarse);
+      }
+      break;
+    }
     sweeps(L, n_pre);
     const Lev<T> C = S[l + 1];
     const size_t cc = (size_t)C.ny * C.nx;
@@ -243,26 +265,18 @@ coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n
   coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
 }
 
-// The coarse part of an FP32 plan's V-cycle in FP64: level l's right-hand
-// side is widened into the FP64 copy of levels l .. nl-1 (operators built
-// from the same FP64 host hierarchy), the single-CTA cycle (restriction,
-// sweeps, the coarsest-level solve, prolongation) runs in FP64, and the
-// correction is rounded back into the FP32 level.
+// An FP32 plan's single-CTA coarse cycle with the coarsest-grid solve (the
+// n_coarse Jacobi sweeps on the coarsest level) in FP64, on the FP64 copy of
+// that level (operators from the same FP64 host hierarchy).
 __global__ void __launch_bounds__(kCoarseThreads)
-coarse_vcycle_f64_kernel(LevArray<float> A, LevArray<double> D, int lc, int nl, int n_pre, int n_post,
-                         int n_coarse, double omega) {
-  __shared__ Lev<double> S[kMaxLevels];
-  if (threadIdx.x < nl) S[threadIdx.x] = D.L[threadIdx.x];
+coarse_vcycle_f64_kernel(LevArray<float> A, Lev<double> D, int lc, int nl, int n_pre, int n_post, int n_coarse,
+                         float omega) {
+  __shared__ Lev<float> S[kMaxLevels];
+  __shared__ Lev<double> E;
+  if (threadIdx.x < nl) S[threadIdx.x] = A.L[threadIdx.x];
+  if (threadIdx.x == 0) E = D;
   __syncthreads();
-  const size_t cells = (size_t)A.L[lc].ny * A.L[lc].nx;
-  const float* f32 = A.L[lc].f;
-  double* f64 = S[lc].f;
-  for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) f64[c] = (double)f32[c];
-  __syncthreads();
-  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
-  float* u32 = A.L[lc].u;
-  const double* u64 = S[lc].u;
-  for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) u32[c] = (float)u64[c];
+  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega, &E);
 }
 
 // Many independent solves of A_lc u = f at level lc, one CTA per right-hand
@@ -641,7 +655,7 @@ struct fvx_mg {
   double omega = 0.95, lam = 0.0;
   std::vector<void*> allocs;
   LevArray<float> A32;
-  LevArray<double> A64;  // FP64 plans: every level; FP32 plans: the coarse levels lc .. nl-1
+  LevArray<double> A64;  // FP64 plans: every level; FP32 plans: the coarsest level only
   Lev<double> L0d;  // finest operator in FP64 (residual checks of FP32 solves)
 };
 
@@ -765,10 +779,9 @@ extern "C" int fvx_mg_create(const double* mask, const double* coeff, int ny, in
   g->lc = n_levels - 1;
   while (g->lc > 0 && (size_t)H[g->lc - 1].ny * H[g->lc - 1].nx <= (size_t)kCoarseCells) --g->lc;
   int rc = dtype == 0 ? upload_levels<float>(g, H) : upload_levels<double>(g, H);
-  // FP32 plans keep an FP64 copy of the single-CTA coarse levels: the
-  // coarse part of every V-cycle, the coarsest-level solve included, runs
-  // in FP64
-  if (!rc && dtype == 0) rc = upload_levels<double>(g, H, g->lc);
+  // FP32 plans keep an FP64 copy of the coarsest level: the coarsest-grid
+  // solve of every V-cycle runs in FP64
+  if (!rc && dtype == 0) rc = upload_levels<double>(g, H, n_levels - 1);
   if (!rc) {
     Lev<double>& D = g->L0d;
     D.ny = ny; D.nx = nx; D.dx2 = dx * dx; D.dy2 = dy * dy; D.rdx2 = 1.0 / (dx * dx); D.rdy2 = 1.0 / (dy * dy);
@@ -838,8 +851,8 @@ static int leg_attr() {
 template <typename T>
 static int coarse_vcycle(fvx_mg* g, int l, cudaStream_t st) {
   if constexpr (sizeof(T) == 4)
-    coarse_vcycle_f64_kernel<<<1, kCoarseThreads, 0, st>>>(g->A32, g->A64, l, g->nl, g->n_pre, g->n_post,
-                                                           g->n_coarse, g->omega);
+    coarse_vcycle_f64_kernel<<<1, kCoarseThreads, 0, st>>>(g->A32, g->A64.L[g->nl - 1], l, g->nl, g->n_pre,
+                                                           g->n_post, g->n_coarse, (float)g->omega);
   else
     coarse_vcycle_kernel<T><<<1, kCoarseThreads, 0, st>>>(levs<T>(g), l, g->nl, g->n_pre, g->n_post, g->n_coarse,
                                                           (T)g->omega);
@@ -1594,7 +1607,9 @@ static int pcg_finish_t(fvx_pcg* P, const T* b, double* x, double bb, double* re
   double rr = 0;
   cudaMemcpyAsync(&rr, P->s + S_RR, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return FVX_ERR_CUDA;
-  *rel_out = bb > 0 ? sqrt(rr / bb) : 0.0;
+  // bb = 0: the zero solution is exact; a NaN (or negative) bb or rr is not
+  // a converged solve: the relative residual stays NaN
+  *rel_out = bb == 0.0 ? 0.0 : sqrt(rr / bb);
   return FVX_OK;
 }
 

@@ -94,18 +94,20 @@ def test_mg_fine_levels_host_driven_path(cuda_ok):
     assert rel(host(mg.v_cycle(None, dev(f))), O.mg_vcycle(ref, np.zeros_like(f), f)) < 1e-10
 
 
-def test_mg_fp32_plan_coarse_part_in_fp64(cuda_ok):
-    # 32^2: the whole V-cycle is the single-CTA coarse part, which FP32
-    # plans run in FP64 (the coarsest-grid solve included): the result is
-    # the FP64 cycle rounded once to FP32 (an FP32 cycle would be ~1e-6 off)
+def test_mg_fp32_plan_coarsest_solve_in_fp64(cuda_ok):
+    # FP32 plans run the coarsest-grid solve (its 50 Jacobi sweeps) in FP64.
+    # With no smoothing on the other levels a V-cycle is restriction ->
+    # coarsest solve -> prolongation, so it matches the FP64 oracle up to the
+    # FP32 rounding of the transfers
     n = 32
     m = basin(n, 17)
     c = coeff(n, 18)
-    mg = fvx.build_multigrid_solver(m, 1.0 / n, 1.0 / n, lambda_=2.0, coeff=c, dtype=torch.float32)
-    ref = O.mg_build(m, 1.0 / n, 1.0 / n, lambda_=2.0, coeff=c)
+    kw = dict(lambda_=1e-3, coeff=c, n_pre=0, n_post=0)
+    mg = fvx.build_multigrid_solver(m, 1.0 / n, 1.0 / n, dtype=torch.float32, **kw)
+    ref = O.mg_build(m, 1.0 / n, 1.0 / n, **kw)
     f = (np.random.default_rng(19).standard_normal((n, n)) * m).astype(np.float32).astype(np.float64)
     got = host(mg.v_cycle(None, dev(f, torch.float32)))
-    assert rel(got, O.mg_vcycle(ref, np.zeros_like(f), f)) < 2e-7
+    assert rel(got, O.mg_vcycle(ref, np.zeros_like(f), f)) < 1e-6
 
 
 def test_mg_shape_error(cuda_ok):
