@@ -130,7 +130,7 @@ def tune_qg_split(model, q, dt: float, use_cache: bool = True) -> dict:
     return res
 
 
-DST_KERNELS = ("single64", "pair", "single32", "persist64")
+DST_KERNELS = ("single64", "pair", "single32")
 
 
 def set_dst_kernel(kind) -> None:

@@ -812,254 +812,6 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
   }
 }
 
-// ---- persistent even/odd product ---------------------------------------------
-// The even/odd product with 64-column tiles (a CTA's tile: 128 rows of X by
-// 64 columns of P and the 64 matching columns of Q) on a persistent grid of
-// one CTA per SM, each CTA taking tiles blockIdx.x, blockIdx.x + gridDim.x,
-// ...  Two TMEM accumulators (columns 0-127 and 128-255, P then Q in each)
-// alternate between tiles, so the epilogue of tile i (TMEM -> P +- Q ->
-// scale, 1/Lambda -> bf16 hi/lo or FP32 -> shared memory -> TMA stores)
-// runs while the MMA warp fills the other accumulator with tile i+1, and
-// the operand ring runs on across tile boundaries.  At 2048^2 the 256 tiles
-// cover all 148 SMs (1.73 per CTA) where the 128-column form's 128 tiles
-// leave 20 idle and expose every epilogue.  Roles: warp 0 TMA producer,
-// warp 1 MMA issuer, warps 2-17 the epilogue in four groups of four (one
-// warp per TMEM lane quadrant; group g converts tile columns 16g..16g+15).
-// The epilogue stages each group's part of the tile in its own 16 KiB slot
-// and writes it with TMA bulk-tensor stores; a slot is rewritten only after
-// the previous tile's stores have read it.  Used when the output layout
-// admits the TMA stores (split and FP32 outputs); other epilogues take the
-// 128-column kernel.
-constexpr int PBN = 64;                       // P (and Q) columns per tile
-constexpr int PR_STAGES = 3;
-constexpr int PR_A = BM * BK * 2;             // 16 KiB
-constexpr int PR_B = PBN * BK * 2;            // 8 KiB
-constexpr int PR_STAGE = 2 * PR_A + 2 * PR_B;  // 48 KiB
-constexpr int PR_SLOT = 16384;                // epilogue staging per group
-constexpr int PR_SMEM = PR_STAGES * PR_STAGE + EPI_GROUPS * PR_SLOT + 1024 + 256;
-constexpr uint32_t kIdesc64 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(PBN >> 3) << 17) |
-                              ((uint32_t)(BM >> 4) << 24);
-static_assert(PR_SMEM <= 227 * 1024, "persistent product exceeds shared memory");
-
-DEV void mbar_arrive(uint32_t a) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
-}
-
-__global__ void __launch_bounds__(S_THREADS, 1)
-gemm_sym_persist_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-                        const __grid_constant__ CUtensorMap mPh, const __grid_constant__ CUtensorMap mPl,
-                        const __grid_constant__ CUtensorMap mQh, const __grid_constant__ CUtensorMap mQl,
-                        const __grid_constant__ CUtensorMap mO0, const __grid_constant__ CUtensorMap mO1, int K,
-                        int tiles_n, int tiles, Epi ep) {
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  uint8_t* stage_area = smem + PR_STAGES * PR_STAGE;                   // EPI_GROUPS slots
-  uint64_t* bars = (uint64_t*)(stage_area + EPI_GROUPS * PR_SLOT);     // full, empty, accf[2], acce[2], fin
-  uint32_t* tmem_slot = (uint32_t*)(bars + 2 * PR_STAGES + 5);
-  volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int KH = K >> 1;
-  const int KT = 2 * (KH / BK);  // P and Q blocks alternate
-  auto full = [&](int s) { return smem_u32(&bars[s]); };
-  auto empty = [&](int s) { return smem_u32(&bars[PR_STAGES + s]); };
-  auto accf = [&](int a) { return smem_u32(&bars[2 * PR_STAGES + a]); };
-  auto acce = [&](int a) { return smem_u32(&bars[2 * PR_STAGES + 2 + a]); };
-  const uint32_t fin = smem_u32(&bars[2 * PR_STAGES + 4]);
-
-  if (threadIdx.x == 0) {
-    prefetch_map(&mAh); prefetch_map(&mAl); prefetch_map(&mPh);
-    prefetch_map(&mPl); prefetch_map(&mQh); prefetch_map(&mQl);
-    prefetch_map(&mO0); prefetch_map(&mO1);
-    for (int s = 0; s < PR_STAGES; ++s) { mbar_init(full(s), 1); mbar_init(empty(s), 1); }
-    for (int a = 0; a < 2; ++a) { mbar_init(accf(a), 1); mbar_init(acce(a), EPI_GROUPS); }
-    mbar_init(fin, 1);
-    *abort_flag = 0;
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 1) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(4 * PBN));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = *tmem_slot;
-  auto tile_mn = [&](int t, int& m0, int& n0) {
-    const int tm = t / tiles_n;
-    m0 = tm * BM;
-    n0 = (t - tm * tiles_n) * PBN;
-  };
-  auto shift_of = [&](int t) {  // staggered K start (even: keeps the P / Q alternation)
-    const int tm = t / tiles_n, tn = t - tm * tiles_n;
-    return 2 * (int)(((unsigned)tn * 5u + (unsigned)tm * 3u) % (unsigned)(KT / 2));
-  };
-
-  if (warp == 0 && lane == 0) {
-    // TMA producer: the ring runs across this CTA's tiles
-    int g = 0;  // ring slot counter
-    bool ok = !ep.stall;
-    bool waited = false;
-    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
-      int m0, n0;
-      tile_mn(t, m0, n0);
-      const int ksh = shift_of(t);
-      for (int kt0 = 0; kt0 < KT; ++kt0, ++g) {
-        const int s = g % PR_STAGES;
-        if (g >= PR_STAGES && !mbar_wait(empty(s), ((g / PR_STAGES) - 1) & 1, abort_flag, ep.err, ep.wait_cycles)) {
-          ok = false;
-          break;
-        }
-        mbar_expect_tx(full(s), PR_STAGE);
-        const uint32_t base = smem_u32(smem + s * PR_STAGE);
-        const int kt = (kt0 + ksh) % KT;
-        const int kb = kt >> 1;
-        const bool odd = kt & 1;
-        // the DST tables are constant: their first loads go out before the
-        // wait for the previous kernel, X (its output) only after
-        tma_load_2d(base + 2 * PR_A, odd ? &mQh : &mPh, full(s), kb * BK, n0);
-        tma_load_2d(base + 2 * PR_A + PR_B, odd ? &mQl : &mPl, full(s), kb * BK, n0);
-        if (!waited) { grid_dep_wait(); waited = true; }
-        const int ac = (odd ? KH : 0) + kb * BK;
-        tma_load_2d(base, &mAh, full(s), ac, m0);
-        tma_load_2d(base + PR_A, &mAl, full(s), ac, m0);
-      }
-    }
-    if (!waited) grid_dep_wait();
-    drain_ring(full(0), PR_STAGES, g);
-  } else if (warp == 1 && lane == 0) {
-    // MMA issuer: tile i into accumulator i % 2
-    int g = 0, it = 0;
-    bool ok = true;
-    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++it) {
-      const int a = it & 1;
-      if (it >= 2 && !mbar_wait(acce(a), ((it >> 1) - 1) & 1, abort_flag, ep.err, ep.wait_cycles)) break;
-      tc_fence_after();
-      const int ksh = shift_of(t);
-      for (int kt0 = 0; kt0 < KT; ++kt0, ++g) {
-        const int s = g % PR_STAGES;
-        if (!mbar_wait(full(s), (g / PR_STAGES) & 1, abort_flag, ep.err, ep.wait_cycles)) {
-          ok = false;
-          break;
-        }
-        tc_fence_after();
-        const uint32_t base = smem_u32(smem + s * PR_STAGE);
-        const uint64_t ah = sdesc_sw128(base), al = sdesc_sw128(base + PR_A);
-        const uint64_t bh = sdesc_sw128(base + 2 * PR_A), bl = sdesc_sw128(base + 2 * PR_A + PR_B);
-        const int kt = (kt0 + ksh) % KT;
-        const uint32_t d = tmem + (uint32_t)(a * 2 * PBN) + ((kt & 1) ? (uint32_t)PBN : 0u);
-        const bool first = kt0 < 2;  // the tile's first P block and first Q block overwrite
-#pragma unroll
-        for (int kk = 0; kk < BK / 16; ++kk) {
-          const uint64_t o = (uint64_t)(kk * 32 >> 4);
-          umma_bf16<COLL_FILL>(d, ah + o, bh + o, kIdesc64, !(first && kk == 0));
-          umma_bf16<COLL_LASTUSE>(d, ah + o, bl + o, kIdesc64, 1u);
-          umma_bf16(d, al + o, bh + o, kIdesc64, 1u);
-        }
-        umma_commit(empty(s));
-      }
-      if (ok) umma_commit(accf(a));
-    }
-    umma_commit(fin);  // arrives once every MMA issued above has completed
-  } else if (warp >= 2) {
-    const int wq = warp & 3;
-    const int grp = (warp - 2) >> 2;
-    const int row = wq * 32 + lane;
-    const int half = row & 1, rl = row >> 1;
-    const uint32_t lanes = (uint32_t)(wq * 32) << 16;
-    const bool leader = lane == 0 && wq == 2;  // one thread per group (warps 2, 6, 10, 14 are quadrant 2)
-    uint8_t* slot = stage_area + grp * PR_SLOT;
-    const int R = ep.rows_per_batch;
-    const float alpha = (float)ep.alpha;
-    const bool scaled = ep.alpha != 1.0;
-    const int c0 = grp * 16;  // this group's tile columns
-    int it = 0;
-    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++it) {
-      const int a = it & 1;
-      int m0, n0;
-      tile_mn(t, m0, n0);
-      const int bb = m0 / R, r0 = m0 - bb * R;
-      const int be = bb % ep.n_eig;
-      // 1/Lambda of this tile's columns while the MMAs run
-      float ivp[16], ivm[16];
-      const float* ie = ep.inv_eig ? ep.inv_eig + (long long)be * ep.n_cols * R + (r0 + row) : nullptr;
-      if (ie) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int k = n0 + c0 + j;
-          ivp[j] = __ldg(ie + (long long)k * R);
-          ivm[j] = __ldg(ie + (long long)(K - 1 - k) * R);
-        }
-      }
-      const bool ok = mbar_wait(accf(a), (it >> 1) & 1, abort_flag, ep.err, ep.wait_cycles);
-      if (ok) tc_fence_after();
-      if (t + (int)gridDim.x >= tiles) grid_dep_launch();  // this CTA's last tile
-      const bool go = ok && !*abort_flag;
-      uint32_t vp[16], vq[16];
-      if (go) {
-        tmem_ld16(tmem + lanes + (uint32_t)(a * 2 * PBN + c0), vp);
-        tmem_ld16(tmem + lanes + (uint32_t)(a * 2 * PBN + PBN + c0), vq);
-        tmem_wait_ld();
-      }
-      // the slot's previous stores have read it; the group's TMEM reads are done
-      if (leader) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-      tc_fence_before();
-      asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
-      if (leader) mbar_arrive(acce(a));  // accumulator a may take the tile after next
-      if (go) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const float P = __uint_as_float(vp[j]), Q = __uint_as_float(vq[j]);
-          float xp = P + Q, xm = P - Q;
-          if (scaled) { xp *= alpha; xm *= alpha; }
-          if (ie) { xp *= ivp[j]; xm *= ivm[j]; }
-          if (ep.mode == EPI_SPLIT) {
-            // [which][half][hi/lo][16 n][64 r] bf16; which 1 (P - Q) rows run backwards
-            bf16* box = (bf16*)slot;
-            const __nv_bfloat162 h2 = __floats2bfloat162_rn(xp, xm);
-            const __nv_bfloat162 l2 = __floats2bfloat162_rn(xp - __low2float(h2), xm - __high2float(h2));
-            const int op = j * 64 + rl, om = (15 - j) * 64 + rl;
-            box[((0 * 2 + half) * 2 + 0) * 1024 + op] = h2.x;
-            box[((0 * 2 + half) * 2 + 1) * 1024 + op] = l2.x;
-            box[((1 * 2 + half) * 2 + 0) * 1024 + om] = h2.y;
-            box[((1 * 2 + half) * 2 + 1) * 1024 + om] = l2.y;
-          } else {
-            float* box = (float*)slot;  // [which][16 n][128 r] fp32
-            box[j * 128 + row] = xp;
-            box[2048 + (15 - j) * 128 + row] = xm;
-          }
-        }
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
-      if (go && leader) {
-        const uint32_t sb = smem_u32(slot);
-        const int y0 = n0 + c0, y1 = K - n0 - c0 - 16;  // first output row of P + Q / P - Q
-        if (ep.mode == EPI_SPLIT) {
-          for (int which = 0; which < 2; ++which)
-            for (int hf = 0; hf < 2; ++hf)
-              for (int hl = 0; hl < 2; ++hl)
-                tma_store_3d(hl ? &mO1 : &mO0, sb + (uint32_t)(((which * 2 + hf) * 2 + hl) * 2048),
-                             (hf ? (R >> 1) : 0) + (r0 >> 1), which ? y1 : y0, bb);
-        } else {
-          tma_store_3d(&mO0, sb, r0, y0, bb);
-          tma_store_3d(&mO0, sb + 8192u, r0, y1, bb);
-        }
-        tma_store_commit();
-      }
-    }
-    if (leader) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 1) {
-    if (lane == 0) mbar_drain(fin, 0);  // no MMA still writes TMEM
-    __syncwarp();
-    tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(4 * PBN));
-  }
-}
-
 // ---- FP64 SIMT GEMM with the same transposed-store epilogue (correctness path)
 constexpr int DT = 64, DK = 16;
 __global__ void __launch_bounds__(256)
@@ -1289,9 +1041,7 @@ static bool make_out_map(CUtensorMap* map, void* base, bool f32, uint64_t R, uin
 
 // Which even/odd kernel runs (fvx_dst_kernel_config): 0 = single CTAs with
 // 64-element K blocks (default), 1 = CTA pairs (row counts that are
-// multiples of 256), 2 = single CTAs with 32-element K blocks, 3 = the
-// persistent kernel with 64-column tiles (products whose epilogue writes
-// through TMA; the others take form 0).
+// multiples of 256), 2 = single CTAs with 32-element K blocks.
 static int g_sym_kernel = 0;
 
 // C[M, K] = X[M, K] S[K, K] by the even/odd product; X's columns
@@ -1327,26 +1077,6 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
                          make_out_map(&o1, ep.out1, false, R, K, B, ep.ld, ep.batch_stride, 64)
                    : make_out_map(&o0, ep.out0, true, R, K, B, ep.ld, ep.batch_stride, 128);
     ep.tma_out = okm ? 1 : 0;
-  }
-  if (g_sym_kernel == 3 && ep.tma_out && M % BM == 0 && KH % PBN == 0) {
-    // persistent 64-column tiles, one CTA per SM
-    static fvx_once_per_device pattr;
-    if (fvx_once_on_device(pattr, [] { return fvx_set_max_smem(gemm_sym_persist_kernel, PR_SMEM); }))
-      return FVX_ERR_CUDA;
-    CUtensorMap p64h, p64l, q64h, q64l;
-    if (!make_map(&p64h, Ph, KH, KH, PBN) || !make_map(&p64l, Pl, KH, KH, PBN) ||
-        !make_map(&q64h, Qh, KH, KH, PBN) || !make_map(&q64l, Ql, KH, KH, PBN))
-      return FVX_ERR_ARG;
-    const int tiles_n = KH / PBN, tiles = tiles_n * (M / BM);
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
-                                                  cudaSuccess)
-      return FVX_ERR_CUDA;
-    const int grid = tiles < sms ? tiles : sms;
-    if (fvx_launch_pdl(gemm_sym_persist_kernel, dim3(grid), dim3(S_THREADS), PR_SMEM, st, a_h, a_l, p64h, p64l,
-                       q64h, q64l, o0, o1, K, tiles_n, tiles, ep) != cudaSuccess)
-      return FVX_ERR_CUDA;
-    return fvx_cuda_status();
   }
   if (M % (2 * BM) == 0 && g_sym_kernel == 1) {
     // CTA pairs: B blocks of 64 table rows per CTA
@@ -1855,7 +1585,7 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
 // Lambda -> W1.  Operands are whatever the workspaces currently hold.
 extern "C" int fvx_dst_kernel_config(int kind) {
   if (kind < 0) return g_sym_kernel;
-  if (kind > 3) return FVX_ERR_ARG;
+  if (kind > 2) return FVX_ERR_ARG;
   g_sym_kernel = kind;
   return FVX_OK;
 }

@@ -228,11 +228,8 @@ int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
  * per 128-row tile with 64-element K blocks (3 ring stages, default), 1 =
  * CTA pairs sharing each B block (cta_group::2; row counts that are
  * multiples of 256), 2 = one CTA per tile with 32-element K blocks (6 ring
- * stages), 3 = persistent grid of one CTA per SM over 128 x 64-column tiles
- * with two TMEM accumulators (a tile's epilogue overlaps the next tile's
- * MMAs; products with TMA-written outputs, the others run form 0); kind < 0
- * returns the current choice.  No counterpart in finitevolX (launch
- * configuration). */
+ * stages); kind < 0 returns the current choice.  No counterpart in
+ * finitevolX (launch configuration). */
 int fvx_dst_kernel_config(int kind);
 
 /* Allocation-free FP32 DST Helmholtz solve.  No counterpart in the

@@ -49,9 +49,8 @@ def test_dst_split_bf16_chain(cuda_ok, shape, lam):
 
 @pytest.mark.parametrize("shape", [(256, 512), (512, 256), (768, 512), (2048, 2048)])
 def test_dst_product_forms_agree(cuda_ok, shape):
-    # the even/odd products on single CTAs (64- and 32-element K blocks), on
-    # CTA pairs (cta_group::2, B blocks shared by the pair) and on the
-    # persistent grid (64-column tiles, two TMEM accumulators): the same
+    # the even/odd products on single CTAs (64- and 32-element K blocks) and
+    # on CTA pairs (cta_group::2, B blocks shared by the pair): the same
     # 3xBF16 sums in another k order.  All within the chain's 1e-4 of the
     # oracle; against each other within 5e-5: an intermediate that differs
     # by one FP32 ulp can round to another bf16 hi/lo pair, which moves it by

@@ -314,3 +314,43 @@ def test_no_host_fallback_without_library(monkeypatch, cuda_ok):
     monkeypatch.setattr(L, "LIB_PATH", pathlib.Path("/nonexistent/libfvx.so"))
     with pytest.raises(RuntimeError):
         fvx.enforce_periodic(dev(np.zeros((5, 5))))
+
+
+# interior tiles: at 150 x 270 most 64 x 16 tiles lie at least the halo from
+# every edge and take the kernels' branch-free interior bodies; the edge
+# tiles keep the boundary ladders -- both against the oracle
+@pytest.mark.parametrize("method", METHODS)
+def test_advection_interior_tiles_fp64(cuda_ok, method):
+    ny, nx = 150, 270
+    h, u, v = rand_fields(ny, nx, 21)
+    ref = O.advection2d(h, u, v, 0.3, 0.2, method)
+    grid = fvx.ArakawaCGrid2D(Nx=nx, Ny=ny, Lx=0.3 * (nx - 2), Ly=0.2 * (ny - 2), dx=0.3, dy=0.2)
+    close_norm(host(fvx.Advection2D(grid)(dev(h), dev(u), dev(v), method=method)), ref, 1e-12)
+
+
+@pytest.mark.parametrize("method", ("weno5", "wenoz5", "weno7", "weno9", "van_leer", "upwind3"))
+def test_advection_interior_tiles_fp32(cuda_ok, method):
+    ny, nx = 150, 270
+    h = O.kminus3_field(ny, nx, 2) + 1.0
+    psi = O.fourier_streamfunction(ny - 2, nx - 2, 1.0, 1.0, 3)
+    u, v = O.diff2d("grad_perp", psi, 1.0, 1.0)
+    ref = O.advection2d(h, u, v, 1.0, 1.0, method)
+    got = fvx.Advection2D(fvx.ArakawaCGrid2D(nx, ny, nx - 2.0, ny - 2.0, 1.0, 1.0))(
+        dev(h, torch.float32), dev(u, torch.float32), dev(v, torch.float32), method=method)
+    close_norm(host(got), ref, 1e-5)
+
+
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 1e-5)])
+def test_biharmonic_jacobian_interior_tiles(cuda_ok, dtype, tol):
+    ny, nx = 150, 270
+    rng = np.random.default_rng(22)
+    h = O.kminus3_field(ny, nx, 4)
+    g = O.kminus3_field(ny, nx, 5)
+    grid = fvx.ArakawaCGrid2D(Nx=nx, Ny=ny, Lx=0.3 * (nx - 2), Ly=0.2 * (ny - 2), dx=0.3, dy=0.2)
+    got = fvx.BiharmonicDiffusion2D(grid)(dev(h, dtype), 1e-3)
+    close_norm(host(got), O.biharmonic2d(h, 1e-3, 0.3, 0.2), tol)
+    mask = rng.random((ny, nx)) > 0.2
+    got = fvx.BiharmonicDiffusion2D(grid, fvx.Mask2D.from_mask(mask))(dev(h, dtype), 1e-3)
+    close_norm(host(got), O.biharmonic2d(h, 1e-3, 0.3, 0.2, O.mask2d_from_mask(mask)), tol)
+    got = fvx.arakawa_jacobian(dev(h, dtype), dev(g, dtype), 0.3, 0.2)
+    close_norm(host(got), O.arakawa_jacobian(h, g, 0.3, 0.2), tol)
