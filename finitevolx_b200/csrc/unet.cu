@@ -47,11 +47,22 @@ __host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
 // Small tiles give enough blocks for single-field inference on coarse grids.
 // Launched as a programmatic dependent of the previous layer (inference), a
 // block stages the weights before waiting for that layer's output.
+// Inference hooks of the first and last layers (null elsewhere): with
+// x0_src, input channel 0 is x0_src * scale[1] (the network input f / s
+// formed while the tile loads); with out_mask, the output is
+// (y * (scale[0] * sigma)) * out_mask (the coarse correction s sigma m y).
+struct ConvHooks {
+  const float* x0_src = nullptr;
+  const float* scale = nullptr;
+  const float* out_mask = nullptr;
+  float sigma = 1.f;
+};
+
 template <int COUT, int CPT, int T>
 __global__ void __launch_bounds__(T * T * (COUT / CPT))
 conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
                  const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
-                 int w, int relu) {
+                 int w, int relu, ConvHooks hk) {
   constexpr int NT = T * T * (COUT / CPT);
   constexpr int TW = T + 2;
   extern __shared__ __align__(16) float sm[];
@@ -78,6 +89,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
   const int nt = cin * TW * TW;
+  const float x0s = hk.x0_src ? hk.scale[1] : 0.f;
   for (int k0 = tid; k0 < nt; k0 += 16 * NT) {
     float v[16];
 #pragma unroll
@@ -85,7 +97,10 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
       const int k = k0 + u * NT;
       const int ci = k / (TW * TW), r = k - ci * (TW * TW);
       const int ly = r / TW, lx = r - ly * TW;
-      v[u] = k < nt ? in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
+      if (hk.x0_src && ci == 0)
+        v[u] = k < nt ? in_at(hk.x0_src, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) * x0s : 0.f;
+      else
+        v[u] = k < nt ? in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < 16; ++u)
@@ -112,12 +127,14 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const int y = y0 + ty, x = x0 + tx;
   if (y >= h || x >= w) return;
   const size_t plane = (size_t)h * w, base = (size_t)b * COUT * plane + (size_t)y * w + x;
+  const float os = hk.out_mask ? hk.scale[0] * hk.sigma : 0.f;
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
     const int co = co0 + c;
     float v = acc[c] + bias[co];
     if (skip) v += skip[base + co * plane];
     if (relu) v = fmaxf(v, 0.f);
+    if (hk.out_mask) v = (v * os) * hk.out_mask[(size_t)y * w + x];
     out[base + co * plane] = v;
   }
 }
@@ -125,7 +142,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
 template <int COUT, int CPT, int T>
 static int launch_conv_tile(const float* in, int mode, int batch, int cin, const __nv_bfloat16* wb,
                             const float* bias, const float* skip, float* out, int h, int w, int relu,
-                            cudaStream_t st, bool pdl) {
+                            cudaStream_t st, bool pdl, ConvHooks hk) {
   constexpr int NT = T * T * (COUT / CPT);
   const size_t smem = ((size_t)cin * 9 * COUT + (size_t)cin * (T + 2) * (T + 2)) * sizeof(float);
   static fvx_once_per_device attr;  // per instantiation; the largest use needs > 48 KB
@@ -137,10 +154,10 @@ static int launch_conv_tile(const float* in, int mode, int batch, int cin, const
   dim3 g((w + T - 1) / T, (h + T - 1) / T, batch);
   if (pdl) {
     if (fvx_launch_pdl(conv_tile_kernel<COUT, CPT, T>, g, dim3(NT), smem, st, in, mode, cin, wb, bias, skip, out, h,
-                       w, relu) != cudaSuccess)
+                       w, relu, hk) != cudaSuccess)
       return FVX_ERR_CUDA;
   } else {
-    conv_tile_kernel<COUT, CPT, T><<<g, NT, smem, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu);
+    conv_tile_kernel<COUT, CPT, T><<<g, NT, smem, st>>>(in, mode, cin, wb, bias, skip, out, h, w, relu, hk);
   }
   return fvx_cuda_status();
 }
@@ -325,7 +342,8 @@ using namespace fvx::nn;
 // before it, which must not have written the weights or biases (the kernel
 // reads them before waiting for it).
 static int conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
-                    const float* skip, float* out, int cout, int h, int w, int relu, cudaStream_t st, bool pdl) {
+                    const float* skip, float* out, int cout, int h, int w, int relu, cudaStream_t st, bool pdl,
+                    ConvHooks hk = ConvHooks{}) {
   if (!in || !w_bf16 || !bias || !out) return FVX_ERR_ARG;
   if (cin < 1 || cin > CMAX || batch < 1 || h < 1 || w < 1 || mode < 0 || mode > 2) return FVX_ERR_SHAPE;
   if ((mode == IN_UP) && ((h % 2) || (w % 2))) return FVX_ERR_SHAPE;
@@ -336,14 +354,14 @@ static int conv_fwd(const float* in, int mode, int batch, int cin, const void* w
   const bool big = (size_t)((h + 7) / 8) * ((w + 7) / 8) * batch >= 148;
   switch (cout) {
     case 1:
-      return big ? launch_conv_tile<1, 1, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
-                 : launch_conv_tile<1, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
+      return big ? launch_conv_tile<1, 1, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk)
+                 : launch_conv_tile<1, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk);
     case 16:
-      return big ? launch_conv_tile<16, 4, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
-                 : launch_conv_tile<16, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
+      return big ? launch_conv_tile<16, 4, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk)
+                 : launch_conv_tile<16, 1, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk);
     case 32:
-      return big ? launch_conv_tile<32, 8, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl)
-                 : launch_conv_tile<32, 2, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl);
+      return big ? launch_conv_tile<32, 8, 8>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk)
+                 : launch_conv_tile<32, 2, 4>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st, pdl, hk);
     default: return FVX_ERR_SHAPE;
   }
 }
@@ -471,10 +489,22 @@ __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const 
                                                           float* scale) {
   __shared__ double sh[2][kRmsThreads / 32];
   double a = 0.0, c = 0.0;
-  for (size_t k = threadIdx.x; k < n; k += kRmsThreads) {
-    const double m = mask[k];
-    a += (double)f[k] * f[k] * m;
-    c += m;
+  // eight cells' loads in flight per thread before they are accumulated (in
+  // the same order as a one-at-a-time loop)
+  for (size_t k0 = threadIdx.x; k0 < n; k0 += 8 * kRmsThreads) {
+    float fv[8], mv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const size_t k = k0 + (size_t)u * kRmsThreads;
+      fv[u] = k < n ? f[k] : 0.f;
+      mv[u] = k < n ? mask[k] : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double m = mv[u];
+      a += (double)fv[u] * fv[u] * m;
+      c += m;
+    }
   }
   for (int o = 16; o; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
@@ -495,21 +525,6 @@ __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const 
       scale[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
     }
   }
-}
-
-// x channel 0 = f / s (channels 1, 2 were set once)
-__global__ void prep_kernel(const float* f, const float* scale, float* x0, size_t n) {
-  const float inv = scale[1];
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    x0[k] = f[k] * inv;
-}
-
-// u = y * s * sigma * mask
-__global__ void finish_kernel(const float* y, const float* scale, const float* mask, float sigma, float* u,
-                              size_t n) {
-  const float s = scale[0] * sigma;
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    u[k] = y[k] * s * mask[k];
 }
 
 }  // namespace nn
@@ -624,14 +639,22 @@ extern "C" int fvx_unet_sync_params(fvx_unet* n, void* stream) {
 
 // pdl: each layer launched as a programmatic dependent of the kernel before
 // it (inference only: no kernel between the layers writes the weights).
-static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = false) {
+// coarse_f / coarse_u (inference on one field): the first layer forms
+// f / s from coarse_f as it loads, the last writes s sigma m y to coarse_u.
+static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = false, const float* coarse_f = nullptr,
+                        float* coarse_u = nullptr) {
   size_t off = 0;
-  for (const LayerDef& L : kNet) {
+  for (int l = 0; l < kLayers; ++l) {
+    const LayerDef& L = kNet[l];
     const int hh = n->h >> L.div, ww = n->w >> L.div;
     const __nv_bfloat16* W = n->wb + off;
     const float* wf_b = n->wf + off + (size_t)L.cout * L.cin * 9;  // biases stay FP32
-    int rc = conv_fwd(n->act[L.in], L.mode, batch, L.cin, W, wf_b, L.skip >= 0 ? n->act[L.skip] : nullptr,
-                      n->act[L.out], L.cout, hh, ww, L.relu, st, pdl);
+    ConvHooks hk;
+    float* dst = n->act[L.out];
+    if (coarse_f && l == 0) { hk.x0_src = coarse_f; hk.scale = n->scale; }
+    if (coarse_u && l == kLayers - 1) { hk.out_mask = n->mask; hk.scale = n->scale; hk.sigma = n->sigma; dst = coarse_u; }
+    int rc = conv_fwd(n->act[L.in], L.mode, batch, L.cin, W, wf_b, L.skip >= 0 ? n->act[L.skip] : nullptr, dst,
+                      L.cout, hh, ww, L.relu, st, pdl, hk);
     if (rc) return rc;
     off += layer_params(L);
   }
@@ -717,9 +740,8 @@ extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) 
   cudaStream_t st = fvx_stream(stream);
   const size_t plane = (size_t)n->h * n->w;
   rms_kernel<<<1, kRmsThreads, 0, st>>>((const float*)f, n->mask, plane, n->scale);
-  prep_kernel<<<blocks_for(plane), 256, 0, st>>>((const float*)f, n->scale, n->act[0], plane);
-  int rc = unet_forward(n, 1, st, true);
+  // the first layer forms f / s, the last writes s sigma m y into u
+  int rc = unet_forward(n, 1, st, true, (const float*)f, (float*)u);
   if (rc) return rc;
-  finish_kernel<<<blocks_for(plane), 256, 0, st>>>(n->act[8], n->scale, n->mask, n->sigma, (float*)u, plane);
   return fvx_cuda_status();
 }
