@@ -235,6 +235,8 @@ class LearnedPreconditioner:
             check(fn("fvx_levelsolve_create")(mg.handle, I(self.lvl), I(mg_cycles), ctypes.byref(self._ls)),
                   "levelsolve_create")
         self._hy = ctypes.c_void_p()
+        self.use_fallback = False  # set by calibrate(): MG-PCG is the faster method here
+        self.calibration = None
         self._make_hybrid()
 
     def _make_hybrid(self):
@@ -313,6 +315,37 @@ class LearnedPreconditioner:
             n_cycles: int = 10):
         F, E = generate_pairs(self.mg, self.lvl, n_pairs, self.n_pre, seed, n_cycles)
         return self.train(F, E, epochs, batch, lr, seed)
+
+    def calibrate(self, pcg, b, rtol: float = 1e-8, reps: int = 3) -> dict:
+        """Time flexible PCG with this preconditioner against MG-PCG (the
+        multigrid V-cycle, its fallback) on a calibration right-hand side
+        ``b`` and the solver ``pcg`` (a MaskedHelmholtzPCG on the same
+        operator); when MG-PCG is faster, later solves given this object use
+        MG-PCG (``use_fallback``).  Both reach ``rtol`` checked in FP64.
+        Returns the two times (median of ``reps``, ms) and iteration counts."""
+        import statistics
+
+        def timed(**kw):
+            pcg.solve(b, rtol=rtol, graph=True, **kw)
+            ts, info = [], None
+            for _ in range(reps):
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                _, info = pcg.solve(b, rtol=rtol, graph=True, **kw)
+                e1.record()
+                e1.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            return statistics.median(ts), info
+
+        self.use_fallback = False
+        t_net, i_net = timed(precond=self, flexible=True, max_iter=500)
+        t_mg, i_mg = timed(precond="mg")
+        self.use_fallback = (not i_net["converged"]) or t_mg < t_net
+        self.calibration = {"learned_ms": t_net, "learned_iterations": i_net["iterations"], "mg_ms": t_mg,
+                            "mg_iterations": i_mg["iterations"], "use_fallback": self.use_fallback}
+        return self.calibration
 
     def activate(self):
         """Point the inference path at this level's mask, coefficient and sigma."""

@@ -172,6 +172,10 @@ class MaskedHelmholtzPCG:
 
     def solve(self, b, rtol: float = 1e-8, max_iter: int = 500, precond="mg", flexible: bool = False,
               replace_every: int | None = None, chunk: int = 8, x=None, graph: bool = False):
+        # a learned preconditioner whose calibration found it slower than
+        # the multigrid one on its operator hands the solve to MG-PCG
+        if getattr(precond, "use_fallback", False):
+            precond, flexible = "mg", False
         # float32 work vectors: the recursively updated residual drifts from
         # b - A x by ~eps32 * cond(A) |b|, so recompute it from the FP64
         # iterate (in FP64) every iteration; float64: every 10

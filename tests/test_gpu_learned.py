@@ -136,3 +136,12 @@ def test_learned_pcg_gain(problem128):
     # graph replay gives the same iterations and tolerance
     xg, infog = pcg.solve(b, rtol=1e-8, precond=pc, flexible=True, max_iter=300, graph=True)
     assert infog["converged"] and abs(infog["iterations"] - info["iterations"]) <= 1, (infog, info)
+    # calibration against MG-PCG: the faster method is kept, and with the
+    # fallback set a solve given the preconditioner runs MG-PCG itself
+    cal = pc.calibrate(pcg, torch.from_numpy(O.kminus3_field(n, n, 25) * m).float().cuda(), reps=1)
+    assert pc.use_fallback == (cal["mg_ms"] < cal["learned_ms"]), cal
+    pc.use_fallback = True
+    xf, infof = pcg.solve(b, rtol=1e-8, precond=pc, flexible=True, max_iter=300, graph=True)
+    xm, infom = pcg.solve(b, rtol=1e-8, precond="mg", max_iter=300, graph=True)
+    assert infof["iterations"] == infom["iterations"] and torch.equal(xf, xm)
+    pc.use_fallback = False
