@@ -2,7 +2,7 @@
 // schemes, with mask-aware tier dispatch), face fluxes, C-grid differences
 // and interpolations, Arakawa Jacobian, harmonic / biharmonic diffusion and
 // the periodic ghost-ring fill.  FP32 and FP64 instantiations of each.
-#include "qg_stage.cuh"  // recon.cuh, the full-reach face values and the packed FP32 WENO5
+#include "recon.cuh"
 
 namespace fvx {
 
@@ -42,103 +42,6 @@ advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __
   __shared__ uint8_t ty_[ATY + 2][ATX];
   const int x0 = blockIdx.x * ATX, y0 = blockIdx.y * ATY;
   const int tid = threadIdx.x;
-  if constexpr (!MASKED) {
-    // Interior tile: the h tile and its halo lie inside the array and every
-    // face is at least the scheme's reach from both ends, so each face takes
-    // the full-reach reconstruction (no boundary ladder, no bounds tests)
-    // and every cell the divergence.  Threads as 64 columns x 4 rows: each
-    // thread's faces sit in its own column (coalesced velocity loads), and
-    // FP32 WENO5 / WENO-Z5 faces go two at a time through the packed form.
-    constexpr int R = SchemeInfo<S>::reach;
-    const bool inner = x0 - AH >= 1 && x0 + ATX + AH - 1 <= nx - 2 && y0 - AH >= 1 && y0 + ATY + AH - 1 <= ny - 2 &&
-                       x0 - 1 >= R && x0 + ATX <= nx - 1 - R && y0 - 1 >= R && y0 + ATY <= ny - 1 - R;
-    if (inner) {
-      const int tx = tid & (ATX - 1), ty = tid >> 6;
-      for (int ly = ty; ly < HH; ly += 4) {
-        const T* row = h + (size_t)(y0 - AH + ly) * nx + (x0 - AH);
-        for (int lx = tx; lx < HW; lx += ATX) hs[ly][lx] = row[lx];
-      }
-      __syncthreads();
-      constexpr bool PACK = sizeof(T) == 4 && (S == FVX_WENO5 || S == FVX_WENOZ5);
-      constexpr bool Z = S == FVX_WENOZ5;
-      // east faces (ly, lf), lf = tx + 1 (face x0 + tx), rows ty, ty + 4, ty + 8, ty + 12
-      {
-        const int lf = tx + 1, gi = x0 + tx;
-        if constexpr (PACK) {
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int la = ty + 8 * k, lb = la + 4;
-            const float ua = (float)u[(size_t)(y0 + la) * nx + gi], ub = (float)u[(size_t)(y0 + lb) * nx + gi];
-            const float* pa = (const float*)&hs[la + AH][lf - 1 + AH];
-            const float* pb = (const float*)&hs[lb + AH][lf - 1 + AH];
-            const bool qa = ua >= 0.f, qb = ub >= 0.f;
-            float2 e[5];
-#pragma unroll
-            for (int j = 0; j < 5; ++j)
-              e[j] = make_float2(qa ? pa[j - 2] : pa[3 - j], qb ? pb[j - 2] : pb[3 - j]);
-            const float2 r = qg::weno5_x2<Z>(e[0], e[1], e[2], e[3], e[4]);
-            fe[la][lf] = (T)(r.x * ua);
-            fe[lb][lf] = (T)(r.y * ub);
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int ly = ty + 4 * k;
-            const T uu = u[(size_t)(y0 + ly) * nx + gi];
-            fe[ly][lf] = qg::face_value_full<T, S>(&hs[ly + AH][lf - 1 + AH], 1, gi, nx, uu >= T(0)) * uu;
-          }
-        }
-        if (tid < ATY) {  // the west-most faces x0 - 1
-          const int ly = tid;
-          const T uu = u[(size_t)(y0 + ly) * nx + x0 - 1];
-          fe[ly][0] = qg::face_value_full<T, S>(&hs[ly + AH][AH - 1], 1, x0 - 1, nx, uu >= T(0)) * uu;
-        }
-      }
-      // north faces (lf, tx): face row lf = 1 + ty + 4k (face y0 + ty + 4k), and lf = 0 (y0 - 1)
-      {
-        const int gi = x0 + tx;
-        if constexpr (PACK) {
-#pragma unroll
-          for (int k = 0; k < 2; ++k) {
-            const int la = 1 + ty + 8 * k, lb = la + 4;
-            const float va = (float)v[(size_t)(y0 - 1 + la) * nx + gi], vb = (float)v[(size_t)(y0 - 1 + lb) * nx + gi];
-            const float* pa = (const float*)&hs[la - 1 + AH][tx + AH];
-            const float* pb = (const float*)&hs[lb - 1 + AH][tx + AH];
-            const bool qa = va >= 0.f, qb = vb >= 0.f;
-            float2 e[5];
-#pragma unroll
-            for (int j = 0; j < 5; ++j)
-              e[j] = make_float2(qa ? pa[(j - 2) * HW] : pa[(3 - j) * HW], qb ? pb[(j - 2) * HW] : pb[(3 - j) * HW]);
-            const float2 r = qg::weno5_x2<Z>(e[0], e[1], e[2], e[3], e[4]);
-            fn[la][tx] = (T)(r.x * va);
-            fn[lb][tx] = (T)(r.y * vb);
-          }
-        } else {
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int lf = 1 + ty + 4 * k, gj = y0 - 1 + lf;
-            const T vv = v[(size_t)gj * nx + gi];
-            fn[lf][tx] = qg::face_value_full<T, S>(&hs[lf - 1 + AH][tx + AH], HW, gj, ny, vv >= T(0)) * vv;
-          }
-        }
-        if (ty == 0) {  // the south-most faces y0 - 1
-          const T vv = v[(size_t)(y0 - 1) * nx + gi];
-          fn[0][tx] = qg::face_value_full<T, S>(&hs[AH - 1][tx + AH], HW, y0 - 1, ny, vv >= T(0)) * vv;
-        }
-      }
-      __syncthreads();
-      const T rdx = T(1) / dx, rdy = T(1) / dy;
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const int ly = ty + 4 * k;
-        const size_t c = (size_t)(y0 + ly) * nx + (x0 + tx);
-        T r = -(qg::divr(fe[ly][tx + 1] - fe[ly][tx], dx, rdx) + qg::divr(fn[ly + 1][tx] - fn[ly][tx], dy, rdy));
-        if (mh != nullptr) r = r * T(mh[c]);
-        out[c] = r;
-      }
-      return;
-    }
-  }
   for (int k = tid; k < HH * HW; k += ATHREADS) {
     int ly = k / HW, lx = k % HW;
     int gy = y0 - AH + ly, gx = x0 - AH + lx;
@@ -321,46 +224,23 @@ __global__ void cgrid_op_kernel(int op, const T* __restrict__ a, const T* __rest
 // ===========================================================================
 // Arakawa Jacobian (operators/jacobian.py:106-131): out [B, Ny-2, Nx-2].
 // ===========================================================================
-// f and g tiles (with a one-cell ring) in shared memory, a 64 x 16 output
-// tile per 256-thread block (64 columns x 4 rows of threads); the final
-// quotient is a product with 1 / (12 dx dy).
-constexpr int JTX = 64, JTY = 16;
 template <typename T>
-__global__ void __launch_bounds__(256)
-jacobian_kernel(const T* __restrict__ f, const T* __restrict__ g, T* __restrict__ out, int ny, int nx, T scale) {
-  __shared__ T fs[JTY + 2][JTX + 2];
-  __shared__ T gs[JTY + 2][JTX + 2];
-  const int b = blockIdx.z;
-  const int i0 = blockIdx.x * JTX, j0 = blockIdx.y * JTY;  // output origin; input origin (j0, i0)
-  const int tx = threadIdx.x & (JTX - 1), ty = threadIdx.x >> 6;
-  const T* F = f + (size_t)b * ny * nx;
-  const T* G = g + (size_t)b * ny * nx;
-  for (int ly = ty; ly < JTY + 2; ly += 4) {
-    const int gy = j0 + ly;
-    for (int lx = tx; lx < JTX + 2; lx += JTX) {
-      const int gx = i0 + lx;
-      const bool in = gy < ny && gx < nx;
-      const size_t c = (size_t)gy * nx + gx;
-      fs[ly][lx] = in ? F[c] : T(0);
-      gs[ly][lx] = in ? G[c] : T(0);
-    }
-  }
-  __syncthreads();
-  const int i = i0 + tx;
-  if (i >= nx - 2) return;
-  for (int ly = ty; ly < JTY; ly += 4) {
-    const int j = j0 + ly;
-    if (j >= ny - 2) break;
-    const int cy = ly + 1, cx = tx + 1;
-    auto f_ = [&](int dj, int di) { return fs[cy + dj][cx + di]; };
-    auto g_ = [&](int dj, int di) { return gs[cy + dj][cx + di]; };
-    T Jpp = (f_(0, 1) - f_(0, -1)) * (g_(1, 0) - g_(-1, 0)) - (f_(1, 0) - f_(-1, 0)) * (g_(0, 1) - g_(0, -1));
-    T Jpx = f_(0, 1) * (g_(1, 1) - g_(-1, 1)) - f_(0, -1) * (g_(1, -1) - g_(-1, -1)) -
-            f_(1, 0) * (g_(1, 1) - g_(1, -1)) + f_(-1, 0) * (g_(-1, 1) - g_(-1, -1));
-    T Jxp = g_(1, 0) * (f_(1, 1) - f_(1, -1)) - g_(-1, 0) * (f_(-1, 1) - f_(-1, -1)) -
-            g_(0, 1) * (f_(1, 1) - f_(-1, 1)) + g_(0, -1) * (f_(1, -1) - f_(-1, -1));
-    out[(size_t)b * (ny - 2) * (nx - 2) + (size_t)j * (nx - 2) + i] = (Jpp + Jpx + Jxp) * scale;
-  }
+__global__ void jacobian_kernel(const T* __restrict__ f, const T* __restrict__ g, T* __restrict__ out,
+                                int ny, int nx, T scale) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;  // output column 0..nx-3
+  int j = blockIdx.y * blockDim.y + threadIdx.y;  // output row 0..ny-3
+  int b = blockIdx.z;
+  if (i >= nx - 2 || j >= ny - 2) return;
+  const T* F = f + (size_t)b * ny * nx + (size_t)(j + 1) * nx + (i + 1);
+  const T* G = g + (size_t)b * ny * nx + (size_t)(j + 1) * nx + (i + 1);
+  auto f_ = [&](int dj, int di) { return ldg(F + dj * nx + di); };
+  auto g_ = [&](int dj, int di) { return ldg(G + dj * nx + di); };
+  T Jpp = (f_(0, 1) - f_(0, -1)) * (g_(1, 0) - g_(-1, 0)) - (f_(1, 0) - f_(-1, 0)) * (g_(0, 1) - g_(0, -1));
+  T Jpx = f_(0, 1) * (g_(1, 1) - g_(-1, 1)) - f_(0, -1) * (g_(1, -1) - g_(-1, -1)) -
+          f_(1, 0) * (g_(1, 1) - g_(1, -1)) + f_(-1, 0) * (g_(-1, 1) - g_(-1, -1));
+  T Jxp = g_(1, 0) * (f_(1, 1) - f_(1, -1)) - g_(-1, 0) * (f_(-1, 1) - f_(-1, -1)) -
+          g_(0, 1) * (f_(1, 1) - f_(-1, 1)) + g_(0, -1) * (f_(1, -1) - f_(-1, -1));
+  out[(size_t)b * (ny - 2) * (nx - 2) + (size_t)j * (nx - 2) + i] = (Jpp + Jpx + Jxp) * scale;  // scale = 1 / (12 dx dy)
 }
 
 // ===========================================================================
@@ -690,8 +570,8 @@ using namespace fvx;
                                             int nx, double dx, double dy, void* stream) {            \
     if (!f || !g || !out) return FVX_ERR_ARG;                                                        \
     if (ny < 3 || nx < 3 || batch < 1 || batch > 65535) return FVX_ERR_SHAPE;                        \
-    dim3 gr((nx - 2 + JTX - 1) / JTX, (ny - 2 + JTY - 1) / JTY, batch);                                \
-    jacobian_kernel<T><<<gr, 256, 0, fvx_stream(stream)>>>(f, g, out, ny, nx, T(1.0 / (12.0 * dx * dy))); \
+    dim3 b(32, 8), gr((nx - 2 + 31) / 32, (ny - 2 + 7) / 8, batch);                                   \
+    jacobian_kernel<T><<<gr, b, 0, fvx_stream(stream)>>>(f, g, out, ny, nx, T(1.0 / (12.0 * dx * dy)));     \
     return fvx_cuda_status();                                                                        \
   }                                                                                                  \
   extern "C" int fvx_diffusion2d_##SFX(const T* h, const T* kappa_field, double kappa, T* out,       \
