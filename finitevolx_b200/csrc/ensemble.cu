@@ -42,6 +42,14 @@ namespace ens {
 
 constexpr int TXE = 64, TYE = 16;
 constexpr int kMaxLayers = 3;
+// Modes with lambda L^2 below this (deformation radius above ~L / 45) are
+// weakly screened: their streamfunction is dominated by the largest scales,
+// and the velocity differences amplify the split DST chain's ~1e-5 relative
+// psi error past the FP32 step bar (a NumPy emulation of the chain: 5e-5 ..
+// 2.6e-4 one-step q error for 64^2 .. 1024^2 members with Rd 670 km or
+// lambda = 0, 2.4e-6 for Ld = 40 km in 5120 km at 2048^2).  They take the
+// FP64-residual refinement pass; strongly screened modes do not need it.
+constexpr double kWeakScreening = 2000.0;
 
 struct FieldDesc {
   qg::StageArgs a[3];  // the three RK stages
@@ -147,6 +155,7 @@ struct fvx_ens {
     fvx_dst_plan* plan = nullptr;
     float* psim = nullptr;
     float* fm = nullptr;  // FP32 modes (refinement right-hand side)
+    int nref = 0;         // the first nref batch entries are the weakly screened modes that take refinement
     ModeDesc* md[3] = {nullptr, nullptr, nullptr};
     LayerDesc* ld = nullptr;
     __nv_bfloat16 *hi = nullptr, *lo = nullptr;
@@ -278,12 +287,22 @@ extern "C" int fvx_ens_create(int n_members, const int* n, const int* nl, const 
     std::vector<ModeDesc> md[3];
     std::vector<LayerDesc> ld;
     double gdx = 0, gdy = 0;
+    // batch order: the weakly screened modes (lambda L^2 < kWeakScreening,
+    // L = n dx the domain width) first, so a refinement pass covers a prefix
+    // of the batch; then the rest
+    for (int m = 0; m < n_members; ++m)
+      if (n[m] == sz) batch_of[m].assign(nl[m], -1);
+    for (int pass = 0; pass < 2; ++pass)
     for (int m = 0; m < n_members; ++m) {
       if (n[m] != sz) continue;
       if (gdx == 0) { gdx = dx[m]; gdy = dy[m]; }
       if (dx[m] != gdx || dy[m] != gdy) { ens_free(e); delete e; return FVX_ERR_ARG; }  // one spacing per size
+      const double L = sz * fmax(dx[m], dy[m]);
       for (int mo = 0; mo < nl[m]; ++mo) {
-        batch_of[m].push_back(g.B++);
+        const bool weak = lam[loff[m] + mo] * L * L < kWeakScreening;
+        if (weak != (pass == 0)) continue;
+        if (weak) ++g.nref;
+        batch_of[m][mo] = g.B++;
         lams.push_back(lam[loff[m] + mo]);
         for (int s = 0; s < 3; ++s) {
           ModeDesc d{};
@@ -411,9 +430,12 @@ extern "C" int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm) {
 // Launches of one step (for the caller's launch count).
 extern "C" int fvx_ens_launches_per_step(fvx_ens* e) {
   if (!e) return -1;
-  // per stage: per group (mode split + 4 DST products + refine passes x
-  // (residual + 4 products) + layer mix) + counter reset + stage kernel
-  return 3 * ((int)e->groups.size() * (6 + 5 * e->refine) + 2);
+  // per stage: per group (mode split + 4 DST products + layer mix, plus
+  // refine passes x (residual + 4 products) when the group has weakly
+  // screened modes) + counter reset + stage kernel
+  int per = 0;
+  for (const auto& g : e->groups) per += 6 + (g.nref ? 5 * e->refine : 0);
+  return 3 * (per + 2);
 }
 
 // FP64-residual refinement passes per DST solve (default 1; 0 leaves the
@@ -455,7 +477,8 @@ extern "C" int fvx_ens_step(fvx_ens* e, int n_steps, void* stream) {
         const long long plane = (long long)g.n * g.n;
         int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, plane, g.n, g.B, gs);
         if (rc) return rc;
-        if (e->refine && (rc = fvx_dst_refine_f32(g.plan, g.fm, plane, g.n, g.psim, plane, g.n, g.B, e->refine, gs)))
+        if (e->refine && g.nref &&
+            (rc = fvx_dst_refine_f32(g.plan, g.fm, plane, g.n, g.psim, plane, g.n, g.nref, e->refine, gs)))
           return rc;
         const size_t tl = (size_t)g.nlay * g.n * g.n;
         ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, gs>>>(g.ld, g.nlay, g.n, g.psim);

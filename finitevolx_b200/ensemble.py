@@ -64,10 +64,13 @@ class QGEnsemble:
         self.set_refine(refine_passes)
 
     def set_refine(self, passes: int) -> None:
-        """FP64-residual refinement passes after each DST solve: the split
+        """FP64-residual refinement passes after the DST solves of the weakly
+        screened modes (lambda (n dx)^2 < 2000: single-layer members with a
+        deformation radius above ~L/45, every barotropic mode): the split
         tensor-core chain carries its intermediates in 16 bits (about 1e-5
-        relative error in psi, amplified by the velocity differences in
-        weakly screened members); one pass brings psi to FP32 rounding."""
+        relative error in psi), which the velocity differences amplify past
+        the FP32 step bar for those modes; one pass brings psi to FP32
+        rounding.  Strongly screened modes skip it."""
         check(fn("fvx_ens_set_refine")(self._h, I(int(passes))), "ensemble refine")
         self.refine_passes = int(passes)
         self._graph = None
