@@ -423,9 +423,11 @@ int fvx_ens_destroy(fvx_ens* e);
 int fvx_ens_io(fvx_ens* e, int member, int layer, const void* src, void* dst, void* stream);
 int fvx_ens_set_blocks_per_sm(fvx_ens* e, int blocks_per_sm);
 int fvx_ens_launches_per_step(fvx_ens* e);
-/* FP64-residual refinement passes after each batched DST solve (0-4,
- * default 1: the members' psi at FP32 rounding instead of the split
- * chain's ~1e-5; no counterpart in finitevolX, whose solve is FP64). */
+/* FP64-residual refinement passes (0-4, default 1) after the batched DST
+ * solves of the weakly screened modes (lambda (n dx)^2 < 2000, batched
+ * first in each size group): their psi at FP32 rounding instead of the
+ * split chain's ~1e-5, which the velocity differences would amplify past
+ * the FP32 step bar; no counterpart in finitevolX, whose solve is FP64. */
 int fvx_ens_set_refine(fvx_ens* e, int passes);
 int fvx_ens_step(fvx_ens* e, int n_steps, void* stream);
 
