@@ -551,10 +551,12 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
 }
 
 // out (tile) <- k sweeps from u_pre + P ec.  Halo k.
+// ec_scale (may be null): the coarse correction is read as ec * (T)*ec_scale
+// (the hybrid cycle's energy-optimal scaling, applied as the tile loads).
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT)
 up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Lev<T> C, const T* __restrict__ ec,
-              int k, T omega, T* __restrict__ out) {
+              int k, T omega, T* __restrict__ out, const double* __restrict__ ec_scale) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   const int H = k;
   const int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
@@ -577,12 +579,13 @@ up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Le
   // kernels before this one
   leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv, omega);
   grid_dep_wait();
+  const T ew = ec_scale ? (T)*ec_scale : T(1);
   for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
     const int J = CY0 + q / CW, I = CX0 + q % CW;
     const bool in = J >= 0 && J < C.ny && I >= 0 && I < C.nx;
     const size_t c = in ? (size_t)J * C.nx + I : 0;
     const T cm = in ? C.mask[c] : T(0);
-    sv[q] = in ? ec[c] * cm : T(0);
+    sv[q] = in ? (ec[c] * ew) * cm : T(0);
     scm[q] = cm;
   }
   leg_load_pair(L, x0, y0, RW, RN, f, sf, u_pre, sa);
@@ -884,7 +887,8 @@ static int leg_down(fvx_mg* g, int l, const T* f, const T* u_init, int k, cudaSt
 
 // Upward leg at host-driven level l: out <- k sweeps on f from L.u + P ec.
 template <typename T>
-static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cudaStream_t st) {
+static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cudaStream_t st,
+                  const double* ec_scale = nullptr) {
   if (k > kLegMaxSweeps) return FVX_ERR_ARG;
   int rc = leg_attr<T>();
   if (rc) return rc;
@@ -895,9 +899,9 @@ static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cuda
   const bool few = (size_t)gr.x * gr.y < (size_t)kLegFewTiles;
   const cudaError_t e =
       few ? fvx_launch_pdl(up_leg_kernel<T, 1024>, gr, dim3(1024), leg_smem<T>(k), st, L, f, (const T*)L.u,
-                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out)
+                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out, ec_scale)
           : fvx_launch_pdl(up_leg_kernel<T, 256>, gr, dim3(256), leg_smem<T>(k), st, L, f, (const T*)L.u,
-                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out);
+                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out, ec_scale);
   if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
@@ -979,12 +983,16 @@ static int hybrid_down(fvx_mg* g, const T* f, int lvl, int n_pre, cudaStream_t s
   return FVX_OK;
 }
 
+// ec_scale (may be null): scale of the level-lvl correction, applied by the
+// first upward leg as it reads it.
 template <typename T>
-static int hybrid_up(fvx_mg* g, const T* f, T* u_out, int lvl, int n_post, cudaStream_t st) {
+static int hybrid_up(fvx_mg* g, const T* f, T* u_out, int lvl, int n_post, cudaStream_t st,
+                     const double* ec_scale = nullptr) {
   LevArray<T>& A = levs<T>(g);
   for (int l = lvl - 1; l >= 0; --l) {
     const T* ec = l + 1 == lvl ? A.L[lvl].u : A.L[l + 1].tmp;
-    int rc = leg_up<T>(g, l, l == 0 ? f : A.L[l].f, ec, n_post, l == 0 ? u_out : A.L[l].tmp, st);
+    int rc = leg_up<T>(g, l, l == 0 ? f : A.L[l].f, ec, n_post, l == 0 ? u_out : A.L[l].tmp, st,
+                       l + 1 == lvl ? ec_scale : nullptr);
     if (rc) return rc;
   }
   return FVX_OK;
@@ -1001,6 +1009,7 @@ static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int
   if (rc) return rc;
   Lev<T>& C = levs<T>(g).L[lvl];
   const size_t nc = (size_t)C.ny * C.nx;
+  const double* omega_in_leg = nullptr;
   if (coarse) {
     if ((rc = coarse(ctx, C.f, C.u, st))) return rc;
     if (scale) {
@@ -1008,7 +1017,10 @@ static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int
       double* om = part + 2 * kOmegaBlocks;
       unsigned* ticket = (unsigned*)(om + 1);
       k_coarse_omega<T><<<kOmegaBlocks, 256, 0, st>>>(C, part, ticket, om);
-      k_scale<T><<<grid_for(nc), 256, 0, st>>>(C.u, nc, om);
+      // without smoothing sweeps at level lvl the first upward leg applies
+      // omega as it reads the correction; the sweeps need it applied first
+      if (n_smooth > 0) k_scale<T><<<grid_for(nc), 256, 0, st>>>(C.u, nc, om);
+      else omega_in_leg = om;
     }
   } else {
     fill_kernel<T><<<grid_for(nc), 256, 0, st>>>(C.u, nc, T(0));
@@ -1022,7 +1034,7 @@ static int hybrid_cycle(fvx_mg* g, const T* f, T* u_out, int lvl, int n_pre, int
     }
     if (a != C.u) copy_kernel<T><<<grid_for(nc), 256, 0, st>>>(C.u, a, nc);
   }
-  return hybrid_up<T>(g, f, u_out, lvl, n_post, st);
+  return hybrid_up<T>(g, f, u_out, lvl, n_post, st, omega_in_leg);
 }
 
 extern "C" int fvx_mg_vcycle_hybrid(fvx_mg* g, const void* f, void* u_out, int lvl, int n_pre, int n_post,
