@@ -29,23 +29,52 @@ DEV T tiered_face(const T* p, int st, int i, int N, bool pos, int code) {
   return face_value<T, S4>(p, st, i, N, pos);
 }
 
+// One load phase per tile: h (tile + halo), u on the tile's east faces and v
+// on its north faces land in one flat shared buffer, four loads in flight
+// per thread (eight raise the FP32 kernels' registers from 31 to 59); the
+// face fluxes then overwrite u and v in place.
 template <typename T, int S, int S4, int S6, bool MASKED>
 __global__ void __launch_bounds__(ATHREADS)
 advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __restrict__ v,
                    T* __restrict__ out, int ny, int nx, T dx, T dy,
                    const uint8_t* __restrict__ tiers, const uint8_t* __restrict__ mh) {
   constexpr int HW = ATX + 2 * AH, HH = ATY + 2 * AH;
-  __shared__ T hs[HH][HW];
-  __shared__ T fe[ATY][ATX + 1];
-  __shared__ T fn[ATY + 1][ATX];
+  constexpr int NH = HH * HW, NU = ATY * (ATX + 1), NV = (ATY + 1) * ATX, NTOT = NH + NU + NV;
+  constexpr int U = 4;
+  __shared__ T tl[NTOT];
   __shared__ uint8_t tx_[ATY][ATX + 2];
   __shared__ uint8_t ty_[ATY + 2][ATX];
+  T* hs = tl;             // [HH][HW], origin (y0 - AH, x0 - AH)
+  T* fe = tl + NH;        // [ATY][ATX + 1]: u on east faces, then the x flux
+  T* fn = tl + NH + NU;   // [ATY + 1][ATX]: v on north faces, then the y flux
   const int x0 = blockIdx.x * ATX, y0 = blockIdx.y * ATY;
   const int tid = threadIdx.x;
-  for (int k = tid; k < HH * HW; k += ATHREADS) {
-    int ly = k / HW, lx = k % HW;
-    int gy = y0 - AH + ly, gx = x0 - AH + lx;
-    hs[ly][lx] = (gy >= 0 && gy < ny && gx >= 0 && gx < nx) ? h[(size_t)gy * nx + gx] : T(0);
+  for (int k0 = tid; k0 < NTOT; k0 += U * ATHREADS) {
+    T val[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      int k = k0 + q * ATHREADS;
+      T x = T(0);
+      if (k < NH) {
+        const int ly = k / HW, lx = k - ly * HW;
+        const int gy = y0 - AH + ly, gx = x0 - AH + lx;
+        if (gy >= 0 && gy < ny && gx >= 0 && gx < nx) x = h[(size_t)gy * nx + gx];
+      } else if (k < NH + NU) {
+        k -= NH;
+        const int ly = k / (ATX + 1), lf = k - ly * (ATX + 1);
+        const int gj = y0 + ly, gi = x0 - 1 + lf;
+        if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) x = u[(size_t)gj * nx + gi];
+      } else if (k < NTOT) {
+        k -= NH + NU;
+        const int lf = k / ATX, lx = k - lf * ATX;
+        const int gj = y0 - 1 + lf, gi = x0 + lx;
+        if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) x = v[(size_t)gj * nx + gi];
+      }
+      val[q] = x;
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q)
+      if (k0 + q * ATHREADS < NTOT) tl[k0 + q * ATHREADS] = val[q];
   }
   if (MASKED) {
     for (int k = tid; k < ATY * (ATX + 2); k += ATHREADS) {
@@ -61,36 +90,36 @@ advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __
   }
   __syncthreads();
   // east faces i = x0-1 .. x0+ATX-1 on rows y0 .. y0+ATY-1
-  for (int k = tid; k < ATY * (ATX + 1); k += ATHREADS) {
+  for (int k = tid; k < NU; k += ATHREADS) {
     int ly = k / (ATX + 1), lf = k % (ATX + 1);
     int gj = y0 + ly, gi = x0 - 1 + lf;
     T f = T(0);
     if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T uu = u[(size_t)gj * nx + gi];
+      T uu = fe[k];
       bool pos = uu >= T(0);
-      const T* p = &hs[ly + AH][lf - 1 + AH];
+      const T* p = &hs[(ly + AH) * HW + lf - 1 + AH];
       T hf;
       if (MASKED) hf = tiered_face<T, S4, S6>(p, 1, gi, nx, pos, pos ? tx_[ly][lf] : tx_[ly][lf + 1]);
       else hf = face_value<T, S>(p, 1, gi, nx, pos);
       f = hf * uu;
     }
-    fe[ly][lf] = f;
+    fe[k] = f;
   }
   // north faces j = y0-1 .. y0+ATY-1 on columns x0 .. x0+ATX-1
-  for (int k = tid; k < (ATY + 1) * ATX; k += ATHREADS) {
+  for (int k = tid; k < NV; k += ATHREADS) {
     int lf = k / ATX, lx = k % ATX;
     int gj = y0 - 1 + lf, gi = x0 + lx;
     T f = T(0);
     if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T vv = v[(size_t)gj * nx + gi];
+      T vv = fn[k];
       bool pos = vv >= T(0);
-      const T* p = &hs[lf - 1 + AH][lx + AH];
+      const T* p = &hs[(lf - 1 + AH) * HW + lx + AH];
       T hf;
       if (MASKED) hf = tiered_face<T, S4, S6>(p, HW, gj, ny, pos, pos ? ty_[lf][lx] : ty_[lf + 1][lx]);
       else hf = face_value<T, S>(p, HW, gj, ny, pos);
       f = hf * vv;
     }
-    fn[lf][lx] = f;
+    fn[k] = f;
   }
   __syncthreads();
   for (int k = tid; k < ATY * ATX; k += ATHREADS) {
@@ -99,7 +128,8 @@ advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __
     if (gj >= ny || gi >= nx) continue;
     T r = T(0);
     if (gj >= 2 && gj <= ny - 3 && gi >= 2 && gi <= nx - 3)
-      r = -((fe[ly][lx + 1] - fe[ly][lx]) / dx + (fn[ly + 1][lx] - fn[ly][lx]) / dy);
+      r = -((fe[ly * (ATX + 1) + lx + 1] - fe[ly * (ATX + 1) + lx]) / dx +
+            (fn[(ly + 1) * ATX + lx] - fn[ly * ATX + lx]) / dy);
     if (MASKED || mh != nullptr) r = r * T(mh[(size_t)gj * nx + gi]);
     out[(size_t)gj * nx + gi] = r;
   }
@@ -303,13 +333,25 @@ biharmonic_kernel(const T* __restrict__ h, T* __restrict__ out, int ny, int nx, 
   const int x0 = blockIdx.x * BTX, y0 = blockIdx.y * BTY;
   const int tx = threadIdx.x & (BTX - 1), ty = threadIdx.x >> 6;
   const bool inner = x0 >= 3 && x0 + BTX <= nx - 3 && y0 >= 3 && y0 + BTY <= ny - 3;
-  for (int ly = ty; ly < BTY + 4; ly += 4) {
-    const int gy = y0 - 2 + ly;
-    const T* row = h + (size_t)gy * nx;
-    for (int lx = tx; lx < BTX + 4; lx += BTX) {
-      const int gx = x0 - 2 + lx;
-      hs[ly][lx] = (inner || (gy >= 0 && gy < ny && gx >= 0 && gx < nx)) ? row[gx] : T(0);
+  {
+    // all of this thread's tile loads in flight before any is stored
+    constexpr int RY = (BTY + 4 + 3) / 4, RX = (BTX + 4 + BTX - 1) / BTX;
+    T v[RY][RX];
+#pragma unroll
+    for (int a = 0; a < RY; ++a) {
+      const int ly = ty + 4 * a, gy = y0 - 2 + ly;
+#pragma unroll
+      for (int b = 0; b < RX; ++b) {
+        const int lx = tx + BTX * b, gx = x0 - 2 + lx;
+        const bool use = ly < BTY + 4 && lx < BTX + 4 && (inner || (gy >= 0 && gy < ny && gx >= 0 && gx < nx));
+        v[a][b] = use ? h[(size_t)gy * nx + gx] : T(0);
+      }
     }
+#pragma unroll
+    for (int a = 0; a < RY; ++a)
+#pragma unroll
+      for (int b = 0; b < RX; ++b)
+        if (ty + 4 * a < BTY + 4 && tx + BTX * b < BTX + 4) hs[ty + 4 * a][tx + BTX * b] = v[a][b];
   }
   __syncthreads();
   // L(H) at (gy, gx) from the tile (ly, lx): fluxes zero off the interior faces

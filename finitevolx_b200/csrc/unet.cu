@@ -527,6 +527,285 @@ __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const 
   }
 }
 
+// ---- single-launch inference -----------------------------------------------
+// The whole coarse solve -- the RMS s of f over wet cells, the eight conv
+// layers, the output scaling -- as one cooperative launch of one CTA per SM.
+// Every layer's weights are staged in shared memory once, while the RMS
+// partial sums run; the layers are phases separated by grid barriers.  A
+// layer's activations go to the same slots as in the layer-by-layer pass and
+// are read back through L2 only (ld.global.cg), so no SM sees a stale L1
+// line of a tensor another SM wrote in the same launch.  Each output is
+// summed in the same order as conv_tile_kernel (input channels outer, taps
+// inner, one fmaf chain per output channel).
+constexpr int kInferThreads = 512;
+constexpr int kWeightFloats = 3 * 9 * 16 + 16 * 9 * 16 + 16 * 9 * 32 + 32 * 9 * 32 + 32 * 9 * 32 + 32 * 9 * 16 +
+                              16 * 9 * 16 + 16 * 9 * 1;
+constexpr int kTileFloats = 8 * 16 * 10 * 10;  // largest phase: OUT, 8 tiles of 16 x 10 x 10
+constexpr int kInferSmem = (kWeightFloats + kTileFloats) * (int)sizeof(float);
+
+struct InferArgs {
+  const float* f;        // right-hand side at the level [h, w]
+  float* u;              // output [h, w]
+  const float* x;        // input slot: channel 1 mask, channel 2 log c (channel 0 formed from f)
+  float* act[kSlots];
+  const __nv_bfloat16* wb;          // all BF16 weights, layer by layer (with the biases' gaps)
+  const float* B[kLayers];          // each layer's FP32 biases
+  const float* mask;
+  float* scale;          // [s, 1/s] (written for inspection)
+  double* part;          // RMS partials [gridDim.x][2]
+  unsigned* bar;         // [0] arrivals, [1] generation
+  int* err;              // set when a barrier wait ran out
+  long long wait_cycles;
+  int stall;             // CTA 0 never arrives at the first barrier (the timeout test)
+  float sigma;
+  int h, w;
+};
+
+DEV unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Returns true once every CTA of the grid has arrived (their global writes
+// before the barrier visible to all); false when the wait ran past `limit`
+// SM cycles, after raising the error flag: the CTA must return.  The last
+// CTA to arrive resets the arrival count and advances the generation word,
+// so the state is ready for the next barrier and the next launch.
+DEV bool grid_barrier(unsigned* bar, int* err, long long limit) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const unsigned g = ld_acquire_u32(bar + 1);  // cannot advance before this CTA arrives
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = clock64();
+      while (ld_acquire_u32(bar + 1) == g) {
+        if (clock64() - t0 > limit) {
+          ok = 0;
+          atomicExch(err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+// in_at through L2 only (the source may have been written in this launch).
+template <int MODE>
+DEV float in_at_cg(const float* src, int h, int w, int y, int x) {
+  if (y < 0 || y >= h || x < 0 || x >= w) return 0.f;
+  if constexpr (MODE == IN_DIRECT) return __ldcg(src + (size_t)y * w + x);
+  if constexpr (MODE == IN_POOL) {
+    const int W2 = 2 * w;
+    const float* p = src + (size_t)(2 * y) * W2 + 2 * x;
+    return 0.25f * ((__ldcg(p) + __ldcg(p + 1)) + (__ldcg(p + W2) + __ldcg(p + W2 + 1)));
+  }
+  return __ldcg(src + (size_t)(y >> 1) * (w >> 1) + (x >> 1));
+}
+
+// One conv layer over the whole grid: T x T output tiles, COUT / CPT
+// threads per pixel (CPT output channels each), kInferThreads / (T T COUT /
+// CPT) tiles per CTA pass; ws: the layer's weights in shared memory as
+// [cin * 9][COUT].  x0_src / out_mask: the first and last layers' hooks of
+// conv_tile_kernel (input channel 0 = x0_src * x0s; output (y * os) *
+// out_mask).
+template <int MODE, int COUT, int CPT, int T>
+DEV void infer_conv(const float* in, int cin, const float* ws, const float* __restrict__ bias, const float* skip,
+                    float* out, int h, int w, int relu, const float* x0_src, float x0s,
+                    const float* __restrict__ out_mask, float os, float* tile) {
+  constexpr int NT = kInferThreads, TW = T + 2, GROUPS = COUT / CPT, TPT = T * T * GROUPS;
+  static_assert(COUT % CPT == 0 && NT % TPT == 0, "tile threads must divide the block");
+  constexpr int TPI = NT / TPT;
+  constexpr int U = 8;  // loads in flight per thread while a tile is staged
+  const int tid = threadIdx.x;
+  const int per = cin * TW * TW, tot = TPI * per;
+  const int tx_n = (w + T - 1) / T, ntiles = tx_n * ((h + T - 1) / T);
+  const size_t sp = src_plane(MODE, h, w);
+  const int slot = tid / TPT, r = tid - slot * TPT;
+  const int p = r % (T * T), co0 = (r / (T * T)) * CPT;
+  const int ty = p / T, tx = p % T;
+  const size_t plane = (size_t)h * w;
+  for (int t0 = blockIdx.x * TPI; t0 < ntiles; t0 += gridDim.x * TPI) {
+    __syncthreads();  // the previous pass is done with the tiles
+    for (int k0 = tid; k0 < tot; k0 += U * NT) {
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int k = k0 + u * NT;
+        const int s = k / per, kk = k - s * per;
+        const int tt = t0 + s;
+        v[u] = 0.f;
+        if (k < tot && tt < ntiles) {
+          const int ci = kk / (TW * TW), rr = kk - ci * (TW * TW);
+          const int ly = rr / TW, lx = rr - ly * TW;
+          const int gy = (tt / tx_n) * T - 1 + ly, gx = (tt % tx_n) * T - 1 + lx;
+          v[u] = (x0_src && ci == 0) ? in_at_cg<MODE>(x0_src, h, w, gy, gx) * x0s
+                                     : in_at_cg<MODE>(in + ci * sp, h, w, gy, gx);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (k0 + u * NT < tot) tile[k0 + u * NT] = v[u];
+    }
+    __syncthreads();
+    const int tt = t0 + slot;
+    if (tt >= ntiles) continue;
+    const int y = (tt / tx_n) * T + ty, x = (tt % tx_n) * T + tx;
+    const float* tb = tile + slot * per;
+    float acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
+    for (int ci = 0; ci < cin; ++ci) {
+      const float* tl = tb + ci * TW * TW + ty * TW + tx;
+      const float* wc = ws + ci * 9 * COUT + co0;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const float v = tl[(t / 3) * TW + t % 3];
+        const float* wr = wc + t * COUT;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
+      }
+    }
+    if (y >= h || x >= w) continue;
+    const size_t base = (size_t)y * w + x;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int co = co0 + c;
+      float v = acc[c] + bias[co];
+      if (skip) v += __ldcg(skip + base + co * plane);
+      if (relu) v = fmaxf(v, 0.f);
+      if (out_mask) v = (v * os) * out_mask[base];
+      out[base + co * plane] = v;
+    }
+  }
+}
+
+static_assert(kNet[0].cin == 3 && kNet[1].cin == 16 && kNet[2].cin == 16 && kNet[3].cin == 32 &&
+                  kNet[4].cin == 32 && kNet[5].cin == 32 && kNet[6].cin == 16 && kNet[7].cin == 16 &&
+                  kNet[0].cout == 16 && kNet[1].cout == 16 && kNet[2].cout == 32 && kNet[3].cout == 32 &&
+                  kNet[4].cout == 32 && kNet[5].cout == 16 && kNet[6].cout == 16 && kNet[7].cout == 1,
+              "unet_infer_kernel's layer table follows kNet");
+
+__global__ void __launch_bounds__(kInferThreads, 1) unet_infer_kernel(InferArgs a) {
+  extern __shared__ __align__(16) float ism[];
+  __shared__ double red[2][kInferThreads / 32];
+  __shared__ float sc[2];
+  float* tile = ism + kWeightFloats;
+  const int h = a.h, w = a.w;
+  const size_t plane = (size_t)h * w;
+  // every layer's weights, [cin * 9][cout] per layer: coalesced BF16 reads
+  // (8 in flight per thread), transposed as they are stored
+  {
+    constexpr int kCin[kLayers] = {3, 16, 16, 32, 32, 32, 16, 16}, kCout[kLayers] = {16, 16, 32, 32, 32, 16, 16, 1};
+    int wo = 0;        // shared-memory offset of the layer
+    size_t go = 0;     // parameter offset of the layer
+#pragma unroll
+    for (int l = 0; l < kLayers; ++l) {
+      const int cin = kCin[l], cout = kCout[l], k9 = cin * 9, n = cout * k9;
+      for (int k0 = threadIdx.x; k0 < n; k0 += 8 * kInferThreads) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = k0 + u * kInferThreads;
+          v[u] = k < n ? __bfloat162float(a.wb[go + k]) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = k0 + u * kInferThreads;  // k = co * k9 + rest
+          if (k < n) {
+            const int co = k / k9, rest = k - co * k9;
+            ism[wo + rest * cout + co] = v[u];
+          }
+        }
+      }
+      wo += n;
+      go += (size_t)n + cout;
+    }
+  }
+  // RMS: FP64 partial sums over one contiguous chunk per CTA, then every
+  // CTA adds the partials in CTA order (the same s everywhere)
+  {
+    const size_t chunk = (plane + gridDim.x - 1) / gridDim.x;
+    const size_t c0 = (size_t)blockIdx.x * chunk, c1 = c0 + chunk < plane ? c0 + chunk : plane;
+    double q2 = 0.0, cm = 0.0;
+    for (size_t c = c0 + threadIdx.x; c < c1; c += kInferThreads) {
+      const double m = a.mask[c], fv = a.f[c];
+      q2 += fv * fv * m;
+      cm += m;
+    }
+    for (int o = 16; o; o >>= 1) {
+      q2 += __shfl_xor_sync(0xffffffffu, q2, o);
+      cm += __shfl_xor_sync(0xffffffffu, cm, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = q2; red[1][threadIdx.x >> 5] = cm; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t2 = 0.0, tc = 0.0;
+      for (int i = 0; i < kInferThreads / 32; ++i) { t2 += red[0][i]; tc += red[1][i]; }
+      a.part[2 * blockIdx.x] = t2;
+      a.part[2 * blockIdx.x + 1] = tc;
+    }
+  }
+  if (a.stall && blockIdx.x == 0) return;  // never arrives: the others' waits run out
+  if (!grid_barrier(a.bar, a.err, a.wait_cycles)) return;
+  if (threadIdx.x < 32) {
+    double t2 = 0.0, tc = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += 32) {
+      t2 += __ldcg(a.part + 2 * i);
+      tc += __ldcg(a.part + 2 * i + 1);
+    }
+    for (int o = 16; o; o >>= 1) {
+      t2 += __shfl_xor_sync(0xffffffffu, t2, o);
+      tc += __shfl_xor_sync(0xffffffffu, tc, o);
+    }
+    if (threadIdx.x == 0) {
+      const double s = sqrt(t2 / (tc > 1.0 ? tc : 1.0));
+      sc[0] = (float)s;
+      sc[1] = s > 0.0 ? (float)(1.0 / s) : 0.f;
+      if (blockIdx.x == 0) { a.scale[0] = sc[0]; a.scale[1] = sc[1]; }
+    }
+  }
+  __syncthreads();
+  const float s = sc[0], rs = sc[1];
+  constexpr int o0 = 0, o1 = o0 + 3 * 9 * 16, o2 = o1 + 16 * 9 * 16, o3 = o2 + 16 * 9 * 32, o4 = o3 + 32 * 9 * 32,
+                o5 = o4 + 32 * 9 * 32, o6 = o5 + 32 * 9 * 16, o7 = o6 + 16 * 9 * 16;
+  const long long lim = a.wait_cycles;
+  infer_conv<IN_DIRECT, 16, 2, 8>(a.x, 3, ism + o0, a.B[0], nullptr, a.act[1], h, w, 1, a.f, rs, nullptr, 0.f,
+                                  tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_POOL, 16, 1, 4>(a.act[1], 16, ism + o1, a.B[1], nullptr, a.act[2], h >> 1, w >> 1, 1, nullptr, 0.f,
+                                nullptr, 0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_POOL, 32, 1, 4>(a.act[2], 16, ism + o2, a.B[2], nullptr, a.act[3], h >> 2, w >> 2, 1, nullptr, 0.f,
+                                nullptr, 0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_POOL, 32, 1, 4>(a.act[3], 32, ism + o3, a.B[3], nullptr, a.act[4], h >> 3, w >> 3, 1, nullptr, 0.f,
+                                nullptr, 0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_UP, 32, 1, 4>(a.act[4], 32, ism + o4, a.B[4], a.act[3], a.act[5], h >> 2, w >> 2, 1, nullptr, 0.f,
+                              nullptr, 0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_UP, 16, 1, 4>(a.act[5], 32, ism + o5, a.B[5], a.act[2], a.act[6], h >> 1, w >> 1, 1, nullptr, 0.f,
+                              nullptr, 0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_UP, 16, 2, 8>(a.act[6], 16, ism + o6, a.B[6], a.act[1], a.act[7], h, w, 1, nullptr, 0.f, nullptr,
+                              0.f, tile);
+  if (!grid_barrier(a.bar, a.err, lim)) return;
+  infer_conv<IN_DIRECT, 1, 1, 8>(a.act[7], 16, ism + o7, a.B[7], nullptr, a.u, h, w, 0, nullptr, 0.f, a.mask,
+                                 s * a.sigma, tile);
+}
+
 }  // namespace nn
 }  // namespace fvx
 
@@ -543,6 +822,13 @@ struct fvx_unet {
   float* mask = nullptr;
   float* scale = nullptr;
   float sigma = 1.f;
+  // single-launch inference: grid barrier state, error flag, RMS partials
+  unsigned* bar = nullptr;
+  int* err = nullptr;
+  double* rms_part = nullptr;
+  int infer_grid = 0;
+  long long wait_cycles = 4000000000LL;  // ~2 s at the boost clock
+  int stall = 0;
   std::vector<void*> allocs;
 };
 
@@ -598,6 +884,18 @@ extern "C" int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out) {
   n->loss = (double*)alloc(8);
   n->mask = (float*)alloc((size_t)h * w * 4);
   n->scale = (float*)alloc(16);
+  int dev = 0, sms = 0, occ = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      fvx_set_max_smem(unet_infer_kernel, kInferSmem) == false ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, unet_infer_kernel, kInferThreads, kInferSmem) !=
+          cudaSuccess ||
+      occ < 1)
+    ok = false;
+  n->infer_grid = sms;  // one CTA per SM: every CTA resident (cooperative launch)
+  n->bar = (unsigned*)alloc(16);
+  n->err = (int*)alloc(16);
+  n->rms_part = (double*)alloc((size_t)2 * (sms > 0 ? sms : 1) * sizeof(double));
   if (!ok || cudaDeviceSynchronize() != cudaSuccess) {
     unet_free(n);
     delete n;
@@ -731,9 +1029,81 @@ extern "C" int fvx_unet_set_level(fvx_unet* n, const float* mask, const float* l
   return fvx_cuda_status();
 }
 
+// The coarse solve of fvx_unet_coarse in one cooperative launch
+// (unet_infer_kernel).  No host synchronisation; a barrier wait that ran
+// out shows in fvx_unet_check.
+extern "C" int fvx_unet_coarse_fused(void* ctx, const void* f, void* u, void* stream) {
+  fvx_unet* n = (fvx_unet*)ctx;
+  if (!n || !f || !u) return FVX_ERR_ARG;
+  InferArgs a;
+  a.f = (const float*)f;
+  a.u = (float*)u;
+  a.x = n->act[0];
+  for (int s = 0; s < kSlots; ++s) a.act[s] = n->act[s];
+  a.wb = n->wb;
+  size_t off = 0;
+  for (int l = 0; l < kLayers; ++l) {
+    a.B[l] = n->wf + off + (size_t)kNet[l].cout * kNet[l].cin * 9;
+    off += layer_params(kNet[l]);
+  }
+  a.mask = n->mask;
+  a.scale = n->scale;
+  a.part = n->rms_part;
+  a.bar = n->bar;
+  a.err = n->err;
+  a.wait_cycles = n->wait_cycles;
+  a.stall = n->stall;
+  a.sigma = n->sigma;
+  a.h = n->h;
+  a.w = n->w;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(n->infer_grid);
+  cfg.blockDim = dim3(kInferThreads);
+  cfg.dynamicSmemBytes = kInferSmem;
+  cfg.stream = fvx_stream(stream);
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  if (cudaLaunchKernelEx(&cfg, unet_infer_kernel, a) != cudaSuccess) return FVX_ERR_CUDA;
+  return fvx_cuda_status();
+}
+
+// FVX_ERR_TIMEOUT (and the barrier state and flag cleared) when a barrier
+// wait of the single-launch inference ran out since the last check.
+// Synchronises the device.
+extern "C" int fvx_unet_check(fvx_unet* n) {
+  if (!n) return FVX_ERR_ARG;
+  int e = 0;
+  if (cudaDeviceSynchronize() != cudaSuccess || cudaMemcpy(&e, n->err, sizeof(int), cudaMemcpyDeviceToHost) !=
+                                                    cudaSuccess)
+    return FVX_ERR_CUDA;
+  if (!e) return FVX_OK;
+  if (cudaMemset(n->bar, 0, 16) != cudaSuccess || cudaMemset(n->err, 0, 16) != cudaSuccess) return FVX_ERR_CUDA;
+  return FVX_ERR_TIMEOUT;
+}
+
+// Bound (SM cycles) on each barrier wait of the single-launch inference.
+extern "C" int fvx_unet_set_wait_limit(fvx_unet* n, long long cycles) {
+  if (!n || cycles < 1) return FVX_ERR_ARG;
+  n->wait_cycles = cycles;
+  return FVX_OK;
+}
+
+// stall != 0: CTA 0 of the next launches never arrives at the first
+// barrier, so the other CTAs' waits run out (the timeout test).
+extern "C" int fvx_unet_inject_stall(fvx_unet* n, int stall) {
+  if (!n) return FVX_ERR_ARG;
+  n->stall = stall != 0;
+  return FVX_OK;
+}
+
 // Coarse solver callback (fvx_precond_fn, ctx = the network): u = s sigma
-// m net([f / s, m, log c]) with s the RMS of f over wet cells.  Launches
-// only; no host synchronisation.
+// m net([f / s, m, log c]) with s the RMS of f over wet cells, as a chain of
+// per-layer launches (the RMS kernel, then conv_tile_kernel per layer, each
+// a programmatic dependent of the one before).  Launches only; no host
+// synchronisation.
 extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) {
   fvx_unet* n = (fvx_unet*)ctx;
   if (!n || !f || !u) return FVX_ERR_ARG;

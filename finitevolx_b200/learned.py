@@ -132,6 +132,16 @@ class UNet:
         check(fn("fvx_unet_backward")(self._h, I(B), P(dy), stream_ptr()), "unet_backward")
         return self.grad()
 
+    def check_device(self) -> None:
+        """Raises if a grid-barrier wait of the single-launch inference gave
+        up since the last check (the barrier state is then reset)."""
+        check(fn("fvx_unet_check")(self._h), "unet inference")
+
+    def set_wait_limit(self, cycles: int) -> None:
+        """Bound, in SM clock cycles, on each grid-barrier wait of the
+        single-launch inference."""
+        check(fn("fvx_unet_set_wait_limit")(self._h, _I64(int(cycles))), "unet wait limit")
+
     def train_step(self, x, target, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8, loss_out=None) -> None:
         """One Adam step on the masked MSE (mask = channel 1 of x)."""
         B = self._load_x(x)
@@ -353,11 +363,13 @@ class LearnedPreconditioner:
               "unet_set_level")
 
     # -- inference ----------------------------------------------------------
-    def coarse_solve(self, f_lvl) -> torch.Tensor:
-        """The network's approximation of A_lvl^{-1} f_lvl."""
+    def coarse_solve(self, f_lvl, fused: bool = False) -> torch.Tensor:
+        """The network's approximation of A_lvl^{-1} f_lvl: one launch per
+        layer (``fused=True``: the same solve as one cooperative launch)."""
         f = L.as_field(f_lvl, dtype=torch.float32)
         u = torch.empty_like(f)
-        check(fn("fvx_unet_coarse")(self.net.handle, P(f), P(u), stream_ptr()), "unet_coarse")
+        name = "fvx_unet_coarse_fused" if fused else "fvx_unet_coarse"
+        check(fn(name)(self.net.handle, P(f), P(u), stream_ptr()), "unet_coarse")
         return u
 
     def __call__(self, r) -> torch.Tensor:

@@ -378,7 +378,18 @@ int fvx_unet_backward(fvx_unet* n, int batch, const float* dy, void* stream);
 int fvx_unet_train_step(fvx_unet* n, int batch, const float* target, double lr, double beta1, double beta2,
                         double eps, int step, double* loss_out, void* stream);
 int fvx_unet_set_level(fvx_unet* n, const float* mask, const float* logc, double sigma, void* stream);
+/* fvx_unet_coarse: one launch per layer.  fvx_unet_coarse_fused: the whole
+ * solve (RMS, 8 layers, output scaling) as one cooperative launch with grid
+ * barriers between the layers; every barrier wait is bounded
+ * (fvx_unet_set_wait_limit, SM cycles) and a wait that ran out shows as
+ * FVX_ERR_TIMEOUT in fvx_unet_check (which synchronises and resets the
+ * barrier state).  fvx_unet_inject_stall: CTA 0 skips the first barrier
+ * (the timeout test). */
 int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream);
+int fvx_unet_coarse_fused(void* ctx, const void* f, void* u, void* stream);
+int fvx_unet_check(fvx_unet* n);
+int fvx_unet_set_wait_limit(fvx_unet* n, long long cycles);
+int fvx_unet_inject_stall(fvx_unet* n, int stall);
 /* Layer-level kernels (conv3x3 with pool/upsample input, backward, MSE, Adam). */
 int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, const void* w_bf16, const float* bias,
                     const float* skip, float* out, int cout, int h, int w, int relu, void* stream);

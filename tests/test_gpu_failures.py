@@ -5,6 +5,8 @@
   barrier nothing completes; with a short wait limit (about 1 ms) the wait
   gives up, the CTA ends without trapping, the plan reports status 7 once,
   and the same plan then solves correctly (the context stays usable).
+  The U-Net's single-launch inference does the same with a grid barrier that
+  one CTA never reaches.
 * Non-convergence is a result, not an exception (finitevolX's
   CGInfo.converged, solvers/iterative.py:32-41,129-136): PCG on a NaN
   right-hand side and on an indefinite operator (lambda < 0 beyond the
@@ -49,6 +51,44 @@ def test_dst_wait_timeout_reports_status_and_recovers(cuda_ok):
     assert np.abs(got - ref).max() / np.abs(ref).max() < 1e-4
     with pytest.raises(FvxError):
         plan.set_wait_limit(10)  # below the accepted minimum
+
+
+def test_unet_barrier_timeout_reports_status_and_recovers(cuda_ok):
+    """The U-Net's single-launch inference: with CTA 0 held back from the first
+    grid barrier and a ~1 ms wait limit, the other CTAs give up, the launch
+    ends, fvx_unet_check reports status 7 once and resets the barrier, and
+    the next solve is bit-identical to one before the fault."""
+    from finitevolx_b200._lib import D, P, check, stream_ptr
+    from finitevolx_b200.learned import UNet
+
+    h = w = 32
+    rng = np.random.default_rng(7)
+    m = np.ones((h, w), np.float32)
+    m[:, :3] = 0.0
+    f = torch.from_numpy((rng.standard_normal((h, w)) * m).astype(np.float32)).cuda()
+    net = UNet(h, w, batch_max=1)
+    mt = torch.from_numpy(m).cuda()
+    lt = torch.zeros_like(mt)
+    check(fn("fvx_unet_set_level")(net.handle, P(mt), P(lt), D(1.0), stream_ptr()), "set_level")
+
+    def solve():
+        u = torch.empty_like(f)
+        check(fn("fvx_unet_coarse_fused")(net.handle, P(f), P(u), stream_ptr()), "unet_coarse_fused")
+        return u
+
+    u0 = solve()
+    net.check_device()
+    net.set_wait_limit(2_000_000)  # ~1 ms
+    assert fn("fvx_unet_inject_stall")(net.handle, 1) == 0
+    try:
+        solve()  # the call itself returns normally
+        assert fn("fvx_unet_check")(net.handle) == 7
+    finally:
+        fn("fvx_unet_inject_stall")(net.handle, 0)
+    net.check_device()
+    u1 = solve()
+    net.check_device()
+    assert torch.equal(u0, u1)
 
 
 def _basin(n=128, seed=3):

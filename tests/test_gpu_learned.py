@@ -83,6 +83,53 @@ def test_unet_train_step_loss_and_adam(cuda_ok):
     np.testing.assert_allclose(net.params().cpu().numpy(), th1, atol=1e-6, rtol=0)
 
 
+def _set_level(net, m, logc, sigma):
+    from finitevolx_b200._lib import D, P, check, fn, stream_ptr
+    mt = torch.from_numpy(m).cuda()
+    lt = torch.from_numpy(logc).cuda()
+    check(fn("fvx_unet_set_level")(net.handle, P(mt), P(lt), D(sigma), stream_ptr()), "set_level")
+    torch.cuda.synchronize()
+
+
+def _coarse(net, f, fused=False):
+    from finitevolx_b200._lib import P, check, fn, stream_ptr
+    ft = torch.from_numpy(f).cuda()
+    u = torch.empty_like(ft)
+    name = "fvx_unet_coarse_fused" if fused else "fvx_unet_coarse"
+    check(fn(name)(net.handle, P(ft), P(u), stream_ptr()), name)
+    return u
+
+
+@pytest.mark.parametrize("h,w", [(64, 64), (40, 56), (128, 128)])
+def test_unet_coarse_single_launch_matches_oracle(cuda_ok, h, w):
+    """The coarse solve (per-layer launches, and the same in one cooperative
+    launch) against the oracle's s sigma m net([f / s, m, log c]);
+    40 x 56 leaves partial tiles on every level."""
+    theta, _, _ = _net_case(5, B=1, h=h, w=w)
+    rng = np.random.default_rng(6)
+    m = (rng.random((h, w)) > 0.3).astype(np.float32)
+    logc = (0.3 * rng.standard_normal((h, w)) * m).astype(np.float32)
+    f = (rng.standard_normal((h, w)) * m).astype(np.float32)
+    net = UNet(h, w, batch_max=1)
+    net.set_params(theta)
+    sigma = 0.37
+    _set_level(net, m, logc, sigma)
+    u = _coarse(net, f, fused=True)
+    u2 = _coarse(net, f, fused=True)
+    ul = _coarse(net, f)
+    net.check_device()
+    fd, md = f.astype(np.float64), m.astype(np.float64)
+    s = np.sqrt((fd * fd * md).sum() / max(md.sum(), 1.0))
+    x = np.stack([fd / s, md, logc.astype(np.float64)])[None]
+    ref = s * sigma * md * U.forward(theta.astype(np.float64), x)[8][0, 0]
+    got = u.cpu().numpy()
+    assert nrel(got, ref) < 2e-5
+    assert nrel(ul.cpu().numpy(), ref) < 2e-5
+    assert nrel(got, ul.cpu().numpy()) < 1e-6
+    assert torch.equal(u, u2)  # fixed reduction order: run-to-run identical
+    assert np.all(got[m == 0] == 0)
+
+
 @pytest.fixture(scope="module")
 def problem128(cuda_ok):
     n = 128
