@@ -364,172 +364,241 @@ constexpr int kOmegaBlocks = 64;
 //   down: u = k Jacobi sweeps from u_init (NULL = 0) on f, then the
 //         restricted residual R (f - A u) into the next level's f;
 //   up:   u = u_pre + P e_coarse, then k Jacobi sweeps, into ``out``.
-// Each CTA loads its output tile plus a halo of k (+1 for the residual) of
-// f, mask, cx, cy and inv_diag into shared memory once and runs all sweeps
-// there (the valid region shrinks by one cell per sweep); the arithmetic of
-// every cell is jacobi_at / restrict_at / prolong_at's, in the same order.
+// A CTA covers its output tile plus a halo of H = k (+1 for the residual):
+// an RW x RH region.  Thread tid owns column c = tid % RW of the region and
+// rows r0 .. r0 + LR - 1 of it (r0 = (tid / RW) LR): those cells' u, f,
+// omega * inv_diag, cx, cy and mask stay in its registers for the whole leg;
+// shared memory holds u (two buffers, for the neighbours' reads) and cx
+// (for the west face).  Every sweep updates the whole region but its outer
+// ring: a cell d cells from the region's edge is exact after d sweeps, so
+// after k sweeps the tile and a ring of H - k around it hold the global
+// Jacobi iterate, as in the shrinking-region form.  The arithmetic of every
+// cell is jacobi_at / restrict_at / prolong_at's, in the same order.
 // ---------------------------------------------------------------------------
 constexpr int kLegMaxSweeps = 16;
-constexpr int kLegFewTiles = 148;  // legs with fewer tiles run 1024-thread CTAs
+constexpr int kLegFewTiles = 148;  // legs with fewer tiles use more threads per CTA
 
 template <typename T> struct LegTile;
 template <> struct LegTile<float> { static constexpr int TX = 64, TY = 32; };
 template <> struct LegTile<double> { static constexpr int TX = 32, TY = 16; };
 
-// One weighted-Jacobi update on a shared-memory tile whose u is already
-// masked (zero on dry cells) and whose winv holds omega * inv_diag (zero on
-// dry cells): jacobi_at's arithmetic with the multiplications by the 0/1
-// mask dropped.  On a wet cell those multiply by 1 (exact); on a dry cell
+// One weighted-Jacobi update of a cell from its own and its neighbours'
+// values: jacobi_at's arithmetic with the multiplications by the 0/1 mask
+// dropped (u is masked -- zero on dry cells -- and winv = omega * inv_diag
+// is zero there).  On a wet cell those multiply by 1 (exact); on a dry cell
 // the result is u + 0 * r = 0, as the masked form gives (up to the sign of
 // zero), so the values are the same.
 template <typename T>
-DEV T jac_s(const T* u, const T* f, const T* cx, const T* cy, const T* winv, int k, int RW, T dx2, T rdx2, T dy2,
-            T rdy2, T lam) {
-  const T um = u[k];
-  const T ue = u[k + 1];
-  const T uw = u[k - 1];
-  const T un = u[k + RW];
-  const T us = u[k - RW];
-  const T lap = divd(cx[k] * (ue - um) - cx[k - 1] * (um - uw), dx2, rdx2) +
-                divd(cy[k] * (un - um) - cy[k - RW] * (um - us), dy2, rdy2);
-  const T r = f[k] - (lap - lam * um);
-  return um + winv[k] * r;
+DEV T jac_v(T um, T ue, T uw, T un, T us, T cx, T cxw, T cy, T cys, T f, T winv, T dx2, T rdx2, T dy2, T rdy2,
+            T lam) {
+  const T lap = divd(cx * (ue - um) - cxw * (um - uw), dx2, rdx2) + divd(cy * (un - um) - cys * (um - us), dy2, rdy2);
+  const T r = f - (lap - lam * um);
+  return um + winv * r;
 }
 
+// Region geometry of a leg with halo H on a TX x TY tile.
+struct LegShape {
+  int RW, RH, RN, LR;  // LR: rows per thread
+};
 template <typename T>
-DEV T res_s(const T* u, const T* f, const T* m, const T* cx, const T* cy, int k, int RW, T dx2, T rdx2, T dy2,
-            T rdy2, T lam) {
-  const T mc = m[k];
-  const T um = u[k] * mc;
-  const T ue = u[k + 1] * m[k + 1];
-  const T uw = u[k - 1] * m[k - 1];
-  const T un = u[k + RW] * m[k + RW];
-  const T us = u[k - RW] * m[k - RW];
-  const T lap = divd(cx[k] * (ue - um) - cx[k - 1] * (um - uw), dx2, rdx2) +
-                divd(cy[k] * (un - um) - cy[k - RW] * (um - us), dy2, rdy2);
-  return (f[k] - (lap - lam * um) * mc) * mc;
+__host__ __device__ inline LegShape leg_shape(int H, int nt) {
+  LegShape g;
+  g.RW = LegTile<T>::TX + 2 * H;
+  g.RH = LegTile<T>::TY + 2 * H;
+  g.RN = g.RW * g.RH;
+  const int nseg = nt / g.RW;
+  g.LR = nseg > 0 ? (g.RH + nseg - 1) / nseg : 1 << 20;
+  return g;
 }
 
-// fnc(ly, lx) on the cells of the w x h region with corner (s, s) that this
-// thread owns (region index tid, tid + blockDim.x, ...), the indices
-// advanced without divisions.
-template <typename F>
-DEV void leg_region(int s, int w, int h, F&& fnc) {
-  const int n = w * h, dq = (int)blockDim.x / w, dr = (int)blockDim.x - dq * w;
-  int j = (int)threadIdx.x / w, i = (int)threadIdx.x - j * w;
-  for (int q = threadIdx.x; q < n; q += blockDim.x) {
-    fnc(s + j, s + i);
-    i += dr;
-    j += dq;
-    if (i >= w) { i -= w; ++j; }
-  }
+// Coarse window of an up leg (prolongation sources of the region).
+struct CoarseWin {
+  int CX0, CY0, CW, CH;
+};
+__host__ __device__ inline CoarseWin coarse_win(int x0, int y0, int RW, int RH) {
+  CoarseWin w;
+  w.CX0 = (x0 >> 1) - 1;
+  w.CY0 = (y0 >> 1) - 1;
+  w.CW = ((x0 + RW - 1) >> 1) + 1 - w.CX0 + 1;
+  w.CH = ((y0 + RH - 1) >> 1) + 1 - w.CY0 + 1;
+  return w;
 }
 
+// Shared memory of a leg with k sweeps (both kinds): cx and two u buffers
+// over the halo-(k + 1) region, and the up leg's coarse window (twice).
 template <typename T>
 static size_t leg_smem(int k) {
-  constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
-  const int H = k + 1;
-  const size_t RN = (size_t)(TX + 2 * H) * (TY + 2 * H);
-  const size_t CN = (size_t)((TX + 2 * H) / 2 + 3) * ((TY + 2 * H) / 2 + 3);
-  return (7 * RN + 2 * CN) * sizeof(T);
+  const LegShape g = leg_shape<T>(k + 1, 1);
+  const size_t CN = (size_t)((g.RW + 1) / 2 + 3) * ((g.RH + 1) / 2 + 3);
+  return (3 * (size_t)g.RN + 2 * CN) * sizeof(T);
 }
 
-// Shared-memory tile (origin (y0, x0), RW wide, RN cells) of the level's
-// mask, cx, cy and omega * inv_diag, zero outside the level.
-template <typename T>
-DEV void leg_load_tile(const Lev<T>& L, int x0, int y0, int RW, int RN, T* sm, T* scx, T* scy, T* sinv, T omega) {
-  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
-    T v[4][4];
+// Per-thread cell state of a leg: R register slots for the thread's rows.
+template <typename T, int R>
+struct LegCells {
+  T u[R], f[R], w[R], cx[R], cy[R];
+  unsigned wet = 0;   // bit i: row slot i is a wet cell
+  T cy_south = T(0);  // cy of the row below the thread's first row
+};
+
+// The level's constants of the thread's cells (zero outside the level):
+// mask bits, cx, cy, omega * inv_diag; cx also into the shared tile.
+template <typename T, int R>
+DEV void leg_load_constants(const Lev<T>& L, LegCells<T, R>& s, T* scx, int x0, int y0, int RW, int RH, int c,
+                            int r0, int LR, bool act, T omega) {
+  const int gx = x0 + c;
+  const bool colg = act && gx >= 0 && gx < L.nx;
+  T mv[R];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      const int ly = q / RW, lx = q - ly * RW;
-      const int gy = y0 + ly, gx = x0 + lx;
-      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-      v[u][0] = in ? L.mask[c] : T(0);
-      v[u][1] = in ? L.cx[c] : T(0);
-      v[u][2] = in ? L.cy[c] : T(0);
-      v[u][3] = in ? L.inv[c] : T(0);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      if (q < RN) { sm[q] = v[u][0]; scx[q] = v[u][1]; scy[q] = v[u][2]; sinv[q] = omega * v[u][3]; }
-    }
+  for (int i = 0; i < R; ++i) {
+    const int r = r0 + i, gy = y0 + r;
+    const bool in = colg && i < LR && r < RH && gy >= 0 && gy < L.ny;
+    const size_t g = in ? (size_t)gy * L.nx + gx : 0;
+    mv[i] = in ? L.mask[g] : T(0);
+    s.cx[i] = in ? L.cx[g] : T(0);
+    s.cy[i] = in ? L.cy[g] : T(0);
+    s.w[i] = in ? L.inv[g] : T(0);
   }
-}
-// The same tile of two level arrays a and b (b may be null: zeros).
-template <typename T>
-DEV void leg_load_pair(const Lev<T>& L, int x0, int y0, int RW, int RN, const T* a, T* sa_, const T* b, T* sb_) {
-  for (int q0 = threadIdx.x; q0 < RN; q0 += 4 * blockDim.x) {
-    T v[4][2];
+  {
+    const int gy = y0 + r0 - 1;
+    const bool in = colg && r0 >= 1 && gy >= 0 && gy < L.ny;
+    s.cy_south = in ? L.cy[(size_t)gy * L.nx + gx] : T(0);
+  }
+  s.wet = 0;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      const int ly = q / RW, lx = q - ly * RW;
-      const int gy = y0 + ly, gx = x0 + lx;
-      const bool in = q < RN && gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-      const size_t c = in ? (size_t)gy * L.nx + gx : 0;
-      v[u][0] = in ? a[c] : T(0);
-      v[u][1] = (in && b) ? b[c] : T(0);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int q = q0 + u * blockDim.x;
-      if (q < RN) { sa_[q] = v[u][0]; sb_[q] = v[u][1]; }
-    }
+  for (int i = 0; i < R; ++i) {
+    s.w[i] = omega * s.w[i];
+    if (mv[i] != T(0)) s.wet |= 1u << i;
+    if (act && i < LR && r0 + i < RH) scx[(r0 + i) * RW + c] = s.cx[i];
   }
 }
 
-// L.u (tile) <- k sweeps; C.f <- restricted residual.  Halo k + 1.
-// NT threads: 256 on the fine levels (two CTAs per SM), 1024 on levels with
-// fewer tiles than SMs, where one CTA's sweeps are the whole leg's latency.
-template <typename T, int NT>
+// k Jacobi sweeps of the region held in (registers, A); returns the buffer
+// holding the final u (the registers hold the thread's own final values).
+template <typename T, int R>
+DEV T* leg_sweeps(const Lev<T>& L, LegCells<T, R>& s, T* A, T* B, const T* scx, int k, int RW, int RH, int c,
+                  int r0, int LR, bool act) {
+  const bool colin = act && c >= 1 && c <= RW - 2;
+  for (int sw = 0; sw < k; ++sw) {
+    T us = (colin && r0 >= 1) ? A[(r0 - 1) * RW + c] : T(0);  // old u of the row below
+    T cys = s.cy_south;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = r0 + i;
+      if (act && i < LR && r < RH) {
+        const T um = s.u[i];
+        T nv = um;
+        if (colin && r >= 1 && r <= RH - 2) {
+          const int q = r * RW + c;
+          const T un = (i + 1 < R && i + 1 < LR) ? s.u[i + 1 < R ? i + 1 : i] : A[q + RW];
+          nv = jac_v(um, A[q + 1], A[q - 1], un, us, s.cx[i], scx[q - 1], s.cy[i], cys, s.f[i], s.w[i], L.dx2,
+                     L.rdx2, L.dy2, L.rdy2, L.lam);
+        }
+        us = um;
+        cys = s.cy[i];
+        s.u[i] = nv;
+        B[r * RW + c] = nv;
+      }
+    }
+    __syncthreads();
+    T* t = A;
+    A = B;
+    B = t;
+  }
+  return A;
+}
+
+// The legs' thread configurations: NT threads with R register rows each; the
+// host takes the first that covers the region (LR <= R).  The legs are
+// programmatic dependents: what the kernel before them wrote (f, u_init,
+// u_pre, ec, ec_scale) is read only after grid_dep_wait, through L2
+// (ld.global.cg), from pointers not marked __restrict__ -- a restrict-const
+// load may be served by the read-only path or moved above the wait.
+template <typename T, int NT, int R>
 __global__ void __launch_bounds__(NT)
-down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init, int k, T omega, Lev<T> C) {
+down_leg_kernel(Lev<T> L, const T* f, const T* u_init, int k, T omega, Lev<T> C) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   const int H = k + 1;
-  const int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
+  const LegShape g = leg_shape<T>(H, NT);
+  const int RW = g.RW, RH = g.RH, LR = g.LR;
   extern __shared__ __align__(16) unsigned char leg_raw[];
-  T* sf = (T*)leg_raw;
-  T* sm = sf + RN;
-  T* scx = sm + RN;
-  T* scy = scx + RN;
-  T* sinv = scy + RN;
-  T* sa = sinv + RN;
-  T* sb = sa + RN;
+  T* scx = (T*)leg_raw;
+  T* A = scx + g.RN;
+  T* B = A + g.RN;
   const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
-  // the level's constant arrays, then (after the previous kernel, which
-  // wrote f and u_init) f and u_init; batches of 4 cells per thread, all
-  // loads of a batch in flight before any store
-  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv, omega);
+  const int seg = threadIdx.x / RW, c = threadIdx.x - seg * RW, r0 = seg * LR;
+  const bool act = r0 < RH;
+  LegCells<T, R> s;
+  // the level's constants, then (after the previous kernel, which wrote f
+  // and u_init) f and u_init
+  leg_load_constants<T, R>(L, s, scx, x0, y0, RW, RH, c, r0, LR, act, omega);
   grid_dep_wait();
-  leg_load_pair(L, x0, y0, RW, RN, f, sf, u_init, sa);
+  {
+    const int gx = x0 + c;
+    const bool colg = act && gx >= 0 && gx < L.nx;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = r0 + i, gy = y0 + r;
+      const bool in = colg && i < LR && r < RH && gy >= 0 && gy < L.ny;
+      const size_t gg = in ? (size_t)gy * L.nx + gx : 0;
+      s.f[i] = in ? __ldcg(f + gg) : T(0);
+      s.u[i] = (in && u_init) ? __ldcg(u_init + gg) : T(0);
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      if (u_init) s.u[i] *= ((s.wet >> i) & 1u) ? T(1) : T(0);  // the sweeps take u masked
+      if (act && i < LR && r0 + i < RH) A[(r0 + i) * RW + c] = s.u[i];
+    }
+  }
   __syncthreads();
   grid_dep_launch();  // the next kernel may start loading its constants
-  if (u_init) {  // the sweeps take u masked (each thread its own cells)
-    for (int q = threadIdx.x; q < RN; q += blockDim.x) sa[q] *= sm[q];
-    __syncthreads();
+  A = leg_sweeps<T, R>(L, s, A, B, scx, k, RW, RH, c, r0, LR, act);
+  B = A == scx + g.RN ? A + g.RN : scx + g.RN;
+  // the tile's u, and its residual * mask (u is masked, so the neighbours'
+  // masks multiply by 1 or meet a zero: res_s's values)
+  T rm[R];
+  {
+    const bool colt = act && c >= H && c < H + TX;
+    const int gx = x0 + c;
+    T us = (colt && r0 >= 1) ? A[(r0 - 1) * RW + c] : T(0);
+    T cys = s.cy_south;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = r0 + i;
+      rm[i] = T(0);
+      if (act && i < LR && r < RH) {
+        const T um = s.u[i];
+        if (colt && r >= H && r < H + TY) {
+          const int gy = y0 + r;
+          if (gy < L.ny && gx < L.nx) L.u[(size_t)gy * L.nx + gx] = um;
+          const int q = r * RW + c;
+          const T un = (i + 1 < R && i + 1 < LR) ? s.u[i + 1 < R ? i + 1 : i] : A[q + RW];
+          const T ue = A[q + 1], uw = A[q - 1];
+          const T mc = ((s.wet >> i) & 1u) ? T(1) : T(0);
+          const T lap = divd(s.cx[i] * (ue - um) - scx[q - 1] * (um - uw), L.dx2, L.rdx2) +
+                        divd(s.cy[i] * (un - um) - cys * (um - us), L.dy2, L.rdy2);
+          rm[i] = ((s.f[i] - (lap - L.lam * um) * mc) * mc) * mc;
+        }
+        us = um;
+        cys = s.cy[i];
+      }
+    }
   }
-  T* a = sa;
-  T* b = sb;
-  for (int s = 1; s <= k; ++s) {
-    leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
-      const int kk = ly * RW + lx;
-      b[kk] = jac_s(a, sf, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
-    });
-    __syncthreads();
-    T* t = a; a = b; b = t;
+  __syncthreads();  // every read of A is done: A <- r * m, B <- m on the tile
+  {
+    const bool colt = act && c >= H && c < H + TX;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int r = r0 + i;
+      if (colt && i < LR && r >= H && r < H + TY) {
+        A[r * RW + c] = rm[i];
+        B[r * RW + c] = ((s.wet >> i) & 1u) ? T(1) : T(0);
+      }
+    }
   }
-  // a is valid on the tile and one ring around it
-  for (int q = threadIdx.x; q < TX * TY; q += blockDim.x) {
-    const int ly = H + q / TX, lx = H + q % TX;
-    const int gy = y0 + ly, gx = x0 + lx;
-    if (gy < L.ny && gx < L.nx) L.u[(size_t)gy * L.nx + gx] = a[ly * RW + lx];
-  }
+  __syncthreads();
   constexpr int CX = TX / 2, CY = TY / 2;
-  for (int q = threadIdx.x; q < CX * CY; q += blockDim.x) {
+  for (int q = threadIdx.x; q < CX * CY; q += NT) {
     const int Jl = q / CX, Il = q % CX;
     const int J = blockIdx.y * CY + Jl, I = blockIdx.x * CX + Il;
     if (J >= C.ny || I >= C.nx) continue;
@@ -538,10 +607,8 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
 #pragma unroll
     for (int t = 0; t < 4; ++t) {
       const int kk = (H + 2 * Jl + dj[t]) * RW + (H + 2 * Il + di[t]);
-      const T mf = sm[kk];
-      const T r = res_s(a, sf, sm, scx, scy, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
-      sv[t] = r * mf;
-      mv[t] = mf;
+      sv[t] = A[kk];
+      mv[t] = B[kk];
     }
     const T sum4 = ((sv[0] + sv[1]) + sv[2]) + sv[3];
     const T cnt = ((mv[0] + mv[1]) + mv[2]) + mv[3];
@@ -552,77 +619,80 @@ down_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_init,
 
 // out (tile) <- k sweeps from u_pre + P ec.  Halo k.
 // ec_scale (may be null): the coarse correction is read as ec * (T)*ec_scale
-// (the hybrid cycle's energy-optimal scaling, applied as the tile loads).
-template <typename T, int NT>
+// (the hybrid cycle's energy-optimal scaling, applied as the window loads).
+template <typename T, int NT, int R>
 __global__ void __launch_bounds__(NT)
-up_leg_kernel(Lev<T> L, const T* __restrict__ f, const T* __restrict__ u_pre, Lev<T> C, const T* __restrict__ ec,
-              int k, T omega, T* __restrict__ out, const double* __restrict__ ec_scale) {
+up_leg_kernel(Lev<T> L, const T* f, const T* u_pre, Lev<T> C, const T* ec, int k, T omega, T* __restrict__ out,
+              const double* ec_scale) {
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   const int H = k;
-  const int RW = TX + 2 * H, RH = TY + 2 * H, RN = RW * RH;
+  const LegShape g = leg_shape<T>(H, NT);
+  const int RW = g.RW, RH = g.RH, LR = g.LR;
   // the buffer layout of leg_smem(k) (sized for halo k + 1)
-  const int RNmax = (TX + 2 * (k + 1)) * (TY + 2 * (k + 1));
+  const int RNmax = leg_shape<T>(k + 1, 1).RN;
   extern __shared__ __align__(16) unsigned char leg_raw[];
-  T* sf = (T*)leg_raw;
-  T* sm = sf + RNmax;
-  T* scx = sm + RNmax;
-  T* scy = scx + RNmax;
-  T* sinv = scy + RNmax;
-  T* sa = sinv + RNmax;
-  T* sb = sa + RNmax;
-  T* sv = sb + RNmax;  // coarse e * mask
+  T* scx = (T*)leg_raw;
+  T* A = scx + RNmax;
+  T* B = A + RNmax;
+  T* sv = B + RNmax;  // coarse e * mask
   const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
-  const int CX0 = (x0 >> 1) - 1, CY0 = (y0 >> 1) - 1;
-  const int CW = ((x0 + RW - 1) >> 1) + 1 - CX0 + 1, CH = ((y0 + RH - 1) >> 1) + 1 - CY0 + 1;
-  T* scm = sv + CW * CH;  // coarse mask
+  const CoarseWin cw = coarse_win(x0, y0, RW, RH);
+  T* scm = sv + cw.CW * cw.CH;  // coarse mask
+  const int seg = threadIdx.x / RW, c = threadIdx.x - seg * RW, r0 = seg * LR;
+  const bool act = r0 < RH;
+  LegCells<T, R> s;
   // constants first; the coarse correction ec, f and u_pre come from the
   // kernels before this one
-  leg_load_tile(L, x0, y0, RW, RN, sm, scx, scy, sinv, omega);
+  leg_load_constants<T, R>(L, s, scx, x0, y0, RW, RH, c, r0, LR, act, omega);
   grid_dep_wait();
-  const T ew = ec_scale ? (T)*ec_scale : T(1);
-  for (int q = threadIdx.x; q < CW * CH; q += blockDim.x) {
-    const int J = CY0 + q / CW, I = CX0 + q % CW;
+  const T ew = ec_scale ? (T)__ldcg(ec_scale) : T(1);
+  for (int q = threadIdx.x; q < cw.CW * cw.CH; q += NT) {
+    const int J = cw.CY0 + q / cw.CW, I = cw.CX0 + q % cw.CW;
     const bool in = J >= 0 && J < C.ny && I >= 0 && I < C.nx;
-    const size_t c = in ? (size_t)J * C.nx + I : 0;
-    const T cm = in ? C.mask[c] : T(0);
-    sv[q] = in ? (ec[c] * ew) * cm : T(0);
+    const size_t cc = in ? (size_t)J * C.nx + I : 0;
+    const T cm = in ? C.mask[cc] : T(0);
+    sv[q] = in ? (__ldcg(ec + cc) * ew) * cm : T(0);
     scm[q] = cm;
   }
-  leg_load_pair(L, x0, y0, RW, RN, f, sf, u_pre, sa);
+  T up[R];
+  const int gx = x0 + c;
+  const bool colg = act && gx >= 0 && gx < L.nx;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = r0 + i, gy = y0 + r;
+    const bool in = colg && i < LR && r < RH && gy >= 0 && gy < L.ny;
+    const size_t gg = in ? (size_t)gy * L.nx + gx : 0;
+    s.f[i] = in ? __ldcg(f + gg) : T(0);
+    up[i] = in ? __ldcg(u_pre + gg) : T(0);
+  }
   __syncthreads();
   grid_dep_launch();
-  leg_region(0, RW, RH, [&](int ly, int lx) {
-    const int q = ly * RW + lx;
-    const int gy = y0 + ly, gx = x0 + lx;
-    const bool in = gy >= 0 && gy < L.ny && gx >= 0 && gx < L.nx;
-    const T mf = sm[q];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = r0 + i, gy = y0 + r;
+    if (!(act && i < LR && r < RH)) continue;
+    const bool in = colg && gy >= 0 && gy < L.ny;
+    const T mf = ((s.wet >> i) & 1u) ? T(1) : T(0);
     T u = T(0);
     if (in) {
       const int J = gy >> 1, I = gx >> 1, sj = 2 * (gy & 1) - 1, si = 2 * (gx & 1) - 1;
-      auto V = [&](int jj, int ii) -> T { return sv[(jj - CY0) * CW + (ii - CX0)]; };
-      auto M = [&](int jj, int ii) -> T { return scm[(jj - CY0) * CW + (ii - CX0)]; };
+      auto V = [&](int jj, int ii) -> T { return sv[(jj - cw.CY0) * cw.CW + (ii - cw.CX0)]; };
+      auto M = [&](int jj, int ii) -> T { return scm[(jj - cw.CY0) * cw.CW + (ii - cw.CX0)]; };
       const T ws = ((T(9) * V(J, I) + T(3) * V(J, I + si)) + T(3) * V(J + sj, I)) + T(1) * V(J + sj, I + si);
       const T ds = ((T(9) * M(J, I) + T(3) * M(J, I + si)) + T(3) * M(J + sj, I)) + T(1) * M(J + sj, I + si);
       const T e = (ws / (ds > T(1) ? ds : T(1))) * mf;
-      u = (sa[q] + e) * mf;
+      u = (up[i] + e) * mf;
     }
-    sb[q] = u;
-  });
-  __syncthreads();
-  T* a = sb;  // u_pre + P e, masked
-  T* b = sa;
-  for (int s = 1; s <= k; ++s) {
-    leg_region(s, RW - 2 * s, RH - 2 * s, [&](int ly, int lx) {
-      const int kk = ly * RW + lx;
-      b[kk] = jac_s(a, sf, scx, scy, sinv, kk, RW, L.dx2, L.rdx2, L.dy2, L.rdy2, L.lam);
-    });
-    __syncthreads();
-    T* t = a; a = b; b = t;
+    s.u[i] = u;
+    A[r * RW + c] = u;
   }
-  for (int q = threadIdx.x; q < TX * TY; q += blockDim.x) {
-    const int ly = H + q / TX, lx = H + q % TX;
-    const int gy = y0 + ly, gx = x0 + lx;
-    if (gy < L.ny && gx < L.nx) out[(size_t)gy * L.nx + gx] = a[ly * RW + lx];
+  __syncthreads();
+  A = leg_sweeps<T, R>(L, s, A, B, scx, k, RW, RH, c, r0, LR, act);
+  const bool colt = act && c >= H && c < H + TX && gx < L.nx;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int r = r0 + i, gy = y0 + r;
+    if (colt && i < LR && r >= H && r < H + TY && gy < L.ny) out[(size_t)gy * L.nx + gx] = s.u[i];
   }
 }
 
@@ -840,13 +910,34 @@ extern "C" int fvx_mg_level(fvx_mg* g, int level, int* ny, int* nx, double* dx2,
 
 extern "C" int fvx_mg_num_levels(fvx_mg* g) { return g ? g->nl : -1; }
 
+// The legs' thread configurations: 0 = (512 threads, 4 register rows),
+// 1 = (512, 8), 2 = (1024, 4), 3 = (1024, 8); the first in the type's order
+// whose rows cover the region is used.  FP32 prefers 1024 x 4 (63 registers:
+// one CTA of 32 warps per SM); FP64 prefers 512 x 4 (1024 x 4 would spill),
+// except on levels with fewer tiles than SMs, where more threads per tile
+// shorten each CTA's sweeps.
+constexpr int kLegNT[4] = {512, 512, 1024, 1024}, kLegR[4] = {4, 8, 4, 8};
+template <typename T>
+static int leg_config(int H, bool few) {
+  static constexpr int order32[4] = {2, 3, 1, 0}, order64[4] = {0, 1, 2, 3}, order_few[4] = {2, 3, 0, 1};
+  const int* order = few ? order_few : (sizeof(T) == 4 ? order32 : order64);
+  for (int j = 0; j < 4; ++j) {
+    const int i = order[j];
+    if (leg_shape<T>(H, kLegNT[i]).LR <= kLegR[i]) return i;
+  }
+  return -1;
+}
+
 template <typename T>
 static int leg_attr() {
   static fvx_once_per_device attr;
   return fvx_once_on_device(attr, [] {
     const int bytes = (int)leg_smem<T>(kLegMaxSweeps);
-    return fvx_set_max_smem(down_leg_kernel<T, 256>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 256>, bytes) &&
-           fvx_set_max_smem(down_leg_kernel<T, 1024>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 1024>, bytes);
+    return fvx_set_max_smem(down_leg_kernel<T, 512, 4>, bytes) && fvx_set_max_smem(down_leg_kernel<T, 512, 8>, bytes) &&
+           fvx_set_max_smem(down_leg_kernel<T, 1024, 4>, bytes) &&
+           fvx_set_max_smem(down_leg_kernel<T, 1024, 8>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 512, 4>, bytes) &&
+           fvx_set_max_smem(up_leg_kernel<T, 512, 8>, bytes) && fvx_set_max_smem(up_leg_kernel<T, 1024, 4>, bytes) &&
+           fvx_set_max_smem(up_leg_kernel<T, 1024, 8>, bytes);
   });
 }
 
@@ -873,14 +964,20 @@ static int leg_down(fvx_mg* g, int l, const T* f, const T* u_init, int k, cudaSt
   Lev<T>& L = A.L[l];
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  // programmatic launch: the constant tiles load while the kernel before
+  // programmatic launch: the constants load while the kernel before
   // finishes (the kernel waits before reading f and u_init)
-  const bool few = (size_t)gr.x * gr.y < (size_t)kLegFewTiles;
-  const cudaError_t e =
-      few ? fvx_launch_pdl(down_leg_kernel<T, 1024>, gr, dim3(1024), leg_smem<T>(k), st, L, f, u_init, k,
-                           (T)g->omega, A.L[l + 1])
-          : fvx_launch_pdl(down_leg_kernel<T, 256>, gr, dim3(256), leg_smem<T>(k), st, L, f, u_init, k,
-                           (T)g->omega, A.L[l + 1]);
+  const int cfg = leg_config<T>(k + 1, (size_t)gr.x * gr.y < (size_t)kLegFewTiles);
+  const size_t sm = leg_smem<T>(k);
+  const Lev<T>& C = A.L[l + 1];
+  const T om = (T)g->omega;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (cfg) {
+    case 0: e = fvx_launch_pdl(down_leg_kernel<T, 512, 4>, gr, dim3(512), sm, st, L, f, u_init, k, om, C); break;
+    case 1: e = fvx_launch_pdl(down_leg_kernel<T, 512, 8>, gr, dim3(512), sm, st, L, f, u_init, k, om, C); break;
+    case 2: e = fvx_launch_pdl(down_leg_kernel<T, 1024, 4>, gr, dim3(1024), sm, st, L, f, u_init, k, om, C); break;
+    case 3: e = fvx_launch_pdl(down_leg_kernel<T, 1024, 8>, gr, dim3(1024), sm, st, L, f, u_init, k, om, C); break;
+    default: return FVX_ERR_ARG;
+  }
   if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
@@ -896,12 +993,19 @@ static int leg_up(fvx_mg* g, int l, const T* f, const T* ec, int k, T* out, cuda
   Lev<T>& L = A.L[l];
   constexpr int TX = LegTile<T>::TX, TY = LegTile<T>::TY;
   dim3 gr((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  const bool few = (size_t)gr.x * gr.y < (size_t)kLegFewTiles;
-  const cudaError_t e =
-      few ? fvx_launch_pdl(up_leg_kernel<T, 1024>, gr, dim3(1024), leg_smem<T>(k), st, L, f, (const T*)L.u,
-                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out, ec_scale)
-          : fvx_launch_pdl(up_leg_kernel<T, 256>, gr, dim3(256), leg_smem<T>(k), st, L, f, (const T*)L.u,
-                           A.L[l + 1], (const T*)ec, k, (T)g->omega, out, ec_scale);
+  const int cfg = leg_config<T>(k + 1, (size_t)gr.x * gr.y < (size_t)kLegFewTiles);
+  const size_t sm = leg_smem<T>(k);
+  const Lev<T>& C = A.L[l + 1];
+  const T om = (T)g->omega;
+  const T* up = L.u;
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (cfg) {
+    case 0: e = fvx_launch_pdl(up_leg_kernel<T, 512, 4>, gr, dim3(512), sm, st, L, f, up, C, ec, k, om, out, ec_scale); break;
+    case 1: e = fvx_launch_pdl(up_leg_kernel<T, 512, 8>, gr, dim3(512), sm, st, L, f, up, C, ec, k, om, out, ec_scale); break;
+    case 2: e = fvx_launch_pdl(up_leg_kernel<T, 1024, 4>, gr, dim3(1024), sm, st, L, f, up, C, ec, k, om, out, ec_scale); break;
+    case 3: e = fvx_launch_pdl(up_leg_kernel<T, 1024, 8>, gr, dim3(1024), sm, st, L, f, up, C, ec, k, om, out, ec_scale); break;
+    default: return FVX_ERR_ARG;
+  }
   if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }

@@ -36,6 +36,19 @@ DEV float in_at(const float* src, int mode, int h, int w, int y, int x) {
   return src[(size_t)(y >> 1) * (w >> 1) + (x >> 1)];  // IN_UP
 }
 
+// in_at through L2 only (ld.global.cg): for tensors the kernel before wrote,
+// read after grid_dep_wait by a programmatic dependent.
+DEV float in_at_l2(const float* src, int mode, int h, int w, int y, int x) {
+  if (y < 0 || y >= h || x < 0 || x >= w) return 0.f;
+  if (mode == IN_DIRECT) return __ldcg(src + (size_t)y * w + x);
+  if (mode == IN_POOL) {
+    const int W2 = 2 * w;
+    const float* p = src + (size_t)(2 * y) * W2 + 2 * x;
+    return 0.25f * ((__ldcg(p) + __ldcg(p + 1)) + (__ldcg(p + W2) + __ldcg(p + W2 + 1)));
+  }
+  return __ldcg(src + (size_t)(y >> 1) * (w >> 1) + (x >> 1));  // IN_UP
+}
+
 __host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
   return mode == IN_DIRECT ? (size_t)h * w : (mode == IN_POOL ? (size_t)4 * h * w : (size_t)(h / 2) * (w / 2));
 }
@@ -46,7 +59,9 @@ __host__ __device__ __forceinline__ size_t src_plane(int mode, int h, int w) {
 // barrier), each thread accumulating CPT output channels of one pixel.
 // Small tiles give enough blocks for single-field inference on coarse grids.
 // Launched as a programmatic dependent of the previous layer (inference), a
-// block stages the weights before waiting for that layer's output.
+// block stages the weights before waiting for that layer's output; the
+// layer's input, skip tensor and scale (written by the kernels before) are
+// read after the wait through L2, from pointers not marked __restrict__.
 // Inference hooks of the first and last layers (null elsewhere): with
 // x0_src, input channel 0 is x0_src * scale[1] (the network input f / s
 // formed while the tile loads); with out_mask, the output is
@@ -60,9 +75,9 @@ struct ConvHooks {
 
 template <int COUT, int CPT, int T>
 __global__ void __launch_bounds__(T * T * (COUT / CPT))
-conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
-                 const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
-                 int w, int relu, ConvHooks hk) {
+conv_tile_kernel(const float* in, int mode, int cin, const __nv_bfloat16* __restrict__ wb,
+                 const float* __restrict__ bias, const float* skip, float* __restrict__ out, int h, int w, int relu,
+                 ConvHooks hk) {
   constexpr int NT = T * T * (COUT / CPT);
   constexpr int TW = T + 2;
   extern __shared__ __align__(16) float sm[];
@@ -89,7 +104,7 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const size_t sp = src_plane(mode, h, w);
   const float* inb = in + (size_t)b * cin * sp;
   const int nt = cin * TW * TW;
-  const float x0s = hk.x0_src ? hk.scale[1] : 0.f;
+  const float x0s = hk.x0_src ? __ldcg(hk.scale + 1) : 0.f;
   for (int k0 = tid; k0 < nt; k0 += 16 * NT) {
     float v[16];
 #pragma unroll
@@ -98,9 +113,9 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
       const int ci = k / (TW * TW), r = k - ci * (TW * TW);
       const int ly = r / TW, lx = r - ly * TW;
       if (hk.x0_src && ci == 0)
-        v[u] = k < nt ? in_at(hk.x0_src, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) * x0s : 0.f;
+        v[u] = k < nt ? in_at_l2(hk.x0_src, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) * x0s : 0.f;
       else
-        v[u] = k < nt ? in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
+        v[u] = k < nt ? in_at_l2(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx) : 0.f;
     }
 #pragma unroll
     for (int u = 0; u < 16; ++u)
@@ -127,12 +142,12 @@ conv_tile_kernel(const float* __restrict__ in, int mode, int cin, const __nv_bfl
   const int y = y0 + ty, x = x0 + tx;
   if (y >= h || x >= w) return;
   const size_t plane = (size_t)h * w, base = (size_t)b * COUT * plane + (size_t)y * w + x;
-  const float os = hk.out_mask ? hk.scale[0] * hk.sigma : 0.f;
+  const float os = hk.out_mask ? __ldcg(hk.scale) * hk.sigma : 0.f;
 #pragma unroll
   for (int c = 0; c < CPT; ++c) {
     const int co = co0 + c;
     float v = acc[c] + bias[co];
-    if (skip) v += skip[base + co * plane];
+    if (skip) v += __ldcg(skip + base + co * plane);
     if (relu) v = fmaxf(v, 0.f);
     if (hk.out_mask) v = (v * os) * hk.out_mask[(size_t)y * w + x];
     out[base + co * plane] = v;
