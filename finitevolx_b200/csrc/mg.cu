@@ -191,6 +191,53 @@ DEV void coarse_cells(int ny, int nx, F&& fnc) {
   }
 }
 
+// The coarsest-grid solve -- n Jacobi sweeps from u = 0 -- of a level of at
+// most kWarpSolveCells cells on shared-memory copies of the level's arrays
+// (sh: 7 * kWarpSolveCells values): one cell per thread of the first
+// ceil(cells / 32) warps, which alone meet at a named barrier between sweeps.
+// jacobi_at's arithmetic on the same values as the block-wide form over
+// global memory.  f_src: the right-hand side (of type F, widened as it is
+// copied); the solution goes to u_dst (of type U, rounded if narrower).
+// Called by the whole CTA; returns with it synchronised.
+constexpr int kWarpSolveCells = 256;
+template <typename T, typename F, typename U>
+DEV void coarsest_warp_solve(const Lev<T>& L, const F* f_src, U* u_dst, int n, T omega, T* sh) {
+  const int cells = L.ny * L.nx;
+  Lev<T> S = L;
+  S.mask = sh;
+  S.cx = sh + kWarpSolveCells;
+  S.cy = sh + 2 * kWarpSolveCells;
+  S.inv = sh + 3 * kWarpSolveCells;
+  S.f = sh + 4 * kWarpSolveCells;
+  S.u = sh + 5 * kWarpSolveCells;
+  S.tmp = sh + 6 * kWarpSolveCells;
+  for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+    S.mask[c] = L.mask[c];
+    S.cx[c] = L.cx[c];
+    S.cy[c] = L.cy[c];
+    S.inv[c] = L.inv[c];
+    S.f[c] = (T)f_src[c];
+    S.u[c] = T(0);
+  }
+  __syncthreads();
+  const int nthr = (cells + 31) & ~31;
+  const int c = threadIdx.x;
+  if (c < nthr) {
+    const int j = c / L.nx, i = c - j * L.nx;
+    T* a = S.u;
+    T* b = S.tmp;
+    for (int s = 0; s < n; ++s) {
+      if (c < cells) jacobi_at(S, a, S.f, b, omega, j, i, (size_t)c);
+      asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory");
+      T* t = a;
+      a = b;
+      b = t;
+    }
+    if (c < cells) u_dst[c] = (U)a[c];
+  }
+  __syncthreads();
+}
+
 // Whole coarse part of a V-cycle in one CTA: levels lc .. nl-1, entered with
 // f[lc] set and u[lc] = 0 (the recursion's zero initial guess).  S is the
 // level table in shared memory; each level's entry is copied to registers
@@ -198,9 +245,12 @@ DEV void coarse_cells(int ny, int nx, F&& fnc) {
 // D (may be null): the coarsest level in FP64; its n_coarse sweeps -- the
 // coarsest-grid solve -- then run in FP64 on the widened right-hand side and
 // the result is rounded back into S[nl-1].u.
+// wsh (may be null): shared memory for coarsest_warp_solve (7 *
+// kWarpSolveCells values of the coarsest solve's type), used when the
+// coarsest level fits it.
 template <typename T>
 DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega,
-                      const Lev<double>* D = nullptr) {
+                      const Lev<double>* D = nullptr, void* wsh = nullptr) {
   const int tid = threadIdx.x;
   auto sweeps = [&](const Lev<T> L, int n) {
     const size_t cells = (size_t)L.ny * L.nx;
@@ -222,7 +272,12 @@ DEV void coarse_cycle(const Lev<T>* S, int lc, int nl, int n_pre, int n_post, in
     for (size_t c = tid; c < cells; c += kCoarseThreads) L.u[c] = T(0);
     __syncthreads();
     if (l == nl - 1) {
-      if (D) {
+      const bool warp = wsh && cells <= (size_t)kWarpSolveCells;
+      if (D && warp) {
+        coarsest_warp_solve<double, T, T>(*D, L.f, L.u, n_coarse, (double)omega, (double*)wsh);
+      } else if (!D && warp) {
+        coarsest_warp_solve<T, T, T>(L, L.f, L.u, n_coarse, omega, (T*)wsh);
+      } else if (D) {
         const Lev<double> E = *D;
         for (size_t c = tid; c < cells; c += kCoarseThreads) { E.f[c] = (double)L.f[c]; E.u[c] = 0.0; }
         __syncthreads();
@@ -260,9 +315,10 @@ template <typename T>
 __global__ void __launch_bounds__(kCoarseThreads)
 coarse_vcycle_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post, int n_coarse, T omega) {
   __shared__ Lev<T> S[kMaxLevels];
+  __shared__ T wsh[7 * kWarpSolveCells];
   if (threadIdx.x < nl) S[threadIdx.x] = A.L[threadIdx.x];
   __syncthreads();
-  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
+  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega, (const Lev<double>*)nullptr, (void*)wsh);
 }
 
 // An FP32 plan's single-CTA coarse cycle with the coarsest-grid solve (the
@@ -273,10 +329,11 @@ coarse_vcycle_f64_kernel(LevArray<float> A, Lev<double> D, int lc, int nl, int n
                          float omega) {
   __shared__ Lev<float> S[kMaxLevels];
   __shared__ Lev<double> E;
+  __shared__ double wsh[7 * kWarpSolveCells];
   if (threadIdx.x < nl) S[threadIdx.x] = A.L[threadIdx.x];
   if (threadIdx.x == 0) E = D;
   __syncthreads();
-  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega, &E);
+  coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega, &E, (void*)wsh);
 }
 
 // Many independent solves of A_lc u = f at level lc, one CTA per right-hand
@@ -289,6 +346,7 @@ coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post
                             const T* __restrict__ f, T* __restrict__ u, T* work, size_t work_per_block,
                             int n_cycles) {
   __shared__ Lev<T> S[kMaxLevels];
+  __shared__ T wsh[7 * kWarpSolveCells];
   if (threadIdx.x == 0) {
     T* w = work + (size_t)blockIdx.x * work_per_block;
     for (int l = lc; l < nl; ++l) {
@@ -310,7 +368,7 @@ coarse_solve_batched_kernel(LevArray<T> A, int lc, int nl, int n_pre, int n_post
   for (int k = 0; k < n_cycles; ++k) {
     coarse_cells(L.ny, L.nx, [&](int j, int i, size_t c) { L.f[c] = (fb[c] - apply_at(L, ub, j, i)) * L.mask[c]; });
     __syncthreads();
-    coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega);
+    coarse_cycle(S, lc, nl, n_pre, n_post, n_coarse, omega, (const Lev<double>*)nullptr, (void*)wsh);
     for (size_t c = threadIdx.x; c < cells; c += kCoarseThreads) ub[c] += L.u[c];
     __syncthreads();
   }
