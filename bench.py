@@ -77,6 +77,9 @@ def parse():
     ap.add_argument("--dst-rhs", type=int, default=64)
     ap.add_argument("--profile", action="store_true",
                     help="only the warm-up and timed QG steps (for ncu launch lists); no extra sections")
+    ap.add_argument("--mg-profile", action="store_true",
+                    help="only a few V-cycles, U-Net coarse solves and hybrid preconditioner applications on the "
+                         "1024^2 masked basin (untrained network; for ncu launch lists of the Helmholtz path)")
     ap.add_argument("--ens-steps", type=int, default=100)
     ap.add_argument("--stage-tile", default=None, help="fix the stage tile (e.g. 64x32) instead of autotuning")
     return ap.parse_args()
@@ -638,6 +641,31 @@ def ensemble_section(members, n_steps):
             "launches_per_step": r["launches_per_step"], "autotuned_blocks_per_sm": tuned.get("blocks_per_sm")}
 
 
+def mg_profile_run(n=1024, reps=3):
+    """The Helmholtz path's kernels in a short run for ncu launch lists:
+    ``reps`` MG V-cycles, U-Net coarse solves (per-layer chain) and hybrid
+    preconditioner applications on the masked basin, Ld 40 km (the network
+    untrained: its launches are what is profiled, not its answer)."""
+    import torch
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200.learned import LearnedPreconditioner
+
+    m, c, f = masked_basin(n, 1)
+    dx = LX / n
+    mg = fvx.build_multigrid_solver(m, dx, dx, lambda_=1.0 / LD ** 2, coeff=c, dtype=torch.float32)
+    b = torch.from_numpy(f).float().cuda()
+    pc = LearnedPreconditioner(mg, n_pre=6, n_post=6, batch_max=1, seed=0)
+    pc.activate()
+    fl = torch.randn(pc.m_lvl.shape, device="cuda")
+    for _ in range(reps):
+        mg.v_cycle(None, b)
+        pc.coarse_solve(fl)
+        pc(b)
+    torch.cuda.synchronize()
+    print(json.dumps({"mg_profile_run": True, "n": n, "reps": reps, "levels": mg.n_levels, "unet_level": pc.lvl}))
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -645,6 +673,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.mg_profile:
+        mg_profile_run(reps=3)
         return
     import numpy as np
     import torch

@@ -177,6 +177,212 @@ static int launch_conv_tile(const float* in, int mode, int batch, int cin, const
   return fvx_cuda_status();
 }
 
+// The network's last two layers in one kernel (single-field inference): the
+// decoder's full-resolution conv (16 -> 16 on the upsampled input, + skip,
+// ReLU) on the output tile and a one-pixel ring around it, kept in shared
+// memory, then the output conv (16 -> 1) and the output hook on the tile.
+// The ring's decoder values are recomputed by the neighbouring tiles (1.56x
+// that layer's work for one launch and one tensor round trip fewer); every
+// value is summed in the same order as conv_tile_kernel, so the result equals
+// the two-launch form.
+constexpr int kD0T = 8, kD0R = kD0T + 2, kD0IN = kD0T + 4;  // tile, decoder ring, decoder input
+constexpr int kD0Threads = 512;
+__global__ void __launch_bounds__(kD0Threads)
+conv_d0_out_kernel(const float* in, const __nv_bfloat16* __restrict__ w0, const float* __restrict__ b0,
+                   const float* skip, const __nv_bfloat16* __restrict__ w1, const float* __restrict__ b1,
+                   float* __restrict__ out, int h, int w, ConvHooks hk) {
+  constexpr int C = 16, CPT = 4, GROUPS = C / CPT;
+  __shared__ float ws0[C * 9 * C];               // [ci * 9][co]
+  __shared__ float ws1[C * 9];                   // [ci * 9]
+  __shared__ float tin[C][kD0IN][kD0IN];         // decoder input (upsampled), origin (y0 - 2, x0 - 2)
+  __shared__ float td[C][kD0R][kD0R];            // decoder output, origin (y0 - 1, x0 - 1)
+  const int tid = threadIdx.x;
+  const int x0 = blockIdx.x * kD0T, y0 = blockIdx.y * kD0T;
+  for (int k = tid; k < C * 9 * C; k += kD0Threads) {
+    const int co = k % C, rest = k / C;
+    ws0[k] = __bfloat162float(w0[(size_t)co * C * 9 + rest]);
+  }
+  for (int k = tid; k < C * 9; k += kD0Threads) ws1[k] = __bfloat162float(w1[k]);
+  grid_dep_wait();  // the input and skip come from the kernels before
+  const size_t sp = src_plane(IN_UP, h, w), plane = (size_t)h * w;
+  {
+    constexpr int NIN = C * kD0IN * kD0IN;
+    for (int k0 = tid; k0 < NIN; k0 += 8 * kD0Threads) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int k = k0 + u * kD0Threads;
+        const int ci = k / (kD0IN * kD0IN), r = k - ci * (kD0IN * kD0IN);
+        const int ly = r / kD0IN, lx = r - ly * kD0IN;
+        v[u] = k < NIN ? in_at_l2(in + ci * sp, IN_UP, h, w, y0 - 2 + ly, x0 - 2 + lx) : 0.f;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+        if (k0 + u * kD0Threads < NIN) (&tin[0][0][0])[k0 + u * kD0Threads] = v[u];
+    }
+  }
+  __syncthreads();
+  grid_dep_launch();
+  // decoder layer on the 10 x 10 ring region: 100 pixels x 4 groups of 4 channels
+  if (tid < kD0R * kD0R * GROUPS) {
+    const int p = tid % (kD0R * kD0R), co0 = (tid / (kD0R * kD0R)) * CPT;
+    const int ry = p / kD0R, rx = p % kD0R;
+    const int y = y0 - 1 + ry, x = x0 - 1 + rx;
+    float acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
+    for (int ci = 0; ci < C; ++ci) {
+      const float* wc = ws0 + ci * 9 * C + co0;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const float v = tin[ci][ry + t / 3][rx + t % 3];
+        const float* wr = wc + t * C;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
+      }
+    }
+    const bool inside = y >= 0 && y < h && x >= 0 && x < w;
+    const size_t base = inside ? (size_t)y * w + x : 0;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int co = co0 + c;
+      float v = 0.f;  // the output conv reads zero outside the grid
+      if (inside) v = fmaxf(acc[c] + b0[co] + __ldcg(skip + base + co * plane), 0.f);
+      td[co][ry][rx] = v;
+    }
+  }
+  __syncthreads();
+  // output layer on the 8 x 8 tile
+  if (tid < kD0T * kD0T) {
+    const int ty = tid / kD0T, tx = tid % kD0T;
+    const int y = y0 + ty, x = x0 + tx;
+    float acc = 0.f;
+    for (int ci = 0; ci < C; ++ci) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) acc = fmaf(ws1[ci * 9 + t], td[ci][ty + t / 3][tx + t % 3], acc);
+    }
+    if (y < h && x < w) {
+      const size_t base = (size_t)y * w + x;
+      float v = acc + b1[0];
+      const float os = __ldcg(hk.scale) * hk.sigma;
+      v = (v * os) * hk.out_mask[base];
+      out[base] = v;
+    }
+  }
+}
+
+// The network's first two layers in one kernel (single-field inference): the
+// input conv (3 -> 16, ReLU; channel 0 = f / s as it loads) on the fine
+// pixels under a 4 x 4 tile of the half-resolution grid and its one-pixel
+// ring, kept in shared memory (the block writes its own 8 x 8 of it, the
+// decoder's skip tensor), then 2 x 2 average pooling and the second conv
+// (16 -> 16, ReLU) on the tile.  The ring's values are recomputed by the
+// neighbouring tiles (2.25x the first layer's 27 products per output for one
+// launch and one tensor read fewer); every value is summed in the same order
+// as conv_tile_kernel, so the result equals the two-launch form.
+constexpr int kE1T = 4, kE1R = kE1T + 2, kE0R = 2 * kE1R, kE0IN = kE0R + 2;
+constexpr int kE01Threads = 288;
+__global__ void __launch_bounds__(kE01Threads)
+conv_e0_e1_kernel(const float* x, const float* f, const __nv_bfloat16* __restrict__ w0,
+                  const float* __restrict__ b0, const __nv_bfloat16* __restrict__ w1, const float* __restrict__ b1,
+                  float* __restrict__ a0, float* __restrict__ a1, int h, int w, const float* scale) {
+  constexpr int C0 = 3, C1 = 16;
+  __shared__ float ws0[C0 * 9 * C1];          // [ci * 9][co]
+  __shared__ float ws1[C1 * 9 * C1];
+  __shared__ float tx[C0][kE0IN][kE0IN];      // input, origin (2 Y0 - 3, 2 X0 - 3)
+  __shared__ float t0[C1][kE0R][kE0R];        // first layer's output, origin (2 Y0 - 2, 2 X0 - 2)
+  __shared__ float tp[C1][kE1R][kE1R];        // pooled, origin (Y0 - 1, X0 - 1)
+  const int tid = threadIdx.x;
+  const int h1 = h >> 1, w1n = w >> 1;
+  const int X0 = blockIdx.x * kE1T, Y0 = blockIdx.y * kE1T;
+  const int fy0 = 2 * Y0 - 2, fx0 = 2 * X0 - 2;
+  for (int k = tid; k < C0 * 9 * C1; k += kE01Threads) {
+    const int co = k % C1, rest = k / C1;
+    ws0[k] = __bfloat162float(w0[(size_t)co * C0 * 9 + rest]);
+  }
+  for (int k = tid; k < C1 * 9 * C1; k += kE01Threads) {
+    const int co = k % C1, rest = k / C1;
+    ws1[k] = __bfloat162float(w1[(size_t)co * C1 * 9 + rest]);
+  }
+  grid_dep_wait();  // f and the scale come from the kernels before
+  const size_t plane = (size_t)h * w;
+  const float rs = __ldcg(scale + 1);
+  {
+    constexpr int NIN = C0 * kE0IN * kE0IN;
+    float v[3];
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int k = tid + u * kE01Threads;
+      v[u] = 0.f;
+      if (k < NIN) {
+        const int ci = k / (kE0IN * kE0IN), r = k - ci * (kE0IN * kE0IN);
+        const int ly = r / kE0IN, lx = r - ly * kE0IN;
+        v[u] = ci == 0 ? in_at_l2(f, IN_DIRECT, h, w, fy0 - 1 + ly, fx0 - 1 + lx) * rs
+                       : in_at_l2(x + ci * plane, IN_DIRECT, h, w, fy0 - 1 + ly, fx0 - 1 + lx);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u)
+      if (tid + u * kE01Threads < NIN) (&tx[0][0][0])[tid + u * kE01Threads] = v[u];
+  }
+  __syncthreads();
+  grid_dep_launch();
+  // first layer on the 12 x 12 fine region: 144 pixels x 2 groups of 8 channels
+  {
+    constexpr int CPT = 8;
+    const int p = tid % (kE0R * kE0R), co0 = (tid / (kE0R * kE0R)) * CPT;
+    const int ry = p / kE0R, rx = p % kE0R;
+    const int y = fy0 + ry, xg = fx0 + rx;
+    float acc[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
+    for (int ci = 0; ci < C0; ++ci) {
+      const float* wc = ws0 + ci * 9 * C1 + co0;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const float v = tx[ci][ry + t / 3][rx + t % 3];
+        const float* wr = wc + t * C1;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
+      }
+    }
+    const bool inside = y >= 0 && y < h && xg >= 0 && xg < w;
+    const bool own = ry >= 2 && ry < 2 + 2 * kE1T && rx >= 2 && rx < 2 + 2 * kE1T;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int co = co0 + c;
+      const float v = fmaxf(acc[c] + b0[co], 0.f);
+      t0[co][ry][rx] = v;
+      if (inside && own) a0[(size_t)co * plane + (size_t)y * w + xg] = v;
+    }
+  }
+  __syncthreads();
+  // 2 x 2 average pooling (zero off the half-resolution grid)
+  for (int k = tid; k < C1 * kE1R * kE1R; k += kE01Threads) {
+    const int ci = k / (kE1R * kE1R), r = k - ci * (kE1R * kE1R);
+    const int ly = r / kE1R, lx = r - ly * kE1R;
+    const int Y = Y0 - 1 + ly, X = X0 - 1 + lx;
+    float v = 0.f;
+    if (Y >= 0 && Y < h1 && X >= 0 && X < w1n)
+      v = 0.25f * ((t0[ci][2 * ly][2 * lx] + t0[ci][2 * ly][2 * lx + 1]) +
+                   (t0[ci][2 * ly + 1][2 * lx] + t0[ci][2 * ly + 1][2 * lx + 1]));
+    tp[ci][ly][lx] = v;
+  }
+  __syncthreads();
+  // second layer on the 4 x 4 tile: 16 pixels x 16 channels
+  if (tid < kE1T * kE1T * C1) {
+    const int p = tid % (kE1T * kE1T), co = tid / (kE1T * kE1T);
+    const int ty = p / kE1T, tx_ = p % kE1T;
+    const int Y = Y0 + ty, X = X0 + tx_;
+    float acc = 0.f;
+    for (int ci = 0; ci < C1; ++ci) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) acc = fmaf(ws1[(ci * 9 + t) * C1 + co], tp[ci][ty + t / 3][tx_ + t % 3], acc);
+    }
+    if (Y < h1 && X < w1n) a1[(size_t)co * h1 * w1n + (size_t)Y * w1n + X] = fmaxf(acc + b1[co], 0.f);
+  }
+}
+
 // G = dL/d(pre-activation) = dY * (y > 0) (or dY when the layer is linear);
 // dskip += G.
 __global__ void act_grad_kernel(const float* dy, const float* y, float* g, float* dskip, size_t n, int relu) {
@@ -930,13 +1136,14 @@ extern "C" int fvx_unet_destroy(fvx_unet* n) {
 
 // Copy ``count`` floats at ``offset`` of one of the network's buffers
 // (0 FP32 master parameters, 1 their gradient, 2 input x [batch_max, 3, h,
-// w], 3 output y [batch_max, 1, h, w]) from ``src`` and/or to ``dst`` (host
-// or device pointers; NULL skips that direction).
+// w], 3 output y [batch_max, 1, h, w], 4 the inference scale pair [s, 1/s]
+// of the last coarse solve) from ``src`` and/or to ``dst`` (host or device
+// pointers; NULL skips that direction).
 extern "C" int fvx_unet_io(fvx_unet* n, int which, long long offset, long long count, const void* src, void* dst,
                            void* stream) {
-  if (!n || which < 0 || which > 3 || offset < 0 || count < 0) return FVX_ERR_ARG;
-  float* buf = which == 0 ? n->wf : which == 1 ? n->grad : which == 2 ? n->act[0] : n->act[8];
-  const size_t len = which < 2 ? n->n_params : slot_elems(n, which == 2 ? 0 : 8, n->batch_max);
+  if (!n || which < 0 || which > 4 || offset < 0 || count < 0) return FVX_ERR_ARG;
+  float* buf = which == 0 ? n->wf : which == 1 ? n->grad : which == 2 ? n->act[0] : which == 3 ? n->act[8] : n->scale;
+  const size_t len = which < 2 ? n->n_params : which == 4 ? 2 : slot_elems(n, which == 2 ? 0 : 8, n->batch_max);
   if ((size_t)(offset + count) > len) return FVX_ERR_SHAPE;
   cudaStream_t st = fvx_stream(stream);
   if (src) cudaMemcpyAsync(buf + offset, src, (size_t)count * 4, cudaMemcpyDefault, st);
@@ -954,11 +1161,54 @@ extern "C" int fvx_unet_sync_params(fvx_unet* n, void* stream) {
 // it (inference only: no kernel between the layers writes the weights).
 // coarse_f / coarse_u (inference on one field): the first layer forms
 // f / s from coarse_f as it loads, the last writes s sigma m y to coarse_u.
+static_assert(kNet[6].cin == 16 && kNet[6].cout == 16 && kNet[6].mode == IN_UP && kNet[6].skip == 1 &&
+                  kNet[6].relu == 1 && kNet[7].cin == 16 && kNet[7].cout == 1 && kNet[7].mode == IN_DIRECT &&
+                  kNet[7].skip < 0 && kNet[7].relu == 0 && kNet[7].in == kNet[6].out,
+              "conv_d0_out_kernel computes layers 6 and 7 of kNet");
+
+static_assert(kNet[0].cin == 3 && kNet[0].cout == 16 && kNet[0].mode == IN_DIRECT && kNet[0].skip < 0 &&
+                  kNet[0].relu == 1 && kNet[1].cin == 16 && kNet[1].cout == 16 && kNet[1].mode == IN_POOL &&
+                  kNet[1].skip < 0 && kNet[1].relu == 1 && kNet[1].in == kNet[0].out,
+              "conv_e0_e1_kernel computes layers 0 and 1 of kNet");
+
+// coarse_u (single-field inference, batch 1): the first two layers run as
+// one conv_e0_e1_kernel launch and the last two as one conv_d0_out_kernel
+// launch.
 static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = false, const float* coarse_f = nullptr,
                         float* coarse_u = nullptr) {
   size_t off = 0;
-  for (int l = 0; l < kLayers; ++l) {
+  int l0 = 0;
+  if (coarse_u && coarse_f) {
+    const LayerDef& L0 = kNet[0];
+    const LayerDef& L1 = kNet[1];
+    const size_t off1 = layer_params(L0);
+    const dim3 g((n->w / 2) / kE1T, (n->h / 2) / kE1T);
+    if (fvx_launch_pdl(conv_e0_e1_kernel, g, dim3(kE01Threads), 0, st, (const float*)n->act[0], coarse_f,
+                       (const __nv_bfloat16*)n->wb, (const float*)(n->wf + (size_t)L0.cout * L0.cin * 9),
+                       (const __nv_bfloat16*)(n->wb + off1), (const float*)(n->wf + off1 + (size_t)L1.cout * L1.cin * 9),
+                       n->act[L0.out], n->act[L1.out], n->h, n->w, (const float*)n->scale) != cudaSuccess)
+      return FVX_ERR_CUDA;
+    off = off1 + layer_params(L1);
+    l0 = 2;
+  }
+  for (int l = l0; l < kLayers; ++l) {
     const LayerDef& L = kNet[l];
+    if (coarse_u && l == kLayers - 2) {
+      const LayerDef& L1 = kNet[l + 1];
+      const size_t off1 = off + layer_params(L);
+      ConvHooks hk;
+      hk.out_mask = n->mask;
+      hk.scale = n->scale;
+      hk.sigma = n->sigma;
+      const dim3 g(n->w / kD0T, n->h / kD0T);
+      const float* b0 = n->wf + off + (size_t)L.cout * L.cin * 9;
+      const float* b1 = n->wf + off1 + (size_t)L1.cout * L1.cin * 9;
+      if (fvx_launch_pdl(conv_d0_out_kernel, g, dim3(kD0Threads), 0, st, (const float*)n->act[L.in],
+                         (const __nv_bfloat16*)(n->wb + off), b0, (const float*)n->act[L.skip],
+                         (const __nv_bfloat16*)(n->wb + off1), b1, coarse_u, n->h, n->w, hk) != cudaSuccess)
+        return FVX_ERR_CUDA;
+      return fvx_cuda_status();
+    }
     const int hh = n->h >> L.div, ww = n->w >> L.div;
     const __nv_bfloat16* W = n->wb + off;
     const float* wf_b = n->wf + off + (size_t)L.cout * L.cin * 9;  // biases stay FP32

@@ -365,7 +365,9 @@ int fvx_hybrid_precond(void* ctx, const void* rho, void* z, void* stream);
 
 /* 4-level U-Net (16/16/32/32 channels), BF16 weights, FP32 accumulation:
  * create / parameter IO / forward / backward / Adam train step, and the
- * inference callback fvx_unet_coarse (an fvx_precond_fn, ctx = the net). */
+ * inference callback fvx_unet_coarse (an fvx_precond_fn, ctx = the net).
+ * fvx_unet_io which: 0 parameters, 1 gradient, 2 input x, 3 output y, 4 the
+ * last coarse solve's scale pair [s, 1/s]. */
 typedef struct fvx_unet fvx_unet;
 long long fvx_unet_num_params(void);
 int fvx_unet_create(int h, int w, int batch_max, fvx_unet** out);

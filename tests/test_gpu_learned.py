@@ -18,6 +18,7 @@ import torch
 import finitevolx_b200 as fvx
 import oracle.fvx_oracle as O
 import oracle.unet_oracle as U
+from finitevolx_b200._lib import P
 from finitevolx_b200.learned import LearnedPreconditioner, UNet, generate_pairs
 
 from test_gpu_solvers import basin, coeff
@@ -128,6 +129,31 @@ def test_unet_coarse_single_launch_matches_oracle(cuda_ok, h, w):
     assert nrel(got, ul.cpu().numpy()) < 1e-6
     assert torch.equal(u, u2)  # fixed reduction order: run-to-run identical
     assert np.all(got[m == 0] == 0)
+
+
+@pytest.mark.parametrize("h,w", [(128, 128), (40, 56)])
+def test_unet_coarse_fused_layers_equal_generic_forward(cuda_ok, h, w):
+    """The coarse solve's fused first-two and last-two layer kernels give
+    exactly the generic per-layer forward pass on x = [f * (1/s), m, log c],
+    scaled by (s sigma) and masked as the output hook does."""
+    theta, _, _ = _net_case(9, B=1, h=h, w=w)
+    rng = np.random.default_rng(10)
+    m = (rng.random((h, w)) > 0.3).astype(np.float32)
+    logc = (0.3 * rng.standard_normal((h, w)) * m).astype(np.float32)
+    f = (rng.standard_normal((h, w)) * m).astype(np.float32)
+    net = UNet(h, w, batch_max=1)
+    net.set_params(theta)
+    sigma = 0.61
+    _set_level(net, m, logc, sigma)
+    u = _coarse(net, f)
+    sc = torch.empty(2, dtype=torch.float32, device="cuda")
+    net._io(4, 0, 2, dst=P(sc))
+    torch.cuda.synchronize()
+    ft, mt = torch.from_numpy(f).cuda(), torch.from_numpy(m).cuda()
+    x = torch.stack([ft * sc[1], mt, torch.from_numpy(logc).cuda()])[None]
+    y = net.forward(x)[0, 0]
+    ref = (y * (sc[0] * torch.tensor(sigma, dtype=torch.float32, device="cuda"))) * mt
+    assert torch.equal(u, ref)
 
 
 @pytest.fixture(scope="module")
