@@ -705,11 +705,13 @@ constexpr int kRmsThreads = 1024;
 // s = sqrt(sum(f^2 m) / max(sum m, 1)), stored as [s, 1/s] (1/s = 0 when
 // s = 0), by one block (the coarse level has tens of thousands of cells):
 // FP64 partial sums per thread, then a fixed-order tree, so the result is
-// deterministic.
+// deterministic.  Launched as a programmatic dependent of the kernel that
+// wrote f (read after the wait, through L2).
 __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const float* mask, size_t n,
                                                           float* scale) {
   __shared__ double sh[2][kRmsThreads / 32];
   double a = 0.0, c = 0.0;
+  grid_dep_wait();
   // eight cells' loads in flight per thread before they are accumulated (in
   // the same order as a one-at-a-time loop)
   for (size_t k0 = threadIdx.x; k0 < n; k0 += 8 * kRmsThreads) {
@@ -717,7 +719,7 @@ __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const 
 #pragma unroll
     for (int u = 0; u < 8; ++u) {
       const size_t k = k0 + (size_t)u * kRmsThreads;
-      fv[u] = k < n ? f[k] : 0.f;
+      fv[u] = k < n ? __ldcg(f + k) : 0.f;
       mv[u] = k < n ? mask[k] : 0.f;
     }
 #pragma unroll
@@ -727,6 +729,7 @@ __global__ void __launch_bounds__(kRmsThreads) rms_kernel(const float* f, const 
       c += m;
     }
   }
+  grid_dep_launch();  // the first layer may stage its weights
   for (int o = 16; o; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
     c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -1374,7 +1377,9 @@ extern "C" int fvx_unet_coarse(void* ctx, const void* f, void* u, void* stream) 
   if (!n || !f || !u) return FVX_ERR_ARG;
   cudaStream_t st = fvx_stream(stream);
   const size_t plane = (size_t)n->h * n->w;
-  rms_kernel<<<1, kRmsThreads, 0, st>>>((const float*)f, n->mask, plane, n->scale);
+  if (fvx_launch_pdl(rms_kernel, dim3(1), dim3(kRmsThreads), 0, st, (const float*)f, (const float*)n->mask, plane,
+                     n->scale) != cudaSuccess)
+    return FVX_ERR_CUDA;
   // the first layer forms f / s, the last writes s sigma m y into u
   int rc = unet_forward(n, 1, st, true, (const float*)f, (float*)u);
   if (rc) return rc;
