@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--mg-profile", action="store_true",
                     help="only a few V-cycles, U-Net coarse solves and hybrid preconditioner applications on the "
                          "1024^2 masked basin (untrained network; for ncu launch lists of the Helmholtz path)")
+    ap.add_argument("--ens-profile", action="store_true",
+                    help="only two eager steps of the 64-member ensemble (for ncu launch lists)")
     ap.add_argument("--ens-steps", type=int, default=100)
     ap.add_argument("--stage-tile", default=None, help="fix the stage tile (e.g. 64x32) instead of autotuning")
     return ap.parse_args()
@@ -641,6 +643,30 @@ def ensemble_section(members, n_steps):
             "launches_per_step": r["launches_per_step"], "autotuned_blocks_per_sm": tuned.get("blocks_per_sm")}
 
 
+def ens_profile_run(steps=2):
+    """The ensemble's kernels in a short run for ncu launch lists: the bench's
+    64 members (seeded states), ``steps`` eager RK3 steps after one warm-up
+    step, default persistent-grid occupancy."""
+    import torch
+
+    import finitevolx_b200 as fvx
+
+    members = ensemble_members()
+    ens = fvx.QGEnsemble(members)
+    for m, (n, nl) in enumerate(members):
+        g = torch.Generator(device="cuda").manual_seed(1000 + m)
+        for k in range(nl):
+            q = torch.zeros((n + 2, n + 2), device="cuda")
+            q[1:-1, 1:-1] = torch.randn((n, n), device="cuda", generator=g) * 1e-5
+            ens.set_layer(m, k, q)
+    ens.step(1)
+    torch.cuda.synchronize()
+    ens.step(steps)
+    torch.cuda.synchronize()
+    print(json.dumps({"ens_profile_run": True, "members": len(members), "steps": steps,
+                      "launches_per_step": ens.launches_per_step}))
+
+
 def mg_profile_run(n=1024, reps=3):
     """The Helmholtz path's kernels in a short run for ncu launch lists:
     ``reps`` MG V-cycles, U-Net coarse solves (per-layer chain) and hybrid
@@ -676,6 +702,9 @@ def main():
         return
     if args.mg_profile:
         mg_profile_run(reps=3)
+        return
+    if args.ens_profile:
+        ens_profile_run(steps=2)
         return
     import numpy as np
     import torch
