@@ -177,93 +177,148 @@ static int launch_conv_tile(const float* in, int mode, int batch, int cin, const
   return fvx_cuda_status();
 }
 
-// The network's last two layers in one kernel (single-field inference): the
-// decoder's full-resolution conv (16 -> 16 on the upsampled input, + skip,
-// ReLU) on the output tile and a one-pixel ring around it, kept in shared
-// memory, then the output conv (16 -> 1) and the output hook on the tile.
-// The ring's decoder values are recomputed by the neighbouring tiles (1.56x
-// that layer's work for one launch and one tensor round trip fewer); every
-// value is summed in the same order as conv_tile_kernel, so the result equals
-// the two-launch form.
-constexpr int kD0T = 8, kD0R = kD0T + 2, kD0IN = kD0T + 4;  // tile, decoder ring, decoder input
-constexpr int kD0Threads = 512;
-__global__ void __launch_bounds__(kD0Threads)
-conv_d0_out_kernel(const float* in, const __nv_bfloat16* __restrict__ w0, const float* __restrict__ b0,
-                   const float* skip, const __nv_bfloat16* __restrict__ w1, const float* __restrict__ b1,
-                   float* __restrict__ out, int h, int w, ConvHooks hk) {
-  constexpr int C = 16, CPT = 4, GROUPS = C / CPT;
-  __shared__ float ws0[C * 9 * C];               // [ci * 9][co]
-  __shared__ float ws1[C * 9];                   // [ci * 9]
-  __shared__ float tin[C][kD0IN][kD0IN];         // decoder input (upsampled), origin (y0 - 2, x0 - 2)
-  __shared__ float td[C][kD0R][kD0R];            // decoder output, origin (y0 - 1, x0 - 1)
+// The network's last three layers in one kernel (single-field inference):
+// the half-resolution decoder conv (nearest upsample of the quarter-
+// resolution tensor, 32 -> 16, + skip, ReLU) on the 6 x 6 half-resolution
+// pixels the next conv's upsampled input touches, the full-resolution
+// decoder conv (16 -> 16, + skip, ReLU) on the 8 x 8 output tile and a
+// one-pixel ring around it, both kept in shared memory, then the output
+// conv (16 -> 1) and the output hook on the tile.  The halo values are
+// recomputed by the neighbouring tiles (2.25x and 1.56x those two layers'
+// products, for two launches and two tensor round trips fewer); every value
+// is summed in the same order as conv_tile_kernel, so the result equals the
+// layer-by-layer form.
+constexpr int kDT = 8;                 // output tile (full resolution)
+constexpr int kDR = kDT + 2;           // full-resolution decoder ring
+constexpr int kDH = kDT / 2 + 2;       // half-resolution decoder pixels per side
+constexpr int kDQ = kDH / 2 + 1;       // quarter-resolution input pixels per side
+constexpr int kDThreads = 512;
+__global__ void __launch_bounds__(kDThreads)
+conv_d1_d0_out_kernel(const float* a4, const float* a1, const float* a0, const __nv_bfloat16* __restrict__ w5,
+                      const float* __restrict__ b5, const __nv_bfloat16* __restrict__ w6,
+                      const float* __restrict__ b6, const __nv_bfloat16* __restrict__ w7,
+                      const float* __restrict__ b7, float* __restrict__ out, int h, int w, ConvHooks hk) {
+  constexpr int C4 = 32, C = 16;
+  __shared__ float ws5[C4 * 9 * C];        // [ci * 9][co]
+  __shared__ float ws6[C * 9 * C];
+  __shared__ float ws7[C * 9];
+  __shared__ float t4[C4][kDQ][kDQ];       // quarter-resolution input, origin (y0 / 4 - 1, x0 / 4 - 1)
+  __shared__ float t1[C][kDH][kDH];        // half-resolution skip, origin (y0 / 2 - 1, x0 / 2 - 1)
+  __shared__ float t5[C][kDH][kDH];        // half-resolution decoder output, same origin
+  __shared__ float td[C][kDR][kDR];        // full-resolution decoder output, origin (y0 - 1, x0 - 1)
   const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * kD0T, y0 = blockIdx.y * kD0T;
-  for (int k = tid; k < C * 9 * C; k += kD0Threads) {
+  const int x0 = blockIdx.x * kDT, y0 = blockIdx.y * kDT;
+  const int h1 = h >> 1, w1 = w >> 1, h2 = h >> 2, w2 = w >> 2;
+  const int H0 = (y0 >> 1) - 1, G0 = (x0 >> 1) - 1;  // half-resolution origin
+  const int Q0 = (y0 >> 2) - 1, P0 = (x0 >> 2) - 1;  // quarter-resolution origin
+  for (int k = tid; k < C4 * 9 * C; k += kDThreads) {
     const int co = k % C, rest = k / C;
-    ws0[k] = __bfloat162float(w0[(size_t)co * C * 9 + rest]);
+    ws5[k] = __bfloat162float(w5[(size_t)co * C4 * 9 + rest]);
   }
-  for (int k = tid; k < C * 9; k += kD0Threads) ws1[k] = __bfloat162float(w1[k]);
-  grid_dep_wait();  // the input and skip come from the kernels before
-  const size_t sp = src_plane(IN_UP, h, w), plane = (size_t)h * w;
+  for (int k = tid; k < C * 9 * C; k += kDThreads) {
+    const int co = k % C, rest = k / C;
+    ws6[k] = __bfloat162float(w6[(size_t)co * C * 9 + rest]);
+  }
+  for (int k = tid; k < C * 9; k += kDThreads) ws7[k] = __bfloat162float(w7[k]);
+  grid_dep_wait();  // the decoder's inputs come from the kernels before
   {
-    constexpr int NIN = C * kD0IN * kD0IN;
-    for (int k0 = tid; k0 < NIN; k0 += 8 * kD0Threads) {
-      float v[8];
+    constexpr int N4 = C4 * kDQ * kDQ, N1 = C * kDH * kDH;
+    float v[3];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int k = k0 + u * kD0Threads;
-        const int ci = k / (kD0IN * kD0IN), r = k - ci * (kD0IN * kD0IN);
-        const int ly = r / kD0IN, lx = r - ly * kD0IN;
-        v[u] = k < NIN ? in_at_l2(in + ci * sp, IN_UP, h, w, y0 - 2 + ly, x0 - 2 + lx) : 0.f;
+    for (int u = 0; u < 3; ++u) {
+      const int k = tid + u * kDThreads;
+      v[u] = 0.f;
+      if (k < N4) {
+        const int ci = k / (kDQ * kDQ), r = k - ci * (kDQ * kDQ);
+        const int ly = r / kDQ, lx = r - ly * kDQ;
+        v[u] = in_at_l2(a4 + (size_t)ci * h2 * w2, IN_DIRECT, h2, w2, Q0 + ly, P0 + lx);
+      } else if (k < N4 + N1) {
+        const int kk = k - N4;
+        const int ci = kk / (kDH * kDH), r = kk - ci * (kDH * kDH);
+        const int ly = r / kDH, lx = r - ly * kDH;
+        v[u] = in_at_l2(a1 + (size_t)ci * h1 * w1, IN_DIRECT, h1, w1, H0 + ly, G0 + lx);
       }
+    }
 #pragma unroll
-      for (int u = 0; u < 8; ++u)
-        if (k0 + u * kD0Threads < NIN) (&tin[0][0][0])[k0 + u * kD0Threads] = v[u];
+    for (int u = 0; u < 3; ++u) {
+      const int k = tid + u * kDThreads;
+      if (k < N4) (&t4[0][0][0])[k] = v[u];
+      else if (k < N4 + N1) (&t1[0][0][0])[k - N4] = v[u];
     }
   }
   __syncthreads();
   grid_dep_launch();
-  // decoder layer on the 10 x 10 ring region: 100 pixels x 4 groups of 4 channels
-  if (tid < kD0R * kD0R * GROUPS) {
-    const int p = tid % (kD0R * kD0R), co0 = (tid / (kD0R * kD0R)) * CPT;
-    const int ry = p / kD0R, rx = p % kD0R;
+  // half-resolution decoder conv: 36 pixels x 8 groups of 2 channels
+  if (tid < kDH * kDH * (C / 2)) {
+    constexpr int CPT = 2;
+    const int p = tid % (kDH * kDH), co0 = (tid / (kDH * kDH)) * CPT;
+    const int hy = p / kDH, hx = p % kDH;
+    const int Y = H0 + hy, X = G0 + hx;
+    float acc[CPT] = {0.f, 0.f};
+    for (int ci = 0; ci < C4; ++ci) {
+      const float* wc = ws5 + ci * 9 * C + co0;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) {
+        const int yy = Y - 1 + t / 3, xx = X - 1 + t % 3;
+        const float v = (yy >= 0 && yy < h1 && xx >= 0 && xx < w1) ? t4[ci][(yy >> 1) - Q0][(xx >> 1) - P0] : 0.f;
+        const float* wr = wc + t * C;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
+      }
+    }
+    const bool inside = Y >= 0 && Y < h1 && X >= 0 && X < w1;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+      const int co = co0 + c;
+      float v = 0.f;  // never read: the next conv's upsampled input is zero off the grid
+      if (inside) v = fmaxf((acc[c] + b5[co]) + t1[co][hy][hx], 0.f);
+      t5[co][hy][hx] = v;
+    }
+  }
+  __syncthreads();
+  // full-resolution decoder conv on the 10 x 10 ring region: 100 pixels x 4 groups of 4 channels
+  if (tid < kDR * kDR * (C / 4)) {
+    constexpr int CPT = 4;
+    const int p = tid % (kDR * kDR), co0 = (tid / (kDR * kDR)) * CPT;
+    const int ry = p / kDR, rx = p % kDR;
     const int y = y0 - 1 + ry, x = x0 - 1 + rx;
     float acc[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
     for (int ci = 0; ci < C; ++ci) {
-      const float* wc = ws0 + ci * 9 * C + co0;
+      const float* wc = ws6 + ci * 9 * C + co0;
 #pragma unroll
       for (int t = 0; t < 9; ++t) {
-        const float v = tin[ci][ry + t / 3][rx + t % 3];
+        const int yy = y - 1 + t / 3, xx = x - 1 + t % 3;
+        const float v = (yy >= 0 && yy < h && xx >= 0 && xx < w) ? t5[ci][(yy >> 1) - H0][(xx >> 1) - G0] : 0.f;
         const float* wr = wc + t * C;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) acc[c] = fmaf(wr[c], v, acc[c]);
       }
     }
     const bool inside = y >= 0 && y < h && x >= 0 && x < w;
-    const size_t base = inside ? (size_t)y * w + x : 0;
+    const size_t base = inside ? (size_t)y * w + x : 0, plane = (size_t)h * w;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
       const int co = co0 + c;
       float v = 0.f;  // the output conv reads zero outside the grid
-      if (inside) v = fmaxf(acc[c] + b0[co] + __ldcg(skip + base + co * plane), 0.f);
+      if (inside) v = fmaxf((acc[c] + b6[co]) + __ldcg(a0 + base + co * plane), 0.f);
       td[co][ry][rx] = v;
     }
   }
   __syncthreads();
-  // output layer on the 8 x 8 tile
-  if (tid < kD0T * kD0T) {
-    const int ty = tid / kD0T, tx = tid % kD0T;
+  // output conv on the 8 x 8 tile
+  if (tid < kDT * kDT) {
+    const int ty = tid / kDT, tx = tid % kDT;
     const int y = y0 + ty, x = x0 + tx;
     float acc = 0.f;
     for (int ci = 0; ci < C; ++ci) {
 #pragma unroll
-      for (int t = 0; t < 9; ++t) acc = fmaf(ws1[ci * 9 + t], td[ci][ty + t / 3][tx + t % 3], acc);
+      for (int t = 0; t < 9; ++t) acc = fmaf(ws7[ci * 9 + t], td[ci][ty + t / 3][tx + t % 3], acc);
     }
     if (y < h && x < w) {
       const size_t base = (size_t)y * w + x;
-      float v = acc + b1[0];
+      float v = acc + b7[0];
       const float os = __ldcg(hk.scale) * hk.sigma;
       v = (v * os) * hk.out_mask[base];
       out[base] = v;
@@ -1164,10 +1219,12 @@ extern "C" int fvx_unet_sync_params(fvx_unet* n, void* stream) {
 // it (inference only: no kernel between the layers writes the weights).
 // coarse_f / coarse_u (inference on one field): the first layer forms
 // f / s from coarse_f as it loads, the last writes s sigma m y to coarse_u.
-static_assert(kNet[6].cin == 16 && kNet[6].cout == 16 && kNet[6].mode == IN_UP && kNet[6].skip == 1 &&
-                  kNet[6].relu == 1 && kNet[7].cin == 16 && kNet[7].cout == 1 && kNet[7].mode == IN_DIRECT &&
-                  kNet[7].skip < 0 && kNet[7].relu == 0 && kNet[7].in == kNet[6].out,
-              "conv_d0_out_kernel computes layers 6 and 7 of kNet");
+static_assert(kNet[5].cin == 32 && kNet[5].cout == 16 && kNet[5].mode == IN_UP && kNet[5].skip == 2 &&
+                  kNet[5].relu == 1 && kNet[5].div == 1 && kNet[6].cin == 16 && kNet[6].cout == 16 &&
+                  kNet[6].mode == IN_UP && kNet[6].in == kNet[5].out && kNet[6].skip == 1 && kNet[6].relu == 1 &&
+                  kNet[7].cin == 16 && kNet[7].cout == 1 && kNet[7].mode == IN_DIRECT && kNet[7].skip < 0 &&
+                  kNet[7].relu == 0 && kNet[7].in == kNet[6].out,
+              "conv_d1_d0_out_kernel computes layers 5, 6 and 7 of kNet");
 
 static_assert(kNet[0].cin == 3 && kNet[0].cout == 16 && kNet[0].mode == IN_DIRECT && kNet[0].skip < 0 &&
                   kNet[0].relu == 1 && kNet[1].cin == 16 && kNet[1].cout == 16 && kNet[1].mode == IN_POOL &&
@@ -1175,8 +1232,8 @@ static_assert(kNet[0].cin == 3 && kNet[0].cout == 16 && kNet[0].mode == IN_DIREC
               "conv_e0_e1_kernel computes layers 0 and 1 of kNet");
 
 // coarse_u (single-field inference, batch 1): the first two layers run as
-// one conv_e0_e1_kernel launch and the last two as one conv_d0_out_kernel
-// launch.
+// one conv_e0_e1_kernel launch and the last three as one
+// conv_d1_d0_out_kernel launch.
 static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = false, const float* coarse_f = nullptr,
                         float* coarse_u = nullptr) {
   size_t off = 0;
@@ -1196,19 +1253,23 @@ static int unet_forward(fvx_unet* n, int batch, cudaStream_t st, bool pdl = fals
   }
   for (int l = l0; l < kLayers; ++l) {
     const LayerDef& L = kNet[l];
-    if (coarse_u && l == kLayers - 2) {
-      const LayerDef& L1 = kNet[l + 1];
-      const size_t off1 = off + layer_params(L);
+    if (coarse_u && l == kLayers - 3) {
+      const LayerDef& L6 = kNet[l + 1];
+      const LayerDef& L7 = kNet[l + 2];
+      const size_t off6 = off + layer_params(L), off7 = off6 + layer_params(L6);
       ConvHooks hk;
       hk.out_mask = n->mask;
       hk.scale = n->scale;
       hk.sigma = n->sigma;
-      const dim3 g(n->w / kD0T, n->h / kD0T);
-      const float* b0 = n->wf + off + (size_t)L.cout * L.cin * 9;
-      const float* b1 = n->wf + off1 + (size_t)L1.cout * L1.cin * 9;
-      if (fvx_launch_pdl(conv_d0_out_kernel, g, dim3(kD0Threads), 0, st, (const float*)n->act[L.in],
-                         (const __nv_bfloat16*)(n->wb + off), b0, (const float*)n->act[L.skip],
-                         (const __nv_bfloat16*)(n->wb + off1), b1, coarse_u, n->h, n->w, hk) != cudaSuccess)
+      const dim3 g(n->w / kDT, n->h / kDT);
+      if (fvx_launch_pdl(conv_d1_d0_out_kernel, g, dim3(kDThreads), 0, st, (const float*)n->act[L.in],
+                         (const float*)n->act[L.skip], (const float*)n->act[L6.skip],
+                         (const __nv_bfloat16*)(n->wb + off), (const float*)(n->wf + off + (size_t)L.cout * L.cin * 9),
+                         (const __nv_bfloat16*)(n->wb + off6),
+                         (const float*)(n->wf + off6 + (size_t)L6.cout * L6.cin * 9),
+                         (const __nv_bfloat16*)(n->wb + off7),
+                         (const float*)(n->wf + off7 + (size_t)L7.cout * L7.cin * 9), coarse_u, n->h, n->w,
+                         hk) != cudaSuccess)
         return FVX_ERR_CUDA;
       return fvx_cuda_status();
     }
