@@ -33,8 +33,16 @@ DEV T tiered_face(const T* p, int st, int i, int N, bool pos, int code) {
 // on its north faces land in one flat shared buffer, four loads in flight
 // per thread (eight raise the FP32 kernels' registers from 31 to 59); the
 // face fluxes then overwrite u and v in place.
+// Resident CTAs per SM the compiler must allow: the FP64 WENO7 / WENO9 face
+// arithmetic otherwise takes ~126 registers (two CTAs per SM); capped at
+// three (WENO7) or four (WENO9) CTAs it spills a little and runs 3 % / 13 %
+// faster at 2048^2.
+template <typename T, int S>
+struct AdvMinBlocks {
+  static constexpr int v = sizeof(T) != 8 ? 1 : (S == FVX_WENO7 ? 3 : (S == FVX_WENO9 ? 4 : 1));
+};
 template <typename T, int S, int S4, int S6, bool MASKED>
-__global__ void __launch_bounds__(ATHREADS)
+__global__ void __launch_bounds__(ATHREADS, AdvMinBlocks<T, S>::v)
 advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __restrict__ v,
                    T* __restrict__ out, int ny, int nx, T dx, T dy,
                    const uint8_t* __restrict__ tiers, const uint8_t* __restrict__ mh) {
