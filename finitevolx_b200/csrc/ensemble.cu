@@ -97,43 +97,51 @@ ens_stage_kernel(const FieldDesc* __restrict__ fields, int nfields, int stage, i
 
 // Layers -> modes, written split into bf16 hi/lo (x de-interleaved when
 // perm) and, when fm is not null, as FP32 in natural order (the right-hand
-// side of the refinement residual).
-__global__ void ens_mode_split_kernel(const ModeDesc* __restrict__ md, int B, int n, __nv_bfloat16* hi,
-                                      __nv_bfloat16* lo, int perm, float* __restrict__ fm) {
-  const size_t plane = (size_t)n * n, total = plane * B;
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
-    const int b = (int)(k / plane);
-    const size_t r = k - (size_t)b * plane;
-    const int y = (int)(r / n), x = (int)(r - (size_t)y * n);
-    const ModeDesc& d = md[b];
-    const size_t g = (size_t)(y + 1) * (n + 2) + (x + 1);
-    float v = d.c[0] * d.q[0][g];
-    for (int l = 1; l < d.nl; ++l) v += d.c[l] * d.q[l][g];
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    const int xs = perm ? ((x & 1) ? (n >> 1) + (x >> 1) : (x >> 1)) : x;
-    const size_t o = (size_t)b * plane + (size_t)y * n + xs;
-    hi[o] = h;
-    lo[o] = __float2bfloat16_rn(v - __bfloat162float(h));
-    if (fm) fm[k] = v;
+// side of the refinement residual).  Grid (row blocks of kMixRows rows,
+// modes): each block reads its mode's descriptor once.
+constexpr int kMixRows = 8;
+__global__ void __launch_bounds__(256)
+ens_mode_split_kernel(const ModeDesc* __restrict__ md, int n, __nv_bfloat16* hi, __nv_bfloat16* lo, int perm,
+                      float* __restrict__ fm) {
+  const int b = blockIdx.y;
+  const ModeDesc d = md[b];
+  const size_t plane = (size_t)n * n;
+  const int y1 = min(n, (int)(blockIdx.x + 1) * kMixRows);
+  for (int y = blockIdx.x * kMixRows; y < y1; ++y) {
+    const size_t grow = (size_t)(y + 1) * (n + 2) + 1, orow = (size_t)b * plane + (size_t)y * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+      const size_t g = grow + x;
+      float v = d.c[0] * d.q[0][g];
+#pragma unroll
+      for (int l = 1; l < kMaxLayers; ++l)
+        if (l < d.nl) v += d.c[l] * d.q[l][g];
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      const int xs = perm ? ((x & 1) ? (n >> 1) + (x >> 1) : (x >> 1)) : x;
+      hi[orow + xs] = h;
+      lo[orow + xs] = __float2bfloat16_rn(v - __bfloat162float(h));
+      if (fm) fm[orow + x] = v;
+    }
   }
 }
 
-__global__ void ens_layer_mix_kernel(const LayerDesc* __restrict__ ld, int nlay, int n,
-                                     const float* __restrict__ psim) {
-  const size_t plane = (size_t)n * n, total = plane * nlay;
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
-    const int f = (int)(k / plane);
-    const size_t r = k - (size_t)f * plane;
-    const LayerDesc& d = ld[f];
-    float v = d.c[0] * psim[(size_t)d.b[0] * plane + r];
-    for (int m = 1; m < d.nl; ++m) v += d.c[m] * psim[(size_t)d.b[m] * plane + r];
-    d.psi[r] = v;
+// Modes -> layers: psi_k = sum_m c[m] psi_mode[b[m]].  Grid (row blocks of
+// kMixRows rows, layers).
+__global__ void __launch_bounds__(256)
+ens_layer_mix_kernel(const LayerDesc* __restrict__ ld, int n, const float* __restrict__ psim) {
+  const LayerDesc d = ld[blockIdx.y];
+  const size_t plane = (size_t)n * n;
+  const int y1 = min(n, (int)(blockIdx.x + 1) * kMixRows);
+  for (int y = blockIdx.x * kMixRows; y < y1; ++y) {
+    const size_t r0 = (size_t)y * n;
+    for (int x = threadIdx.x; x < n; x += blockDim.x) {
+      const size_t r = r0 + x;
+      float v = d.c[0] * psim[(size_t)d.b[0] * plane + r];
+#pragma unroll
+      for (int m = 1; m < kMaxLayers; ++m)
+        if (m < d.nl) v += d.c[m] * psim[(size_t)d.b[m] * plane + r];
+      d.psi[r] = v;
+    }
   }
-}
-
-static int grid_blocks(size_t n) {
-  size_t b = (n + 255) / 256;
-  return (int)(b > 148 * 8 ? 148 * 8 : (b < 1 ? 1 : b));
 }
 
 }  // namespace ens
@@ -471,17 +479,15 @@ extern "C" int fvx_ens_step(fvx_ens* e, int n_steps, void* stream) {
         auto& g = e->groups[k];
         cudaStream_t gs = k == 0 ? st : e->gst[k - 1];
         if (k > 0 && cudaStreamWaitEvent(gs, e->fork, 0) != cudaSuccess) return FVX_ERR_CUDA;
-        const size_t tot = (size_t)g.B * g.n * g.n;
-        ens_mode_split_kernel<<<grid_blocks(tot), 256, 0, gs>>>(g.md[s], g.B, g.n, g.hi, g.lo, g.perm,
-                                                                  e->refine ? g.fm : nullptr);
+        ens_mode_split_kernel<<<dim3((g.n + kMixRows - 1) / kMixRows, g.B), 256, 0, gs>>>(
+            g.md[s], g.n, g.hi, g.lo, g.perm, e->refine ? g.fm : nullptr);
         const long long plane = (long long)g.n * g.n;
         int rc = fvx_dst_solve_presplit_f32(g.plan, g.psim, plane, g.n, g.B, gs);
         if (rc) return rc;
         if (e->refine && g.nref &&
             (rc = fvx_dst_refine_f32(g.plan, g.fm, plane, g.n, g.psim, plane, g.n, g.nref, e->refine, gs)))
           return rc;
-        const size_t tl = (size_t)g.nlay * g.n * g.n;
-        ens_layer_mix_kernel<<<grid_blocks(tl), 256, 0, gs>>>(g.ld, g.nlay, g.n, g.psim);
+        ens_layer_mix_kernel<<<dim3((g.n + kMixRows - 1) / kMixRows, g.nlay), 256, 0, gs>>>(g.ld, g.n, g.psim);
         if (k > 0 && cudaEventRecord(e->gdone[k - 1], gs) != cudaSuccess) return FVX_ERR_CUDA;
       }
       for (int k = 1; k < ng; ++k)  // join before the stage kernel reads every psi

@@ -46,6 +46,28 @@ DEV double block_sum(double v) {
   return v;
 }
 
+// Grid-stride walk over the cells of an ny x nx array: f(c, j, i) for
+// c = global thread index, + stride, ... with the row j and column i
+// advanced by additions (one division per thread, at the start), so the
+// loop body carries no 64-bit division.
+template <typename F>
+DEV void grid_cells(int ny, int nx, F&& f) {
+  const size_t n = (size_t)ny * nx, stride = (size_t)gridDim.x * blockDim.x;
+  size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  int j = (int)(c / (size_t)nx), i = (int)(c - (size_t)j * nx);
+  const int dj = (int)(stride / (size_t)nx), di = (int)(stride - (size_t)dj * nx);
+  for (; c < n; c += stride) {
+    f(c, j, i);
+    i += di;
+    j += dj;
+    if (i >= nx) {
+      i -= nx;
+      ++j;
+    }
+  }
+}
+
 // True in the one block that finishes last (an atomic ticket taken after a
 // fence); that block then sums the partials in block order.
 DEV bool pcg_last_block(unsigned* ticket) {
@@ -383,12 +405,12 @@ __global__ void __launch_bounds__(256)
 k_coarse_omega(Lev<T> C, double* part, unsigned* ticket, double* omega) {
   const size_t n = (size_t)C.ny * C.nx;
   double df = 0.0, dad = 0.0;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(c / C.nx), i = (int)(c - (size_t)j * C.nx);
+  (void)n;
+  grid_cells(C.ny, C.nx, [&](size_t c, int j, int i) {
     const double d = (double)C.u[c];
     df += d * (double)C.f[c];
     dad += d * (double)apply_at(C, C.u, j, i);
-  }
+  });
   df = block_sum(df);
   dad = block_sum(dad);
   if (threadIdx.x == 0) { part[2 * blockIdx.x] = df; part[2 * blockIdx.x + 1] = dad; }
@@ -1391,12 +1413,12 @@ __global__ void k_apply_dot(Lev<T> L, const T* p, T* Ap, double* part, const dou
   if (s[S_CONV] != 0.0) return;
   const size_t n = (size_t)L.ny * L.nx;
   double acc = 0.0;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+  (void)n;
+  grid_cells(L.ny, L.nx, [&](size_t c, int j, int i) {
     const T a = apply_at(L, p, j, i);
     Ap[c] = a;
     acc += (double)p[c] * (double)a;
-  }
+  });
   acc = block_sum(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
@@ -1425,12 +1447,12 @@ __global__ void k_residual64(Lev<double> D, const double* x, const T* b, T* rho,
   if (!force && s[S_CONV] != 0.0) return;
   const size_t n = (size_t)D.ny * D.nx;
   double acc = 0.0;
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(c / D.nx), i = (int)(c - (size_t)j * D.nx);
+  (void)n;
+  grid_cells(D.ny, D.nx, [&](size_t c, int j, int i) {
     const double r = (double)b[c] - apply_at(D, x, j, i);
     if (rho) rho[c] = (T)r;
     acc += r * r;
-  }
+  });
   acc = block_sum(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
 }
@@ -1542,14 +1564,14 @@ k_dir_apply(Lev<T> L, const T* __restrict__ z, T* p0, T* p1, T* __restrict__ Ap,
   const size_t n = (size_t)L.ny * L.nx;
   double acc = 0.0;
   auto P = [&](size_t k) -> T { return z[k] + beta * po[k]; };
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
-    const int j = (int)(c / L.nx), i = (int)(c - (size_t)j * L.nx);
+  (void)n;
+  grid_cells(L.ny, L.nx, [&](size_t c, int j, int i) {
     const T pc = P(c);
     const T a = apply_fn(L, j, i, P);
     pn[c] = pc;
     Ap[c] = a;
     acc += (double)pc * (double)a;
-  }
+  });
   acc = block_sum(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
   if (pcg_last_block(ticket)) {
@@ -1581,13 +1603,13 @@ k_step(Lev<double> D, const T* p0, const T* p1, const T* __restrict__ Ap, double
   const size_t n = (size_t)D.ny * D.nx;
   double acc = 0.0;
   auto X = [&](size_t k) -> double { return xo[k] + a * (double)pn[k]; };
-  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) {
+  (void)n;
+  grid_cells(D.ny, D.nx, [&](size_t c, int j, int i) {
     const double xc = X(c);
     xn[c] = xc;
     const T ro = rho[c];
     if (rho_prev) rho_prev[c] = ro;
     if (true_res) {
-      const int j = (int)(c / D.nx), i = (int)(c - (size_t)j * D.nx);
       const double r = (double)b[c] - apply_fn(D, j, i, X);
       rho[c] = (T)r;
       acc += r * r;
@@ -1596,7 +1618,7 @@ k_step(Lev<double> D, const T* p0, const T* p1, const T* __restrict__ Ap, double
       rho[c] = r;
       acc += (double)r * (double)r;
     }
-  }
+  });
   acc = block_sum(acc);
   if (threadIdx.x == 0) part[blockIdx.x] = acc;
   if (pcg_last_block(ticket)) {
