@@ -80,6 +80,9 @@ def parse():
     ap.add_argument("--mg-profile", action="store_true",
                     help="only a few V-cycles, U-Net coarse solves and hybrid preconditioner applications on the "
                          "1024^2 masked basin (untrained network; for ncu launch lists of the Helmholtz path)")
+    ap.add_argument("--fp64-profile", action="store_true",
+                    help="only three eager FP64 QG steps at 256^2 (the metric's own configuration; for ncu launch "
+                         "lists)")
     ap.add_argument("--ens-profile", action="store_true",
                     help="only two eager steps of the 64-member ensemble (for ncu launch lists)")
     ap.add_argument("--ens-steps", type=int, default=100)
@@ -315,6 +318,8 @@ def fp64_metric_section(method, steps, flush, n=256):
     q0 = initial_q(n, seed=7)
     qd = torch.as_tensor(q0, device="cuda")
     got = model.step(qd, dt).cpu().numpy()
+    from finitevolx_b200 import autotune
+    tile = autotune.tune_qg_stage(model, qd, dt)["tile"]  # the FP64 stage tile, as the FP32 line's
     ref, times, cores = _oracle_steps(n, method, 3, q=q0)
     err = float(np.abs(got - ref).max() / np.abs(ref).max())
     qa, qb = qd.clone(), torch.empty_like(qd)
@@ -322,7 +327,7 @@ def fp64_metric_section(method, steps, flush, n=256):
     ms = _time_graphs(graphs, steps, flush)
     return {"workload": f"qg1.5_rk3ssp_{method}_dst_{n}x{n}", "dtype": "f64", "steps": steps,
             "ms_per_step": ms / steps, "value": n * n * steps / (ms * 1e-3) / 1e6, "unit": UNIT,
-            "launches_per_step": per_step, "dst": "FP64 SIMT transform-matrix chain",
+            "launches_per_step": per_step, "dst": "FP64 SIMT transform-matrix chain", "stage_tile": tile,
             "parity": {"rel_err_vs_fp64_oracle": err, "bar": 1e-12},
             "cpu_oracle": {"value": n * n * len(times) / sum(times) / 1e6, "unit": UNIT, "cores": cores}}
 
@@ -643,6 +648,27 @@ def ensemble_section(members, n_steps):
             "launches_per_step": r["launches_per_step"], "autotuned_blocks_per_sm": tuned.get("blocks_per_sm")}
 
 
+def fp64_profile_run(method, n=256, steps=3):
+    """The FP64 step's kernels (the metric's own configuration) in a short
+    run for ncu launch lists: one warm-up step and ``steps`` eager steps."""
+    import torch
+
+    import finitevolx_b200 as fvx
+    from finitevolx_b200.qg import QGModel
+    grid = fvx.ArakawaCGrid2D.from_interior(n, n, LX, LX)
+    dt = 0.5 * grid.dx
+    model = QGModel(grid, BETA, 1.0 / LD ** 2, method=method, dtype=torch.float64)
+    qa = torch.as_tensor(initial_q(n, seed=7), device="cuda")
+    qb = torch.empty_like(qa)
+    model.step(qa, dt, out=qb)
+    torch.cuda.synchronize()
+    for _ in range(steps):
+        model.step(qb, dt, out=qa)
+        qa, qb = qb, qa
+    torch.cuda.synchronize()
+    print(json.dumps({"fp64_profile_run": True, "n": n, "steps": steps}))
+
+
 def ens_profile_run(steps=2):
     """The ensemble's kernels in a short run for ncu launch lists: the bench's
     64 members (seeded states), ``steps`` eager RK3 steps after one warm-up
@@ -705,6 +731,9 @@ def main():
         return
     if args.ens_profile:
         ens_profile_run(steps=2)
+        return
+    if args.fp64_profile:
+        fp64_profile_run(args.method)
         return
     import numpy as np
     import torch

@@ -813,44 +813,64 @@ gemm_sym_pair_kernel(const __grid_constant__ CUtensorMap mAh, const __grid_const
 }
 
 // ---- FP64 SIMT GEMM with the same transposed-store epilogue (correctness path)
-constexpr int DT = 64, DK = 16;
+// TDT x TDT output tiles, 256 threads, each (TDT / 16)^2 outputs; every
+// output's FMA chain runs over k in order, so the tile size does not change
+// the result.  The largest tile that still gives at least one CTA per SM is
+// used (64, else 32, else 16).
+template <int TDT> struct F64Cfg {
+  // k-block: small tiles stage long k-blocks (few dependent load round trips
+  // per output); large tiles are bound by their FMAs
+  static constexpr int DK = TDT == 16 ? 128 : 16;
+};
+template <int TDT>
 __global__ void __launch_bounds__(256)
 gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict__ S, int lds, int M, int N, int K,
                 Epi ep) {
-  __shared__ double As[DK][DT + 1];
-  __shared__ double Ss[DK][DT + 1];
+  constexpr int R = TDT / 16, DK = F64Cfg<TDT>::DK, NL = TDT * DK / 256;  // loads per thread per operand
+  static_assert(TDT * DK % 256 == 0, "whole loads per thread");
+  __shared__ double As[DK][TDT + 1];
+  __shared__ double Ss[DK][TDT + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-  const int m0 = blockIdx.y * DT, n0 = blockIdx.x * DT;
-  double acc[4][4] = {};
+  const int m0 = blockIdx.y * TDT, n0 = blockIdx.x * TDT;
+  double acc[R][R] = {};
   for (int k0 = 0; k0 < K; k0 += DK) {
-    for (int t = threadIdx.x; t < DT * DK; t += 256) {
-      int mm = t / DK, kk = t % DK;
-      int gm = m0 + mm, gk = k0 + kk;
-      As[kk][mm] = (gm < M && gk < K) ? A[(long long)gm * lda + gk] : 0.0;
-      int kk2 = t / DT, nn = t % DT;
-      int gk2 = k0 + kk2, gn = n0 + nn;
-      Ss[kk2][nn] = (gk2 < K && gn < N) ? S[(long long)gk2 * lds + gn] : 0.0;
+    {  // every load of the k-block in flight before any is stored
+      double va[NL], vs[NL];
+#pragma unroll
+      for (int u = 0; u < NL; ++u) {
+        const int t = threadIdx.x + u * 256;
+        const int mm = t / DK, kk = t % DK, gm = m0 + mm, gk = k0 + kk;
+        va[u] = (gm < M && gk < K) ? A[(long long)gm * lda + gk] : 0.0;
+        const int kk2 = t / TDT, nn = t % TDT, gk2 = k0 + kk2, gn = n0 + nn;
+        vs[u] = (gk2 < K && gn < N) ? S[(long long)gk2 * lds + gn] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < NL; ++u) {
+        const int t = threadIdx.x + u * 256;
+        As[t % DK][t / DK] = va[u];
+        Ss[t / TDT][t % TDT] = vs[u];
+      }
     }
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < DK; ++kk) {
-      double a[4], s[4];
+      double a[R], s[R];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) { a[i] = As[kk][ty + 16 * i]; s[i] = Ss[kk][tx + 16 * i]; }
+      for (int i = 0; i < R; ++i) { a[i] = As[kk][ty + 16 * i]; s[i] = Ss[kk][tx + 16 * i]; }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < R; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], s[j], acc[i][j]);
+        for (int j = 0; j < R; ++j) acc[i][j] = fma(a[i], s[j], acc[i][j]);
     }
     __syncthreads();
   }
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < R; ++i) {
     const int m = m0 + ty + 16 * i;
     if (m >= M) continue;
     const int b = m / ep.rows_per_batch, r = m - b * ep.rows_per_batch;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < R; ++j) {
       const int n = n0 + tx + 16 * j;
       if (n >= N) continue;
       double x = acc[i][j] * ep.alpha;
@@ -1108,9 +1128,13 @@ static int gemm_sym(const bf16* Xh, const bf16* Xl, int M, int K, const bf16* Ph
 }
 
 static int gemm_f64(const double* A, int lda, int M, int K, const double* S, int N, const Epi& ep, cudaStream_t st) {
-  dim3 grid((N + DT - 1) / DT, (M + DT - 1) / DT);
+  auto tiles = [&](int t) { return (long long)((N + t - 1) / t) * ((M + t - 1) / t); };
+  const int t = tiles(64) >= 148 ? 64 : (tiles(32) >= 148 ? 32 : 16);
+  dim3 grid((N + t - 1) / t, (M + t - 1) / t);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  gemm_f64_kernel<<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
+  if (t == 64) gemm_f64_kernel<64><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
+  else if (t == 32) gemm_f64_kernel<32><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
+  else gemm_f64_kernel<16><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
   return fvx_cuda_status();
 }
 
