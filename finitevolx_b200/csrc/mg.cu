@@ -635,7 +635,7 @@ down_leg_kernel(Lev<T> L, const T* f, const T* u_init, int k, T omega, Lev<T> C)
   A = leg_sweeps<T, R>(L, s, A, B, scx, k, RW, RH, c, r0, LR, act);
   B = A == scx + g.RN ? A + g.RN : scx + g.RN;
   // the tile's u, and its residual * mask (u is masked, so the neighbours'
-  // masks multiply by 1 or meet a zero: res_s's values)
+  // masks multiply by 1 or meet a zero: restrict_at's values)
   T rm[R];
   {
     const bool colt = act && c >= H && c < H + TX;

@@ -8,7 +8,10 @@ tests check the kernels themselves against the oracle).
   weno5_x2), and stencils whose products overflow are the ones the kernels
   send to the four-division fallback.
 * Division-free (row, column) walks of the multigrid kernels (csrc/mg.cu
-  coarse_cells, leg_region): the same cells as c -> (c / w, c % w).
+  coarse_cells, grid_cells): the same cells as c -> (c / w, c % w).
+* The multigrid legs' thread layout (csrc/mg.cu leg_shape, leg_config):
+  every cell of a leg's region is owned by exactly one thread, within that
+  thread's register rows, for every sweep count a leg accepts.
 """
 
 import numpy as np
@@ -121,3 +124,32 @@ def test_mask_free_jacobi_equals_masked_form():
     r = f - (lap - 2.0 * um)
     got = um + (omega * L["inv"]) * r
     np.testing.assert_array_equal(got, ref)
+
+
+def _leg_shape(tx, ty, halo, nt):
+    rw, rh = tx + 2 * halo, ty + 2 * halo
+    nseg = nt // rw
+    return rw, rh, (-(-rh // nseg) if nseg > 0 else 1 << 20)
+
+
+@pytest.mark.parametrize("tile", [(64, 32), (32, 16)])
+def test_leg_threads_own_every_region_cell_once(tile):
+    nt_r = [(512, 4), (512, 8), (1024, 4), (1024, 8)]  # leg_config's candidates
+    for k in range(0, 17):  # sweeps per leg (kLegMaxSweeps = 16)
+        for halo in (k + 1, k):  # down leg, up leg
+            for order in ((2, 3, 1, 0), (0, 1, 2, 3)):
+                cfg = next(i for i in order if _leg_shape(*tile, k + 1, nt_r[i][0])[2] <= nt_r[i][1])
+                nt, rows = nt_r[cfg]
+                rw, rh, lr = _leg_shape(*tile, halo, nt)
+                assert lr <= rows
+                owned = np.zeros((rh, rw), np.int64)
+                for tid in range(nt):
+                    seg, c = divmod(tid, rw)
+                    r0 = seg * lr
+                    if r0 >= rh:
+                        continue
+                    for i in range(rows):
+                        r = r0 + i
+                        if i < lr and r < rh:
+                            owned[r, c] += 1
+                assert (owned == 1).all(), (tile, k, halo, cfg)
