@@ -76,7 +76,11 @@ def test_dst_product_forms_agree(cuda_ok, shape):
         assert rel_err(o, outs[0]) < 5e-5
 
 
-@pytest.mark.parametrize("shape", [(40, 56), (37, 29), (128, 128)])
+# The FP64 products take 16-, 32- or 64-element output tiles by problem size
+# (the largest giving at least 148 tiles): the first three shapes run on
+# 16-tiles, (420, 388) on 32-tiles and (790, 780) on 64-tiles, both with
+# partial edge tiles.
+@pytest.mark.parametrize("shape", [(40, 56), (37, 29), (128, 128), (420, 388), (790, 780)])
 def test_dst_fp64_chain(cuda_ok, shape):
     ny, nx = shape
     f = np.random.default_rng(1).standard_normal((ny, nx))
@@ -286,6 +290,23 @@ def test_qg_step_fp64_256_within_1e12(cuda_ok):
     got = host(m.step(dev(q), dt))
     assert rel_err(got, ref) < 1e-12
     assert rel_err(got - q, ref - q) < 1e-9
+
+
+def test_qg_step_fp64_every_stage_tile(cuda_ok):
+    # the FP64 stage tile is autotuned: every shape the tuner may pick meets
+    # the FP64 bar at the metric's configuration
+    from finitevolx_b200 import autotune
+    n = 256
+    grid, q = qg_setup(n, torch.float64, 14)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method="weno5", dtype=torch.float64)
+    ref = O.qg_step(q, grid.dx, grid.dy, beta, lam, dt, "weno5")
+    try:
+        for cfg in range(len(autotune._TILES)):
+            autotune.set_stage_tile("weno5", torch.float64, cfg)
+            assert rel_err(host(m.step(dev(q), dt)), ref) < 1e-12, autotune._TILES[cfg]
+    finally:
+        autotune.set_stage_tile("weno5", torch.float64, 0)
 
 
 @pytest.mark.parametrize("n,ld", [(128, 6.7e5), (512, 4.0e6)])

@@ -94,6 +94,28 @@ def test_mg_fine_levels_host_driven_path(cuda_ok):
     assert rel(host(mg.v_cycle(None, dev(f))), O.mg_vcycle(ref, np.zeros_like(f), f)) < 1e-10
 
 
+@pytest.mark.parametrize("dtype,sweeps,bar", [(torch.float64, 12, 1e-10), (torch.float64, 16, 1e-10),
+                                              (torch.float32, 12, 1e-5), (torch.float32, 16, 1e-5)])
+def test_mg_vcycle_many_sweeps(cuda_ok, dtype, sweeps, bar):
+    # 12 and 16 sweeps per leg widen each tile's region past what four rows
+    # per thread cover: the legs run their eight-row thread layouts (FP64
+    # 512 threads x 8 rows at 512^2, FP32 1024 x 8)
+    n = 512
+    m = basin(n, 21)
+    c = coeff(n, 22)
+    kw = dict(lambda_=0.5, coeff=c, n_pre=sweeps, n_post=sweeps)
+    mg = fvx.build_multigrid_solver(m, 1.0 / n, 1.0 / n, dtype=dtype, **kw)
+    ref = O.mg_build(m, 1.0 / n, 1.0 / n, **kw)
+    f = np.random.default_rng(23).standard_normal((n, n)) * m
+    if dtype == torch.float32:
+        f = f.astype(np.float32).astype(np.float64)
+    u = np.random.default_rng(24).standard_normal((n, n)) * m
+    if dtype == torch.float32:
+        u = u.astype(np.float32).astype(np.float64)
+    assert rel(host(mg.v_cycle(None, dev(f, dtype))), O.mg_vcycle(ref, np.zeros_like(f), f)) < bar
+    assert rel(host(mg.v_cycle(dev(u, dtype), dev(f, dtype))), O.mg_vcycle(ref, u, f)) < bar
+
+
 def test_mg_fp32_plan_coarsest_solve_in_fp64(cuda_ok):
     # FP32 plans run the coarsest-grid solve (its 50 Jacobi sweeps) in FP64.
     # With no smoothing on the other levels a V-cycle is restriction ->
