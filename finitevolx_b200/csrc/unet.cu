@@ -516,53 +516,158 @@ __global__ void in_adjoint_kernel(const float* dxin, float* dsrc, int mode, int 
   }
 }
 
-// dW partials: block (tile, b) sums G[co] * Xin[ci] shifted over its 16x16
-// pixels for every (co, ci, t); db partials likewise.
+// dW and db partials.  dW[co][ci][t] = sum over samples and pixels of
+// G[co](p) Xin[ci](p + shift t), db[co] = sum of G[co]: a contraction over
+// B h w pixels with Cout x Cin x 9 outputs.  Block j of P accumulates the
+// (sample, 16 x 16 tile) items j, j + P, j + 2P, ... in registers, in that
+// order; a thread owns COT output channels x one input channel x the nine
+// taps and a residue class of the tile's rows, walking each row with a 3 x 3
+// window of the input that gains one column per pixel (per pixel: COT + 3
+// shared loads for 9 COT FMAs).  The row classes are summed at the end in a
+// fixed order and the block writes its partial row [Cout Cin 9 | Cout]:
+// every partial, and the fixed-order sum over P that follows, is run-to-run
+// identical.
+constexpr int kWgradRows = 296;  // P at most: two partial rows per SM
+constexpr int kWgradGS = TILE * TILE + 1;                   // padded G row
+constexpr int kWgradXS = ((TILE + 2) * (TILE + 2)) | 1;     // padded input plane (odd: ci spreads over banks)
+
+struct WgradShape {
+  int ncog, ot, pg;  // channel groups, threads per row class, row classes
+};
+__host__ __device__ inline WgradShape wgrad_shape(int cin, int cout, int cot) {
+  WgradShape s;
+  s.ncog = (cout + cot - 1) / cot;
+  s.ot = s.ncog * cin;
+  s.pg = THREADS / s.ot < TILE ? THREADS / s.ot : TILE;
+  return s;
+}
+static int wgrad_cot(int cout) { return cout >= 4 ? 4 : (cout >= 2 ? 2 : 1); }
+static size_t wgrad_smem(int cin, int cout, int cot) {
+  const WgradShape s = wgrad_shape(cin, cout, cot);
+  const size_t stage = (size_t)s.ncog * cot * kWgradGS + (size_t)cin * kWgradXS;
+  const size_t comb = (size_t)s.pg * s.ot * cot * 10;
+  return (stage > comb ? stage : comb) * sizeof(float);
+}
+
+template <int COT>
 __global__ void __launch_bounds__(THREADS)
-conv_bwd_weight_kernel(const float* __restrict__ in, int mode, int cin, const float* __restrict__ g, int cout, int h,
-                       int w, float* __restrict__ part_w, float* __restrict__ part_b) {
-  __shared__ float gs[CMAX][TILE * TILE];
-  __shared__ float xs[TILE + 2][TILE + 2];
-  const int b = blockIdx.z;
-  const int x0 = blockIdx.x * TILE, y0 = blockIdx.y * TILE;
-  const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  const size_t plane = (size_t)h * w;
-  for (int k = threadIdx.x; k < cout * TILE * TILE; k += THREADS) {
-    const int co = k / (TILE * TILE), p = k % (TILE * TILE);
-    const int y = y0 + p / TILE, x = x0 + p % TILE;
-    gs[co][p] = (y < h && x < w) ? g[((size_t)b * cout + co) * plane + (size_t)y * w + x] : 0.f;
+conv_wgrad_kernel(const float* __restrict__ in, int mode, int cin, const float* __restrict__ g, int cout, int h,
+                  int w, int batch, float* __restrict__ part) {
+  extern __shared__ float wsm[];
+  const WgradShape S = wgrad_shape(cin, cout, COT);
+  const int coutp = S.ncog * COT;
+  float* gs = wsm;                          // [coutp][kWgradGS]
+  float* xs = wsm + (size_t)coutp * kWgradGS;  // [cin][kWgradXS], (TILE+2)^2 used
+  const int tid = threadIdx.x;
+  const int pg = tid / S.ot, r = tid - pg * S.ot;
+  const int cog = r / cin, ci = r - cog * cin;
+  const bool act = pg < S.pg;
+  float acc[COT][9], accb[COT];
+#pragma unroll
+  for (int j = 0; j < COT; ++j) {
+    accb[j] = 0.f;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) acc[j][t] = 0.f;
   }
-  __syncthreads();
-  if (threadIdx.x < cout) {
-    float s = 0.f;
-    for (int p = 0; p < TILE * TILE; ++p) s += gs[threadIdx.x][p];
-    part_b[(size_t)blk * cout + threadIdx.x] = s;
-  }
-  const size_t sp = src_plane(mode, h, w);
-  const float* inb = in + (size_t)b * cin * sp;
-  const int combos = cout * 9;
-  for (int ci = 0; ci < cin; ++ci) {
-    __syncthreads();
-    for (int k = threadIdx.x; k < (TILE + 2) * (TILE + 2); k += THREADS) {
-      const int ly = k / (TILE + 2), lx = k % (TILE + 2);
-      xs[ly][lx] = in_at(inb + ci * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+  const int tx = (w + TILE - 1) / TILE, ty = (h + TILE - 1) / TILE;
+  const int nitems = tx * ty * batch;
+  const size_t plane = (size_t)h * w, sp = src_plane(mode, h, w);
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int b = it / (tx * ty), rr = it - b * (tx * ty);
+    const int y0 = (rr / tx) * TILE, x0 = (rr - (rr / tx) * tx) * TILE;
+    __syncthreads();  // the previous item's reads are done
+    for (int k = tid; k < coutp * TILE * TILE; k += THREADS) {
+      const int co = k / (TILE * TILE), p = k - co * (TILE * TILE);
+      const int y = y0 + p / TILE, x = x0 + p % TILE;
+      gs[co * kWgradGS + p] =
+          (co < cout && y < h && x < w) ? g[((size_t)b * cout + co) * plane + (size_t)y * w + x] : 0.f;
+    }
+    const float* inb = in + (size_t)b * cin * sp;
+    for (int k = tid; k < cin * (TILE + 2) * (TILE + 2); k += THREADS) {
+      const int c = k / ((TILE + 2) * (TILE + 2)), q = k - c * ((TILE + 2) * (TILE + 2));
+      const int ly = q / (TILE + 2), lx = q - ly * (TILE + 2);
+      xs[c * kWgradXS + q] = in_at(inb + c * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
     }
     __syncthreads();
-    for (int c = threadIdx.x; c < combos; c += THREADS) {
-      const int co = c / 9, t = c % 9, dy = t / 3, dx = t % 3;
-      float s = 0.f;
-      for (int p = 0; p < TILE * TILE; ++p) s = fmaf(gs[co][p], xs[p / TILE + dy][p % TILE + dx], s);
-      part_w[(size_t)blk * cout * cin * 9 + ((size_t)co * cin + ci) * 9 + t] = s;
+    if (act) {
+      const float* gp = gs + (size_t)cog * COT * kWgradGS;
+      const float* xp = xs + (size_t)ci * kWgradXS;
+      for (int py = pg; py < TILE; py += S.pg) {
+        // window columns c0, c1 (and c2 loaded per pixel) of rows py .. py+2
+        const float* xr = xp + py * (TILE + 2);
+        float a0 = xr[0], a1 = xr[TILE + 2], a2 = xr[2 * (TILE + 2)];
+        float b0 = xr[1], b1 = xr[TILE + 3], b2 = xr[2 * (TILE + 2) + 1];
+#pragma unroll 4
+        for (int px = 0; px < TILE; ++px) {
+          const float c0 = xr[px + 2], c1 = xr[TILE + 2 + px + 2], c2 = xr[2 * (TILE + 2) + px + 2];
+#pragma unroll
+          for (int j = 0; j < COT; ++j) {
+            const float gv = gp[j * kWgradGS + py * TILE + px];
+            acc[j][0] = fmaf(gv, a0, acc[j][0]);
+            acc[j][1] = fmaf(gv, b0, acc[j][1]);
+            acc[j][2] = fmaf(gv, c0, acc[j][2]);
+            acc[j][3] = fmaf(gv, a1, acc[j][3]);
+            acc[j][4] = fmaf(gv, b1, acc[j][4]);
+            acc[j][5] = fmaf(gv, c1, acc[j][5]);
+            acc[j][6] = fmaf(gv, a2, acc[j][6]);
+            acc[j][7] = fmaf(gv, b2, acc[j][7]);
+            acc[j][8] = fmaf(gv, c2, acc[j][8]);
+            accb[j] += gv;
+          }
+          a0 = b0; a1 = b1; a2 = b2;
+          b0 = c0; b1 = c1; b2 = c2;
+        }
+      }
+    }
+  }
+  // row classes summed in a fixed order through shared memory
+  __syncthreads();
+  float* comb = wsm;  // [pg][ot][COT * 10]
+  if (act) {
+    float* c = comb + ((size_t)pg * S.ot + r) * (COT * 10);
+#pragma unroll
+    for (int j = 0; j < COT; ++j) {
+#pragma unroll
+      for (int t = 0; t < 9; ++t) c[j * 10 + t] = acc[j][t];
+      c[j * 10 + 9] = accb[j];
+    }
+  }
+  __syncthreads();
+  if (tid < S.ot) {
+    float* row = part + (size_t)blockIdx.x * ((size_t)cout * cin * 9 + cout);
+    for (int j = 0; j < COT; ++j) {
+      const int co = cog * COT + j;
+      if (co >= cout) break;
+      for (int t = 0; t < 10; ++t) {
+        float s = 0.f;
+        for (int q = 0; q < S.pg; ++q) s += comb[((size_t)q * S.ot + r) * (COT * 10) + j * 10 + t];
+        if (t < 9) row[((size_t)co * cin + ci) * 9 + t] = s;
+        else if (ci == 0) row[(size_t)cout * cin * 9 + co] = s;
+      }
     }
   }
 }
 
-// sum over blocks (fixed order) of the partials into grad
-__global__ void reduce_parts_kernel(const float* part, int nblk, int len, float* grad) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < len; k += gridDim.x * blockDim.x) {
-    float s = 0.f;
-    for (int j = 0; j < nblk; ++j) s += part[(size_t)j * len + k];
-    grad[k] = s;
+// Sum of the P partial rows (fixed order) into dW (the first nw entries of
+// a row) and db (the rest): a block per 32 consecutive entries, its eight
+// warps taking the rows in residue classes mod 8, then the eight class sums
+// in order.
+__global__ void __launch_bounds__(256)
+reduce_rows_kernel(const float* __restrict__ part, int nrows, int len, int nw, float* dw, float* db) {
+  __shared__ float sh[8][32];
+  const int lane = threadIdx.x & 31, wq = threadIdx.x >> 5;
+  const int k = blockIdx.x * 32 + lane;
+  float s = 0.f;
+  if (k < len)
+    for (int j = wq; j < nrows; j += 8) s += part[(size_t)j * len + k];
+  sh[wq][lane] = s;
+  __syncthreads();
+  if (wq == 0 && k < len) {
+    float t = sh[0][lane];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) t += sh[q][lane];
+    if (k < nw) dw[k] = t;
+    else db[k - nw] = t;
   }
 }
 
@@ -652,6 +757,7 @@ extern "C" int fvx_nn_conv_fwd(const float* in, int mode, int batch, int cin, co
 // skip gradient into dskip (if non-null), adds the input gradient into
 // dsrc (if non-null; dxin scratch [B, Cin, h, w]), and writes dW, db.
 // part: scratch of nblocks * Cout * (Cin * 9 + 1) floats.
+extern "C" int fvx_nn_conv_bwd_blocks(int batch, int h, int w);
 extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, const void* wb, const float* dy,
                                const float* y, int cout, int h, int w, int relu, float* g, float* dskip, float* dxin,
                                float* dsrc, float* dw, float* db, float* part, void* stream) {
@@ -662,12 +768,22 @@ extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, co
   const size_t n = (size_t)batch * cout * h * w;
   act_grad_kernel<<<blocks_for(n), 256, 0, st>>>(dy, y, g, dskip, n, relu);
   dim3 gr((w + TILE - 1) / TILE, (h + TILE - 1) / TILE, batch);
-  const int nblk = gr.x * gr.y * gr.z;
-  float* pw = part;
-  float* pb = part + (size_t)nblk * cout * cin * 9;
-  conv_bwd_weight_kernel<<<gr, THREADS, 0, st>>>(in, mode, cin, g, cout, h, w, pw, pb);
-  reduce_parts_kernel<<<blocks_for((size_t)cout * cin * 9), 256, 0, st>>>(pw, nblk, cout * cin * 9, dw);
-  reduce_parts_kernel<<<1, 256, 0, st>>>(pb, nblk, cout, db);
+  // weight and bias gradients: P partial rows, then their fixed-order sum
+  static fvx_once_per_device attr;
+  if (fvx_once_on_device(attr, [] {
+        return fvx_set_max_smem(conv_wgrad_kernel<4>, (int)wgrad_smem(CMAX, CMAX, 4)) &&
+               fvx_set_max_smem(conv_wgrad_kernel<2>, (int)wgrad_smem(CMAX, 3, 2)) &&
+               fvx_set_max_smem(conv_wgrad_kernel<1>, (int)wgrad_smem(CMAX, 1, 1));
+      }))
+    return FVX_ERR_CUDA;
+  const int nrows = fvx_nn_conv_bwd_blocks(batch, h, w);
+  const int cot = wgrad_cot(cout);
+  const size_t wsm = wgrad_smem(cin, cout, cot);
+  if (cot == 4) conv_wgrad_kernel<4><<<nrows, THREADS, wsm, st>>>(in, mode, cin, g, cout, h, w, batch, part);
+  else if (cot == 2) conv_wgrad_kernel<2><<<nrows, THREADS, wsm, st>>>(in, mode, cin, g, cout, h, w, batch, part);
+  else conv_wgrad_kernel<1><<<nrows, THREADS, wsm, st>>>(in, mode, cin, g, cout, h, w, batch, part);
+  const int len = cout * (cin * 9 + 1);
+  reduce_rows_kernel<<<(len + 31) / 32, 256, 0, st>>>(part, nrows, len, cout * cin * 9, dw, db);
   if (dsrc) {
     if (!dxin) return FVX_ERR_ARG;
     switch (cin) {
@@ -684,9 +800,11 @@ extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, co
   return fvx_cuda_status();
 }
 
-// Number of blocks a conv_bwd call uses for its partials (scratch sizing).
+// Number of partial rows a conv_bwd call writes (scratch sizing): one per
+// (sample, 16 x 16 tile) item, at most kWgradRows.
 extern "C" int fvx_nn_conv_bwd_blocks(int batch, int h, int w) {
-  return ((w + TILE - 1) / TILE) * ((h + TILE - 1) / TILE) * batch;
+  const long long items = (long long)((w + TILE - 1) / TILE) * ((h + TILE - 1) / TILE) * batch;
+  return (int)(items < kWgradRows ? (items < 1 ? 1 : items) : kWgradRows);
 }
 
 extern "C" int fvx_nn_mse(const float* pred, const float* target, const float* mask, long long plane, int batch,
