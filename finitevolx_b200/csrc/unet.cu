@@ -13,6 +13,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 namespace fvx {
@@ -493,6 +494,270 @@ conv_bwd_data_kernel(const float* __restrict__ g, int cout, const __nv_bfloat16*
   for (int ci = 0; ci < CIN; ++ci) dxin[base + ci * plane] = acc[ci];
 }
 
+// Batched 3x3 convolution for training (many samples):
+//   out[b][co] = act(sum_ci sum_t W[co][ci][t] in~[b][ci](p + shift t) + bias[co] (+ skip)),
+// in~ the mode-transformed input.  A block covers a TH x 32 pixel tile of
+// one sample and every output channel; a thread owns 8 consecutive pixels
+// of one row x 8 output channels (64 FMA accumulators), walks the input
+// channels in chunks of 8 staged in shared memory, and per (channel, tap
+// row) loads one 10-value input window and per tap 8 weights as two
+// float4: 33 shared loads per 576 FMAs.  WT = bf16: the forward weights
+// W[co][ci][9]; WT = float: any [co][ci][9] FP32 table (the data gradient's
+// transposed, flipped weights).  bias and skip may be null.
+constexpr int kBcPX = 8, kBcCO = 8, kBcTW = 32, kBcKC = 8, kBcPitch = kBcTW + 2;
+template <int COUT> struct BcCfg {
+  static constexpr int NCG = COUT / kBcCO;        // channel groups
+  static constexpr int TH = THREADS / (4 * NCG);   // tile rows (4 threads cover a row of 32 pixels)
+  static constexpr int IN_FLOATS = kBcKC * (TH + 2) * kBcPitch;
+  static_assert(IN_FLOATS % 4 == 0, "the weight table starts 16-byte aligned");
+};
+template <int COUT>
+static size_t bc_smem(int cin, bool adjoint = false) {
+  const size_t main = (size_t)BcCfg<COUT>::IN_FLOATS + (size_t)cin * 9 * COUT;
+  const size_t adj = adjoint ? (size_t)COUT * BcCfg<COUT>::TH * (kBcTW + 1) : 0;  // the adjoint epilogue's tile
+  return (main > adj ? main : adj) * sizeof(float);
+}
+
+// Adjoint epilogue of the data gradient: the tile's 8 channels of dX (in
+// shared memory, [8][TH][EP]) go straight into the gradient of the layer's
+// source, dsrc += T^T dX, instead of through a dX tensor: IN_DIRECT adds
+// them, IN_POOL spreads each value / 4 over its 2 x 2 source pixels, IN_UP
+// gathers each source pixel's 2 x 2 children (the tile holds whole groups:
+// y0 and x0 even, h and w even).  Every dsrc element is updated by one
+// thread, in the order of the separate adjoint pass.  A thread takes runs of
+// 4 destination pixels along a row (float4 read-modify-writes when aligned)
+// and issues the loads of 4 runs before any store.
+template <int COUT, int TH, int EP>
+DEV void conv_batch_adjoint(const float* e, float* dsrc, int amode, int b, int grp, int y0, int x0, int h, int w) {
+  // destination runs per channel: rows x (columns / 4) of the tile's image
+  // in dsrc (IN_POOL: two source rows per tile row, each 8 wide per run of 4)
+  const bool up = amode == IN_UP, pool = amode == IN_POOL;
+  const int drows = up ? TH / 2 : TH, druns = up ? kBcTW / 8 : kBcTW / 4;
+  const int dh = up ? h >> 1 : (pool ? 2 * h : h), dw = up ? w >> 1 : (pool ? 2 * w : w);
+  const bool v4 = (dw & 3) == 0 && ((uintptr_t)dsrc & 15) == 0;
+  const int n = kBcCO * drows * druns;
+  for (int base = threadIdx.x; base < n; base += 4 * THREADS) {
+    float4 add[4][2];
+    float4 cur[4][2];
+    size_t off[4];
+    int valid[4], dxs[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = base + u * THREADS;
+      valid[u] = 0;
+      if (k >= n) continue;
+      const int q = k / (drows * druns), rem = k - q * (drows * druns);
+      const int rr = rem / druns, j = rem - rr * druns;
+      const size_t pl = (size_t)b * COUT + grp * kBcCO + q;
+      int dy, dx;  // first destination pixel of the run
+      if (up) {
+        dy = (y0 >> 1) + rr;
+        dx = (x0 >> 1) + 4 * j;
+        const float* c = e + (q * TH + 2 * rr) * EP + 8 * j;
+        float v[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = (c[2 * i] + c[2 * i + 1]) + (c[EP + 2 * i] + c[EP + 2 * i + 1]);
+        add[u][0] = make_float4(v[0], v[1], v[2], v[3]);
+        add[u][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        const float* c = e + (q * TH + rr) * EP + 4 * j;
+        if (pool) {
+          dy = 2 * (y0 + rr);
+          dx = 2 * (x0 + 4 * j);
+          const float a0 = 0.25f * c[0], a1 = 0.25f * c[1], a2 = 0.25f * c[2], a3 = 0.25f * c[3];
+          add[u][0] = make_float4(a0, a0, a1, a1);
+          add[u][1] = make_float4(a2, a2, a3, a3);
+        } else {
+          dy = y0 + rr;
+          dx = x0 + 4 * j;
+          add[u][0] = make_float4(c[0], c[1], c[2], c[3]);
+          add[u][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+      }
+      if (dy >= dh || dx >= dw) continue;
+      dxs[u] = dx;
+      valid[u] = (v4 && dx + (pool ? 8 : 4) <= dw) ? 2 : 1;
+      off[u] = (pl * dh + dy) * dw + dx;
+      if (valid[u] == 2) {
+        cur[u][0] = *(const float4*)(dsrc + off[u]);
+        if (pool) {
+          cur[u][1] = *(const float4*)(dsrc + off[u] + 4);
+        }
+      }
+    }
+    // IN_POOL also needs the second source row: loaded with the first
+    float4 cur2[4][2];
+    if (pool) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (valid[u] == 2) {
+          cur2[u][0] = *(const float4*)(dsrc + off[u] + dw);
+          cur2[u][1] = *(const float4*)(dsrc + off[u] + dw + 4);
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (valid[u] == 2) {
+        const int nv = pool ? 2 : 1;
+        for (int h2 = 0; h2 < nv; ++h2) {
+          float4 a = cur[u][h2];
+          const float4 d = add[u][h2];
+          a.x += d.x; a.y += d.y; a.z += d.z; a.w += d.w;
+          *(float4*)(dsrc + off[u] + 4 * h2) = a;
+          if (pool) {
+            float4 a2 = cur2[u][h2];
+            a2.x += d.x; a2.y += d.y; a2.z += d.z; a2.w += d.w;
+            *(float4*)(dsrc + off[u] + dw + 4 * h2) = a2;
+          }
+        }
+      } else if (valid[u] == 1) {
+        // ragged or unaligned run: element by element, inside the row
+        const float4 d0 = add[u][0], d1 = add[u][1];
+        const float vals[8] = {d0.x, d0.y, d0.z, d0.w, d1.x, d1.y, d1.z, d1.w};
+        const int len = pool ? 8 : 4;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          if (i >= len || dxs[u] + i >= dw) break;
+          dsrc[off[u] + i] += vals[i];
+          if (pool) dsrc[off[u] + dw + i] += vals[i];
+        }
+      }
+    }
+  }
+}
+
+template <int COUT, typename WT>
+__global__ void __launch_bounds__(THREADS)
+conv_batch_kernel(const float* __restrict__ in, int mode, int cin, const WT* __restrict__ wt,
+                  const float* __restrict__ bias, const float* __restrict__ skip, float* __restrict__ out, int h,
+                  int w, int relu, int amode) {
+  using C = BcCfg<COUT>;
+  constexpr int TH = C::TH, NCG = C::NCG;
+  extern __shared__ __align__(16) float bsm[];
+  float* xin = bsm;               // [kBcKC][TH + 2][kBcPitch], origin (y0 - 1, x0 - 1)
+  float* ws = bsm + C::IN_FLOATS;  // [cin][9][COUT]
+  const int tid = threadIdx.x;
+  const int g = tid % NCG, c = (tid / NCG) % 4, r = tid / (4 * NCG);
+  const int b = blockIdx.z, x0 = blockIdx.x * kBcTW, y0 = blockIdx.y * TH;
+  for (int k = tid; k < cin * 9 * COUT; k += THREADS) {
+    const int co = k % COUT, rest = k / COUT;  // rest = ci * 9 + t
+    if constexpr (std::is_same<WT, float>::value) ws[k] = wt[(size_t)co * cin * 9 + rest];
+    else ws[k] = __bfloat162float(wt[(size_t)co * cin * 9 + rest]);
+  }
+  float acc[kBcPX][kBcCO];
+#pragma unroll
+  for (int p = 0; p < kBcPX; ++p)
+#pragma unroll
+    for (int q = 0; q < kBcCO; ++q) acc[p][q] = 0.f;
+  const size_t sp = src_plane(mode, h, w);
+  const float* inb = in + (size_t)b * cin * sp;
+  for (int c0 = 0; c0 < cin; c0 += kBcKC) {
+    const int kc = cin - c0 < kBcKC ? cin - c0 : kBcKC;
+    __syncthreads();  // the previous chunk's reads are done
+    stage8(
+        kc * (TH + 2) * kBcPitch,
+        [&](int k) {
+          const int cc = k / ((TH + 2) * kBcPitch), q = k - cc * ((TH + 2) * kBcPitch);
+          const int ly = q / kBcPitch, lx = q - ly * kBcPitch;
+          return in_at(inb + (size_t)(c0 + cc) * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+        },
+        [&](int k, float v) { xin[k] = v; });
+    __syncthreads();
+    for (int cc = 0; cc < kc; ++cc) {
+      const float* xr = xin + (cc * (TH + 2) + r) * kBcPitch + c * kBcPX;
+      const float* wr = ws + (size_t)(c0 + cc) * 9 * COUT + g * kBcCO;
+#pragma unroll
+      for (int dy = 0; dy < 3; ++dy) {
+        float row[kBcPX + 2];
+#pragma unroll
+        for (int j = 0; j < kBcPX + 2; j += 2) {
+          const float2 v = *(const float2*)(xr + dy * kBcPitch + j);
+          row[j] = v.x;
+          row[j + 1] = v.y;
+        }
+#pragma unroll
+        for (int dx = 0; dx < 3; ++dx) {
+          const float4 wa = *(const float4*)(wr + (dy * 3 + dx) * COUT);
+          const float4 wb = *(const float4*)(wr + (dy * 3 + dx) * COUT + 4);
+          const float wv[kBcCO] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};
+#pragma unroll
+          for (int p = 0; p < kBcPX; ++p)
+#pragma unroll
+            for (int q = 0; q < kBcCO; ++q) acc[p][q] = fmaf(row[p + dx], wv[q], acc[p][q]);
+        }
+      }
+    }
+  }
+  // epilogue: each group of 8 output channels passes through shared memory
+  // ([8][TH][33], reusing the input tile) so that the stores and the skip
+  // loads run along whole tile rows, four pixels per thread
+  constexpr int EP = kBcTW + 1;
+  static_assert(kBcCO * TH * EP <= C::IN_FLOATS, "epilogue staging fits the input tile");
+  if (amode >= 0) {
+    // data gradient: every channel of the tile into shared memory at once
+    // ([COUT][TH][EP], launched with room for it), then dsrc += T^T dX
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kBcCO; ++q)
+#pragma unroll
+      for (int p = 0; p < kBcPX; ++p) xin[((g * kBcCO + q) * TH + r) * EP + c * kBcPX + p] = acc[p][q];
+    __syncthreads();
+    for (int grp = 0; grp < NCG; ++grp)
+      conv_batch_adjoint<COUT, TH, EP>(xin + grp * kBcCO * TH * EP, out, amode, b, grp, y0, x0, h, w);
+    return;
+  }
+  const bool v4 = (w & 3) == 0 && (((uintptr_t)out | (uintptr_t)skip) & 15) == 0;
+  for (int grp = 0; grp < NCG; ++grp) {
+    __syncthreads();
+    if (g == grp) {
+#pragma unroll
+      for (int q = 0; q < kBcCO; ++q)
+#pragma unroll
+        for (int p = 0; p < kBcPX; ++p) xin[(q * TH + r) * EP + c * kBcPX + p] = acc[p][q];
+    }
+    __syncthreads();
+    for (int k = tid; k < kBcCO * TH * (kBcTW / 4); k += THREADS) {
+      const int q = k / (TH * (kBcTW / 4)), rem = k - q * (TH * (kBcTW / 4));
+      const int rr = rem / (kBcTW / 4), x4 = (rem - rr * (kBcTW / 4)) * 4;
+      const int co = grp * kBcCO + q, y = y0 + rr, x = x0 + x4;
+      if (y >= h || x >= w) continue;
+      const float bq = bias ? bias[co] : 0.f;
+      const float* e = xin + (q * TH + rr) * EP + x4;
+      float v[4] = {e[0] + bq, e[1] + bq, e[2] + bq, e[3] + bq};
+      const size_t o = (((size_t)b * COUT + co) * h + y) * w + x;
+      if (v4 && x + 4 <= w) {
+        if (skip) {
+          const float4 s = *(const float4*)(skip + o);
+          v[0] += s.x; v[1] += s.y; v[2] += s.z; v[3] += s.w;
+        }
+        if (relu) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) v[j] = fmaxf(v[j], 0.f);
+        }
+        *(float4*)(out + o) = make_float4(v[0], v[1], v[2], v[3]);
+      } else {
+        for (int j = 0; j < 4 && x + j < w; ++j) {
+          float t = v[j];
+          if (skip) t += skip[o + j];
+          if (relu) t = fmaxf(t, 0.f);
+          out[o + j] = t;
+        }
+      }
+    }
+  }
+}
+
+// The data gradient's weights for conv_batch_kernel: wt[ci][co][t] =
+// W[co][ci][8 - t] (input pixel p receives G at p - shift t).
+__global__ void flip_transpose_kernel(const __nv_bfloat16* __restrict__ wb, int cin, int cout,
+                                      float* __restrict__ wt) {
+  const int n = cin * cout * 9;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int ci = k / (cout * 9), rest = k - ci * (cout * 9), co = rest / 9, t = rest - co * 9;
+    wt[k] = __bfloat162float(wb[((size_t)co * cin + ci) * 9 + (8 - t)]);
+  }
+}
+
 // Adjoint of the input transform: dsrc += T^T dxin.
 __global__ void in_adjoint_kernel(const float* dxin, float* dsrc, int mode, int bc, int h, int w) {
   // bc = B * Cin planes; conv grid h x w
@@ -527,7 +792,27 @@ __global__ void in_adjoint_kernel(const float* dxin, float* dsrc, int mode, int 
 // fixed order and the block writes its partial row [Cout Cin 9 | Cout]:
 // every partial, and the fixed-order sum over P that follows, is run-to-run
 // identical.
-constexpr int kWgradRows = 296;  // P at most: two partial rows per SM
+// store(k, load(k)) for k < n over the block, eight loads in flight per
+// thread (all issued before any is stored), so staging a tile costs about
+// n / (8 THREADS) memory latencies instead of n / THREADS.
+template <typename L, typename S>
+DEV void stage8(int n, L load, S store) {
+  for (int base = threadIdx.x; base < n; base += 8 * THREADS) {
+    float v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = base + u * THREADS;
+      v[u] = k < n ? load(k) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = base + u * THREADS;
+      if (k < n) store(k, v[u]);
+    }
+  }
+}
+
+constexpr int kWgradRows = 592;  // P at most: four partial rows per SM
 constexpr int kWgradGS = TILE * TILE + 1;                   // padded G row
 constexpr int kWgradXS = ((TILE + 2) * (TILE + 2)) | 1;     // padded input plane (odd: ci spreads over banks)
 
@@ -541,12 +826,26 @@ __host__ __device__ inline WgradShape wgrad_shape(int cin, int cout, int cot) {
   s.pg = THREADS / s.ot < TILE ? THREADS / s.ot : TILE;
   return s;
 }
-static int wgrad_cot(int cout) { return cout >= 4 ? 4 : (cout >= 2 ? 2 : 1); }
 static size_t wgrad_smem(int cin, int cout, int cot) {
   const WgradShape s = wgrad_shape(cin, cout, cot);
   const size_t stage = (size_t)s.ncog * cot * kWgradGS + (size_t)cin * kWgradXS;
   const size_t comb = (size_t)s.pg * s.ot * cot * 10;
   return (stage > comb ? stage : comb) * sizeof(float);
+}
+// Output channels per thread: 2 while Cout / 2 x Cin threads fit the block
+// (fewer registers, four blocks per SM), else 4 (always fits: 8 x 32); 1
+// for a single output channel.
+static int wgrad_cot(int cin, int cout) {
+  if (cout == 1) return 1;
+  return wgrad_shape(cin, cout, 2).ot <= THREADS ? 2 : 4;
+}
+// Largest dynamic shared memory a COT instantiation is launched with.
+static size_t wgrad_smem_max(int cot) {
+  size_t m = 0;
+  for (int ci = 1; ci <= CMAX; ++ci)
+    for (int co = 1; co <= CMAX; ++co)
+      if (wgrad_cot(ci, co) == cot) m = std::max(m, wgrad_smem(ci, co, cot));
+  return m;
 }
 
 template <int COT>
@@ -576,18 +875,26 @@ conv_wgrad_kernel(const float* __restrict__ in, int mode, int cin, const float* 
     const int b = it / (tx * ty), rr = it - b * (tx * ty);
     const int y0 = (rr / tx) * TILE, x0 = (rr - (rr / tx) * tx) * TILE;
     __syncthreads();  // the previous item's reads are done
-    for (int k = tid; k < coutp * TILE * TILE; k += THREADS) {
-      const int co = k / (TILE * TILE), p = k - co * (TILE * TILE);
-      const int y = y0 + p / TILE, x = x0 + p % TILE;
-      gs[co * kWgradGS + p] =
-          (co < cout && y < h && x < w) ? g[((size_t)b * cout + co) * plane + (size_t)y * w + x] : 0.f;
-    }
+    stage8(
+        coutp * TILE * TILE,
+        [&](int k) {
+          const int co = k / (TILE * TILE), p = k - co * (TILE * TILE);
+          const int y = y0 + p / TILE, x = x0 + p % TILE;
+          return (co < cout && y < h && x < w) ? g[((size_t)b * cout + co) * plane + (size_t)y * w + x] : 0.f;
+        },
+        [&](int k, float v) { gs[(k / (TILE * TILE)) * kWgradGS + k % (TILE * TILE)] = v; });
     const float* inb = in + (size_t)b * cin * sp;
-    for (int k = tid; k < cin * (TILE + 2) * (TILE + 2); k += THREADS) {
-      const int c = k / ((TILE + 2) * (TILE + 2)), q = k - c * ((TILE + 2) * (TILE + 2));
-      const int ly = q / (TILE + 2), lx = q - ly * (TILE + 2);
-      xs[c * kWgradXS + q] = in_at(inb + c * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
-    }
+    stage8(
+        cin * (TILE + 2) * (TILE + 2),
+        [&](int k) {
+          const int c = k / ((TILE + 2) * (TILE + 2)), q = k - c * ((TILE + 2) * (TILE + 2));
+          const int ly = q / (TILE + 2), lx = q - ly * (TILE + 2);
+          return in_at(inb + c * sp, mode, h, w, y0 - 1 + ly, x0 - 1 + lx);
+        },
+        [&](int k, float v) {
+          const int c = k / ((TILE + 2) * (TILE + 2));
+          xs[c * kWgradXS + (k - c * ((TILE + 2) * (TILE + 2)))] = v;
+        });
     __syncthreads();
     if (act) {
       const float* gp = gs + (size_t)cog * COT * kWgradGS;
@@ -719,6 +1026,26 @@ static int blocks_for(size_t n) {
 using namespace fvx;
 using namespace fvx::nn;
 
+template <int COUT, typename WT>
+static int launch_conv_batch(const float* in, int mode, int batch, int cin, const WT* wt, const float* bias,
+                             const float* skip, float* out, int h, int w, int relu, cudaStream_t st,
+                             int amode = -1) {
+  static fvx_once_per_device attr;  // per instantiation; 32 input channels need > 48 KB
+  if (fvx_once_on_device(attr, [] {
+        return fvx_set_max_smem(conv_batch_kernel<COUT, WT>, (int)bc_smem<COUT>(CMAX, true));
+      }))
+    return FVX_ERR_CUDA;
+  const dim3 g((w + kBcTW - 1) / kBcTW, (h + BcCfg<COUT>::TH - 1) / BcCfg<COUT>::TH, batch);
+  conv_batch_kernel<COUT, WT><<<g, THREADS, bc_smem<COUT>(cin, amode >= 0), st>>>(in, mode, cin, wt, bias, skip, out,
+                                                                                  h, w, relu, amode);
+  return fvx_cuda_status();
+}
+// Training batches (several samples, grids of 32 x 32 and up) take the
+// register-blocked batch kernel; single samples (inference) the tile kernels.
+static bool conv_batch_ok(int batch, int h, int w, int cout) {
+  return batch > 1 && h >= 32 && w >= 32 && (cout == 16 || cout == 32);
+}
+
 // One conv layer; pdl: launched as a programmatic dependent of the kernel
 // before it, which must not have written the weights or biases (the kernel
 // reads them before waiting for it).
@@ -729,6 +1056,9 @@ static int conv_fwd(const float* in, int mode, int batch, int cin, const void* w
   if (cin < 1 || cin > CMAX || batch < 1 || h < 1 || w < 1 || mode < 0 || mode > 2) return FVX_ERR_SHAPE;
   if ((mode == IN_UP) && ((h % 2) || (w % 2))) return FVX_ERR_SHAPE;
   const __nv_bfloat16* wb = (const __nv_bfloat16*)w_bf16;
+  if (!pdl && !hk.x0_src && !hk.scale && !hk.out_mask && conv_batch_ok(batch, h, w, cout))
+    return cout == 16 ? launch_conv_batch<16>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st)
+                      : launch_conv_batch<32>(in, mode, batch, cin, wb, bias, skip, out, h, w, relu, st);
   // 8 x 8 tiles with 4 or 8 output channels per thread while that gives at
   // least one block per SM; else 4 x 4 tiles with 1 or 2 channels per
   // thread (256 threads, 4-8x the blocks) for the coarse levels
@@ -771,13 +1101,13 @@ extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, co
   // weight and bias gradients: P partial rows, then their fixed-order sum
   static fvx_once_per_device attr;
   if (fvx_once_on_device(attr, [] {
-        return fvx_set_max_smem(conv_wgrad_kernel<4>, (int)wgrad_smem(CMAX, CMAX, 4)) &&
-               fvx_set_max_smem(conv_wgrad_kernel<2>, (int)wgrad_smem(CMAX, 3, 2)) &&
-               fvx_set_max_smem(conv_wgrad_kernel<1>, (int)wgrad_smem(CMAX, 1, 1));
+        return fvx_set_max_smem(conv_wgrad_kernel<4>, (int)wgrad_smem_max(4)) &&
+               fvx_set_max_smem(conv_wgrad_kernel<2>, (int)wgrad_smem_max(2)) &&
+               fvx_set_max_smem(conv_wgrad_kernel<1>, (int)wgrad_smem_max(1));
       }))
     return FVX_ERR_CUDA;
   const int nrows = fvx_nn_conv_bwd_blocks(batch, h, w);
-  const int cot = wgrad_cot(cout);
+  const int cot = wgrad_cot(cin, cout);
   const size_t wsm = wgrad_smem(cin, cout, cot);
   if (cot == 4) conv_wgrad_kernel<4><<<nrows, THREADS, wsm, st>>>(in, mode, cin, g, cout, h, w, batch, part);
   else if (cot == 2) conv_wgrad_kernel<2><<<nrows, THREADS, wsm, st>>>(in, mode, cin, g, cout, h, w, batch, part);
@@ -786,16 +1116,28 @@ extern "C" int fvx_nn_conv_bwd(const float* in, int mode, int batch, int cin, co
   reduce_rows_kernel<<<(len + 31) / 32, 256, 0, st>>>(part, nrows, len, cout * cin * 9, dw, db);
   if (dsrc) {
     if (!dxin) return FVX_ERR_ARG;
-    switch (cin) {
-      case 1: conv_bwd_data_kernel<1><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
-      case 2: conv_bwd_data_kernel<2><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
-      case 3: conv_bwd_data_kernel<3><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
-      case 16: conv_bwd_data_kernel<16><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
-      case 32: conv_bwd_data_kernel<32><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
-      default: return FVX_ERR_SHAPE;
+    if (conv_batch_ok(batch, h, w, cin) && (mode != IN_UP || ((h | w) & 1) == 0)) {
+      // the data gradient as a convolution of G with the transposed,
+      // flipped weights (staged in the partial-row scratch, whose sum is
+      // done), its epilogue adding T^T dX into dsrc (no dX tensor)
+      flip_transpose_kernel<<<blocks_for((size_t)cin * cout * 9), 256, 0, st>>>(wf, cin, cout, part);
+      const int rc = cin == 16 ? launch_conv_batch<16>(g, IN_DIRECT, batch, cout, (const float*)part, nullptr, nullptr,
+                                                        dsrc, h, w, 0, st, mode)
+                               : launch_conv_batch<32>(g, IN_DIRECT, batch, cout, (const float*)part, nullptr, nullptr,
+                                                        dsrc, h, w, 0, st, mode);
+      if (rc) return rc;
+    } else {
+      switch (cin) {
+        case 1: conv_bwd_data_kernel<1><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+        case 2: conv_bwd_data_kernel<2><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+        case 3: conv_bwd_data_kernel<3><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+        case 16: conv_bwd_data_kernel<16><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+        case 32: conv_bwd_data_kernel<32><<<gr, THREADS, 0, st>>>(g, cout, wf, dxin, h, w); break;
+        default: return FVX_ERR_SHAPE;
+      }
+      const size_t sp = src_plane(mode, h, w);
+      in_adjoint_kernel<<<blocks_for((size_t)batch * cin * sp), 256, 0, st>>>(dxin, dsrc, mode, batch * cin, h, w);
     }
-    const size_t sp = src_plane(mode, h, w);
-    in_adjoint_kernel<<<blocks_for((size_t)batch * cin * sp), 256, 0, st>>>(dxin, dsrc, mode, batch * cin, h, w);
   }
   return fvx_cuda_status();
 }
