@@ -85,6 +85,9 @@ def parse():
                          "lists)")
     ap.add_argument("--ens-profile", action="store_true",
                     help="only two eager steps of the 64-member ensemble (for ncu launch lists)")
+    ap.add_argument("--train-profile", action="store_true",
+                    help="only U-Net training steps at batch 64 on 128^2 (seeded synthetic inputs; for ncu launch "
+                         "lists and the per-step time)")
     ap.add_argument("--ens-steps", type=int, default=100)
     ap.add_argument("--stage-tile", default=None, help="fix the stage tile (e.g. 64x32) instead of autotuning")
     return ap.parse_args()
@@ -693,6 +696,33 @@ def ens_profile_run(steps=2):
                       "launches_per_step": ens.launches_per_step}))
 
 
+def train_profile_run(steps=20, batch=64, n=128):
+    """U-Net training steps (forward, backward, Adam) at the bench's training
+    batch on a 128^2 level, seeded synthetic inputs and targets (channel 1 a
+    0/1 mask): three warm-up steps, then ``steps`` steps timed with CUDA
+    events on the current stream; prints the milliseconds per step."""
+    import torch
+
+    from finitevolx_b200.learned import UNet
+    net = UNet(n, n, batch_max=batch, seed=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.randn((batch, 3, n, n), generator=g, device="cuda")
+    x[:, 1] = (torch.rand((batch, n, n), generator=g, device="cuda") > 0.3).float()
+    t = torch.randn((batch, 1, n, n), generator=g, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        net.train_step(x, t, lr=1e-3, loss_out=loss)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        net.train_step(x, t, lr=1e-3, loss_out=loss)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"train_profile_run": True, "batch": batch, "n": n, "steps": steps,
+                      "ms_per_step": e0.elapsed_time(e1) / steps}))
+
+
 def mg_profile_run(n=1024, reps=3):
     """The Helmholtz path's kernels in a short run for ncu launch lists:
     ``reps`` MG V-cycles, U-Net coarse solves (per-layer chain) and hybrid
@@ -734,6 +764,9 @@ def main():
         return
     if args.fp64_profile:
         fp64_profile_run(args.method)
+        return
+    if args.train_profile:
+        train_profile_run(steps=args.steps)
         return
     import numpy as np
     import torch
