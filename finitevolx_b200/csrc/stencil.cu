@@ -33,16 +33,26 @@ DEV T tiered_face(const T* p, int st, int i, int N, bool pos, int code) {
 // on its north faces land in one flat shared buffer, four loads in flight
 // per thread (eight raise the FP32 kernels' registers from 31 to 59); the
 // face fluxes then overwrite u and v in place.
-// Resident CTAs per SM the compiler must allow: the FP64 WENO7 / WENO9 face
-// arithmetic otherwise takes ~126 registers (two CTAs per SM); capped at
-// three (WENO7) or four (WENO9) CTAs it spills a little and runs 3 % / 13 %
-// faster at 2048^2.
-template <typename T, int S>
-struct AdvMinBlocks {
-  static constexpr int v = sizeof(T) != 8 ? 1 : (S == FVX_WENO7 ? 3 : (S == FVX_WENO9 ? 4 : 1));
+// WENO7 / WENO9 faces are evaluated through a call: inlined into the face
+// loops, the compiler hoists the schemes' ~84 table coefficients out of the
+// loop into registers (FP64 WENO7: 134 registers, or spills under a cap of
+// three CTAs per SM); behind the call they stay constant-bank operands
+// (60 registers, no spills).
+template <int S>
+struct AdvFaceCall {
+  static constexpr bool v = S == FVX_WENO7 || S == FVX_WENO9;
 };
+template <typename T, int S>
+__noinline__ __device__ T face_value_call(const T* p, int st, int i, int N, bool pos) {
+  return face_value<T, S>(p, st, i, N, pos);
+}
+template <typename T, int S>
+DEV T adv_face(const T* p, int st, int i, int N, bool pos) {
+  if constexpr (AdvFaceCall<S>::v) return face_value_call<T, S>(p, st, i, N, pos);
+  else return face_value<T, S>(p, st, i, N, pos);
+}
 template <typename T, int S, int S4, int S6, bool MASKED>
-__global__ void __launch_bounds__(ATHREADS, AdvMinBlocks<T, S>::v)
+__global__ void __launch_bounds__(ATHREADS)
 advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __restrict__ v,
                    T* __restrict__ out, int ny, int nx, T dx, T dy,
                    const uint8_t* __restrict__ tiers, const uint8_t* __restrict__ mh) {
@@ -97,37 +107,45 @@ advect_tile_kernel(const T* __restrict__ h, const T* __restrict__ u, const T* __
     }
   }
   __syncthreads();
-  // east faces i = x0-1 .. x0+ATX-1 on rows y0 .. y0+ATY-1
-  for (int k = tid; k < NU; k += ATHREADS) {
-    int ly = k / (ATX + 1), lf = k % (ATX + 1);
-    int gj = y0 + ly, gi = x0 - 1 + lf;
-    T f = T(0);
-    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T uu = fe[k];
-      bool pos = uu >= T(0);
-      const T* p = &hs[(ly + AH) * HW + lf - 1 + AH];
-      T hf;
-      if (MASKED) hf = tiered_face<T, S4, S6>(p, 1, gi, nx, pos, pos ? tx_[ly][lf] : tx_[ly][lf + 1]);
-      else hf = face_value<T, S>(p, 1, gi, nx, pos);
-      f = hf * uu;
-    }
-    fe[k] = f;
+  // Face fluxes, overwriting u / v in place.  East face (ly, lf) is the
+  // face between cells x0-2+lf and x0-1+lf of row y0+ly; north face (lf, lx)
+  // the one between rows y0-2+lf and y0-1+lf of column x0+lx.  Each trip of
+  // the first loop takes cell (y0+ly, x0+lx)'s east and north faces (two
+  // independent reconstructions; ATY x ATX / ATHREADS whole trips), the
+  // second the tile's west-most east faces and south-most north faces.
+  auto east = [&](int ly, int lf) -> T {
+    const int gj = y0 + ly, gi = x0 - 1 + lf;
+    if (!(gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)) return T(0);
+    const T uu = fe[ly * (ATX + 1) + lf];
+    const bool pos = uu >= T(0);
+    const T* p = &hs[(ly + AH) * HW + lf - 1 + AH];
+    T hf;
+    if (MASKED) hf = tiered_face<T, S4, S6>(p, 1, gi, nx, pos, pos ? tx_[ly][lf] : tx_[ly][lf + 1]);
+    else hf = adv_face<T, S>(p, 1, gi, nx, pos);
+    return hf * uu;
+  };
+  auto north = [&](int lf, int lx) -> T {
+    const int gj = y0 - 1 + lf, gi = x0 + lx;
+    if (!(gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)) return T(0);
+    const T vv = fn[lf * ATX + lx];
+    const bool pos = vv >= T(0);
+    const T* p = &hs[(lf - 1 + AH) * HW + lx + AH];
+    T hf;
+    if (MASKED) hf = tiered_face<T, S4, S6>(p, HW, gj, ny, pos, pos ? ty_[lf][lx] : ty_[lf + 1][lx]);
+    else hf = adv_face<T, S>(p, HW, gj, ny, pos);
+    return hf * vv;
+  };
+  static_assert((ATY * ATX) % ATHREADS == 0, "whole trips over the tile's cells");
+#pragma unroll 1
+  for (int k = tid; k < ATY * ATX; k += ATHREADS) {
+    const int ly = k / ATX, lx = k - ly * ATX;
+    const T a = east(ly, lx + 1), b = north(ly + 1, lx);
+    fe[ly * (ATX + 1) + lx + 1] = a;
+    fn[(ly + 1) * ATX + lx] = b;
   }
-  // north faces j = y0-1 .. y0+ATY-1 on columns x0 .. x0+ATX-1
-  for (int k = tid; k < NV; k += ATHREADS) {
-    int lf = k / ATX, lx = k % ATX;
-    int gj = y0 - 1 + lf, gi = x0 + lx;
-    T f = T(0);
-    if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
-      T vv = fn[k];
-      bool pos = vv >= T(0);
-      const T* p = &hs[(lf - 1 + AH) * HW + lx + AH];
-      T hf;
-      if (MASKED) hf = tiered_face<T, S4, S6>(p, HW, gj, ny, pos, pos ? ty_[lf][lx] : ty_[lf + 1][lx]);
-      else hf = face_value<T, S>(p, HW, gj, ny, pos);
-      f = hf * vv;
-    }
-    fn[k] = f;
+  for (int k = tid; k < ATY + ATX; k += ATHREADS) {
+    if (k < ATY) fe[k * (ATX + 1)] = east(k, 0);
+    else fn[k - ATY] = north(0, k - ATY);
   }
   __syncthreads();
   for (int k = tid; k < ATY * ATX; k += ATHREADS) {
