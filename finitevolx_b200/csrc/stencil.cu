@@ -33,14 +33,15 @@ DEV T tiered_face(const T* p, int st, int i, int N, bool pos, int code) {
 // on its north faces land in one flat shared buffer, four loads in flight
 // per thread (eight raise the FP32 kernels' registers from 31 to 59); the
 // face fluxes then overwrite u and v in place.
-// WENO7 / WENO9 faces are evaluated through a call: inlined into the face
-// loops, the compiler hoists the schemes' ~84 table coefficients out of the
-// loop into registers (FP64 WENO7: 134 registers, or spills under a cap of
-// three CTAs per SM); behind the call they stay constant-bank operands
-// (60 registers, no spills).
-template <int S>
+// FP64 WENO7 / WENO9 faces are evaluated through a call: inlined into the
+// face loops, the compiler hoists the schemes' ~84 table coefficients out of
+// the loop into registers (FP64 WENO7: 134 registers, or spills under a cap
+// of three CTAs per SM); behind the call they stay constant-bank operands
+// (56-60 registers, no spills).  FP32 inlined needs 39 registers and runs
+// faster than through the call.
+template <typename T, int S>
 struct AdvFaceCall {
-  static constexpr bool v = S == FVX_WENO7 || S == FVX_WENO9;
+  static constexpr bool v = sizeof(T) == 8 && (S == FVX_WENO7 || S == FVX_WENO9);
 };
 template <typename T, int S>
 __noinline__ __device__ T face_value_call(const T* p, int st, int i, int N, bool pos) {
@@ -48,7 +49,7 @@ __noinline__ __device__ T face_value_call(const T* p, int st, int i, int N, bool
 }
 template <typename T, int S>
 DEV T adv_face(const T* p, int st, int i, int N, bool pos) {
-  if constexpr (AdvFaceCall<S>::v) return face_value_call<T, S>(p, st, i, N, pos);
+  if constexpr (AdvFaceCall<T, S>::v) return face_value_call<T, S>(p, st, i, N, pos);
   else return face_value<T, S>(p, st, i, N, pos);
 }
 template <typename T, int S, int S4, int S6, bool MASKED>
