@@ -70,6 +70,33 @@ DEV T face_value_full(const T* p, int st, int i, int N, bool pos) {
   }
 }
 
+// WENO7 / WENO9 faces through calls: inlined into the stage's face loops,
+// the compiler hoists the schemes' table coefficients out of the loops into
+// registers (FP32 WENO9: 195 registers per thread); behind a call they stay
+// constant-bank operands.
+template <int S>
+struct StageFaceCall {
+  static constexpr bool v = S == FVX_WENO7 || S == FVX_WENO9;
+};
+template <typename T, int S>
+__noinline__ __device__ T stage_face_full_call(const T* p, int st, int i, int N, bool pos) {
+  return face_value_full<T, S>(p, st, i, N, pos);
+}
+template <typename T, int S>
+__noinline__ __device__ T stage_face_ladder_call(const T* p, int st, int i, int N, bool pos) {
+  return face_value<T, S>(p, st, i, N, pos);
+}
+template <typename T, int S>
+DEV T stage_face_full(const T* p, int st, int i, int N, bool pos) {
+  if constexpr (StageFaceCall<S>::v) return stage_face_full_call<T, S>(p, st, i, N, pos);
+  else return face_value_full<T, S>(p, st, i, N, pos);
+}
+template <typename T, int S>
+DEV T stage_face(const T* p, int st, int i, int N, bool pos) {
+  if constexpr (StageFaceCall<S>::v) return stage_face_ladder_call<T, S>(p, st, i, N, pos);
+  else return face_value<T, S>(p, st, i, N, pos);
+}
+
 // ---- asynchronous global -> shared copies (cp.async, no register staging) --
 // Interior tiles' loads are plain copies: issue them all, then wait once, so
 // the tile load costs one memory latency instead of one per loop iteration.
@@ -398,12 +425,12 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
         const int ly = k, gi = x0 - 1;
         const float* a = ps + ly * (TX + 2);  // psi rows j-1 and j+1 at columns x0-1, x0
         const T uu = (T)(cu * ((a[2 * (TX + 2)] - a[0]) + (a[2 * (TX + 2) + 1] - a[1])));
-        fe[ly * (TX + 1)] = face_value_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
+        fe[ly * (TX + 1)] = stage_face_full<T, S>(qt + (ly + H) * QW + (H - 1), 1, gi, nx, uu >= T(0)) * uu;
       } else {
         const int lx = k - TY, gj = y0 - 1;
         const float* a = ps + lx;  // psi rows y0-1, y0 at columns i-1, i+1
         const T vv = (T)(cv * ((a[2] - a[0]) + (a[(TX + 2) + 2] - a[TX + 2])));
-        fn[lx] = face_value_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+        fn[lx] = stage_face_full<T, S>(qt + (H - 1) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
         vs[lx] = vv;
       }
     }
@@ -414,10 +441,10 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     T f = T(0);
     if (IN) {
       T uu = uvel(gj, gi);
-      f = face_value_full<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
+      f = stage_face_full<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
     } else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2) {
       T uu = uvel(gj, gi);
-      f = face_value<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
+      f = stage_face<T, S>(qt + (ly + H) * QW + (lf - 1 + H), 1, gi, nx, uu >= T(0)) * uu;
     }
     fe[k] = f;
   }
@@ -427,9 +454,9 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     T f = T(0);
     T vv = vvel(gj, gi);
     if (IN)
-      f = face_value_full<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+      f = stage_face_full<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
     else if (gj >= 1 && gj <= ny - 2 && gi >= 1 && gi <= nx - 2)
-      f = face_value<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
+      f = stage_face<T, S>(qt + (lf - 1 + H) * QW + (lx + H), QW, gj, ny, vv >= T(0)) * vv;
     fn[k] = f;
     vs[k] = vv;
   }
