@@ -113,7 +113,11 @@ def set_stage_tile(method: str, dtype: torch.dtype, cfg: int) -> None:
 
 def tune_qg_stage(model, q, dt: float, use_cache: bool = True) -> dict:
     """Pick the stage kernel's tile shape for ``model`` (a QGModel) on
-    state ``q``; returns {"tile": name, "ms": {name: median ms}}."""
+    state ``q``; returns {"tile": name, "ms": {name: median ms per step}}.
+    Candidates are timed as whole steps (graph-replayed): inside a step the
+    stage reads inputs the DST products just wrote, which the stage timed
+    alone does not reproduce (at 2048^2 the two orderings of 64x16 and
+    64x32 disagree)."""
     g = model.grid
     key = f"{_device_key()}/qg_stage/{model.method}/{model.dtype}/{g.Ny}x{g.Nx}"
     if use_cache:
@@ -126,7 +130,7 @@ def tune_qg_stage(model, q, dt: float, use_cache: bool = True) -> dict:
     ms = {}
     for cfg in range(n_cfg):
         set_stage_tile(model.method, model.dtype, cfg)
-        ms[_TILES[cfg]] = _time_graph(lambda: model._stage(q, q, out, 0.75, 0.25, 0.25 * dt, True, False))
+        ms[_TILES[cfg]] = _time_graph(lambda: model.step(q, dt, out=out), batch=4)
     best = min(ms, key=ms.get)
     set_stage_tile(model.method, model.dtype, _TILES.index(best))
     res = {"tile": best, "ms": ms}
