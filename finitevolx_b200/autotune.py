@@ -152,8 +152,8 @@ def tune_qg_split(model, q, dt: float, use_cache: bool = True) -> dict:
     out = torch.empty_like(q)
     ms = {}
     model.step(q, dt, out=out)  # leaves split(out) in the workspace for the fused chain
-    ms["fused"] = _time(lambda: model.step(out, dt, out=out, presplit=True))
-    ms["unfused"] = _time(lambda: model.step(q, dt, out=out, presplit=False))
+    ms["fused"] = _time_graph(lambda: model.step(out, dt, out=out, presplit=True), batch=4)
+    ms["unfused"] = _time_graph(lambda: model.step(q, dt, out=out, presplit=False), batch=4)
     fused = ms["fused"] <= ms["unfused"]
     model.fuse_split = fused
     res = {"fused": fused, "ms": ms}
@@ -182,14 +182,10 @@ def tune_dst_kernel(model, q, dt: float, use_cache: bool = True) -> dict:
             return hit
     out = torch.empty_like(q)
 
-    def steps():
-        for _ in range(3):
-            model.step(q, dt, out=out)
-
     ms = {}
     for name in DST_KERNELS:
         set_dst_kernel(name)
-        ms[name] = _time(steps)
+        ms[name] = _time_graph(lambda: model.step(q, dt, out=out), batch=4)
     best = min(ms, key=ms.get)
     set_dst_kernel(best)
     res = {"kernel": best, "ms": ms}
