@@ -441,8 +441,49 @@ conv_e0_e1_kernel(const float* x, const float* f, const __nv_bfloat16* __restric
 
 // G = dL/d(pre-activation) = dY * (y > 0) (or dY when the layer is linear);
 // dskip += G.
+DEV float4 relu_mask4(float4 d, float4 yv, int relu) {
+  if (relu) {
+    d.x = yv.x > 0.f ? d.x : 0.f;
+    d.y = yv.y > 0.f ? d.y : 0.f;
+    d.z = yv.z > 0.f ? d.z : 0.f;
+    d.w = yv.w > 0.f ? d.w : 0.f;
+  }
+  return d;
+}
+// g = dL/dy masked by the ReLU (y > 0), dskip += g.  Four elements per
+// access and two accesses per trip when every pointer is 16-byte aligned
+// (each trip's loads issued before its stores); else one element at a time.
 __global__ void act_grad_kernel(const float* dy, const float* y, float* g, float* dskip, size_t n, int relu) {
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+  const size_t t0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  const bool v4 = (((uintptr_t)dy | (uintptr_t)y | (uintptr_t)g | (uintptr_t)dskip) & 15) == 0;
+  size_t head = 0;
+  if (v4) {
+    const size_t n4 = n / 4;
+    const float4* dy4 = (const float4*)dy;
+    const float4* y4 = (const float4*)y;
+    float4* g4 = (float4*)g;
+    float4* s4 = (float4*)dskip;
+    for (size_t k = t0; k < n4; k += 2 * stride) {
+      const size_t k2 = k + stride;
+      const bool two = k2 < n4;
+      const float4 d0 = dy4[k], y0 = y4[k];
+      float4 d1 = make_float4(0.f, 0.f, 0.f, 0.f), y1 = d1, a0 = d1, a1 = d1;
+      if (two) { d1 = dy4[k2]; y1 = y4[k2]; }
+      if (dskip) {
+        a0 = s4[k];
+        if (two) a1 = s4[k2];
+      }
+      const float4 v0 = relu_mask4(d0, y0, relu), v1 = relu_mask4(d1, y1, relu);
+      g4[k] = v0;
+      if (two) g4[k2] = v1;
+      if (dskip) {
+        s4[k] = make_float4(a0.x + v0.x, a0.y + v0.y, a0.z + v0.z, a0.w + v0.w);
+        if (two) s4[k2] = make_float4(a1.x + v1.x, a1.y + v1.y, a1.z + v1.z, a1.w + v1.w);
+      }
+    }
+    head = n4 * 4;
+  }
+  for (size_t k = head + t0; k < n; k += stride) {
     const float v = relu ? (y[k] > 0.f ? dy[k] : 0.f) : dy[k];
     g[k] = v;
     if (dskip) dskip[k] += v;
