@@ -824,12 +824,15 @@ template <int TDT> struct F64Cfg {
 };
 template <int TDT>
 __global__ void __launch_bounds__(256)
-gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict__ S, int lds, int M, int N, int K,
-                Epi ep) {
+gemm_f64_kernel(const double* A, int lda, const double* __restrict__ S, int lds, int M, int N, int K, Epi ep) {
   constexpr int R = TDT / 16, DK = F64Cfg<TDT>::DK, NL = TDT * DK / 256;  // loads per thread per operand
   static_assert(TDT * DK % 256 == 0, "whole loads per thread");
   __shared__ double As[DK][TDT + 1];
   __shared__ double Ss[DK][TDT + 1];
+  // launched as a programmatic dependent: A (and the output) belong to the
+  // kernel before until the wait; A is then read through L2 (__ldcg, no
+  // restrict), so no load of it can be placed before the wait
+  grid_dep_wait();
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
   const int m0 = blockIdx.y * TDT, n0 = blockIdx.x * TDT;
   double acc[R][R] = {};
@@ -840,7 +843,7 @@ gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict_
       for (int u = 0; u < NL; ++u) {
         const int t = threadIdx.x + u * 256;
         const int mm = t / DK, kk = t % DK, gm = m0 + mm, gk = k0 + kk;
-        va[u] = (gm < M && gk < K) ? A[(long long)gm * lda + gk] : 0.0;
+        va[u] = (gm < M && gk < K) ? __ldcg(A + (long long)gm * lda + gk) : 0.0;
         const int kk2 = t / TDT, nn = t % TDT, gk2 = k0 + kk2, gn = n0 + nn;
         vs[u] = (gk2 < K && gn < N) ? S[(long long)gk2 * lds + gn] : 0.0;
       }
@@ -864,6 +867,8 @@ gemm_f64_kernel(const double* __restrict__ A, int lda, const double* __restrict_
     }
     __syncthreads();
   }
+  // the next kernel may launch while this one stores its results
+  grid_dep_launch();
 #pragma unroll
   for (int i = 0; i < R; ++i) {
     const int m = m0 + ty + 16 * i;
@@ -1132,9 +1137,13 @@ static int gemm_f64(const double* A, int lda, int M, int K, const double* S, int
   const int t = tiles(64) >= 148 ? 64 : (tiles(32) >= 148 ? 32 : 16);
   dim3 grid((N + t - 1) / t, (M + t - 1) / t);
   if (grid.y > 65535) return FVX_ERR_SHAPE;
-  if (t == 64) gemm_f64_kernel<64><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
-  else if (t == 32) gemm_f64_kernel<32><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
-  else gemm_f64_kernel<16><<<grid, 256, 0, st>>>(A, lda, S, N, M, N, K, ep);
+  // programmatic dependent launch: the set-up overlaps the previous
+  // kernel's tail (the kernel waits before touching its data)
+  cudaError_t e;
+  if (t == 64) e = fvx_launch_pdl(gemm_f64_kernel<64>, grid, dim3(256), 0, st, A, lda, S, N, M, N, K, ep);
+  else if (t == 32) e = fvx_launch_pdl(gemm_f64_kernel<32>, grid, dim3(256), 0, st, A, lda, S, N, M, N, K, ep);
+  else e = fvx_launch_pdl(gemm_f64_kernel<16>, grid, dim3(256), 0, st, A, lda, S, N, M, N, K, ep);
+  if (e != cudaSuccess) return FVX_ERR_CUDA;
   return fvx_cuda_status();
 }
 
