@@ -919,17 +919,23 @@ __global__ void split_input_kernel(const T* __restrict__ in, long long bstride, 
 }
 
 template <typename T>
-__global__ void copy_in_f64_kernel(const T* __restrict__ in, long long bstride, long long ld, int ny, int nx,
-                                   int batch, double* __restrict__ out) {
-  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  long long n = (long long)batch * ny * nx;
-  for (; k < n; k += (long long)gridDim.x * blockDim.x) {
-    long long b = k / ((long long)ny * nx);
-    long long rem = k - b * ny * nx;
-    int y = (int)(rem / nx), x = (int)(rem - (long long)y * nx);
-    out[k] = (double)in[b * bstride + (long long)y * ld + x];
+__global__ void copy_in_f64_kernel(const T* in, long long bstride, long long ld, int ny, int nx, int batch,
+                                   double* __restrict__ out) {
+  // rows of the [batch][ny][nx] input over the grid, a row's elements over
+  // the threads (no per-element divisions).  Launched as a programmatic
+  // dependent: the input is the previous kernel's output, read after the
+  // wait through L2.
+  grid_dep_wait();
+  const int rows = batch * ny;
+  for (int r = blockIdx.x; r < rows; r += gridDim.x) {
+    const int b = r / ny, y = r - b * ny;
+    const T* src = in + (long long)b * bstride + (long long)y * ld;
+    double* dst = out + (long long)r * nx;
+    for (int x = threadIdx.x; x < nx; x += blockDim.x) dst[x] = (double)__ldcg(src + x);
   }
+  grid_dep_launch();
 }
+static int copy_rows_grid(long long rows) { return (int)(rows < 148 * 16 ? (rows < 1 ? 1 : rows) : 148 * 16); }
 
 __global__ void zero_f64_kernel(double* p, long long bstride, long long ld, int ny, int nx, int batch) {
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1504,7 +1510,9 @@ extern "C" int fvx_dst_solve_f32(fvx_dst_plan* p, const float* rhs, long long rh
   cudaStream_t st = fvx_stream(stream);
   long long n = (long long)batch * p->ny * p->nx;
   if (!p->split_ok) {  // sizes the TMA tiles cannot address: FP64 SIMT chain, FP32 output
-    copy_in_f64_kernel<float><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, p->ny, p->nx, batch, p->V1);
+    if (fvx_launch_pdl(copy_in_f64_kernel<float>, dim3(copy_rows_grid((long long)batch * p->ny)), dim3(256), 0, st,
+                       rhs, rhs_bstride, rhs_ld, p->ny, p->nx, batch, p->V1) != cudaSuccess)
+      return FVX_ERR_CUDA;
     int rc0 = fvx_cuda_status();
     if (rc0) return rc0;
     return chain_f64(p, batch, EPI_F32, psi, psi_bstride, psi_ld, st);
@@ -1578,7 +1586,9 @@ extern "C" int fvx_dst_solve_f64(fvx_dst_plan* p, const double* rhs, long long r
   int rc;
   if (method == 0 || !p->split_ok) {
     if (!p->V1) return FVX_ERR_ARG;
-    copy_in_f64_kernel<double><<<grid1d(n), 256, 0, st>>>(rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->V1);
+    if (fvx_launch_pdl(copy_in_f64_kernel<double>, dim3(copy_rows_grid((long long)batch * ny)), dim3(256), 0, st,
+                       rhs, rhs_bstride, rhs_ld, ny, nx, batch, p->V1) != cudaSuccess)
+      return FVX_ERR_CUDA;
     if ((rc = fvx_cuda_status())) return rc;
     rc = chain_f64(p, batch, EPI_F64, psi, psi_bstride, psi_ld, st);
     if (info) { info[0] = 1; info[1] = -1; info[2] = -1; }
