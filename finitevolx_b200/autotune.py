@@ -30,7 +30,7 @@ import torch
 
 from finitevolx_b200._lib import I, SCHEMES, check, fn
 
-_TILES = ("64x16", "32x16", "128x8", "64x32", "128x16")
+_TILES = ("64x16", "32x16", "128x8", "64x32", "128x16", "16x16")
 
 
 def _cache_path() -> pathlib.Path:

@@ -41,6 +41,7 @@ static int launch(const StageArgs& a, cudaStream_t st) {
     case 2: return launch_t<T, S, kTileTX[2], kTileTY[2]>(a, st);
     case 3: return launch_t<T, S, kTileTX[3], kTileTY[3]>(a, st);
     case 4: return launch_t<T, S, kTileTX[4], kTileTY[4]>(a, st);
+    case 5: return launch_t<T, S, kTileTX[5], kTileTY[5]>(a, st);
     default: return launch_t<T, S, kTileTX[0], kTileTY[0]>(a, st);
   }
 }

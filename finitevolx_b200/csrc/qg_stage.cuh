@@ -12,9 +12,10 @@ namespace qg {
 
 constexpr int THREADS = 256;
 // Tile shapes the autotuner chooses from (fvx_qg_tile_config): TX x TY cells.
-constexpr int kTileTX[5] = {64, 32, 128, 64, 128};
-constexpr int kTileTY[5] = {16, 16, 8, 32, 16};
-constexpr int kTileConfigs = 5;
+// (16 x 16: small FP64 grids, where 32 x 16 tiles leave SMs idle.)
+constexpr int kTileTX[6] = {64, 32, 128, 64, 128, 16};
+constexpr int kTileTY[6] = {16, 16, 8, 32, 16, 16};
+constexpr int kTileConfigs = 6;
 
 // a / d: exact division in FP64; multiplication by the rounded reciprocal in
 // FP32 (<= 1 ulp from the quotient).

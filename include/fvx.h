@@ -416,7 +416,7 @@ int fvx_qg_snapshot_pack_f64(const double* q, const double* psi, const double* u
                              const double* z, int ny, int nx, double eta_scale, double* out, void* stream);
 
 /* ---- QG fused-stage tile shape (autotuner) -------------------------------- */
-/* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8, 3 = 64x32, 4 = 128x16 cells for (method, dtype 0 FP32 / 1
+/* cfg 0 = 64x16, 1 = 32x16, 2 = 128x8, 3 = 64x32, 4 = 128x16, 5 = 16x16 cells for (method, dtype 0 FP32 / 1
  * FP64); cfg < 0 returns the number of configurations.  No counterpart in
  * finitevolX (launch configuration). */
 int fvx_qg_tile_config(int method, int dtype, int cfg);
