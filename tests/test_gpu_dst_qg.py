@@ -89,6 +89,20 @@ def test_dst_fp64_chain(cuda_ok, shape):
     assert rel_err(host(got), ref) < 1e-12
 
 
+def test_dst_fp64_chain_tile_size_keeps_result(cuda_ok):
+    # one 128^2 right-hand side runs the FP64 products on 16 x 16 tiles
+    # (128-long k-blocks); a batch of ten on 32 x 32 tiles (16-long
+    # k-blocks).  Every output's FMA chain over k keeps its order in both, so
+    # the results are bit-identical
+    n = 128
+    f = np.random.default_rng(9).standard_normal((n, n))
+    one = host(solve_helmholtz_dst(dev(f), 0.1, 0.2, 1.5))
+    batch = host(solve_helmholtz_dst(dev(np.stack([f] * 10)), 0.1, 0.2, 1.5))
+    for k in range(10):
+        np.testing.assert_array_equal(batch[k], one)
+    assert rel_err(one, O.solve_helmholtz_dst(f, 0.1, 0.2, 1.5)) < 1e-12
+
+
 def test_dst_odd_size_fp32_uses_fp64_chain(cuda_ok):
     f = np.random.default_rng(2).standard_normal((37, 29))
     ref = O.solve_helmholtz_dst(f, 0.1, 0.2, 0.0)
