@@ -189,6 +189,19 @@ def test_qg_step_fp32_within_1e5(cuda_ok):
     m.plan.check_device()
 
 
+@pytest.mark.parametrize("method", ("weno7", "weno9"))
+def test_qg_step_fp32_wide_schemes_within_1e5(cuda_ok, method):
+    # the stage kernel's wide WENO faces (evaluated through calls) in FP32:
+    # one step at 256^2 within the FP32 bar of the FP64 oracle
+    n = 256
+    grid, q = qg_setup(n, torch.float32, 15)
+    lam, beta, dt = 1.0 / 4e4 ** 2, 1.7e-11, 0.5 * (5.12e6 / n)
+    m = QGModel(grid, beta, lam, method=method, dtype=torch.float32)
+    ref = O.qg_step(q.astype(np.float32).astype(np.float64), grid.dx, grid.dy, beta, lam, dt, method)
+    got = m.step(dev(q, torch.float32), dt)
+    assert rel_err(host(got), ref) < 1e-5
+
+
 def test_autotuner_choices_keep_results(cuda_ok, tmp_path, monkeypatch):
     # every tile shape and both split placements give the same step (FP32,
     # 1e-6 relative: only accumulation order may differ), and the tuner
