@@ -91,6 +91,25 @@ def test_ensemble_single_layer_matches_qgmodel(cuda_ok):
         assert err < 1e-5, (m, err)
 
 
+@pytest.mark.parametrize("method", ("wenoz5", "weno3", "van_leer", "upwind1"))
+def test_ensemble_other_schemes_match_qgmodel(cuda_ok, method):
+    # the persistent stage kernel's other schemes against QGModel's stage
+    # kernel (the same tile body), single-layer members of two sizes
+    members = [(64, 1), (256, 1)]
+    ens = fvx.QGEnsemble(members, method=method)
+    qs = init_state(ens, 3)
+    ens.step(1)
+    torch.cuda.synchronize()
+    for m, (n, nl) in enumerate(members):
+        grid = fvx.ArakawaCGrid2D.from_interior(n, n, ens.Lx, ens.Lx)
+        lam = float(ens.modes[m][2][0])
+        model = fvx.QGModel(grid, ens.beta, lam, method=method, dtype=torch.float32, dst_refine=1)
+        ref = model.step(torch.from_numpy(qs[m][0]).float().cuda(), ens.dt[m]).double().cpu().numpy()
+        got = ens.get_layer(m, 0).double().cpu().numpy()
+        err = np.abs(got - ref).max() / np.abs(ref).max()
+        assert err < 1e-5, (method, m, err)
+
+
 def test_ensemble_graph_replay_matches_eager(cuda_ok):
     a = fvx.QGEnsemble(MEMBERS[:3])
     b = fvx.QGEnsemble(MEMBERS[:3])
