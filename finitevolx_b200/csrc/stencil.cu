@@ -281,23 +281,41 @@ __global__ void cgrid_op_kernel(int op, const T* __restrict__ a, const T* __rest
 // ===========================================================================
 // Arakawa Jacobian (operators/jacobian.py:106-131): out [B, Ny-2, Nx-2].
 // ===========================================================================
+// A thread per output column walking kJacRows rows with a 3 x 3 window of f
+// and g in registers (three new values of each per row instead of eight):
+// the warp's loads of a row are consecutive columns.  Each output keeps the
+// reference's three-form expression and operand order.
+constexpr int kJacCols = 128, kJacRows = 16;
 template <typename T>
-__global__ void jacobian_kernel(const T* __restrict__ f, const T* __restrict__ g, T* __restrict__ out,
-                                int ny, int nx, T scale) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;  // output column 0..nx-3
-  int j = blockIdx.y * blockDim.y + threadIdx.y;  // output row 0..ny-3
-  int b = blockIdx.z;
-  if (i >= nx - 2 || j >= ny - 2) return;
-  const T* F = f + (size_t)b * ny * nx + (size_t)(j + 1) * nx + (i + 1);
-  const T* G = g + (size_t)b * ny * nx + (size_t)(j + 1) * nx + (i + 1);
-  auto f_ = [&](int dj, int di) { return ldg(F + dj * nx + di); };
-  auto g_ = [&](int dj, int di) { return ldg(G + dj * nx + di); };
-  T Jpp = (f_(0, 1) - f_(0, -1)) * (g_(1, 0) - g_(-1, 0)) - (f_(1, 0) - f_(-1, 0)) * (g_(0, 1) - g_(0, -1));
-  T Jpx = f_(0, 1) * (g_(1, 1) - g_(-1, 1)) - f_(0, -1) * (g_(1, -1) - g_(-1, -1)) -
-          f_(1, 0) * (g_(1, 1) - g_(1, -1)) + f_(-1, 0) * (g_(-1, 1) - g_(-1, -1));
-  T Jxp = g_(1, 0) * (f_(1, 1) - f_(1, -1)) - g_(-1, 0) * (f_(-1, 1) - f_(-1, -1)) -
-          g_(0, 1) * (f_(1, 1) - f_(-1, 1)) + g_(0, -1) * (f_(1, -1) - f_(-1, -1));
-  out[(size_t)b * (ny - 2) * (nx - 2) + (size_t)j * (nx - 2) + i] = (Jpp + Jpx + Jxp) * scale;  // scale = 1 / (12 dx dy)
+__global__ void __launch_bounds__(kJacCols)
+jacobian_kernel(const T* __restrict__ f, const T* __restrict__ g, T* __restrict__ out, int ny, int nx, T scale) {
+  const int i = blockIdx.x * kJacCols + threadIdx.x;  // output column 0..nx-3
+  const int j0 = blockIdx.y * kJacRows;               // first output row
+  const int b = blockIdx.z;
+  if (i >= nx - 2 || j0 >= ny - 2) return;
+  const int j1 = min(j0 + kJacRows, ny - 2);
+  // padded row j0 + r, columns i .. i + 2: window rows a (top), m (middle), c (bottom)
+  const T* F = f + (size_t)b * ny * nx + (size_t)j0 * nx + i;
+  const T* G = g + (size_t)b * ny * nx + (size_t)j0 * nx + i;
+  T fa0 = ldg(F), fa1 = ldg(F + 1), fa2 = ldg(F + 2), ga0 = ldg(G), ga1 = ldg(G + 1), ga2 = ldg(G + 2);
+  F += nx;
+  G += nx;
+  T fm0 = ldg(F), fm1 = ldg(F + 1), fm2 = ldg(F + 2), gm0 = ldg(G), gm1 = ldg(G + 1), gm2 = ldg(G + 2);
+  T* o = out + (size_t)b * (ny - 2) * (nx - 2) + (size_t)j0 * (nx - 2) + i;
+#pragma unroll 4
+  for (int j = j0; j < j1; ++j) {
+    F += nx;
+    G += nx;
+    const T fc0 = ldg(F), fc1 = ldg(F + 1), fc2 = ldg(F + 2), gc0 = ldg(G), gc1 = ldg(G + 1), gc2 = ldg(G + 2);
+    // f_(dj, di): dj = -1, 0, 1 -> a, m, c; di = -1, 0, 1 -> 0, 1, 2
+    const T Jpp = (fm2 - fm0) * (gc1 - ga1) - (fc1 - fa1) * (gm2 - gm0);
+    const T Jpx = fm2 * (gc2 - ga2) - fm0 * (gc0 - ga0) - fc1 * (gc2 - gc0) + fa1 * (ga2 - ga0);
+    const T Jxp = gc1 * (fc2 - fc0) - ga1 * (fa2 - fa0) - gm2 * (fc2 - fa2) + gm0 * (fc0 - fa0);
+    *o = (Jpp + Jpx + Jxp) * scale;  // scale = 1 / (12 dx dy)
+    o += nx - 2;
+    fa0 = fm0; fa1 = fm1; fa2 = fm2; ga0 = gm0; ga1 = gm1; ga2 = gm2;
+    fm0 = fc0; fm1 = fc1; fm2 = fc2; gm0 = gc0; gm1 = gc1; gm2 = gc2;
+  }
 }
 
 // ===========================================================================
@@ -639,8 +657,8 @@ using namespace fvx;
                                             int nx, double dx, double dy, void* stream) {            \
     if (!f || !g || !out) return FVX_ERR_ARG;                                                        \
     if (ny < 3 || nx < 3 || batch < 1 || batch > 65535) return FVX_ERR_SHAPE;                        \
-    dim3 b(32, 8), gr((nx - 2 + 31) / 32, (ny - 2 + 7) / 8, batch);                                   \
-    jacobian_kernel<T><<<gr, b, 0, fvx_stream(stream)>>>(f, g, out, ny, nx, T(1.0 / (12.0 * dx * dy)));     \
+    dim3 gr((nx - 2 + kJacCols - 1) / kJacCols, (ny - 2 + kJacRows - 1) / kJacRows, batch);              \
+    jacobian_kernel<T><<<gr, kJacCols, 0, fvx_stream(stream)>>>(f, g, out, ny, nx, T(1.0 / (12.0 * dx * dy))); \
     return fvx_cuda_status();                                                                        \
   }                                                                                                  \
   extern "C" int fvx_diffusion2d_##SFX(const T* h, const T* kappa_field, double kappa, T* out,       \
