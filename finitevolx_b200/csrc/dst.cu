@@ -1557,6 +1557,24 @@ extern "C" int fvx_dst_refine_f32(fvx_dst_plan* p, const float* rhs, long long r
   return FVX_OK;
 }
 
+// FP64 chain on the input the caller already wrote into the plan's FP64
+// workspace (fvx_dst_workspace_f64; the FP64 QG stage kernel writes it):
+// the FP64 solve without its input copy.  psi: FP64 interior view.
+extern "C" int fvx_dst_solve_presplit_f64(fvx_dst_plan* p, double* psi, long long psi_bstride, long long psi_ld,
+                                          int batch, void* stream) {
+  if (!p || !psi || !p->V1) return FVX_ERR_ARG;
+  if (batch < 1 || batch > p->batch_max) return FVX_ERR_SHAPE;
+  return chain_f64(p, batch, EPI_F64, psi, psi_bstride, psi_ld, fvx_stream(stream));
+}
+
+// The FP64 chain's input workspace: [batch_max][ny][nx] doubles, natural
+// layout (what fvx_dst_solve_presplit_f64 reads).
+extern "C" int fvx_dst_workspace_f64(fvx_dst_plan* p, void** v1) {
+  if (!p || !v1) return FVX_ERR_ARG;
+  *v1 = p->V1;
+  return p->V1 ? FVX_OK : FVX_ERR_SHAPE;
+}
+
 // Layout of the chain's first operand (the fvx_dst_workspace buffers): 0
 // natural [b][y][x]; 1 x de-interleaved, x stored at x / 2 (even x) or
 // nx / 2 + x / 2 (odd x) -- the even/odd products of plans whose ny and nx

@@ -75,7 +75,9 @@ using namespace fvx;
                                     double a, double b, double c, int method, int periodic, int write_ghost, \
                                     void* stream) {                                                          \
     if (!q_stage || !psi_interior || !q_out) return FVX_ERR_ARG;                                             \
-    if ((split_hi == nullptr) != (split_lo == nullptr)) return FVX_ERR_ARG;                                  \
+    if (sizeof(T) == 8 ? (split_lo != nullptr || (split_hi && split_layout)) /* FP64: hi = interior copy */  \
+                       : ((split_hi == nullptr) != (split_lo == nullptr)))                                      \
+      return FVX_ERR_ARG;                                                                                    \
     if (ny < 6 || nx < 6) return FVX_ERR_SHAPE;                                                              \
     qg::StageArgs A;                                                                                         \
     A.qs = q_stage; A.qn = q_start; A.psi = psi_interior; A.forcing = forcing; A.out = q_out;              \

@@ -30,8 +30,8 @@ struct StageArgs {
   const void* psi;     // interior-only [Ny-2][Nx-2]
   const void* forcing; // [Ny][Nx] or null
   void* out;           // [Ny][Nx]
-  __nv_bfloat16* split_hi;  // [Ny-2][Nx-2] or null
-  __nv_bfloat16* split_lo;
+  __nv_bfloat16* split_hi;  // [Ny-2][Nx-2] or null (FP64 stages: a double [Ny-2][Nx-2] interior copy)
+  __nv_bfloat16* split_lo;  // (FP64 stages: null)
   int split_layout;         // 1: x de-interleaved (the even/odd DST operand layout)
   int ny, nx;
   double a, b, c;      // out = a*qn + b*qs + c*rhs
@@ -491,6 +491,7 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
         const T* qnp = decltype(has_qn)::value ? qn + g : nullptr;
         T* op = out + g;
         __nv_bfloat16* hp = decltype(do_split)::value ? A.split_hi + sidx : nullptr;
+        double* dp = (sizeof(T) == 8 && decltype(do_split)::value) ? (double*)(void*)A.split_hi + sidx : nullptr;
         __nv_bfloat16* lp = decltype(do_split)::value ? A.split_lo + sidx : nullptr;
 #pragma unroll
         for (int f = 0; f < SEGT; ++f) {
@@ -502,10 +503,14 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
           r = r + cc * rhs;
           op[(size_t)f * nx] = r;
           if constexpr (decltype(do_split)::value) {
-            const float fv = (float)r;
-            const __nv_bfloat16 h = __float2bfloat16_rn(fv);
-            hp[(size_t)f * nxi] = h;
-            lp[(size_t)f * nxi] = __float2bfloat16_rn(fv - __bfloat162float(h));
+            if constexpr (sizeof(T) == 8) {
+              dp[(size_t)f * nxi] = r;  // FP64: the interior itself (the FP64 chain's input)
+            } else {
+              const float fv = (float)r;
+              const __nv_bfloat16 h = __float2bfloat16_rn(fv);
+              hp[(size_t)f * nxi] = h;
+              lp[(size_t)f * nxi] = __float2bfloat16_rn(fv - __bfloat162float(h));
+            }
           }
           fs = fnn;
           vsv = vn;
@@ -555,10 +560,14 @@ DEV void stage_body(const StageArgs& A, uint8_t* sm, const int x0, const int y0)
     if (A.split_hi) {
       const int xi = gi - 1;
       size_t s = (size_t)(gj - 1) * nxi + (A.split_layout ? ((xi & 1) ? (nxi >> 1) + (xi >> 1) : (xi >> 1)) : xi);
-      float fv = (float)r;
-      __nv_bfloat16 h = __float2bfloat16_rn(fv);
-      A.split_hi[s] = h;
-      A.split_lo[s] = __float2bfloat16_rn(fv - __bfloat162float(h));
+      if constexpr (sizeof(T) == 8) {
+        ((double*)(void*)A.split_hi)[s] = r;  // FP64: the interior itself
+      } else {
+        float fv = (float)r;
+        __nv_bfloat16 h = __float2bfloat16_rn(fv);
+        A.split_hi[s] = h;
+        A.split_lo[s] = __float2bfloat16_rn(fv - __bfloat162float(h));
+      }
     }
     if (!IN && A.write_ghost && A.periodic) {
       // copies of this interior cell into the ghost ring (S, N, W, E fill)

@@ -58,6 +58,11 @@ class QGModel:
             check(fn("fvx_dst_workspace")(self.plan.handle, ctypes.byref(hi), ctypes.byref(lo)), "workspace")
             self._layout = fn("fvx_dst_operand_layout")(self.plan.handle)
         self._w1 = (hi, lo)
+        # FP64: the stage kernel writes its output's interior straight into
+        # the FP64 chain's input workspace, so the next solve skips its copy
+        self._v1 = ctypes.c_void_p()
+        self._fused_copy64 = (dtype == torch.float64 and
+                              fn("fvx_dst_workspace_f64")(self.plan.handle, ctypes.byref(self._v1)) == 0)
         # FP64-residual refinement passes after each FP32 DST solve (the
         # split chain's ~1e-5 relative psi error, amplified by the velocity
         # differences, exceeds the FP32 step bar in weakly screened fields:
@@ -89,6 +94,11 @@ class QGModel:
         self.kernel_launches += 4
         self._refine(q)
 
+    def _dst_presplit64(self):
+        check(fn("fvx_dst_solve_presplit_f64")(self.plan.handle, P(self.psi), I64(self.psi.numel()),
+                                               I64(self.grid.Nx - 2), I(1), stream_ptr()), "DST solve")
+        self.kernel_launches += 4
+
     def _refine(self, q):
         if not self.dst_refine:
             return
@@ -102,6 +112,8 @@ class QGModel:
     def _stage(self, qs, qn, out, a, b, c, split, write_ghost):
         g = self.grid
         hi, lo = self._w1 if split else (ctypes.c_void_p(0), ctypes.c_void_p(0))
+        if split and self._fused_copy64:
+            hi = self._v1  # FP64: the interior copy for the FP64 chain
         check(fn(f"fvx_qg_stage_{sfx(qs)}")(P(qs), P(qn), P(self.psi), P(self.forcing), P(out), hi, lo,
                                             I(self._layout if split else 0), I(g.Ny),
                                             I(g.Nx), D(g.dx), D(g.dy), D(self.beta), D(self.drag), D(self.visc),
@@ -130,15 +142,20 @@ class QGModel:
         q = L.as_field(q, dtype=self.dtype)
         out = torch.empty_like(q) if out is None else out
         split = self._fused_split and self.fuse_split
-        presplit = presplit and split
+        copy64 = self._fused_copy64 and self.fuse_split
+        presplit = presplit and (split or copy64)
         stages = ((q, self.y1), (self.y1, self.y2), (self.y2, out))
         for s, ((a, b, c), (qs, qo)) in enumerate(zip(RK3, stages)):
-            # the stage kernel before this one left qs's interior split in the workspace
+            # the stage kernel before this one left qs's interior (split, or
+            # as FP64) in the workspace
             if split and (s > 0 or presplit):
                 self._dst_presplit(qs)
+            elif copy64 and (s > 0 or presplit):
+                self._dst_presplit64()
             else:
                 self._dst_from(qs)
-            self._stage(qs, None if s == 0 else q, qo, a, b, c * dt, split, s == 2)
+            # the layout argument stays 0 for FP64 (_layout is 0 there)
+            self._stage(qs, None if s == 0 else q, qo, a, b, c * dt, split or copy64, s == 2)
         return out
 
     # -- unfused baseline: the reference's operator sequence ------------------

@@ -221,6 +221,14 @@ int fvx_dst_solve_presplit_f32(fvx_dst_plan* plan, float* psi, long long psi_bst
 int fvx_dst_refine_f32(fvx_dst_plan* plan, const float* rhs, long long rhs_bstride, long long rhs_ld, float* psi,
                        long long psi_bstride, long long psi_ld, int batch, int passes, void* stream);
 int fvx_dst_workspace(fvx_dst_plan* plan, void** w1_hi, void** w1_lo);
+/* The FP64 chain's input workspace ([batch_max][ny][nx] doubles, natural
+ * layout; plans with an FP64 chain) and the FP64 solve that starts from it
+ * (fvx_dst_solve_f64's FP64 chain without its input copy): the FP64 QG
+ * stage kernel writes its output's interior there.  Launch plumbing with no
+ * counterpart in finitevolX. */
+int fvx_dst_workspace_f64(fvx_dst_plan* plan, void** v1);
+int fvx_dst_solve_presplit_f64(fvx_dst_plan* plan, double* psi, long long psi_bstride, long long psi_ld, int batch,
+                               void* stream);
 int fvx_dst_operand_layout(fvx_dst_plan* plan);
 /* One product of the chain on the current workspaces (timing only). */
 int fvx_dst_gemm_step(fvx_dst_plan* plan, int which, int batch, void* stream);
@@ -265,7 +273,10 @@ int fvx_dst_noalloc_check(void* stream);
  * geostrophic velocity of psi_interior (zero outside).  periodic: 1 periodic
  * ghost ring, 0 zero ring.  write_ghost refills q_out's ring.  split_hi/lo
  * (bf16 [ny-2][nx-2], may be NULL) receive q_out's interior for the next DST,
- * in the layout split_layout (fvx_dst_operand_layout of the plan).
+ * in the layout split_layout (fvx_dst_operand_layout of the plan).  FP64
+ * stages: split_hi (may be NULL) receives q_out's interior as doubles
+ * [ny-2][nx-2] (the FP64 chain's input, fvx_dst_workspace_f64), split_lo
+ * must be NULL and split_layout 0.
  * method: 1 upwind1, 3 upwind3, 4 weno3, 5 weno5, 6 wenoz5, 7 weno7,
  * 8 weno9, 9 minmod, 10 van_leer. */
 int fvx_qg_stage_f32(const float* q_stage, const float* q_start, const float* psi_interior, const float* forcing,

@@ -319,6 +319,26 @@ def test_qg_step_fp64_256_within_1e12(cuda_ok):
     assert rel_err(got - q, ref - q) < 1e-9
 
 
+def test_qg_step_fp64_stage_writes_chain_input(cuda_ok):
+    # FP64: the stage kernel writes its output's interior into the FP64
+    # chain's input (no copy pass before the next solve); the same step as
+    # with the copy pass, bit for bit, and across steps with presplit
+    n = 256
+    grid, q = qg_setup(n, torch.float64, 16)
+    dt = 0.5 * (5.12e6 / n)
+    m = QGModel(grid, 1.7e-11, 1.0 / 4e4 ** 2, method="weno5", dtype=torch.float64)
+    assert m._fused_copy64
+    fused = m.step(dev(q), dt)
+    m.fuse_split = False
+    plain = m.step(dev(q), dt)
+    np.testing.assert_array_equal(host(fused), host(plain))
+    m.fuse_split = True
+    q1 = m.step(dev(q), dt)
+    q2a = m.step(q1, dt, presplit=True)
+    q2b = m.step(q1.clone(), dt, presplit=False)
+    np.testing.assert_array_equal(host(q2a), host(q2b))
+
+
 def test_qg_step_fp64_every_stage_tile(cuda_ok):
     # the FP64 stage tile is autotuned: every shape the tuner may pick meets
     # the FP64 bar at the metric's configuration
