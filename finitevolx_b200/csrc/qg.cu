@@ -92,7 +92,8 @@ FVX_DEF_QG(f32, float)
 FVX_DEF_QG(f64, double)
 
 // Tile shape of the fused stage kernel for one scheme and dtype (0 FP32, 1
-// FP64): cfg 0 = 64x16, 1 = 32x16, 2 = 128x8 cells.  Returns the number of
+// FP64): cfg 0 = 64x16, 1 = 32x16, 2 = 128x8, 3 = 64x32, 4 = 128x16, 5 = 16x16
+// cells.  Returns the number of
 // configurations when cfg < 0 (and changes nothing).
 extern "C" int fvx_qg_tile_config(int method, int dtype, int cfg) {
   if (cfg < 0) return qg::kTileConfigs;
